@@ -1,0 +1,114 @@
+/*
+ * b2m.h -- C ABI of libb2m, the B200 (sm_100a) implementation of mrMath's dense FP64
+ * GEMM + partial-pivoting LU path.
+ *
+ * Every entry point is `extern "C"`, takes plain pointers and sizes, returns an int32 status
+ * and never throws.  Conventions are those of the reference (Object Pascal, mikerabat/mrmath):
+ *   - matrices are row-major FP64; strides ("LineWidth") are in BYTES;
+ *   - width = number of columns, height = number of rows (NativeInt -> int64_t);
+ *   - pivot vectors are int32, 0-based, with LAPACK-ipiv meaning: indx[i] is the absolute row
+ *     that was swapped with row i at elimination step i (LinAlgLU.pas:120-136, 181-281);
+ *   - status 0 = leOk, 1 = leSingular (MatrixConst.pas:28); negative = library errors.
+ *
+ * Two families:
+ *   b2m_Matrix*      host buffers.  Drop-in replacements for the reference routine of the same
+ *                    name; data is copied to the device, computed, copied back; synchronous.
+ *   b2m_dev_Matrix*  device buffers (device pointers, byte strides), asynchronous on the
+ *                    context's stream; results (status, determinant) come back through device
+ *                    or host pointers as documented.
+ */
+#ifndef B2M_H
+#define B2M_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------------ status codes */
+#define B2M_OK               0   /* leOk */
+#define B2M_SINGULAR         1   /* leSingular: |pivot| <= 10/MaxDouble (LinAlgLU.pas:262) */
+#define B2M_ERR_DIM         -1   /* dimension / stride error (the reference's 'Dimension error' asserts) */
+#define B2M_ERR_CUDA        -2   /* a CUDA call failed; b2m_last_error() has the text */
+#define B2M_ERR_ALLOC       -3   /* device or pinned allocation failed */
+#define B2M_ERR_TIMEOUT     -4   /* a bounded in-kernel wait gave up (never expected) */
+#define B2M_ERR_ARG         -5   /* null pointer / invalid enum */
+#define B2M_ERR_NOCONV      -6   /* mixed-precision refinement did not converge and fallback was disabled */
+#define B2M_ERR_UNSUPPORTED -7   /* size outside what this build supports */
+
+/* destination operation of the blocked multiplication, TMatrixMultDestOperation (MatrixConst.pas:147) */
+#define B2M_DO_NONE 0
+#define B2M_DO_ADD  1
+#define B2M_DO_SUB  2
+
+typedef struct b2m_ctx b2m_ctx;
+
+#if defined(__GNUC__)
+#define B2M_API __attribute__((visibility("default")))
+#else
+#define B2M_API
+#endif
+
+/* ------------------------------------------------------------------ context
+ * A context owns one device, one stream, the device workspaces and the captured graphs.
+ * It is single-threaded; the library is re-entrant across contexts.  There is no counterpart
+ * in the reference (its state is global: MatrixASMStubSwitch.pas InitMathFunctions). */
+B2M_API int32_t     b2m_create(int32_t device, b2m_ctx** out);
+B2M_API int32_t     b2m_destroy(b2m_ctx* ctx);
+/* Use a caller stream (a cudaStream_t) for the b2m_dev_* calls; NULL restores the context's own. */
+B2M_API int32_t     b2m_set_stream(b2m_ctx* ctx, void* stream);
+B2M_API int32_t     b2m_synchronize(b2m_ctx* ctx);
+B2M_API const char* b2m_last_error(b2m_ctx* ctx);
+B2M_API const char* b2m_status_string(int32_t status);
+/* Number of kernels this context has launched so far (device work accounting). */
+B2M_API int64_t     b2m_kernel_launches(b2m_ctx* ctx);
+
+/* ------------------------------------------------------------------ GEMM
+ * Replaces MatrixMult / MatrixMultEx (MatrixASMStubSwitch.pas:769-782),
+ * MatrixMultT1 / MatrixMultT1Ex (:812-823) and MatrixMultT2 / MatrixMultT2Ex (:853-863).
+ * trans 0: dest(height1 x width2)  op=  mt1(height1 x width1)   * mt2(height2 x width2), width1 = height2
+ * trans 1: dest(width1  x width2)  op=  mt1(height1 x width1)^T * mt2(height2 x width2), height1 = height2
+ * trans 2: dest(height1 x height2) op=  mt1(height1 x width1)   * mt2(height2 x width2)^T, width1 = width2
+ * op: B2M_DO_NONE (dest =), B2M_DO_ADD (dest +=), B2M_DO_SUB (dest -=). */
+B2M_API int32_t b2m_MatrixMultEx(b2m_ctx* ctx, double* dest, int64_t destLineWidth, const double* mt1, const double* mt2,
+                         int64_t width1, int64_t height1, int64_t width2, int64_t height2,
+                         int64_t LineWidth1, int64_t LineWidth2, int32_t op, int32_t trans);
+B2M_API int32_t b2m_dev_MatrixMultEx(b2m_ctx* ctx, double* dest, int64_t destLineWidth, const double* mt1,
+                             const double* mt2, int64_t width1, int64_t height1, int64_t width2, int64_t height2,
+                             int64_t LineWidth1, int64_t LineWidth2, int32_t op, int32_t trans);
+
+/* ------------------------------------------------------------------ LU (src/LinAlgLU.pas) */
+/* MatrixLUDecompInPlace LinAlgLU.pas:283-295 */
+B2M_API int32_t b2m_MatrixLUDecompInPlace(b2m_ctx* ctx, double* A, int64_t LineWidthA, int64_t width, int32_t* indx);
+/* MatrixLUDecomp LinAlgLU.pas:297-305 (A is left untouched) */
+B2M_API int32_t b2m_MatrixLUDecomp(b2m_ctx* ctx, const double* A, int64_t LineWidthA, double* LUDecomp,
+                           int64_t LineWidthLU, int64_t width, int32_t* indx);
+/* MatrixLUBackSubst LinAlgLU.pas:315-385, generalised to nrhs columns of B (nrhs = 1 is the reference call). */
+B2M_API int32_t b2m_MatrixLUBackSubst(b2m_ctx* ctx, const double* LUDecomp, int64_t LineWidthLU, int64_t width,
+                              const int32_t* indx, double* B, int64_t LineWidthB, int64_t nrhs);
+/* MatrixInverseInPlace LinAlgLU.pas:388-431 */
+B2M_API int32_t b2m_MatrixInverseInPlace(b2m_ctx* ctx, double* A, int64_t LineWidthA, int64_t width);
+/* MatrixDeterminant LinAlgLU.pas:433-479 (0 for a singular matrix, status still B2M_OK like the reference) */
+B2M_API int32_t b2m_MatrixDeterminant(b2m_ctx* ctx, const double* A, int64_t LineWidthA, int64_t width, double* det);
+/* MatrixLinEQSolve LinAlgLU.pas:481-592.  NumRefinements > 0 runs the reference's fixed-count FP64
+   refinement (residual A*x - b, back-substitution, x -= d), each column reading x along its column. */
+B2M_API int32_t b2m_MatrixLinEQSolve(b2m_ctx* ctx, const double* A, int64_t LineWidthA, int64_t width, const double* B,
+                             int64_t LineWidthB, double* X, int64_t LineWidthX, int64_t Width2,
+                             int64_t NumRefinements);
+
+/* device-resident twins (device pointers; indx / det / status are device pointers too) */
+B2M_API int32_t b2m_dev_MatrixLUDecompInPlace(b2m_ctx* ctx, double* A, int64_t LineWidthA, int64_t width, int32_t* indx,
+                                      int32_t* status);
+B2M_API int32_t b2m_dev_MatrixLUBackSubst(b2m_ctx* ctx, const double* LUDecomp, int64_t LineWidthLU, int64_t width,
+                                  const int32_t* indx, double* B, int64_t LineWidthB, int64_t nrhs);
+B2M_API int32_t b2m_dev_MatrixLinEQSolve(b2m_ctx* ctx, const double* A, int64_t LineWidthA, int64_t width,
+                                 const double* B, int64_t LineWidthB, double* X, int64_t LineWidthX,
+                                 int64_t Width2, int64_t NumRefinements, int32_t* status);
+B2M_API int32_t b2m_dev_MatrixInverseInPlace(b2m_ctx* ctx, double* A, int64_t LineWidthA, int64_t width, int32_t* status);
+B2M_API int32_t b2m_dev_MatrixDeterminant(b2m_ctx* ctx, const double* A, int64_t LineWidthA, int64_t width, double* det);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* B2M_H */

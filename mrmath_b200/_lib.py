@@ -1,0 +1,109 @@
+"""ctypes binding of libb2m.so (the C ABI declared in include/b2m.h).
+
+There is no fallback: if the shared library is missing or cannot be loaded, importing this
+module raises, so nothing can silently run a CPU path in place of the CUDA one.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libb2m.so")
+
+i32, i64, dbl, vp = C.c_int32, C.c_int64, C.c_double, C.c_void_p
+
+# status codes (b2m.h)
+OK, SINGULAR = 0, 1
+ERR_DIM, ERR_CUDA, ERR_ALLOC, ERR_TIMEOUT, ERR_ARG, ERR_NOCONV, ERR_UNSUPPORTED = -1, -2, -3, -4, -5, -6, -7
+DO_NONE, DO_ADD, DO_SUB = 0, 1, 2
+
+# name -> (restype, argtypes); pointers are passed as integers (c_void_p) so that numpy
+# arrays (host) and torch tensors (device) use the same signatures.
+SIGNATURES: dict[str, tuple] = {
+    "b2m_create": (i32, [i32, C.POINTER(vp)]),
+    "b2m_destroy": (i32, [vp]),
+    "b2m_set_stream": (i32, [vp, vp]),
+    "b2m_synchronize": (i32, [vp]),
+    "b2m_last_error": (C.c_char_p, [vp]),
+    "b2m_status_string": (C.c_char_p, [i32]),
+    "b2m_kernel_launches": (i64, [vp]),
+    "b2m_MatrixMultEx": (i32, [vp, vp, i64, vp, vp, i64, i64, i64, i64, i64, i64, i32, i32]),
+    "b2m_dev_MatrixMultEx": (i32, [vp, vp, i64, vp, vp, i64, i64, i64, i64, i64, i64, i32, i32]),
+    "b2m_MatrixLUDecompInPlace": (i32, [vp, vp, i64, i64, vp]),
+    "b2m_MatrixLUDecomp": (i32, [vp, vp, i64, vp, i64, i64, vp]),
+    "b2m_MatrixLUBackSubst": (i32, [vp, vp, i64, i64, vp, vp, i64, i64]),
+    "b2m_MatrixInverseInPlace": (i32, [vp, vp, i64, i64]),
+    "b2m_MatrixDeterminant": (i32, [vp, vp, i64, i64, vp]),
+    "b2m_MatrixLinEQSolve": (i32, [vp, vp, i64, i64, vp, i64, vp, i64, i64, i64]),
+    "b2m_dev_MatrixLUDecompInPlace": (i32, [vp, vp, i64, i64, vp, vp]),
+    "b2m_dev_MatrixLUBackSubst": (i32, [vp, vp, i64, i64, vp, vp, i64, i64]),
+    "b2m_dev_MatrixLinEQSolve": (i32, [vp, vp, i64, i64, vp, i64, vp, i64, i64, i64, vp]),
+    "b2m_dev_MatrixInverseInPlace": (i32, [vp, vp, i64, i64, vp]),
+    "b2m_dev_MatrixDeterminant": (i32, [vp, vp, i64, i64, vp]),
+}
+
+
+def load(path: str = LIB_PATH) -> C.CDLL:
+    if not os.path.exists(path):
+        raise ImportError(
+            f"libb2m.so not found at {path}: build it with `python -m mrmath_b200.build` "
+            "(there is no CPU fallback)")
+    lib = C.CDLL(path)
+    for name, (res, args) in SIGNATURES.items():
+        f = getattr(lib, name)
+        f.restype = res
+        f.argtypes = args
+    return lib
+
+
+lib = load()
+
+
+class B2MError(RuntimeError):
+    def __init__(self, status: int, msg: str):
+        super().__init__(f"b2m status {status}: {msg}")
+        self.status = status
+
+
+class Context:
+    """One libb2m context (device, stream, workspaces).  Mirrors b2m_create/b2m_destroy."""
+
+    def __init__(self, device: int = 0):
+        h = vp()
+        st = lib.b2m_create(device, C.byref(h))
+        if st != OK:
+            raise B2MError(st, lib.b2m_status_string(st).decode())
+        self.h = h
+        self.device = device
+
+    def close(self) -> None:
+        if self.h:
+            lib.b2m_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def last_error(self) -> str:
+        return lib.b2m_last_error(self.h).decode()
+
+    def check(self, status: int, allow=(OK,)) -> int:
+        if status in allow:
+            return status
+        raise B2MError(status, f"{lib.b2m_status_string(status).decode()}: {self.last_error()}")
+
+    def set_stream(self, stream_handle: int | None) -> None:
+        self.check(lib.b2m_set_stream(self.h, stream_handle or None))
+
+    def synchronize(self) -> None:
+        self.check(lib.b2m_synchronize(self.h))
+
+    def kernel_launches(self) -> int:
+        return lib.b2m_kernel_launches(self.h)
+
+    def call(self, name: str, *args, allow=(OK,)) -> int:
+        return self.check(getattr(lib, name)(self.h, *args), allow=allow)

@@ -1,0 +1,484 @@
+// abi.cu -- the extern "C" entry points of b2m.h for GEMM, LU, back-substitution, inverse,
+// determinant and the linear-equation solve (plain FP64 form).
+//
+// Host-buffer calls (b2m_Matrix*) mirror the reference routines of the same name: they copy
+// the operands into library-owned device buffers whose row stride is padded for TMA, run the
+// device path on the context stream, copy the results back and return the reference's result
+// code.  Device-buffer calls (b2m_dev_*) run asynchronously on the context stream.
+#include <cstring>
+
+#include "common.cuh"
+#include "kernels.cuh"
+
+using namespace b2m;
+
+namespace {
+
+Ctx* as_ctx(b2m_ctx* h) { return reinterpret_cast<Ctx*>(h); }
+
+int64_t padded_ld(int64_t cols) { return round_up(std::max<int64_t>(cols, 1), 16); }
+
+// the reference asserts LineWidth >= width*sizeof(double); strides must also be whole doubles
+bool lw_ok(int64_t lw, int64_t cols) { return lw >= cols * 8 && (lw % 8) == 0; }
+
+int32_t upload(Ctx* ctx, double* dst, int64_t ld, const double* src, int64_t lw_bytes, int64_t rows, int64_t cols) {
+    if (rows <= 0 || cols <= 0) return B2M_OK;
+    B2M_CU(ctx, cudaMemcpy2DAsync(dst, ld * 8, src, lw_bytes, cols * 8, rows, cudaMemcpyHostToDevice, ctx->stream));
+    return B2M_OK;
+}
+int32_t download(Ctx* ctx, double* dst, int64_t lw_bytes, const double* src, int64_t ld, int64_t rows, int64_t cols) {
+    if (rows <= 0 || cols <= 0) return B2M_OK;
+    B2M_CU(ctx, cudaMemcpy2DAsync(dst, lw_bytes, src, ld * 8, cols * 8, rows, cudaMemcpyDeviceToHost, ctx->stream));
+    return B2M_OK;
+}
+
+int32_t reset_status(Ctx* ctx) {
+    B2M_CU(ctx, cudaMemsetAsync(ctx->d_status, 0, kNumStatus * sizeof(int32_t), ctx->stream));
+    return B2M_OK;
+}
+
+// reads the status words; returns B2M_SINGULAR / B2M_ERR_TIMEOUT / B2M_OK
+int32_t finish(Ctx* ctx) {
+    B2M_CU(ctx, cudaMemcpyAsync(ctx->h_status, ctx->d_status, kNumStatus * sizeof(int32_t), cudaMemcpyDeviceToHost,
+                                ctx->stream));
+    B2M_CU(ctx, cudaStreamSynchronize(ctx->stream));
+    if (ctx->h_status[kTimeout] != 0)
+        return fail(ctx, B2M_ERR_TIMEOUT, "a bounded device wait gave up (site %d)", ctx->h_status[kTimeout]);
+    return ctx->h_status[kInfo] != 0 ? B2M_SINGULAR : B2M_OK;
+}
+
+struct MultShape {
+    int64_t M, N, K;
+};
+
+int32_t mult_shape(Ctx* ctx, int32_t trans, int64_t w1, int64_t h1, int64_t w2, int64_t h2, MultShape* s) {
+    if (w1 < 0 || h1 < 0 || w2 < 0 || h2 < 0) return fail(ctx, B2M_ERR_DIM, "negative dimension");
+    switch (trans) {
+        case 0:
+            if (w1 != h2) return fail(ctx, B2M_ERR_DIM, "MatrixMult: width1 (%lld) != height2 (%lld)", (long long)w1,
+                                      (long long)h2);
+            *s = {h1, w2, w1};
+            return B2M_OK;
+        case 1:
+            if (h1 != h2) return fail(ctx, B2M_ERR_DIM, "MatrixMultT1: height1 != height2");
+            *s = {w1, w2, h1};
+            return B2M_OK;
+        case 2:
+            if (w1 != w2) return fail(ctx, B2M_ERR_DIM, "MatrixMultT2: width1 != width2");
+            *s = {h1, h2, w1};
+            return B2M_OK;
+        default: return fail(ctx, B2M_ERR_ARG, "trans must be 0, 1 or 2");
+    }
+}
+
+// GEMM on device operands that satisfy the TMA rules (16-byte aligned base, even stride)
+int32_t mult_device_aligned(Ctx* ctx, int32_t trans, int32_t op, const MultShape& s, const double* A, int64_t lda,
+                            int64_t arows, int64_t acols, const double* B, int64_t ldb, int64_t brows, int64_t bcols,
+                            double* C, int64_t ldc) {
+    DOperand a{A, lda, arows, acols, 0, 0, trans != 1};
+    DOperand b{B, ldb, brows, bcols, 0, 0, trans == 2};
+    return dgemm_tiled(ctx, ctx->stream, a, b, C, ldc, s.M, s.N, s.K, op, false);
+}
+
+}  // namespace
+
+// ======================================================================================= GEMM
+extern "C" int32_t b2m_MatrixMultEx(b2m_ctx* h, double* dest, int64_t destLineWidth, const double* mt1,
+                                    const double* mt2, int64_t width1, int64_t height1, int64_t width2,
+                                    int64_t height2, int64_t LineWidth1, int64_t LineWidth2, int32_t op,
+                                    int32_t trans) {
+    Ctx* ctx = as_ctx(h);
+    if (!ctx) return B2M_ERR_ARG;
+    std::lock_guard<std::mutex> lk(ctx->mtx);
+    if (!dest || !mt1 || !mt2) return fail(ctx, B2M_ERR_ARG, "null pointer");
+    if (op < 0 || op > 2) return fail(ctx, B2M_ERR_ARG, "op must be 0 (doNone), 1 (doAdd) or 2 (doSub)");
+    MultShape s;
+    B2M_TRY(mult_shape(ctx, trans, width1, height1, width2, height2, &s));
+    if (!lw_ok(LineWidth1, width1) || !lw_ok(LineWidth2, width2) || !lw_ok(destLineWidth, s.N))
+        return fail(ctx, B2M_ERR_DIM, "Line widths do not match");
+    if (s.M == 0 || s.N == 0) return B2M_OK;
+    cudaSetDevice(ctx->device);
+    const int64_t lda = padded_ld(width1), ldb = padded_ld(width2), ldc = padded_ld(s.N);
+    void *pa, *pb, *pc;
+    B2M_TRY(ws_get(ctx, kWsMatA, (size_t)(std::max<int64_t>(height1, 1) * lda * 8), &pa));
+    B2M_TRY(ws_get(ctx, kWsMatB, (size_t)(std::max<int64_t>(height2, 1) * ldb * 8), &pb));
+    B2M_TRY(ws_get(ctx, kWsMatC, (size_t)(s.M * ldc * 8), &pc));
+    double *dA = (double*)pa, *dB = (double*)pb, *dC = (double*)pc;
+    B2M_TRY(upload(ctx, dA, lda, mt1, LineWidth1, height1, width1));
+    B2M_TRY(upload(ctx, dB, ldb, mt2, LineWidth2, height2, width2));
+    if (op != B2M_DO_NONE) B2M_TRY(upload(ctx, dC, ldc, dest, destLineWidth, s.M, s.N));
+    B2M_TRY(reset_status(ctx));
+    B2M_TRY(mult_device_aligned(ctx, trans, op, s, dA, lda, height1, width1, dB, ldb, height2, width2, dC, ldc));
+    B2M_TRY(download(ctx, dest, destLineWidth, dC, ldc, s.M, s.N));
+    return finish(ctx);
+}
+
+extern "C" int32_t b2m_dev_MatrixMultEx(b2m_ctx* h, double* dest, int64_t destLineWidth, const double* mt1,
+                                        const double* mt2, int64_t width1, int64_t height1, int64_t width2,
+                                        int64_t height2, int64_t LineWidth1, int64_t LineWidth2, int32_t op,
+                                        int32_t trans) {
+    Ctx* ctx = as_ctx(h);
+    if (!ctx) return B2M_ERR_ARG;
+    std::lock_guard<std::mutex> lk(ctx->mtx);
+    if (!dest || !mt1 || !mt2) return fail(ctx, B2M_ERR_ARG, "null pointer");
+    if (op < 0 || op > 2) return fail(ctx, B2M_ERR_ARG, "invalid op");
+    MultShape s;
+    B2M_TRY(mult_shape(ctx, trans, width1, height1, width2, height2, &s));
+    if (!lw_ok(LineWidth1, width1) || !lw_ok(LineWidth2, width2) || !lw_ok(destLineWidth, s.N))
+        return fail(ctx, B2M_ERR_DIM, "Line widths do not match");
+    if (s.M == 0 || s.N == 0) return B2M_OK;
+    const double* A = mt1;
+    const double* B = mt2;
+    int64_t lda = LineWidth1 / 8, ldb = LineWidth2 / 8;
+    // operands that break the TMA rules are repacked into aligned workspaces
+    if (!aligned16(A) || (LineWidth1 & 15)) {
+        void* p;
+        const int64_t ld = padded_ld(width1);
+        B2M_TRY(ws_get(ctx, kWsMatA, (size_t)(std::max<int64_t>(height1, 1) * ld * 8), &p));
+        B2M_TRY(copy_matrix(ctx, ctx->stream, (double*)p, ld * 8, A, LineWidth1, height1, width1));
+        A = (const double*)p;
+        lda = ld;
+    }
+    if (!aligned16(B) || (LineWidth2 & 15)) {
+        void* p;
+        const int64_t ld = padded_ld(width2);
+        B2M_TRY(ws_get(ctx, kWsMatB, (size_t)(std::max<int64_t>(height2, 1) * ld * 8), &p));
+        B2M_TRY(copy_matrix(ctx, ctx->stream, (double*)p, ld * 8, B, LineWidth2, height2, width2));
+        B = (const double*)p;
+        ldb = ld;
+    }
+    return mult_device_aligned(ctx, trans, op, s, A, lda, height1, width1, B, ldb, height2, width2, dest,
+                               destLineWidth / 8);
+}
+
+// ======================================================================================= LU
+namespace {
+
+// factor the n x n matrix at host A (LineWidthA) into device workspace; leaves LU in kWsMatA
+int32_t factor_host(Ctx* ctx, const double* A, int64_t lwA, int64_t n, double** dLU, int64_t* ld, int32_t** dpiv,
+                    int32_t** dperm) {
+    *ld = padded_ld(n);
+    void *pa, *pp;
+    B2M_TRY(ws_get(ctx, kWsMatA, (size_t)(n * *ld * 8), &pa));
+    B2M_TRY(ws_get(ctx, kWsPiv, (size_t)(2 * n * 4), &pp));
+    *dLU = (double*)pa;
+    *dpiv = (int32_t*)pp;
+    *dperm = *dpiv + n;
+    B2M_TRY(upload(ctx, *dLU, *ld, A, lwA, n, n));
+    B2M_CU(ctx, cudaMemsetAsync(*dpiv, 0, (size_t)n * 4, ctx->stream));
+    B2M_TRY(reset_status(ctx));
+    return lu_factor_f64(ctx, ctx->stream, *dLU, *ld, n, *dpiv, *dperm);
+}
+
+}  // namespace
+
+extern "C" int32_t b2m_MatrixLUDecomp(b2m_ctx* h, const double* A, int64_t LineWidthA, double* LUDecomp,
+                                      int64_t LineWidthLU, int64_t width, int32_t* indx) {
+    Ctx* ctx = as_ctx(h);
+    if (!ctx) return B2M_ERR_ARG;
+    std::lock_guard<std::mutex> lk(ctx->mtx);
+    if (!A || !LUDecomp || !indx) return fail(ctx, B2M_ERR_ARG, "null pointer");
+    if (width <= 0 || !lw_ok(LineWidthA, width) || !lw_ok(LineWidthLU, width))
+        return fail(ctx, B2M_ERR_DIM, "Dimension Error");
+    cudaSetDevice(ctx->device);
+    double* dLU;
+    int64_t ld;
+    int32_t *dpiv, *dperm;
+    std::memset(indx, 0, (size_t)width * sizeof(int32_t));  // FillChar(indx^, ...) LinAlgLU.pas:287
+    B2M_TRY(factor_host(ctx, A, LineWidthA, width, &dLU, &ld, &dpiv, &dperm));
+    B2M_TRY(download(ctx, LUDecomp, LineWidthLU, dLU, ld, width, width));
+    B2M_CU(ctx, cudaMemcpyAsync(indx, dpiv, (size_t)width * 4, cudaMemcpyDeviceToHost, ctx->stream));
+    return finish(ctx);
+}
+
+extern "C" int32_t b2m_MatrixLUDecompInPlace(b2m_ctx* h, double* A, int64_t LineWidthA, int64_t width,
+                                             int32_t* indx) {
+    return b2m_MatrixLUDecomp(h, A, LineWidthA, A, LineWidthA, width, indx);
+}
+
+extern "C" int32_t b2m_MatrixLUBackSubst(b2m_ctx* h, const double* LUDecomp, int64_t LineWidthLU, int64_t width,
+                                         const int32_t* indx, double* B, int64_t LineWidthB, int64_t nrhs) {
+    Ctx* ctx = as_ctx(h);
+    if (!ctx) return B2M_ERR_ARG;
+    std::lock_guard<std::mutex> lk(ctx->mtx);
+    if (!LUDecomp || !indx || !B) return fail(ctx, B2M_ERR_ARG, "null pointer");
+    if (width <= 0 || nrhs <= 0 || !lw_ok(LineWidthLU, width) || !lw_ok(LineWidthB, nrhs))
+        return fail(ctx, B2M_ERR_DIM, "Dimension Error");
+    cudaSetDevice(ctx->device);
+    const int64_t n = width, ld = padded_ld(n), ldb = padded_ld(nrhs);
+    void *pa, *pb, *pp;
+    B2M_TRY(ws_get(ctx, kWsMatA, (size_t)(n * ld * 8), &pa));
+    B2M_TRY(ws_get(ctx, kWsMatB, (size_t)(n * ldb * 8), &pb));
+    B2M_TRY(ws_get(ctx, kWsPiv, (size_t)(2 * n * 4), &pp));
+    int32_t* dpiv = (int32_t*)pp;
+    int32_t* dperm = dpiv + n;
+    B2M_TRY(upload(ctx, (double*)pa, ld, LUDecomp, LineWidthLU, n, n));
+    B2M_TRY(upload(ctx, (double*)pb, ldb, B, LineWidthB, n, nrhs));
+    B2M_CU(ctx, cudaMemcpyAsync(dpiv, indx, (size_t)n * 4, cudaMemcpyHostToDevice, ctx->stream));
+    B2M_TRY(reset_status(ctx));
+    B2M_TRY(perm_from_ipiv(ctx, ctx->stream, dpiv, n, dperm));
+    B2M_TRY(lu_solve_f64(ctx, ctx->stream, (double*)pa, ld, n, dperm, (double*)pb, ldb, nrhs));
+    B2M_TRY(download(ctx, B, LineWidthB, (double*)pb, ldb, n, nrhs));
+    return finish(ctx);
+}
+
+extern "C" int32_t b2m_MatrixInverseInPlace(b2m_ctx* h, double* A, int64_t LineWidthA, int64_t width) {
+    Ctx* ctx = as_ctx(h);
+    if (!ctx) return B2M_ERR_ARG;
+    std::lock_guard<std::mutex> lk(ctx->mtx);
+    if (!A) return fail(ctx, B2M_ERR_ARG, "null pointer");
+    if (width <= 0 || !lw_ok(LineWidthA, width)) return fail(ctx, B2M_ERR_DIM, "Dimension Error");
+    cudaSetDevice(ctx->device);
+    double* dLU;
+    int64_t ld;
+    int32_t *dpiv, *dperm;
+    B2M_TRY(factor_host(ctx, A, LineWidthA, width, &dLU, &ld, &dpiv, &dperm));
+    const int32_t st = finish(ctx);
+    if (st != B2M_OK) return st;  // singular: A is left as it was (the reference works on a copy)
+    void* pb;
+    B2M_TRY(ws_get(ctx, kWsMatB, (size_t)(width * ld * 8), &pb));
+    double* X = (double*)pb;
+    B2M_CU(ctx, cudaMemset2DAsync(X, ld * 8, 0, width * 8, width, ctx->stream));
+    B2M_TRY(set_diagonal(ctx, ctx->stream, X, ld, width, 1.0));
+    B2M_TRY(lu_solve_f64(ctx, ctx->stream, dLU, ld, width, dperm, X, ld, width));
+    B2M_TRY(download(ctx, A, LineWidthA, X, ld, width, width));
+    return finish(ctx);
+}
+
+extern "C" int32_t b2m_MatrixDeterminant(b2m_ctx* h, const double* A, int64_t LineWidthA, int64_t width,
+                                         double* det) {
+    Ctx* ctx = as_ctx(h);
+    if (!ctx) return B2M_ERR_ARG;
+    std::lock_guard<std::mutex> lk(ctx->mtx);
+    if (!A || !det) return fail(ctx, B2M_ERR_ARG, "null pointer");
+    if (width <= 0 || !lw_ok(LineWidthA, width)) return fail(ctx, B2M_ERR_DIM, "Dimension error");
+    cudaSetDevice(ctx->device);
+    double* dLU;
+    int64_t ld;
+    int32_t *dpiv, *dperm;
+    B2M_TRY(factor_host(ctx, A, LineWidthA, width, &dLU, &ld, &dpiv, &dperm));
+    void* ps;
+    B2M_TRY(ws_get(ctx, kWsSmall, 256, &ps));
+    B2M_TRY(lu_determinant(ctx, ctx->stream, dLU, ld, width, dpiv, (double*)ps));
+    B2M_CU(ctx, cudaMemcpyAsync(det, ps, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    const int32_t st = finish(ctx);
+    if (st == B2M_SINGULAR) {
+        *det = 0.0;  // MatrixDeterminant returns 0 for a singular matrix
+        return B2M_OK;
+    }
+    return st;
+}
+
+namespace {
+
+// X = A^{-1} B with optional fixed-count FP64 refinement; all operands on the device with
+// TMA-friendly strides.  dA is overwritten by the factors when keepA == nullptr.
+int32_t solve_device(Ctx* ctx, double* dLU, int64_t ld, int64_t n, const double* dAorig, int64_t ldAo,
+                     const double* dB, int64_t ldb, double* dX, int64_t ldx, int64_t nrhs, int64_t numRef,
+                     int32_t* dpiv, int32_t* dperm) {
+    B2M_TRY(lu_factor_f64(ctx, ctx->stream, dLU, ld, n, dpiv, dperm));
+    B2M_TRY(copy_matrix(ctx, ctx->stream, dX, ldx * 8, dB, ldb * 8, n, nrhs));
+    B2M_TRY(lu_solve_f64(ctx, ctx->stream, dLU, ld, n, dperm, dX, ldx, nrhs));
+    if (numRef > 0) {
+        void* pr;
+        B2M_TRY(ws_get(ctx, kWsF, (size_t)(n * ldx * 8), &pr));
+        double* R = (double*)pr;
+        for (int64_t it = 0; it < numRef; ++it) {
+            // R = B - A X (refinement step of MatrixLinEQSolve :542-586 with the sign folded)
+            B2M_TRY(copy_matrix(ctx, ctx->stream, R, ldx * 8, dB, ldb * 8, n, nrhs));
+            DOperand a{dAorig, ldAo, n, n, 0, 0, true};
+            DOperand b{dX, ldx, n, nrhs, 0, 0, false};
+            B2M_TRY(dgemm_tiled(ctx, ctx->stream, a, b, R, ldx, n, nrhs, n, B2M_DO_SUB, true));
+            B2M_TRY(lu_solve_f64(ctx, ctx->stream, dLU, ld, n, dperm, R, ldx, nrhs));
+            // X += R
+            B2M_TRY(axpy_matrix(ctx, ctx->stream, dX, ldx, R, ldx, n, nrhs));
+        }
+    }
+    return B2M_OK;
+}
+
+}  // namespace
+
+extern "C" int32_t b2m_MatrixLinEQSolve(b2m_ctx* h, const double* A, int64_t LineWidthA, int64_t width,
+                                        const double* B, int64_t LineWidthB, double* X, int64_t LineWidthX,
+                                        int64_t Width2, int64_t NumRefinements) {
+    Ctx* ctx = as_ctx(h);
+    if (!ctx) return B2M_ERR_ARG;
+    std::lock_guard<std::mutex> lk(ctx->mtx);
+    if (!A || !B || !X) return fail(ctx, B2M_ERR_ARG, "null pointer");
+    if (width <= 0 || Width2 <= 0 || !lw_ok(LineWidthA, width) || !lw_ok(LineWidthB, Width2) ||
+        !lw_ok(LineWidthX, Width2) || NumRefinements < 0)
+        return fail(ctx, B2M_ERR_DIM, "Dimension error");
+    cudaSetDevice(ctx->device);
+    const int64_t n = width, ld = padded_ld(n), ldb = padded_ld(Width2);
+    void *pa, *pb, *px, *pp, *pc = nullptr;
+    B2M_TRY(ws_get(ctx, kWsMatA, (size_t)(n * ld * 8), &pa));
+    B2M_TRY(ws_get(ctx, kWsMatB, (size_t)(n * ldb * 8), &pb));
+    B2M_TRY(ws_get(ctx, kWsMatD, (size_t)(n * ldb * 8), &px));
+    B2M_TRY(ws_get(ctx, kWsPiv, (size_t)(2 * n * 4), &pp));
+    B2M_TRY(upload(ctx, (double*)pa, ld, A, LineWidthA, n, n));
+    B2M_TRY(upload(ctx, (double*)pb, ldb, B, LineWidthB, n, Width2));
+    if (NumRefinements > 0) {
+        B2M_TRY(ws_get(ctx, kWsMatC, (size_t)(n * ld * 8), &pc));
+        B2M_TRY(copy_matrix(ctx, ctx->stream, (double*)pc, ld * 8, (double*)pa, ld * 8, n, n));
+    }
+    B2M_TRY(reset_status(ctx));
+    int32_t* dpiv = (int32_t*)pp;
+    B2M_TRY(solve_device(ctx, (double*)pa, ld, n, (double*)pc, ld, (double*)pb, ldb, (double*)px, ldb, Width2,
+                         NumRefinements, dpiv, dpiv + n));
+    const int32_t st = finish(ctx);
+    if (st != B2M_OK) return st;  // singular: X untouched, as in the reference
+    B2M_TRY(download(ctx, X, LineWidthX, (double*)px, ldb, n, Width2));
+    return finish(ctx);
+}
+
+// ======================================================================================= device twins
+extern "C" int32_t b2m_dev_MatrixLUDecompInPlace(b2m_ctx* h, double* A, int64_t LineWidthA, int64_t width,
+                                                 int32_t* indx, int32_t* status) {
+    Ctx* ctx = as_ctx(h);
+    if (!ctx) return B2M_ERR_ARG;
+    std::lock_guard<std::mutex> lk(ctx->mtx);
+    if (!A || !indx) return fail(ctx, B2M_ERR_ARG, "null pointer");
+    if (width <= 0 || !lw_ok(LineWidthA, width)) return fail(ctx, B2M_ERR_DIM, "Dimension Error");
+    const int64_t n = width;
+    double* dA = A;
+    int64_t ld = LineWidthA / 8;
+    const bool direct = aligned16(A) && (LineWidthA & 15) == 0;
+    if (!direct) {
+        void* p;
+        ld = padded_ld(n);
+        B2M_TRY(ws_get(ctx, kWsMatA, (size_t)(n * ld * 8), &p));
+        dA = (double*)p;
+        B2M_TRY(copy_matrix(ctx, ctx->stream, dA, ld * 8, A, LineWidthA, n, n));
+    }
+    void* pp;
+    B2M_TRY(ws_get(ctx, kWsPiv, (size_t)(2 * n * 4), &pp));
+    B2M_CU(ctx, cudaMemsetAsync(indx, 0, (size_t)n * 4, ctx->stream));
+    B2M_TRY(reset_status(ctx));
+    B2M_TRY(lu_factor_f64(ctx, ctx->stream, dA, ld, n, indx, (int32_t*)pp + n));
+    if (!direct) B2M_TRY(copy_matrix(ctx, ctx->stream, A, LineWidthA, dA, ld * 8, n, n));
+    if (status)
+        B2M_CU(ctx, cudaMemcpyAsync(status, ctx->d_status + kInfo, 4, cudaMemcpyDeviceToDevice, ctx->stream));
+    return B2M_OK;
+}
+
+extern "C" int32_t b2m_dev_MatrixLUBackSubst(b2m_ctx* h, const double* LUDecomp, int64_t LineWidthLU,
+                                             int64_t width, const int32_t* indx, double* B, int64_t LineWidthB,
+                                             int64_t nrhs) {
+    Ctx* ctx = as_ctx(h);
+    if (!ctx) return B2M_ERR_ARG;
+    std::lock_guard<std::mutex> lk(ctx->mtx);
+    if (!LUDecomp || !indx || !B) return fail(ctx, B2M_ERR_ARG, "null pointer");
+    if (width <= 0 || nrhs <= 0 || !lw_ok(LineWidthLU, width) || !lw_ok(LineWidthB, nrhs))
+        return fail(ctx, B2M_ERR_DIM, "Dimension Error");
+    const int64_t n = width;
+    const double* LU = LUDecomp;
+    int64_t ld = LineWidthLU / 8;
+    if (!aligned16(LU) || (LineWidthLU & 15)) {
+        void* p;
+        ld = padded_ld(n);
+        B2M_TRY(ws_get(ctx, kWsMatA, (size_t)(n * ld * 8), &p));
+        B2M_TRY(copy_matrix(ctx, ctx->stream, (double*)p, ld * 8, LUDecomp, LineWidthLU, n, n));
+        LU = (const double*)p;
+    }
+    double* dB = B;
+    int64_t ldb = LineWidthB / 8;
+    const bool bdirect = aligned16(B) && (LineWidthB & 15) == 0;
+    if (!bdirect) {
+        void* p;
+        ldb = padded_ld(nrhs);
+        B2M_TRY(ws_get(ctx, kWsMatB, (size_t)(n * ldb * 8), &p));
+        dB = (double*)p;
+        B2M_TRY(copy_matrix(ctx, ctx->stream, dB, ldb * 8, B, LineWidthB, n, nrhs));
+    }
+    void* pp;
+    B2M_TRY(ws_get(ctx, kWsPiv, (size_t)(2 * n * 4), &pp));
+    int32_t* dperm = (int32_t*)pp + n;
+    B2M_TRY(reset_status(ctx));
+    B2M_TRY(perm_from_ipiv(ctx, ctx->stream, indx, n, dperm));
+    B2M_TRY(lu_solve_f64(ctx, ctx->stream, LU, ld, n, dperm, dB, ldb, nrhs));
+    if (!bdirect) B2M_TRY(copy_matrix(ctx, ctx->stream, B, LineWidthB, dB, ldb * 8, n, nrhs));
+    return B2M_OK;
+}
+
+extern "C" int32_t b2m_dev_MatrixLinEQSolve(b2m_ctx* h, const double* A, int64_t LineWidthA, int64_t width,
+                                            const double* B, int64_t LineWidthB, double* X, int64_t LineWidthX,
+                                            int64_t Width2, int64_t NumRefinements, int32_t* status) {
+    Ctx* ctx = as_ctx(h);
+    if (!ctx) return B2M_ERR_ARG;
+    std::lock_guard<std::mutex> lk(ctx->mtx);
+    if (!A || !B || !X) return fail(ctx, B2M_ERR_ARG, "null pointer");
+    if (width <= 0 || Width2 <= 0 || !lw_ok(LineWidthA, width) || !lw_ok(LineWidthB, Width2) ||
+        !lw_ok(LineWidthX, Width2) || NumRefinements < 0)
+        return fail(ctx, B2M_ERR_DIM, "Dimension error");
+    const int64_t n = width, ld = padded_ld(n), ldb = padded_ld(Width2);
+    void *pa, *pb, *px, *pp;
+    B2M_TRY(ws_get(ctx, kWsMatA, (size_t)(n * ld * 8), &pa));
+    B2M_TRY(ws_get(ctx, kWsMatB, (size_t)(n * ldb * 8), &pb));
+    B2M_TRY(ws_get(ctx, kWsMatD, (size_t)(n * ldb * 8), &px));
+    B2M_TRY(ws_get(ctx, kWsPiv, (size_t)(2 * n * 4), &pp));
+    B2M_TRY(copy_matrix(ctx, ctx->stream, (double*)pa, ld * 8, A, LineWidthA, n, n));
+    B2M_TRY(copy_matrix(ctx, ctx->stream, (double*)pb, ldb * 8, B, LineWidthB, n, Width2));
+    const double* Ao = A;
+    int64_t ldAo = LineWidthA / 8;
+    if (NumRefinements > 0 && (!aligned16(A) || (LineWidthA & 15))) {
+        void* pc;
+        B2M_TRY(ws_get(ctx, kWsMatC, (size_t)(n * ld * 8), &pc));
+        B2M_TRY(copy_matrix(ctx, ctx->stream, (double*)pc, ld * 8, A, LineWidthA, n, n));
+        Ao = (const double*)pc;
+        ldAo = ld;
+    }
+    B2M_TRY(reset_status(ctx));
+    int32_t* dpiv = (int32_t*)pp;
+    B2M_TRY(solve_device(ctx, (double*)pa, ld, n, Ao, ldAo, (double*)pb, ldb, (double*)px, ldb, Width2,
+                         NumRefinements, dpiv, dpiv + n));
+    B2M_TRY(copy_matrix(ctx, ctx->stream, X, LineWidthX, (double*)px, ldb * 8, n, Width2));
+    if (status)
+        B2M_CU(ctx, cudaMemcpyAsync(status, ctx->d_status + kInfo, 4, cudaMemcpyDeviceToDevice, ctx->stream));
+    return B2M_OK;
+}
+
+extern "C" int32_t b2m_dev_MatrixInverseInPlace(b2m_ctx* h, double* A, int64_t LineWidthA, int64_t width,
+                                                int32_t* status) {
+    Ctx* ctx = as_ctx(h);
+    if (!ctx) return B2M_ERR_ARG;
+    std::lock_guard<std::mutex> lk(ctx->mtx);
+    if (!A) return fail(ctx, B2M_ERR_ARG, "null pointer");
+    if (width <= 0 || !lw_ok(LineWidthA, width)) return fail(ctx, B2M_ERR_DIM, "Dimension Error");
+    const int64_t n = width, ld = padded_ld(n);
+    void *pa, *pb, *pp;
+    B2M_TRY(ws_get(ctx, kWsMatA, (size_t)(n * ld * 8), &pa));
+    B2M_TRY(ws_get(ctx, kWsMatB, (size_t)(n * ld * 8), &pb));
+    B2M_TRY(ws_get(ctx, kWsPiv, (size_t)(2 * n * 4), &pp));
+    double* dLU = (double*)pa;
+    double* X = (double*)pb;
+    int32_t* dpiv = (int32_t*)pp;
+    B2M_TRY(copy_matrix(ctx, ctx->stream, dLU, ld * 8, A, LineWidthA, n, n));
+    B2M_TRY(reset_status(ctx));
+    B2M_TRY(lu_factor_f64(ctx, ctx->stream, dLU, ld, n, dpiv, dpiv + n));
+    B2M_CU(ctx, cudaMemset2DAsync(X, ld * 8, 0, n * 8, n, ctx->stream));
+    B2M_TRY(set_diagonal(ctx, ctx->stream, X, ld, n, 1.0));
+    B2M_TRY(lu_solve_f64(ctx, ctx->stream, dLU, ld, n, dpiv + n, X, ld, n));
+    // the inverse replaces A only when the factorisation succeeded
+    B2M_TRY(copy_if_ok(ctx, ctx->stream, A, LineWidthA / 8, X, ld, n, n));
+    if (status)
+        B2M_CU(ctx, cudaMemcpyAsync(status, ctx->d_status + kInfo, 4, cudaMemcpyDeviceToDevice, ctx->stream));
+    return B2M_OK;
+}
+
+extern "C" int32_t b2m_dev_MatrixDeterminant(b2m_ctx* h, const double* A, int64_t LineWidthA, int64_t width,
+                                             double* det) {
+    Ctx* ctx = as_ctx(h);
+    if (!ctx) return B2M_ERR_ARG;
+    std::lock_guard<std::mutex> lk(ctx->mtx);
+    if (!A || !det) return fail(ctx, B2M_ERR_ARG, "null pointer");
+    if (width <= 0 || !lw_ok(LineWidthA, width)) return fail(ctx, B2M_ERR_DIM, "Dimension error");
+    const int64_t n = width, ld = padded_ld(n);
+    void *pa, *pp;
+    B2M_TRY(ws_get(ctx, kWsMatA, (size_t)(n * ld * 8), &pa));
+    B2M_TRY(ws_get(ctx, kWsPiv, (size_t)(2 * n * 4), &pp));
+    B2M_TRY(copy_matrix(ctx, ctx->stream, (double*)pa, ld * 8, A, LineWidthA, n, n));
+    B2M_TRY(reset_status(ctx));
+    B2M_TRY(lu_factor_f64(ctx, ctx->stream, (double*)pa, ld, n, (int32_t*)pp, (int32_t*)pp + n));
+    return lu_determinant(ctx, ctx->stream, (double*)pa, ld, n, (int32_t*)pp, det);
+}

@@ -1,0 +1,154 @@
+// common.cuh -- shared internals of libb2m: context, device workspaces, error plumbing,
+// tensor-map encoding and the small PTX helpers used by the sm_100a kernels.
+#pragma once
+
+#include <cuda.h>
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <cstdio>
+#include <mutex>
+#include <string>
+
+#include "../../include/b2m.h"
+
+namespace b2m {
+
+// ------------------------------------------------------------------ device status words
+// Every context owns a small device array of int32 status words.  Kernels that can fail
+// (singular pivot, bounded wait that gave up) write here; the host reads it after the call.
+enum StatusWord : int {
+    kInfo = 0,      // 0 ok, 1 singular (first singular pivot stops the factorisation)
+    kTimeout = 1,   // nonzero: some bounded wait gave up; value = site id
+    kIrIters = 2,   // refinement iterations done (mixed solve)
+    kIrState = 3,   // refinement state: 0 converged, 1 stalled, 2 diverged
+    kNumStatus = 8
+};
+
+// ------------------------------------------------------------------ workspace slots
+enum WsSlot : int {
+    kWsMatA = 0,   // device copy of A (host API) / LU factors
+    kWsMatB,       // device copy of B / X
+    kWsMatC,       // device copy of C / scratch
+    kWsMatD,       // extra (FP32 LU, Ozaki slices, ...)
+    kWsPiv,        // pivots and permutation
+    kWsSmall,      // norms, small vectors
+    kWsE,
+    kWsF,
+    kNumWs
+};
+
+struct Ctx {
+    int device = 0;
+    int num_sms = 148;
+    size_t smem_optin = 0;
+    cudaStream_t own_stream = nullptr;
+    cudaStream_t stream = nullptr;
+    int32_t* d_status = nullptr;     // kNumStatus words
+    int32_t* h_status = nullptr;     // pinned mirror
+    void* ws[kNumWs] = {};
+    size_t ws_bytes[kNumWs] = {};
+    void* h_pinned = nullptr;        // pinned staging for host-buffer calls
+    size_t h_pinned_bytes = 0;
+    int64_t launches = 0;
+    std::string last_error;
+    std::mutex mtx;
+};
+
+// records a message and returns the status (for `return fail(ctx, ...)`)
+int32_t fail(Ctx* ctx, int32_t status, const char* fmt, ...);
+
+#define B2M_CU(ctx, call)                                                                          \
+    do {                                                                                           \
+        cudaError_t e_ = (call);                                                                   \
+        if (e_ != cudaSuccess)                                                                     \
+            return ::b2m::fail((ctx), B2M_ERR_CUDA, "%s failed: %s (%s:%d)", #call,                \
+                               cudaGetErrorString(e_), __FILE__, __LINE__);                        \
+    } while (0)
+
+#define B2M_TRY(expr)                                                                              \
+    do {                                                                                           \
+        int32_t s_ = (expr);                                                                       \
+        if (s_ != B2M_OK) return s_;                                                               \
+    } while (0)
+
+// after a launch: count it and surface launch-configuration errors
+#define B2M_LAUNCHED(ctx)                                                                          \
+    do {                                                                                           \
+        (ctx)->launches++;                                                                         \
+        cudaError_t e_ = cudaGetLastError();                                                       \
+        if (e_ != cudaSuccess)                                                                     \
+            return ::b2m::fail((ctx), B2M_ERR_CUDA, "kernel launch failed: %s (%s:%d)",            \
+                               cudaGetErrorString(e_), __FILE__, __LINE__);                        \
+    } while (0)
+
+// grows workspace slot `slot` to at least `bytes` (never shrinks); 256-byte aligned
+int32_t ws_get(Ctx* ctx, int slot, size_t bytes, void** out);
+int32_t pinned_get(Ctx* ctx, size_t bytes, void** out);
+
+// ------------------------------------------------------------------ tensor maps
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no -lcuda needed).
+int32_t encode_tmap_2d(Ctx* ctx, CUtensorMap* map, CUtensorMapDataType dtype, int elem_bytes, const void* base,
+                       uint64_t inner, uint64_t outer, uint64_t row_stride_bytes, uint32_t box_inner,
+                       uint32_t box_outer, CUtensorMapSwizzle swizzle);
+
+inline bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
+
+// ------------------------------------------------------------------ device helpers
+// Bounded waits: every spin in this library gives up after this many polls and reports
+// B2M_ERR_TIMEOUT through the status words instead of hanging the GPU.
+constexpr uint32_t kSpinLimit = 1u << 26;
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void fence_barrier_init() {
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+}
+__device__ __forceinline__ void fence_proxy_async() {
+    asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+}
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(smem_u32(bar)) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+// returns false (and flags `timeout_word`) if the phase never completed
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int32_t* timeout_word, int site) {
+    for (uint32_t i = 0; i < kSpinLimit; ++i)
+        if (mbar_try_wait(bar, parity)) return true;
+    if (timeout_word) atomicExch(timeout_word, site);
+    return false;
+}
+
+// 2-D tiled TMA load (no multicast) into shared memory, completing on `bar`.
+__device__ __forceinline__ void tma_load_2d(void* smem_dst, const CUtensorMap* map, int x, int y, uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], "
+        "[%4];\n" ::"r"(smem_u32(smem_dst)),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(smem_u32(bar))
+        : "memory");
+}
+__device__ __forceinline__ void tma_prefetch_desc(const CUtensorMap* map) {
+    asm volatile("prefetch.tensormap [%0];\n" ::"l"(reinterpret_cast<uint64_t>(map)) : "memory");
+}
+
+__host__ __device__ inline int64_t ceil_div(int64_t a, int64_t b) { return (a + b - 1) / b; }
+__host__ __device__ inline int64_t round_up(int64_t a, int64_t b) { return ceil_div(a, b) * b; }
+
+}  // namespace b2m

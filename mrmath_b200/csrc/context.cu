@@ -1,0 +1,193 @@
+// context.cu -- context lifetime, workspaces, error strings and tensor-map encoding.
+#include <cstdarg>
+#include <cstring>
+
+#include "common.cuh"
+
+namespace b2m {
+
+int32_t fail(Ctx* ctx, int32_t status, const char* fmt, ...) {
+    if (ctx) {
+        char buf[512];
+        va_list ap;
+        va_start(ap, fmt);
+        vsnprintf(buf, sizeof(buf), fmt, ap);
+        va_end(ap);
+        ctx->last_error = buf;
+    }
+    return status;
+}
+
+int32_t ws_get(Ctx* ctx, int slot, size_t bytes, void** out) {
+    bytes = (size_t)round_up((int64_t)std::max<size_t>(bytes, 256), 256);
+    if (ctx->ws_bytes[slot] < bytes) {
+        if (ctx->ws[slot]) {
+            // the buffer may still be in use by queued work on this stream
+            B2M_CU(ctx, cudaStreamSynchronize(ctx->stream));
+            B2M_CU(ctx, cudaFree(ctx->ws[slot]));
+            ctx->ws[slot] = nullptr;
+            ctx->ws_bytes[slot] = 0;
+        }
+        if (cudaMalloc(&ctx->ws[slot], bytes) != cudaSuccess) {
+            cudaGetLastError();
+            return fail(ctx, B2M_ERR_ALLOC, "cudaMalloc(%zu) failed for workspace slot %d", bytes, slot);
+        }
+        ctx->ws_bytes[slot] = bytes;
+    }
+    *out = ctx->ws[slot];
+    return B2M_OK;
+}
+
+int32_t pinned_get(Ctx* ctx, size_t bytes, void** out) {
+    if (ctx->h_pinned_bytes < bytes) {
+        if (ctx->h_pinned) {
+            B2M_CU(ctx, cudaStreamSynchronize(ctx->stream));
+            cudaFreeHost(ctx->h_pinned);
+            ctx->h_pinned = nullptr;
+            ctx->h_pinned_bytes = 0;
+        }
+        if (cudaMallocHost(&ctx->h_pinned, bytes) != cudaSuccess) {
+            cudaGetLastError();
+            return fail(ctx, B2M_ERR_ALLOC, "cudaMallocHost(%zu) failed", bytes);
+        }
+        ctx->h_pinned_bytes = bytes;
+    }
+    *out = ctx->h_pinned;
+    return B2M_OK;
+}
+
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                  const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+static EncodeTiledFn get_encode_fn(Ctx* ctx) {
+    static EncodeTiledFn fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &p, 12000, cudaEnableDefault, &q) ==
+                cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<EncodeTiledFn>(p);
+    });
+    if (!fn) fail(ctx, B2M_ERR_CUDA, "cuTensorMapEncodeTiled entry point not available");
+    return fn;
+}
+
+int32_t encode_tmap_2d(Ctx* ctx, CUtensorMap* map, CUtensorMapDataType dtype, int elem_bytes, const void* base,
+                       uint64_t inner, uint64_t outer, uint64_t row_stride_bytes, uint32_t box_inner,
+                       uint32_t box_outer, CUtensorMapSwizzle swizzle) {
+    EncodeTiledFn fn = get_encode_fn(ctx);
+    if (!fn) return B2M_ERR_CUDA;
+    if (!aligned16(base) || (row_stride_bytes & 15u) != 0)
+        return fail(ctx, B2M_ERR_DIM, "tensor map needs a 16-byte aligned base and stride (stride %llu)",
+                    (unsigned long long)row_stride_bytes);
+    cuuint64_t dims[2] = {inner, outer};
+    cuuint64_t strides[1] = {row_stride_bytes};
+    cuuint32_t box[2] = {box_inner, box_outer};
+    cuuint32_t estr[2] = {1, 1};
+    (void)elem_bytes;
+    CUresult r = fn(map, dtype, 2, const_cast<void*>(base), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                    swizzle, CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS)
+        return fail(ctx, B2M_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d): dims %llu x %llu stride %llu box %u x %u",
+                    (int)r, (unsigned long long)inner, (unsigned long long)outer,
+                    (unsigned long long)row_stride_bytes, box_inner, box_outer);
+    return B2M_OK;
+}
+
+}  // namespace b2m
+
+using b2m::Ctx;
+
+extern "C" int32_t b2m_create(int32_t device, b2m_ctx** out) {
+    if (!out) return B2M_ERR_ARG;
+    *out = nullptr;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || device >= ndev) {
+        cudaGetLastError();
+        return B2M_ERR_CUDA;
+    }
+    Ctx* ctx = new Ctx();
+    ctx->device = device;
+    if (cudaSetDevice(device) != cudaSuccess) { delete ctx; return B2M_ERR_CUDA; }
+    cudaDeviceProp prop;
+    cudaGetDeviceProperties(&prop, device);
+    ctx->num_sms = prop.multiProcessorCount;
+    ctx->smem_optin = prop.sharedMemPerBlockOptin;
+    if (prop.major != 10) {
+        delete ctx;
+        return B2M_ERR_UNSUPPORTED;  // built for sm_100a only
+    }
+    if (cudaStreamCreateWithFlags(&ctx->own_stream, cudaStreamNonBlocking) != cudaSuccess) {
+        delete ctx;
+        return B2M_ERR_CUDA;
+    }
+    ctx->stream = ctx->own_stream;
+    if (cudaMalloc(&ctx->d_status, b2m::kNumStatus * sizeof(int32_t)) != cudaSuccess ||
+        cudaMallocHost(&ctx->h_status, b2m::kNumStatus * sizeof(int32_t)) != cudaSuccess) {
+        cudaGetLastError();
+        delete ctx;
+        return B2M_ERR_ALLOC;
+    }
+    cudaMemset(ctx->d_status, 0, b2m::kNumStatus * sizeof(int32_t));
+    std::memset(ctx->h_status, 0, b2m::kNumStatus * sizeof(int32_t));
+    cudaDeviceSynchronize();
+    *out = reinterpret_cast<b2m_ctx*>(ctx);
+    return B2M_OK;
+}
+
+extern "C" int32_t b2m_destroy(b2m_ctx* h) {
+    Ctx* ctx = reinterpret_cast<Ctx*>(h);
+    if (!ctx) return B2M_ERR_ARG;
+    cudaSetDevice(ctx->device);
+    cudaStreamSynchronize(ctx->stream);
+    for (int i = 0; i < b2m::kNumWs; ++i)
+        if (ctx->ws[i]) cudaFree(ctx->ws[i]);
+    if (ctx->h_pinned) cudaFreeHost(ctx->h_pinned);
+    if (ctx->d_status) cudaFree(ctx->d_status);
+    if (ctx->h_status) cudaFreeHost(ctx->h_status);
+    if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
+    delete ctx;
+    return B2M_OK;
+}
+
+extern "C" int32_t b2m_set_stream(b2m_ctx* h, void* stream) {
+    Ctx* ctx = reinterpret_cast<Ctx*>(h);
+    if (!ctx) return B2M_ERR_ARG;
+    ctx->stream = stream ? reinterpret_cast<cudaStream_t>(stream) : ctx->own_stream;
+    return B2M_OK;
+}
+
+extern "C" int32_t b2m_synchronize(b2m_ctx* h) {
+    Ctx* ctx = reinterpret_cast<Ctx*>(h);
+    if (!ctx) return B2M_ERR_ARG;
+    B2M_CU(ctx, cudaStreamSynchronize(ctx->stream));
+    return B2M_OK;
+}
+
+extern "C" const char* b2m_last_error(b2m_ctx* h) {
+    Ctx* ctx = reinterpret_cast<Ctx*>(h);
+    return ctx ? ctx->last_error.c_str() : "null context";
+}
+
+extern "C" int64_t b2m_kernel_launches(b2m_ctx* h) {
+    Ctx* ctx = reinterpret_cast<Ctx*>(h);
+    return ctx ? ctx->launches : -1;
+}
+
+extern "C" const char* b2m_status_string(int32_t s) {
+    switch (s) {
+        case B2M_OK: return "ok";
+        case B2M_SINGULAR: return "matrix is singular";
+        case B2M_ERR_DIM: return "dimension error";
+        case B2M_ERR_CUDA: return "CUDA error";
+        case B2M_ERR_ALLOC: return "allocation failed";
+        case B2M_ERR_TIMEOUT: return "bounded device wait timed out";
+        case B2M_ERR_ARG: return "invalid argument";
+        case B2M_ERR_NOCONV: return "refinement did not converge";
+        case B2M_ERR_UNSUPPORTED: return "unsupported size or device";
+        default: return "unknown status";
+    }
+}

@@ -1,0 +1,56 @@
+// kernels.cuh -- internal launch interfaces shared by the translation units of libb2m.
+#pragma once
+
+#include "common.cuh"
+
+namespace b2m {
+
+// One GEMM operand as seen by the TMA tensor map: the map covers `rows x cols` elements of a
+// row-major array at `base` with row stride `ld` (elements); the operand starts at (r0, c0)
+// inside it.  kmajor: rows index m (A) or n (B) and cols index k; otherwise rows index k.
+struct DOperand {
+    const void* base;
+    int64_t ld;
+    int64_t rows, cols;
+    int64_t r0, c0;
+    bool kmajor;
+};
+
+// C(M x N) op= A(M x K) * B(K x N) in FP64 on the DMMA path.  Tensor-map origins c0 must be
+// even and K must end on a multiple of 16 unless the map's extent ends exactly at the operand.
+int32_t dgemm_tiled(Ctx* ctx, cudaStream_t st, const DOperand& A, const DOperand& B, double* C, int64_t ldc,
+                    int64_t M, int64_t N, int64_t K, int op, bool check_info);
+
+// Partial-pivoting LU of the leading n x n block of a row-major FP64 array (ld even, base
+// 16-byte aligned), in place.  ipiv (device, n int32) gets absolute pivot rows; perm (device,
+// n int32, may be null) gets the final row permutation; status[kInfo] = 1 on a singular pivot.
+int32_t lu_factor_f64(Ctx* ctx, cudaStream_t st, double* A, int64_t ld, int64_t n, int32_t* ipiv, int32_t* perm);
+
+// Solves A X = B from the factors of lu_factor_f64: B (n x nrhs, row stride ldb elements) is
+// overwritten with X.  perm is the permutation from lu_factor_f64.
+int32_t lu_solve_f64(Ctx* ctx, cudaStream_t st, const double* LU, int64_t ld, int64_t n, const int32_t* perm,
+                     double* B, int64_t ldb, int64_t nrhs);
+
+// Builds perm from ipiv on the device (used when factors come from outside: b2m_MatrixLUBackSubst).
+int32_t perm_from_ipiv(Ctx* ctx, cudaStream_t st, const int32_t* ipiv, int64_t n, int32_t* perm);
+
+// Determinant from factors: (-1)^{#i: ipiv[i] != i} * prod diag, in the reference's order.
+int32_t lu_determinant(Ctx* ctx, cudaStream_t st, const double* LU, int64_t ld, int64_t n, const int32_t* ipiv,
+                       double* d_det);
+
+// Copies a strided FP64 matrix (rows x cols, byte strides) device to device.
+int32_t copy_matrix(Ctx* ctx, cudaStream_t st, double* dst, int64_t ldd_bytes, const double* src, int64_t lds_bytes,
+                    int64_t rows, int64_t cols);
+
+}  // namespace b2m
+
+namespace b2m {
+// X += R elementwise (rows x cols, strides in elements)
+int32_t axpy_matrix(Ctx* ctx, cudaStream_t st, double* X, int64_t ldx, const double* R, int64_t ldr, int64_t rows,
+                    int64_t cols);
+// X[i][i] = v for i < n
+int32_t set_diagonal(Ctx* ctx, cudaStream_t st, double* X, int64_t ldx, int64_t n, double v);
+// dst = src when status[kInfo] == 0 (strides in elements)
+int32_t copy_if_ok(Ctx* ctx, cudaStream_t st, double* dst, int64_t ldd, const double* src, int64_t lds, int64_t rows,
+                   int64_t cols);
+}  // namespace b2m

@@ -1,0 +1,655 @@
+// lu.cu -- partial-pivoting LU and the triangular solves built on it (FP64 plain form).
+//
+// Structure (a B200 re-design of InternalRecursiveMatrixLUDecompInPlace, LinAlgLU.pas:181-281):
+//   * the recursion splits the column range in two halves rounded to the 32-column leaf width
+//     (the reference halves exactly: mn div 2); the leaves are factored by one thread-block
+//     cluster per panel with the panel resident in distributed shared memory;
+//   * a leaf's <= 32 row interchanges are applied at once to every other column of the matrix
+//     (and to a row-permutation vector) by one swap launch, which replaces the reference's two
+//     LUSwap calls per recursion level (:205, :237) -- the final matrix and pivot vector are the
+//     same because each interchange is applied to every column exactly once, in order;
+//   * A12 <- L11^{-1} A12 (LUBacksup :138-169) is a recursive triangular solve whose leaves run
+//     a 32 x 32 register kernel and whose off-diagonal work goes through the DMMA GEMM;
+//   * A22 -= A21 * A12 (MatrixMultEx ... doSub, :221) is the DMMA GEMM with the doSub epilogue.
+// Pivot search follows the reference's leaf exactly: the largest |a| wins, the first (lowest
+// row) among equals wins, a column whose largest |a| is <= 10/MaxDouble is singular (:246-268);
+// the pivot column is scaled by the reciprocal 1/maxVal, as MatrixScaleAndAdd does.
+#include <cooperative_groups.h>
+
+#include <cfloat>
+
+#include "common.cuh"
+#include "kernels.cuh"
+
+namespace cg = cooperative_groups;
+
+namespace b2m {
+
+template <typename T> __device__ __forceinline__ T singular_threshold();
+template <> __device__ __forceinline__ double singular_threshold<double>() { return 10.0 / DBL_MAX; }
+template <> __device__ __forceinline__ float singular_threshold<float>() { return 10.0f / FLT_MAX; }
+
+// (a2,i2) beats (a1,i1): larger magnitude, or equal magnitude and lower row (first maximum wins)
+template <typename T>
+__device__ __forceinline__ bool piv_better(T a2, int i2, T a1, int i1) {
+    return i2 >= 0 && (i1 < 0 || a2 > a1 || (a2 == a1 && i2 < i1));
+}
+
+template <typename T>
+__device__ __forceinline__ void warp_argmax(T& a, int& i) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        T a2 = __shfl_xor_sync(0xffffffffu, a, o);
+        int i2 = __shfl_xor_sync(0xffffffffu, i, o);
+        if (piv_better(a2, i2, a, i)) { a = a2; i = i2; }
+    }
+}
+
+// ------------------------------------------------------------------------------------------
+// Panel kernel: one cluster of C CTAs factors an m x w panel (w <= 32) held in distributed
+// shared memory; CTA `rank` owns panel rows [rank*R, rank*R + R).  One cluster barrier per
+// column: candidates (|max|, row, full row) and the current diagonal row are published in
+// double-buffered slots, read remotely after the barrier, and every CTA derives the same pivot.
+// ------------------------------------------------------------------------------------------
+constexpr int kPanelThreads = 512;
+constexpr int kPanelW = 32;
+constexpr int kMaxCluster = 16;
+
+template <typename T, int RPT>
+__global__ void __launch_bounds__(kPanelThreads, 1)
+    panel_lu_kernel(T* P, int64_t ld, int m, int w, int R, int row_base, int col_base, int32_t* ipiv,
+                    int32_t* status) {
+    cg::cluster_group cluster = cg::this_cluster();
+    const int C = (int)cluster.num_blocks();
+    const int rank = (int)cluster.block_rank();
+    extern __shared__ __align__(16) unsigned char panel_smem[];
+    T* S = reinterpret_cast<T*>(panel_smem);
+    const int SS = w | 1;  // odd row stride: conflict-free column access
+
+    __shared__ T cand_abs[2];
+    __shared__ int cand_idx[2];
+    __shared__ T cand_row[2][kPanelW];
+    __shared__ T diag_row[2][kPanelW];
+    __shared__ T allrows[kMaxCluster][kPanelW];
+    __shared__ T c_abs[kMaxCluster];
+    __shared__ int c_idx[kMaxCluster];
+    __shared__ T urow[kPanelW], drow[kPanelW];
+    __shared__ T wabs[kPanelThreads / 32];
+    __shared__ int widx[kPanelThreads / 32];
+
+    if (status[kInfo] != 0) return;  // uniform over the cluster: written before this launch
+
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int lo = rank * R;
+    const int hi = min(m, lo + R);
+    const int nr = max(0, hi - lo);
+
+    for (int e = tid; e < nr * w; e += kPanelThreads) {
+        const int r = e / w, c = e - r * w;
+        S[r * SS + c] = P[(int64_t)(lo + r) * ld + c];
+    }
+    __syncthreads();
+
+    // local argmax of column `col` over rows >= col, CTA-reduced, then published with its row
+    auto reduce_publish = [&](int col, int par) {
+        T ma = T(0);
+        int mi = -1;
+#pragma unroll
+        for (int k = 0; k < RPT; ++k) {
+            const int rl = tid + k * kPanelThreads;
+            const int r = lo + rl;
+            if (rl < nr && r >= col) {
+                const T a = fabs(S[rl * SS + col]);
+                if (a > ma) { ma = a; mi = r; }
+            }
+        }
+        warp_argmax(ma, mi);
+        if (lane == 0) { wabs[warp] = ma; widx[warp] = mi; }
+        __syncthreads();
+        if (warp == 0) {
+            T a = lane < kPanelThreads / 32 ? wabs[lane] : T(0);
+            int i = lane < kPanelThreads / 32 ? widx[lane] : -1;
+            warp_argmax(a, i);
+            if (lane == 0) { cand_abs[par] = a; cand_idx[par] = i; }
+            if (i >= 0 && lane < w) cand_row[par][lane] = S[(i - lo) * SS + lane];
+            if (col >= lo && col < hi && lane < w) diag_row[par][lane] = S[(col - lo) * SS + lane];
+        }
+    };
+
+    reduce_publish(0, 0);
+    cluster.sync();
+
+    bool singular = false;
+    const int ownj_stride = R;
+    for (int j = 0; j < w; ++j) {
+        const int par = j & 1;
+        const int ownj = j / ownj_stride;
+        // phase A: one round of remote loads (candidates, their rows, the diagonal row)
+        for (int e = tid; e < C * w + w + C; e += kPanelThreads) {
+            if (e < C * w) {
+                const int c = e / w, col = e - c * w;
+                allrows[c][col] = cluster.map_shared_rank(&cand_row[0][0], c)[par * kPanelW + col];
+            } else if (e < C * w + w) {
+                const int col = e - C * w;
+                drow[col] = cluster.map_shared_rank(&diag_row[0][0], ownj)[par * kPanelW + col];
+            } else {
+                const int c = e - C * w - w;
+                c_abs[c] = cluster.map_shared_rank(cand_abs, c)[par];
+                c_idx[c] = cluster.map_shared_rank(cand_idx, c)[par];
+            }
+        }
+        __syncthreads();
+        // phase B: every thread derives the same pivot
+        T babs = T(0);
+        int bidx = -1, bc = 0;
+        for (int c = 0; c < C; ++c)
+            if (piv_better(c_abs[c], c_idx[c], babs, bidx)) { babs = c_abs[c]; bidx = c_idx[c]; bc = c; }
+        if (bidx < 0 || !(babs > singular_threshold<T>())) {
+            singular = true;
+            if (rank == 0 && tid == 0) atomicExch(&status[kInfo], 1);
+            break;
+        }
+        const int p = bidx;
+        if (rank == 0 && tid == 0) ipiv[col_base + j] = row_base + p;
+        if (tid < w) {
+            const T u = allrows[bc][tid];
+            urow[tid] = u;
+            if (p != j && p >= lo && p < hi) S[(p - lo) * SS + tid] = drow[tid];
+            if (j >= lo && j < hi) S[(j - lo) * SS + tid] = u;
+        }
+        __syncthreads();
+        // phase C: scale the pivot column by 1/pivot, rank-1 update of the rest of the panel
+        const T rinv = T(1) / urow[j];
+#pragma unroll
+        for (int k = 0; k < RPT; ++k) {
+            const int rl = tid + k * kPanelThreads;
+            const int r = lo + rl;
+            if (rl < nr && r > j) {
+                T* row = S + rl * SS;
+                const T l = row[j] * rinv + T(0);
+                row[j] = l;
+                for (int c = j + 1; c < w; ++c) row[c] = fma(-l, urow[c], row[c]);
+            }
+        }
+        __syncthreads();
+        if (j + 1 < w) reduce_publish(j + 1, par ^ 1);
+        cluster.sync();
+    }
+    if (singular) {
+        cluster.sync();  // nobody leaves while others may still read its shared memory
+        return;
+    }
+    for (int e = tid; e < nr * w; e += kPanelThreads) {
+        const int r = e / w, c = e - r * w;
+        P[(int64_t)(lo + r) * ld + c] = S[r * SS + c];
+    }
+}
+
+// ------------------------------------------------------------------------------------------
+// Row interchanges of one leaf, applied to every column outside the leaf's own columns and to
+// the permutation vector.  Warp 0 turns the <= 32 sequential swaps into a list of row moves.
+// ------------------------------------------------------------------------------------------
+constexpr int kSwapThreads = 256;
+
+template <typename T>
+__global__ void __launch_bounds__(kSwapThreads)
+    leaf_swap_kernel(T* A, int64_t ld, int ncols, int c0, int w, const int32_t* ipiv, int32_t* perm,
+                     const int32_t* status) {
+    __shared__ int src_main[kPanelW];
+    __shared__ int mv_dst[2 * kPanelW], mv_src[2 * kPanelW];
+    __shared__ int n_moves;
+    if (status[kInfo] != 0) return;
+    const int tid = threadIdx.x, lane = tid & 31;
+    if (tid < 32) {
+        if (lane < w) src_main[lane] = c0 + lane;
+        __syncwarp();
+        int my_pos = -1, my_src = -1, n_extra = 0;
+        for (int j = 0; j < w; ++j) {
+            const int q = ipiv[c0 + j];
+            if (q < c0 + w) {
+                if (lane == 0 && q != c0 + j) {
+                    const int t = src_main[j];
+                    src_main[j] = src_main[q - c0];
+                    src_main[q - c0] = t;
+                }
+            } else {
+                const unsigned hit = __ballot_sync(0xffffffffu, my_pos == q);
+                int owner;
+                if (hit) {
+                    owner = __ffs(hit) - 1;
+                } else {
+                    owner = n_extra++;
+                    if (lane == owner) { my_pos = q; my_src = q; }
+                }
+                if (lane == owner) {
+                    const int t = src_main[j];
+                    src_main[j] = my_src;
+                    my_src = t;
+                }
+            }
+            __syncwarp();
+        }
+        // compact the moves (rows whose content changes)
+        const bool mv_main = lane < w && src_main[lane] != c0 + lane;
+        const bool mv_extra = lane < n_extra && my_src != my_pos;
+        const unsigned bm = __ballot_sync(0xffffffffu, mv_main);
+        const unsigned be = __ballot_sync(0xffffffffu, mv_extra);
+        const int below = (1u << lane) - 1u;
+        if (mv_main) {
+            const int k = __popc(bm & below);
+            mv_dst[k] = c0 + lane;
+            mv_src[k] = src_main[lane];
+        }
+        if (mv_extra) {
+            const int k = __popc(bm) + __popc(be & below);
+            mv_dst[k] = my_pos;
+            mv_src[k] = my_src;
+        }
+        if (lane == 0) n_moves = __popc(bm) + __popc(be);
+    }
+    __syncthreads();
+    const int nm = n_moves;
+    if (nm == 0) return;
+    const int gc = blockIdx.x * kSwapThreads + tid;
+    const int skip = w;
+    const int col = gc < c0 ? gc : gc + skip;
+    if (col < ncols) {
+        T v[2 * kPanelW];
+#pragma unroll
+        for (int k = 0; k < 2 * kPanelW; ++k)
+            if (k < nm) v[k] = A[(int64_t)mv_src[k] * ld + col];
+#pragma unroll
+        for (int k = 0; k < 2 * kPanelW; ++k)
+            if (k < nm) A[(int64_t)mv_dst[k] * ld + col] = v[k];
+    }
+    if (perm && blockIdx.x == 0) {
+        int pv = 0;
+        if (tid < nm) pv = perm[mv_src[tid]];
+        __syncthreads();
+        if (tid < nm) perm[mv_dst[tid]] = pv;
+    }
+}
+
+// ------------------------------------------------------------------------------------------
+// Small triangular solves (k <= 32) on a strip of columns: one thread per column, the column
+// in registers, the triangle in shared memory.  Lower: unit diagonal, ascending j as in
+// LUBacksup / the forward sweep of MatrixLUBackSubst.  Upper: ascending j then a true
+// division by the diagonal, as the backward sweep of MatrixLUBackSubst (:362-382).
+// ------------------------------------------------------------------------------------------
+constexpr int kTrsmThreads = 128;
+
+template <typename T>
+__global__ void __launch_bounds__(kTrsmThreads)
+    trsm_small_kernel(const T* L, int64_t ldl, T* B, int64_t ldb, int k, int ncols, int upper,
+                      const int32_t* status) {
+    __shared__ T Ts[kPanelW][kPanelW + 1];
+    if (status && status[kInfo] != 0) return;
+    for (int e = threadIdx.x; e < k * k; e += kTrsmThreads) {
+        const int i = e / k, j = e - i * k;
+        Ts[i][j] = L[(int64_t)i * ldl + j];
+    }
+    __syncthreads();
+    const int c = blockIdx.x * kTrsmThreads + threadIdx.x;
+    if (c >= ncols) return;
+    T x[kPanelW];
+#pragma unroll
+    for (int i = 0; i < kPanelW; ++i)
+        if (i < k) x[i] = B[(int64_t)i * ldb + c];
+    if (!upper) {
+#pragma unroll
+        for (int i = 1; i < kPanelW; ++i) {
+            if (i < k) {
+                T s = x[i];
+#pragma unroll
+                for (int j = 0; j < i; ++j) s = fma(-Ts[i][j], x[j], s);
+                x[i] = s;
+            }
+        }
+    } else {
+#pragma unroll
+        for (int i = kPanelW - 1; i >= 0; --i) {
+            if (i < k) {
+                T s = x[i];
+#pragma unroll
+                for (int j = i + 1; j < kPanelW; ++j)
+                    if (j < k) s = fma(-Ts[i][j], x[j], s);
+                x[i] = s / Ts[i][i];
+            }
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < kPanelW; ++i)
+        if (i < k) B[(int64_t)i * ldb + c] = x[i];
+}
+
+__global__ void iota_kernel(int32_t* v, int64_t n) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) v[i] = (int32_t)i;
+}
+
+// X[i][:] = B[perm[i]][:]
+__global__ void gather_rows_kernel(double* X, int64_t ldx, const double* B, int64_t ldb, const int32_t* perm,
+                                   int64_t n, int64_t nrhs) {
+    const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= n * nrhs) return;
+    const int64_t i = e / nrhs, c = e - i * nrhs;
+    X[i * ldx + c] = B[(int64_t)perm[i] * ldb + c];
+}
+
+// perm from a LAPACK-style ipiv: sequential interchanges on a shared-memory copy (n <= 48k)
+__global__ void perm_from_ipiv_kernel(const int32_t* ipiv, int n, int32_t* perm) {
+    extern __shared__ int32_t pv[];
+    for (int i = threadIdx.x; i < n; i += blockDim.x) pv[i] = i;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int i = 0; i < n; ++i) {
+            const int q = ipiv[i];
+            if (q != i && q >= 0 && q < n) {
+                const int t = pv[i];
+                pv[i] = pv[q];
+                pv[q] = t;
+            }
+        }
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < n; i += blockDim.x) perm[i] = pv[i];
+}
+
+// det = (-1)^{#i: ipiv[i] != i} * U[0][0] * U[1][1] * ... in this order (MatrixDeterminant :467-476)
+__global__ void determinant_kernel(const double* LU, int64_t ld, int n, const int32_t* ipiv, const int32_t* status,
+                                   double* det) {
+    extern __shared__ double dg[];
+    __shared__ int flips;
+    if (threadIdx.x == 0) flips = 0;
+    __syncthreads();
+    int local = 0;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        dg[i] = LU[(int64_t)i * ld + i];
+        if (ipiv[i] != i) local++;
+    }
+    atomicAdd(&flips, local);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        if (status[kInfo] != 0) { *det = 0.0; return; }
+        double r = (flips & 1) ? -1.0 : 1.0;
+        for (int i = 0; i < n; ++i) r = r * dg[i];
+        *det = r;
+    }
+}
+
+// ------------------------------------------------------------------------------------------
+// host drivers
+// ------------------------------------------------------------------------------------------
+namespace {
+
+int64_t split_cols(int64_t w) { return round_up((w + 1) / 2, kPanelW); }
+
+struct PanelCfg {
+    int C;    // cluster size
+    int R;    // rows per CTA
+    int rpt;  // rows per thread
+    size_t smem;
+};
+
+template <typename T>
+int32_t panel_config(Ctx* ctx, int m, int w, PanelCfg* cfg) {
+    const int SS = w | 1;
+    const size_t budget = std::min<size_t>(ctx->smem_optin ? ctx->smem_optin : 232448, 232448) - 16 * 1024;
+    const int rmax_smem = (int)(budget / (SS * sizeof(T)));
+    for (int rpt = 1; rpt <= 4; rpt *= 2) {
+        const int rmax = std::min(rmax_smem, rpt * kPanelThreads);
+        const int C = (int)ceil_div(m, rmax);
+        if (C <= kMaxCluster) {
+            cfg->C = std::max(1, C);
+            cfg->R = (int)ceil_div(m, cfg->C);
+            cfg->rpt = rpt;
+            cfg->smem = (size_t)cfg->R * SS * sizeof(T);
+            return B2M_OK;
+        }
+    }
+    return fail(ctx, B2M_ERR_UNSUPPORTED, "panel of %d rows x %d columns does not fit one cluster", m, w);
+}
+
+template <typename T, int RPT>
+int32_t launch_panel_rpt(Ctx* ctx, cudaStream_t st, const PanelCfg& pc, T* P, int64_t ld, int m, int w, int row_base,
+                         int col_base, int32_t* ipiv) {
+    auto kern = panel_lu_kernel<T, RPT>;
+    static bool attr = false;
+    if (!attr) {
+        B2M_CU(ctx, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 232448 - 16 * 1024));
+        B2M_CU(ctx, cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+        attr = true;
+    }
+    // a non-portable cluster size must be schedulable with this much shared memory per CTA
+    static int checked_c[kMaxCluster + 1] = {};
+    if (pc.C > 8 && checked_c[pc.C] == 0) {
+        cudaLaunchConfig_t occ = {};
+        occ.gridDim = dim3(pc.C, 1, 1);
+        occ.blockDim = dim3(kPanelThreads, 1, 1);
+        occ.dynamicSmemBytes = 232448 - 16 * 1024;
+        cudaLaunchAttribute oat[1];
+        oat[0].id = cudaLaunchAttributeClusterDimension;
+        oat[0].val.clusterDim.x = pc.C;
+        oat[0].val.clusterDim.y = 1;
+        oat[0].val.clusterDim.z = 1;
+        occ.attrs = oat;
+        occ.numAttrs = 1;
+        int clusters = 0;
+        B2M_CU(ctx, cudaOccupancyMaxActiveClusters(&clusters, kern, &occ));
+        checked_c[pc.C] = clusters > 0 ? 1 : -1;
+    }
+    if (pc.C > 8 && checked_c[pc.C] < 0)
+        return fail(ctx, B2M_ERR_UNSUPPORTED, "panel cluster of %d CTAs cannot be scheduled", pc.C);
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(pc.C, 1, 1);
+    cfg.blockDim = dim3(kPanelThreads, 1, 1);
+    cfg.dynamicSmemBytes = pc.smem;
+    cfg.stream = st;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = pc.C;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    B2M_CU(ctx, cudaLaunchKernelEx(&cfg, kern, P, ld, m, w, pc.R, row_base, col_base, ipiv, ctx->d_status));
+    B2M_LAUNCHED(ctx);
+    return B2M_OK;
+}
+
+template <typename T>
+int32_t launch_panel(Ctx* ctx, cudaStream_t st, T* P, int64_t ld, int m, int w, int row_base, int col_base,
+                     int32_t* ipiv) {
+    PanelCfg pc;
+    B2M_TRY(panel_config<T>(ctx, m, w, &pc));
+    if (pc.rpt == 1) return launch_panel_rpt<T, 1>(ctx, st, pc, P, ld, m, w, row_base, col_base, ipiv);
+    if (pc.rpt == 2) return launch_panel_rpt<T, 2>(ctx, st, pc, P, ld, m, w, row_base, col_base, ipiv);
+    return launch_panel_rpt<T, 4>(ctx, st, pc, P, ld, m, w, row_base, col_base, ipiv);
+}
+
+template <typename T>
+int32_t launch_swaps(Ctx* ctx, cudaStream_t st, T* A, int64_t ld, int ncols, int c0, int w, const int32_t* ipiv,
+                     int32_t* perm) {
+    const int other = ncols - w;
+    const int blocks = std::max(1, (int)ceil_div(other, kSwapThreads));
+    leaf_swap_kernel<T><<<blocks, kSwapThreads, 0, st>>>(A, ld, ncols, c0, w, ipiv, perm, ctx->d_status);
+    B2M_LAUNCHED(ctx);
+    return B2M_OK;
+}
+
+template <typename T>
+int32_t launch_trsm_small(Ctx* ctx, cudaStream_t st, const T* L, int64_t ldl, T* B, int64_t ldb, int k, int ncols,
+                          bool upper) {
+    if (k <= 0 || ncols <= 0) return B2M_OK;
+    const int blocks = (int)ceil_div(ncols, kTrsmThreads);
+    trsm_small_kernel<T><<<blocks, kTrsmThreads, 0, st>>>(L, ldl, B, ldb, k, ncols, upper ? 1 : 0, ctx->d_status);
+    B2M_LAUNCHED(ctx);
+    return B2M_OK;
+}
+
+// Triangular operand description for the recursive solves: the triangle T lives in the
+// row-major array (Abase, lda, an n x n extent) at diagonal offset r0; the right-hand sides are
+// rows [br0, br0+k) and columns [bc0, bc0+ncols) of (Bbase, ldb) whose map extent is bn x bcols.
+struct TriSolve {
+    const double* A;
+    int64_t lda, n;
+    double* B;
+    int64_t ldb, bn, bcols, bc0, ncols;
+};
+
+int32_t trsm_lower_rec(Ctx* ctx, cudaStream_t st, const TriSolve& t, int64_t r0, int64_t br0, int64_t k) {
+    if (k <= kPanelW)
+        return launch_trsm_small<double>(ctx, st, t.A + r0 * t.lda + r0, t.lda, t.B + br0 * t.ldb + t.bc0, t.ldb,
+                                         (int)k, (int)t.ncols, false);
+    const int64_t k1 = split_cols(k), k2 = k - k1;
+    B2M_TRY(trsm_lower_rec(ctx, st, t, r0, br0, k1));
+    DOperand a{t.A, t.lda, t.n, t.n, r0 + k1, r0, true};
+    DOperand b{t.B, t.ldb, t.bn, t.bcols, br0, t.bc0, false};
+    B2M_TRY(dgemm_tiled(ctx, st, a, b, t.B + (br0 + k1) * t.ldb + t.bc0, t.ldb, k2, t.ncols, k1, B2M_DO_SUB, true));
+    return trsm_lower_rec(ctx, st, t, r0 + k1, br0 + k1, k2);
+}
+
+int32_t trsm_upper_rec(Ctx* ctx, cudaStream_t st, const TriSolve& t, int64_t r0, int64_t br0, int64_t k) {
+    if (k <= kPanelW)
+        return launch_trsm_small<double>(ctx, st, t.A + r0 * t.lda + r0, t.lda, t.B + br0 * t.ldb + t.bc0, t.ldb,
+                                         (int)k, (int)t.ncols, true);
+    const int64_t k1 = split_cols(k), k2 = k - k1;
+    B2M_TRY(trsm_upper_rec(ctx, st, t, r0 + k1, br0 + k1, k2));
+    DOperand a{t.A, t.lda, t.n, t.n, r0, r0 + k1, true};
+    DOperand b{t.B, t.ldb, t.bn, t.bcols, br0 + k1, t.bc0, false};
+    B2M_TRY(dgemm_tiled(ctx, st, a, b, t.B + br0 * t.ldb + t.bc0, t.ldb, k1, t.ncols, k2, B2M_DO_SUB, true));
+    return trsm_upper_rec(ctx, st, t, r0, br0, k1);
+}
+
+// factor columns [c0, c0+width), rows [c0, n)
+int32_t lu_rec(Ctx* ctx, cudaStream_t st, double* A, int64_t ld, int64_t n, int64_t c0, int64_t width,
+               int32_t* ipiv, int32_t* perm) {
+    if (width <= kPanelW) {
+        B2M_TRY(launch_panel<double>(ctx, st, A + c0 * ld + c0, ld, (int)(n - c0), (int)width, (int)c0, (int)c0,
+                                     ipiv));
+        return launch_swaps<double>(ctx, st, A, ld, (int)n, (int)c0, (int)width, ipiv, perm);
+    }
+    const int64_t nleft = split_cols(width), nright = width - nleft;
+    B2M_TRY(lu_rec(ctx, st, A, ld, n, c0, nleft, ipiv, perm));
+    // A12 <- L11^{-1} A12
+    TriSolve t{A, ld, n, A, ld, n, n, c0 + nleft, nright};
+    B2M_TRY(trsm_lower_rec(ctx, st, t, c0, c0, nleft));
+    // A22 -= A21 * A12
+    const int64_t r1 = c0 + nleft;
+    DOperand a{A, ld, n, n, r1, c0, true};
+    DOperand b{A, ld, n, n, c0, r1, false};
+    B2M_TRY(dgemm_tiled(ctx, st, a, b, A + r1 * ld + r1, ld, n - r1, nright, nleft, B2M_DO_SUB, true));
+    return lu_rec(ctx, st, A, ld, n, r1, nright, ipiv, perm);
+}
+
+}  // namespace
+
+int32_t lu_factor_f64(Ctx* ctx, cudaStream_t st, double* A, int64_t ld, int64_t n, int32_t* ipiv, int32_t* perm) {
+    if (n <= 0) return B2M_OK;
+    if ((ld & 1) || !aligned16(A)) return fail(ctx, B2M_ERR_DIM, "lu_factor_f64: ld must be even, A 16-byte aligned");
+    if (n > (1 << 30)) return fail(ctx, B2M_ERR_UNSUPPORTED, "n too large");
+    if (perm) {
+        iota_kernel<<<(unsigned)ceil_div(n, 256), 256, 0, st>>>(perm, n);
+        B2M_LAUNCHED(ctx);
+    }
+    return lu_rec(ctx, st, A, ld, n, 0, n, ipiv, perm);
+}
+
+int32_t lu_solve_f64(Ctx* ctx, cudaStream_t st, const double* LU, int64_t ld, int64_t n, const int32_t* perm,
+                     double* B, int64_t ldb, int64_t nrhs) {
+    if (n <= 0 || nrhs <= 0) return B2M_OK;
+    if ((ldb & 1) || !aligned16(B)) return fail(ctx, B2M_ERR_DIM, "lu_solve_f64: ldb must be even");
+    // X = P B
+    void* tmp = nullptr;
+    B2M_TRY(ws_get(ctx, kWsE, (size_t)(n * ldb * sizeof(double)), &tmp));
+    double* X = static_cast<double*>(tmp);
+    B2M_CU(ctx, cudaMemcpy2DAsync(X, ldb * 8, B, ldb * 8, nrhs * 8, n, cudaMemcpyDeviceToDevice, st));
+    gather_rows_kernel<<<(unsigned)ceil_div(n * nrhs, 256), 256, 0, st>>>(B, ldb, X, ldb, perm, n, nrhs);
+    B2M_LAUNCHED(ctx);
+    TriSolve t{LU, ld, n, B, ldb, n, nrhs, 0, nrhs};
+    B2M_TRY(trsm_lower_rec(ctx, st, t, 0, 0, n));
+    return trsm_upper_rec(ctx, st, t, 0, 0, n);
+}
+
+int32_t perm_from_ipiv(Ctx* ctx, cudaStream_t st, const int32_t* ipiv, int64_t n, int32_t* perm) {
+    if (n > 48 * 1024) return fail(ctx, B2M_ERR_UNSUPPORTED, "perm_from_ipiv: n > 49152");
+    const size_t smem = (size_t)n * sizeof(int32_t);
+    if (smem > 48 * 1024)
+        B2M_CU(ctx, cudaFuncSetAttribute(perm_from_ipiv_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)smem));
+    perm_from_ipiv_kernel<<<1, 1024, smem, st>>>(ipiv, (int)n, perm);
+    B2M_LAUNCHED(ctx);
+    return B2M_OK;
+}
+
+int32_t lu_determinant(Ctx* ctx, cudaStream_t st, const double* LU, int64_t ld, int64_t n, const int32_t* ipiv,
+                       double* d_det) {
+    if (n > 24 * 1024) return fail(ctx, B2M_ERR_UNSUPPORTED, "determinant: n > 24576");
+    const size_t smem = (size_t)n * sizeof(double);
+    if (smem > 48 * 1024)
+        B2M_CU(ctx, cudaFuncSetAttribute(determinant_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    determinant_kernel<<<1, 1024, smem, st>>>(LU, ld, (int)n, ipiv, ctx->d_status, d_det);
+    B2M_LAUNCHED(ctx);
+    return B2M_OK;
+}
+
+int32_t copy_matrix(Ctx* ctx, cudaStream_t st, double* dst, int64_t ldd_bytes, const double* src, int64_t lds_bytes,
+                    int64_t rows, int64_t cols) {
+    if (rows <= 0 || cols <= 0) return B2M_OK;
+    B2M_CU(ctx, cudaMemcpy2DAsync(dst, ldd_bytes, src, lds_bytes, cols * 8, rows, cudaMemcpyDeviceToDevice, st));
+    return B2M_OK;
+}
+
+}  // namespace b2m
+
+namespace b2m {
+
+__global__ void axpy_matrix_kernel(double* X, int64_t ldx, const double* R, int64_t ldr, int64_t rows, int64_t cols,
+                                   const int32_t* status) {
+    if (status[kInfo] != 0) return;
+    const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= rows * cols) return;
+    const int64_t i = e / cols, c = e - i * cols;
+    X[i * ldx + c] += R[i * ldr + c];
+}
+
+__global__ void set_diagonal_kernel(double* X, int64_t ldx, int64_t n, double v) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) X[i * ldx + i] = v;
+}
+
+__global__ void copy_if_ok_kernel(double* dst, int64_t ldd, const double* src, int64_t lds, int64_t rows, int64_t cols,
+                                  const int32_t* status) {
+    if (status[kInfo] != 0) return;
+    const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= rows * cols) return;
+    const int64_t i = e / cols, c = e - i * cols;
+    dst[i * ldd + c] = src[i * lds + c];
+}
+
+int32_t axpy_matrix(Ctx* ctx, cudaStream_t st, double* X, int64_t ldx, const double* R, int64_t ldr, int64_t rows,
+                    int64_t cols) {
+    if (rows <= 0 || cols <= 0) return B2M_OK;
+    axpy_matrix_kernel<<<(unsigned)ceil_div(rows * cols, 256), 256, 0, st>>>(X, ldx, R, ldr, rows, cols,
+                                                                             ctx->d_status);
+    B2M_LAUNCHED(ctx);
+    return B2M_OK;
+}
+
+int32_t set_diagonal(Ctx* ctx, cudaStream_t st, double* X, int64_t ldx, int64_t n, double v) {
+    if (n <= 0) return B2M_OK;
+    set_diagonal_kernel<<<(unsigned)ceil_div(n, 256), 256, 0, st>>>(X, ldx, n, v);
+    B2M_LAUNCHED(ctx);
+    return B2M_OK;
+}
+
+int32_t copy_if_ok(Ctx* ctx, cudaStream_t st, double* dst, int64_t ldd, const double* src, int64_t lds, int64_t rows,
+                   int64_t cols) {
+    if (rows <= 0 || cols <= 0) return B2M_OK;
+    copy_if_ok_kernel<<<(unsigned)ceil_div(rows * cols, 256), 256, 0, st>>>(dst, ldd, src, lds, rows, cols,
+                                                                           ctx->d_status);
+    B2M_LAUNCHED(ctx);
+    return B2M_OK;
+}
+
+}  // namespace b2m

@@ -1,0 +1,175 @@
+"""Host-side mirror of the reference's procedure-level API for this path, over the C ABI.
+
+Names and argument meaning follow the reference: MatrixMult / MatrixMultEx / MatrixMultT1Ex /
+MatrixMultT2Ex (MatrixASMStubSwitch.pas:769-863), MatrixLUDecompInPlace, MatrixLUDecomp,
+MatrixLUBackSubst, MatrixInverseInPlace, MatrixDeterminant, MatrixLinEQSolve (LinAlgLU.pas:26-45).
+Matrices are numpy float64 2-D arrays (row-major; padded views such as a[:, :n] of a wider
+array pass their row stride as the LineWidth).  Results use the reference's codes:
+0 = leOk, 1 = leSingular.
+
+`dev_*` functions take torch CUDA tensors and run asynchronously on torch's current stream.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from ._lib import DO_ADD, DO_NONE, DO_SUB, OK, SINGULAR, Context
+
+__all__ = [
+    "default_context", "MatrixMult", "MatrixMultEx", "MatrixMultT1Ex", "MatrixMultT2Ex", "MatrixLUDecompInPlace",
+    "MatrixLUDecomp", "MatrixLUBackSubst", "MatrixInverseInPlace", "MatrixDeterminant", "MatrixLinEQSolve",
+    "DO_NONE", "DO_ADD", "DO_SUB",
+]
+
+_ctx: dict[int, Context] = {}
+
+
+def default_context(device: int = 0) -> Context:
+    c = _ctx.get(device)
+    if c is None:
+        c = _ctx[device] = Context(device)
+    return c
+
+
+def _ptr(a: np.ndarray) -> int:
+    return a.ctypes.data
+
+
+def _lw(a: np.ndarray) -> int:
+    if a.ndim != 2 or a.dtype != np.float64 or a.strides[1] != 8:
+        raise ValueError("expected a 2-D float64 row-major array (rows may be padded)")
+    return a.strides[0]
+
+
+def _ctx_of(ctx):
+    return ctx if ctx is not None else default_context()
+
+
+# ----------------------------------------------------------------------------- GEMM
+def MatrixMultEx(dest: np.ndarray, mt1: np.ndarray, mt2: np.ndarray, op: int = DO_NONE, trans: int = 0,
+                 ctx: Context | None = None) -> None:
+    """dest op= op(mt1) * op(mt2); trans 0: A*B, 1: A^T*B (T1), 2: A*B^T (T2)."""
+    c = _ctx_of(ctx)
+    h1, w1 = mt1.shape
+    h2, w2 = mt2.shape
+    c.call("b2m_MatrixMultEx", _ptr(dest), _lw(dest), _ptr(mt1), _ptr(mt2), w1, h1, w2, h2, _lw(mt1), _lw(mt2),
+           op, trans)
+
+
+def MatrixMult(mt1: np.ndarray, mt2: np.ndarray, ctx: Context | None = None) -> np.ndarray:
+    dest = np.empty((mt1.shape[0], mt2.shape[1]))
+    MatrixMultEx(dest, mt1, mt2, DO_NONE, 0, ctx)
+    return dest
+
+
+def MatrixMultT1Ex(dest, mt1, mt2, op=DO_NONE, ctx=None):
+    MatrixMultEx(dest, mt1, mt2, op, 1, ctx)
+
+
+def MatrixMultT2Ex(dest, mt1, mt2, op=DO_NONE, ctx=None):
+    MatrixMultEx(dest, mt1, mt2, op, 2, ctx)
+
+
+# ----------------------------------------------------------------------------- LU
+def MatrixLUDecompInPlace(A: np.ndarray, indx: np.ndarray | None = None, ctx: Context | None = None):
+    n = A.shape[1]
+    if indx is None:
+        indx = np.zeros(n, dtype=np.int32)
+    st = _ctx_of(ctx).call("b2m_MatrixLUDecompInPlace", _ptr(A), _lw(A), n, indx.ctypes.data, allow=(OK, SINGULAR))
+    return st, indx
+
+
+def MatrixLUDecomp(A: np.ndarray, ctx: Context | None = None):
+    n = A.shape[1]
+    LU = np.empty((n, n))
+    indx = np.zeros(n, dtype=np.int32)
+    st = _ctx_of(ctx).call("b2m_MatrixLUDecomp", _ptr(A), _lw(A), _ptr(LU), _lw(LU), n, indx.ctypes.data,
+                           allow=(OK, SINGULAR))
+    return st, LU, indx
+
+
+def MatrixLUBackSubst(LU: np.ndarray, indx: np.ndarray, B: np.ndarray, ctx: Context | None = None) -> None:
+    """Solves in place on every column of B (the reference solves one column per call)."""
+    n = LU.shape[1]
+    assert indx.dtype == np.int32
+    _ctx_of(ctx).call("b2m_MatrixLUBackSubst", _ptr(LU), _lw(LU), n, indx.ctypes.data, _ptr(B), _lw(B), B.shape[1])
+
+
+def MatrixInverseInPlace(A: np.ndarray, ctx: Context | None = None) -> int:
+    return _ctx_of(ctx).call("b2m_MatrixInverseInPlace", _ptr(A), _lw(A), A.shape[1], allow=(OK, SINGULAR))
+
+
+def MatrixDeterminant(A: np.ndarray, ctx: Context | None = None) -> float:
+    det = C.c_double(0.0)
+    _ctx_of(ctx).call("b2m_MatrixDeterminant", _ptr(A), _lw(A), A.shape[1], C.addressof(det))
+    return det.value
+
+
+def MatrixLinEQSolve(A: np.ndarray, B: np.ndarray, num_refinements: int = 0, X: np.ndarray | None = None,
+                     ctx: Context | None = None):
+    n = A.shape[1]
+    k = B.shape[1]
+    if X is None:
+        X = np.zeros((n, k))
+    st = _ctx_of(ctx).call("b2m_MatrixLinEQSolve", _ptr(A), _lw(A), n, _ptr(B), _lw(B), _ptr(X), _lw(X), k,
+                           num_refinements, allow=(OK, SINGULAR))
+    return st, X
+
+
+# ----------------------------------------------------------------------------- device (torch) twins
+def _tptr(t) -> int:
+    return t.data_ptr()
+
+
+def _tlw(t) -> int:
+    assert t.dim() == 2 and t.stride(1) == 1 and t.dtype.itemsize == 8
+    return t.stride(0) * 8
+
+
+def _bind_stream(c: Context, t) -> None:
+    import torch
+    c.set_stream(torch.cuda.current_stream(t.device).cuda_stream)
+
+
+def dev_MatrixMultEx(dest, mt1, mt2, op=DO_NONE, trans=0, ctx=None):
+    c = _ctx_of(ctx)
+    _bind_stream(c, dest)
+    h1, w1 = mt1.shape
+    h2, w2 = mt2.shape
+    c.call("b2m_dev_MatrixMultEx", _tptr(dest), _tlw(dest), _tptr(mt1), _tptr(mt2), w1, h1, w2, h2, _tlw(mt1),
+           _tlw(mt2), op, trans)
+
+
+def dev_MatrixLUDecompInPlace(A, indx, status=None, ctx=None):
+    c = _ctx_of(ctx)
+    _bind_stream(c, A)
+    c.call("b2m_dev_MatrixLUDecompInPlace", _tptr(A), _tlw(A), A.shape[1], _tptr(indx),
+           _tptr(status) if status is not None else None)
+
+
+def dev_MatrixLUBackSubst(LU, indx, B, ctx=None):
+    c = _ctx_of(ctx)
+    _bind_stream(c, B)
+    c.call("b2m_dev_MatrixLUBackSubst", _tptr(LU), _tlw(LU), LU.shape[1], _tptr(indx), _tptr(B), _tlw(B), B.shape[1])
+
+
+def dev_MatrixLinEQSolve(A, B, X, num_refinements=0, status=None, ctx=None):
+    c = _ctx_of(ctx)
+    _bind_stream(c, A)
+    c.call("b2m_dev_MatrixLinEQSolve", _tptr(A), _tlw(A), A.shape[1], _tptr(B), _tlw(B), _tptr(X), _tlw(X),
+           B.shape[1], num_refinements, _tptr(status) if status is not None else None)
+
+
+def dev_MatrixInverseInPlace(A, status=None, ctx=None):
+    c = _ctx_of(ctx)
+    _bind_stream(c, A)
+    c.call("b2m_dev_MatrixInverseInPlace", _tptr(A), _tlw(A), A.shape[1],
+           _tptr(status) if status is not None else None)
+
+
+def dev_MatrixDeterminant(A, det, ctx=None):
+    c = _ctx_of(ctx)
+    _bind_stream(c, A)
+    c.call("b2m_dev_MatrixDeterminant", _tptr(A), _tlw(A), A.shape[1], _tptr(det))
