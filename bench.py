@@ -1,0 +1,362 @@
+#!/usr/bin/env python
+"""Headline benchmark: LU-solve GFLOP/s at n = 8192 to FP64 backward error.
+
+Workload (one step): solve A X = B for a resident 8192 x 8192 FP64 matrix A = U diag(s) V^T,
+s_i = kappa^(-i/(n-1)) with kappa = 1e5 (the hardest of {1e2, 1e4, 1e5}), and 16 Gaussian
+right-hand sides, to normwise backward error <= n * 2^-53.  GFLOP/s charges the LAPACK nominal
+2/3 n^3 + 2 n^2 k flops per solve to every form.  A is 512 MiB, larger than L2, so no flush is
+needed between steps.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--form mixed|plain] [--impl b200|reference]
+
+--impl reference times the reference's own algorithm restated in C++ (the oracle's threaded
+ThrMatrixLinEQSolve, all host cores) on a bounded sample of the same workload.
+With N > 1 (torchrun) every rank solves its own system: replicas, no collective on the data path.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+N_DEFAULT, NRHS_DEFAULT, KAPPA_DEFAULT = 8192, 16, 1e5
+METRIC = "LU-solve GFLOP/s at n=8192 to FP64 backward error: mixed-precision IR vs plain FP64"
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=5)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", choices=["b200", "reference"], default="b200")
+    p.add_argument("--form", choices=["mixed", "plain"], default=None)
+    p.add_argument("--n", type=int, default=N_DEFAULT)
+    p.add_argument("--nrhs", type=int, default=NRHS_DEFAULT)
+    p.add_argument("--kappa", type=float, default=KAPPA_DEFAULT)
+    p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--no-cpu", action="store_true")
+    p.add_argument("--cpu-n", type=int, default=4096, help="order of the CPU-baseline sample")
+    return p.parse_args()
+
+
+# ----------------------------------------------------------------------------- clocks
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons, sampled every 200 ms during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines: list[str] = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self) -> dict:
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx.append(float(f[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ----------------------------------------------------------------------------- distributed plumbing
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    return world, rank, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(world, value: float) -> float:
+    if world == 1:
+        return value
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([value], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+# ----------------------------------------------------------------------------- CPU baseline (oracle)
+def cpu_baseline(n: int, nrhs: int, seconds: float = 10.0, reps_max: int = 50) -> dict:
+    """The reference's threaded solve (ThrMatrixLinEQSolve, LinAlgLU.pas:986-1128) restated in C++,
+    on all host cores, on an n x n Gaussian system with nrhs right-hand sides."""
+    import numpy as np
+
+    import oracle
+    from mrmath_b200 import inputs
+    oracle.set_num_threads(os.cpu_count() or 1)
+    r = inputs.rng(15)
+    a = r.standard_normal((n, n))
+    b = r.standard_normal((n, nrhs))
+    fl = inputs.lu_solve_flops(n, nrhs)
+    times = []
+    t_end = time.perf_counter() + seconds
+    while len(times) < reps_max and (not times or time.perf_counter() < t_end):
+        t0 = time.perf_counter()
+        rc, x = oracle.thr_lineq_solve(a, b)
+        times.append(time.perf_counter() - t0)
+    best = min(times)
+    return {"value": fl / best / 1e9, "unit": "GFLOP/s", "cores": oracle.num_threads(), "kind": "port",
+            "sample": f"oracle ThrMatrixLinEQSolve restatement, n={n}, {nrhs} RHS, best of {len(times)} runs "
+                      f"({sum(times):.1f} s of CPU work); rate at this order stands in for n=8192",
+            "backward_error": float(oracle.backward_error(a, x, b))}
+
+
+def run_reference(args, world, rank):
+    if rank != 0:
+        return 0
+    n = min(args.cpu_n, args.n)
+    import oracle  # noqa: F401  (fails loudly if the oracle is not built)
+    vals = []
+    for i in range(args.warmup + args.steps):
+        cb = cpu_baseline(n, args.nrhs, seconds=0.0, reps_max=1)
+        if i >= args.warmup:
+            vals.append(cb["value"])
+    v = statistics.median(vals)
+    fl = __import__("mrmath_b200.inputs", fromlist=["x"]).lu_solve_flops(n, args.nrhs)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": v, "unit": "GFLOP/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": fl / v / 1e6, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (MT19937 seed 15, Gaussian)",
+        "config": {"workload": f"FP64 LU solve, n={n} (bounded CPU sample of n={args.n}), {args.nrhs} RHS",
+                   "n": n, "nrhs": args.nrhs, "parallelism": "host threads"},
+        "cpu_baseline": {"value": v, "unit": "GFLOP/s", "cores": cb["cores"], "kind": "port",
+                         "sample": cb["sample"]},
+        "e2e": {"value": v, "unit": "GFLOP/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ----------------------------------------------------------------------------- B200 arm
+def backward_error_torch(A, X, B) -> float:
+    import torch
+    R = B - A @ X
+    na = A.abs().sum(dim=1).max()
+    eta = R.abs().amax(dim=0) / (na * X.abs().amax(dim=0) + B.abs().amax(dim=0))
+    return float(eta.max().item())
+
+
+def fp64_peak_tflops() -> float:
+    """cuBLAS DGEMM 8192^3 (torch.matmul float64), best of 5: the measured FP64 peak of this GPU."""
+    import torch
+    a = torch.randn(8192, 8192, dtype=torch.float64, device="cuda")
+    b = torch.randn(8192, 8192, dtype=torch.float64, device="cuda")
+    torch.matmul(a, b)
+    best = 1e9
+    for _ in range(5):
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record()
+        torch.matmul(a, b)
+        e.record()
+        torch.cuda.synchronize()
+        best = min(best, s.elapsed_time(e))
+    del a, b
+    return 2.0 * 8192 ** 3 / best / 1e9
+
+
+def run_b200(args, world, rank, local):
+    import numpy as np
+    import torch
+
+    import mrmath_b200
+    from mrmath_b200 import inputs, linalg as L
+
+    torch.cuda.set_device(local)
+    ctx = mrmath_b200.Context(local)
+    n, k = args.n, args.nrhs
+    form = args.form or ("mixed" if hasattr(L, "dev_MatrixLinEQSolveMixed") else "plain")
+    A, B = inputs.c2_kappa(n, args.kappa, k, seed=15 + rank, device=f"cuda:{local}")
+    X = torch.empty_like(B)
+    status = torch.zeros(1, dtype=torch.int32, device=A.device)
+    flops = inputs.lu_solve_flops(n, k)
+
+    def step():
+        if form == "mixed":
+            L.dev_MatrixLinEQSolveMixed(A, B, X, status=status, ctx=ctx)
+        else:
+            L.dev_MatrixLinEQSolve(A, B, X, status=status, ctx=ctx)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    eta = backward_error_torch(A, X, B)
+
+    # ---- timed region: K resident steps, events on torch's stream (the stream libb2m is bound to)
+    l0 = ctx.kernel_launches()
+    barrier(world)
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ev0.record()
+        for _ in range(args.steps):
+            step()
+        ev1.record()
+        torch.cuda.synchronize()
+    ms = ev0.elapsed_time(ev1)
+    barrier(world)
+    launches = ctx.kernel_launches() - l0
+    ms_max = max_over_ranks(world, ms)
+    # the same K steps again with every launch bracketed by CUDA events on its stream: per kernel
+    # class device time and algorithmic work for the roofline (kept out of the timed region above)
+    ctx.profile(True)
+    for _ in range(args.steps):
+        step()
+    prof = ctx.profile_read()
+    ctx.profile(False)
+    value = args.steps * world * flops / (ms_max / 1e3) / 1e9
+
+    # ---- end to end through the host-buffer C ABI (pinned host buffers, copies inside the region)
+    e2e = None
+    if not args.no_e2e:
+        hA = torch.empty((n, n), dtype=torch.float64, pin_memory=True)
+        hB = torch.empty((n, k), dtype=torch.float64, pin_memory=True)
+        hX = torch.empty((n, k), dtype=torch.float64, pin_memory=True)
+        hA.copy_(A)
+        hB.copy_(B)
+        a_np, b_np, x_np = hA.numpy(), hB.numpy(), hX.numpy()
+        ctx.set_stream(0)  # host API on the legacy stream so the events below bracket it
+        fn = L.MatrixLinEQSolveMixed if form == "mixed" else L.MatrixLinEQSolve
+        fn(a_np, b_np, X=x_np, ctx=ctx)
+        torch.cuda.synchronize()
+        barrier(world)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(torch.cuda.default_stream())
+        for _ in range(args.steps):
+            fn(a_np, b_np, X=x_np, ctx=ctx)
+        e1.record(torch.cuda.default_stream())
+        torch.cuda.synchronize()
+        ems = max_over_ranks(world, e0.elapsed_time(e1))
+        eta_e2e = backward_error_torch(A, torch.from_numpy(x_np).to(A.device), B)
+        e2e = {"value": args.steps * world * flops / (ems / 1e3) / 1e9, "unit": "GFLOP/s",
+               "h2d_bytes_per_step": int(a_np.nbytes + b_np.nbytes), "d2h_bytes_per_step": int(x_np.nbytes),
+               "backward_error": eta_e2e, "api": "b2m_MatrixLinEQSolve" + ("Mixed" if form == "mixed" else "")}
+        del hA, hB, hX
+
+    # ---- roofline of the dominant kernel class (by device time in the timed region)
+    dom = max(prof.items(), key=lambda kv: kv[1]["ms"])
+    dom_name, d = dom
+    peak_f64 = fp64_peak_tflops()
+    peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))) if os.path.exists(
+        os.path.join(ROOT, "MEASURED_PEAKS.json")) else {}
+    if dom_name in ("gemm_f64", "panel", "trsm"):
+        achieved = d["work"] / (d["ms"] / 1e3) / 1e12 if d["ms"] > 0 else 0.0
+        roof = {"kernel_class": dom_name, "bound": "tensor", "achieved": achieved, "peak": peak_f64,
+                "unit": "TFLOP/s", "frac": achieved / peak_f64, "traffic": None,
+                "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (MEASURED_PEAKS.json has no FP64 figure)",
+                "launches": d["launches"], "share": d["ms"] / max(1e-9, sum(v["ms"] for v in prof.values()))}
+    elif dom_name == "gemm_tc":
+        pk = peaks.get("bf16_tflops", 1590.0) / 2.0
+        achieved = d["work"] / (d["ms"] / 1e3) / 1e12 if d["ms"] > 0 else 0.0
+        roof = {"kernel_class": dom_name, "bound": "tensor", "achieved": achieved, "peak": pk, "unit": "TFLOP/s",
+                "frac": achieved / pk, "traffic": None,
+                "peak_source": "TF32 dense = half of measured bf16_tflops (MEASURED_PEAKS.json)",
+                "launches": d["launches"]}
+    else:
+        bw = peaks.get("hbm_gbs", 6650.0)
+        achieved = d["work"] / (d["ms"] / 1e3) / 1e9 if d["ms"] > 0 else 0.0
+        roof = {"kernel_class": dom_name, "bound": "hbm", "achieved": achieved, "peak": bw, "unit": "GB/s",
+                "frac": achieved / bw, "traffic": None, "peak_source": "MEASURED_PEAKS.json hbm_gbs",
+                "launches": d["launches"]}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        try:
+            cpu = cpu_baseline(min(args.cpu_n, n), k, seconds=10.0)
+        except Exception as exc:  # the oracle is test infrastructure; report why it is missing
+            cpu = {"value": None, "unit": "GFLOP/s", "cores": 0, "kind": "port", "sample": f"unavailable: {exc}"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "GFLOP/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64" if form == "plain" else "f32/tf32 factor + f64 refinement",
+            "data": "synthetic: A = U diag(s) V^T from MT19937-seeded Gaussians (seed 15 + rank), 16 Gaussian RHS",
+            "config": {"workload": f"{'mixed-precision IR' if form == 'mixed' else 'plain FP64'} LU solve, "
+                                   f"n={n}, {k} RHS, kappa={args.kappa:g}", "n": n, "nrhs": k,
+                       "kappa": args.kappa, "form": form, "parallelism": f"replicas x{world}",
+                       "l2": "A (512 MiB) exceeds L2; no flush needed"},
+            "backward_error": eta, "backward_error_bound": n * 2.0 ** -53,
+            "e2e": e2e, "gpu_launches": launches, "roofline": roof, "cpu_baseline": cpu,
+            "kernel_classes": {kname: {"launches": v["launches"], "ms": round(v["ms"], 4)}
+                               for kname, v in prof.items() if v["launches"]},
+            "clocks": clk.summary(),
+        }
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    return 0
+
+
+def main():
+    args = parse()
+    world, rank, local = dist_setup()
+    try:
+        if args.impl == "reference":
+            return run_reference(args, world, rank)
+        return run_b200(args, world, rank, local)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -56,13 +56,22 @@ typedef struct b2m_ctx b2m_ctx;
  * in the reference (its state is global: MatrixASMStubSwitch.pas InitMathFunctions). */
 B2M_API int32_t     b2m_create(int32_t device, b2m_ctx** out);
 B2M_API int32_t     b2m_destroy(b2m_ctx* ctx);
-/* Use a caller stream (a cudaStream_t) for the b2m_dev_* calls; NULL restores the context's own. */
+/* Run subsequent calls on a caller stream (a cudaStream_t; NULL is the legacy default stream). */
 B2M_API int32_t     b2m_set_stream(b2m_ctx* ctx, void* stream);
+/* Go back to the context's own (non-blocking) stream. */
+B2M_API int32_t     b2m_use_own_stream(b2m_ctx* ctx);
 B2M_API int32_t     b2m_synchronize(b2m_ctx* ctx);
 B2M_API const char* b2m_last_error(b2m_ctx* ctx);
 B2M_API const char* b2m_status_string(int32_t status);
 /* Number of kernels this context has launched so far (device work accounting). */
 B2M_API int64_t     b2m_kernel_launches(b2m_ctx* ctx);
+/* Event profiler: when enabled, every launch is bracketed by CUDA events on its own stream and
+ * its algorithmic work is recorded per kernel class (0 FP64 GEMM, 1 panel, 2 row swaps,
+ * 3 triangular solve, 4 tensor-core GEMM, 5 solve/refinement kernels, 6 other).  Enabling (or
+ * disabling) resets the counters.  Reading synchronizes the device. */
+B2M_API int32_t     b2m_profile(b2m_ctx* ctx, int32_t enable);
+B2M_API int32_t     b2m_profile_read(b2m_ctx* ctx, int32_t kernel_class, int64_t* launches, double* ms,
+                                     double* work);
 
 /* ------------------------------------------------------------------ GEMM
  * Replaces MatrixMult / MatrixMultEx (MatrixASMStubSwitch.pas:769-782),

@@ -24,10 +24,13 @@ SIGNATURES: dict[str, tuple] = {
     "b2m_create": (i32, [i32, C.POINTER(vp)]),
     "b2m_destroy": (i32, [vp]),
     "b2m_set_stream": (i32, [vp, vp]),
+    "b2m_use_own_stream": (i32, [vp]),
     "b2m_synchronize": (i32, [vp]),
     "b2m_last_error": (C.c_char_p, [vp]),
     "b2m_status_string": (C.c_char_p, [i32]),
     "b2m_kernel_launches": (i64, [vp]),
+    "b2m_profile": (i32, [vp, i32]),
+    "b2m_profile_read": (i32, [vp, i32, C.POINTER(i64), C.POINTER(dbl), C.POINTER(dbl)]),
     "b2m_MatrixMultEx": (i32, [vp, vp, i64, vp, vp, i64, i64, i64, i64, i64, i64, i32, i32]),
     "b2m_dev_MatrixMultEx": (i32, [vp, vp, i64, vp, vp, i64, i64, i64, i64, i64, i64, i32, i32]),
     "b2m_MatrixLUDecompInPlace": (i32, [vp, vp, i64, i64, vp]),
@@ -47,7 +50,7 @@ SIGNATURES: dict[str, tuple] = {
 def load(path: str = LIB_PATH) -> C.CDLL:
     if not os.path.exists(path):
         raise ImportError(
-            f"libb2m.so not found at {path}: build it with `python -m mrmath_b200.build` "
+            f"libb2m.so not found at {path}: build it with `python mrmath_b200/build.py` "
             "(there is no CPU fallback)")
     lib = C.CDLL(path)
     for name, (res, args) in SIGNATURES.items():
@@ -97,13 +100,30 @@ class Context:
         raise B2MError(status, f"{lib.b2m_status_string(status).decode()}: {self.last_error()}")
 
     def set_stream(self, stream_handle: int | None) -> None:
+        """Bind a cudaStream_t (0 / None = the legacy default stream)."""
         self.check(lib.b2m_set_stream(self.h, stream_handle or None))
+
+    def use_own_stream(self) -> None:
+        self.check(lib.b2m_use_own_stream(self.h))
 
     def synchronize(self) -> None:
         self.check(lib.b2m_synchronize(self.h))
 
     def kernel_launches(self) -> int:
         return lib.b2m_kernel_launches(self.h)
+
+    KERNEL_CLASSES = ("gemm_f64", "panel", "row_swap", "trsm", "gemm_tc", "solve", "other")
+
+    def profile(self, enable: bool) -> None:
+        self.check(lib.b2m_profile(self.h, int(enable)))
+
+    def profile_read(self) -> dict:
+        out = {}
+        for i, name in enumerate(self.KERNEL_CLASSES):
+            n, ms, w = i64(0), dbl(0.0), dbl(0.0)
+            self.check(lib.b2m_profile_read(self.h, i, C.byref(n), C.byref(ms), C.byref(w)))
+            out[name] = {"launches": n.value, "ms": ms.value, "work": w.value}
+        return out
 
     def call(self, name: str, *args, allow=(OK,)) -> int:
         return self.check(getattr(lib, name)(self.h, *args), allow=allow)

@@ -1,7 +1,7 @@
 """Builds libb2m.so (all CUDA sources under csrc/) for sm_100a with nvcc, in-tree.
 
-    python -m mrmath_b200.build          # incremental (skips when the .so is newer than every source)
-    python -m mrmath_b200.build --force
+    python mrmath_b200/build.py          # incremental (skips when the .so is newer than every source)
+    python mrmath_b200/build.py --force
 
 Objects go to csrc/_build/ (git-ignored); the shared library lands next to this file so that it
 travels with the repository snapshot.

@@ -9,6 +9,7 @@
 #include <cstdio>
 #include <mutex>
 #include <string>
+#include <vector>
 
 #include "../../include/b2m.h"
 
@@ -38,6 +39,16 @@ enum WsSlot : int {
     kNumWs
 };
 
+// kernel classes for the optional event profiler (b2m_profile / b2m_profile_read)
+enum KernelClass : int { kClsGemm = 0, kClsPanel, kClsSwap, kClsTrsm, kClsTcGemm, kClsSolve, kClsOther, kNumCls };
+
+struct Prof {
+    bool on = false;
+    std::vector<cudaEvent_t> ev[kNumCls];  // start/end pairs
+    size_t used[kNumCls] = {};
+    double work[kNumCls] = {};             // algorithmic flops (or bytes) recorded with the launches
+};
+
 struct Ctx {
     int device = 0;
     int num_sms = 148;
@@ -51,6 +62,7 @@ struct Ctx {
     void* h_pinned = nullptr;        // pinned staging for host-buffer calls
     size_t h_pinned_bytes = 0;
     int64_t launches = 0;
+    Prof prof;
     std::string last_error;
     std::mutex mtx;
 };
@@ -81,6 +93,10 @@ int32_t fail(Ctx* ctx, int32_t status, const char* fmt, ...);
             return ::b2m::fail((ctx), B2M_ERR_CUDA, "kernel launch failed: %s (%s:%d)",            \
                                cudaGetErrorString(e_), __FILE__, __LINE__);                        \
     } while (0)
+
+// Event profiler: brackets one launch on stream `st` (no-ops unless enabled).
+void prof_begin(Ctx* ctx, cudaStream_t st, int cls);
+void prof_end(Ctx* ctx, cudaStream_t st, int cls, double work);
 
 // grows workspace slot `slot` to at least `bytes` (never shrinks); 256-byte aligned
 int32_t ws_get(Ctx* ctx, int slot, size_t bytes, void** out);

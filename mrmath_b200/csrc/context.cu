@@ -56,6 +56,27 @@ int32_t pinned_get(Ctx* ctx, size_t bytes, void** out) {
     return B2M_OK;
 }
 
+void prof_begin(Ctx* ctx, cudaStream_t st, int cls) {
+    Prof& p = ctx->prof;
+    if (!p.on) return;
+    if (p.used[cls] + 2 > p.ev[cls].size()) {
+        for (int i = 0; i < 64; ++i) {
+            cudaEvent_t e;
+            if (cudaEventCreate(&e) != cudaSuccess) return;
+            p.ev[cls].push_back(e);
+        }
+    }
+    cudaEventRecord(p.ev[cls][p.used[cls]], st);
+}
+
+void prof_end(Ctx* ctx, cudaStream_t st, int cls, double work) {
+    Prof& p = ctx->prof;
+    if (!p.on || p.used[cls] + 2 > p.ev[cls].size()) return;
+    cudaEventRecord(p.ev[cls][p.used[cls] + 1], st);
+    p.used[cls] += 2;
+    p.work[cls] += work;
+}
+
 typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
                                   const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
@@ -149,6 +170,8 @@ extern "C" int32_t b2m_destroy(b2m_ctx* h) {
     if (ctx->d_status) cudaFree(ctx->d_status);
     if (ctx->h_status) cudaFreeHost(ctx->h_status);
     if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
+    for (int c = 0; c < b2m::kNumCls; ++c)
+        for (cudaEvent_t e : ctx->prof.ev[c]) cudaEventDestroy(e);
     delete ctx;
     return B2M_OK;
 }
@@ -156,7 +179,42 @@ extern "C" int32_t b2m_destroy(b2m_ctx* h) {
 extern "C" int32_t b2m_set_stream(b2m_ctx* h, void* stream) {
     Ctx* ctx = reinterpret_cast<Ctx*>(h);
     if (!ctx) return B2M_ERR_ARG;
-    ctx->stream = stream ? reinterpret_cast<cudaStream_t>(stream) : ctx->own_stream;
+    ctx->stream = reinterpret_cast<cudaStream_t>(stream);
+    return B2M_OK;
+}
+
+extern "C" int32_t b2m_use_own_stream(b2m_ctx* h) {
+    Ctx* ctx = reinterpret_cast<Ctx*>(h);
+    if (!ctx) return B2M_ERR_ARG;
+    ctx->stream = ctx->own_stream;
+    return B2M_OK;
+}
+
+extern "C" int32_t b2m_profile(b2m_ctx* h, int32_t enable) {
+    Ctx* ctx = reinterpret_cast<Ctx*>(h);
+    if (!ctx) return B2M_ERR_ARG;
+    B2M_CU(ctx, cudaStreamSynchronize(ctx->stream));
+    ctx->prof.on = enable != 0;
+    for (int c = 0; c < b2m::kNumCls; ++c) {
+        ctx->prof.used[c] = 0;
+        ctx->prof.work[c] = 0.0;
+    }
+    return B2M_OK;
+}
+
+extern "C" int32_t b2m_profile_read(b2m_ctx* h, int32_t cls, int64_t* launches, double* ms, double* work) {
+    Ctx* ctx = reinterpret_cast<Ctx*>(h);
+    if (!ctx || cls < 0 || cls >= b2m::kNumCls) return B2M_ERR_ARG;
+    B2M_CU(ctx, cudaDeviceSynchronize());
+    b2m::Prof& p = ctx->prof;
+    double tot = 0.0;
+    for (size_t i = 0; i + 1 < p.used[cls]; i += 2) {
+        float t = 0.f;
+        if (cudaEventElapsedTime(&t, p.ev[cls][i], p.ev[cls][i + 1]) == cudaSuccess) tot += t;
+    }
+    if (launches) *launches = (int64_t)(p.used[cls] / 2);
+    if (ms) *ms = tot;
+    if (work) *work = p.work[cls];
     return B2M_OK;
 }
 

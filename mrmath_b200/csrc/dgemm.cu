@@ -193,7 +193,9 @@ int32_t launch_variant(Ctx* ctx, cudaStream_t st, const CUtensorMap& ta, const C
         attr_set = true;
     }
     const int tiles = (int)(ceil_div(a.M, BM) * ceil_div(a.N, BN));
+    prof_begin(ctx, st, kClsGemm);
     dgemm_tma_kernel<AK, BKM><<<tiles, kThreads, kSmemBytes, st>>>(ta, tb, a);
+    prof_end(ctx, st, kClsGemm, 2.0 * a.M * a.N * a.K);
     B2M_LAUNCHED(ctx);
     return B2M_OK;
 }

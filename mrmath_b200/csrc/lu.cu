@@ -452,7 +452,12 @@ int32_t launch_panel_rpt(Ctx* ctx, cudaStream_t st, const PanelCfg& pc, T* P, in
     at[0].val.clusterDim.z = 1;
     cfg.attrs = at;
     cfg.numAttrs = 1;
+    prof_begin(ctx, st, kClsPanel);
     B2M_CU(ctx, cudaLaunchKernelEx(&cfg, kern, P, ld, m, w, pc.R, row_base, col_base, ipiv, ctx->d_status));
+    // algorithmic flops of an m x w partial-pivoting panel: sum_j 2(m-j-1)(w-j-1) + (m-j-1)
+    double fl = 0.0;
+    for (int j = 0; j < w; ++j) fl += 2.0 * (m - j - 1) * (w - j - 1) + (m - j - 1);
+    prof_end(ctx, st, kClsPanel, fl);
     B2M_LAUNCHED(ctx);
     return B2M_OK;
 }
@@ -472,7 +477,9 @@ int32_t launch_swaps(Ctx* ctx, cudaStream_t st, T* A, int64_t ld, int ncols, int
                      int32_t* perm) {
     const int other = ncols - w;
     const int blocks = std::max(1, (int)ceil_div(other, kSwapThreads));
+    prof_begin(ctx, st, kClsSwap);
     leaf_swap_kernel<T><<<blocks, kSwapThreads, 0, st>>>(A, ld, ncols, c0, w, ipiv, perm, ctx->d_status);
+    prof_end(ctx, st, kClsSwap, 4.0 * w * other * sizeof(T));  // <= 2w rows read + written
     B2M_LAUNCHED(ctx);
     return B2M_OK;
 }
@@ -482,7 +489,9 @@ int32_t launch_trsm_small(Ctx* ctx, cudaStream_t st, const T* L, int64_t ldl, T*
                           bool upper) {
     if (k <= 0 || ncols <= 0) return B2M_OK;
     const int blocks = (int)ceil_div(ncols, kTrsmThreads);
+    prof_begin(ctx, st, kClsTrsm);
     trsm_small_kernel<T><<<blocks, kTrsmThreads, 0, st>>>(L, ldl, B, ldb, k, ncols, upper ? 1 : 0, ctx->d_status);
+    prof_end(ctx, st, kClsTrsm, (double)k * k * ncols);
     B2M_LAUNCHED(ctx);
     return B2M_OK;
 }

@@ -133,11 +133,9 @@ extern "C" void orc_fill_gauss(orc_rng* r, double* dst, int64_t count) {
     for (int64_t i = 0; i < count; ++i) dst[i] = orc_rng_gauss(r);
 }
 extern "C" void orc_fill_gauss_exp(orc_rng* r, double* dst, int64_t count) {
-    for (int64_t i = 0; i < count; ++i) {
-        double g = orc_rng_gauss(r);
-        int e = (int)orc_rng_lw(r, 17u) - 8;
-        dst[i] = std::ldexp(g, e);
-    }
+    // all Gaussians first, then all exponents e = RandLW(17) - 8, applied element by element
+    for (int64_t i = 0; i < count; ++i) dst[i] = orc_rng_gauss(r);
+    for (int64_t i = 0; i < count; ++i) dst[i] = std::ldexp(dst[i], (int)orc_rng_lw(r, 17u) - 8);
 }
 
 extern "C" void orc_set_mode(int32_t mode) { g_mode = mode ? 1 : 0; }

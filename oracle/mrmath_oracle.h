@@ -44,7 +44,7 @@ double   orc_rng_gauss(orc_rng* r);                                           /*
    (DblMatrix.pas:2751-2759): uniform [0,1) and Gaussian. */
 void     orc_fill_uniform(orc_rng* r, double* dst, int64_t count);
 void     orc_fill_gauss(orc_rng* r, double* dst, int64_t count);
-/* C3 GEMM inputs: g*2^e with g = RandGauss and e = RandLW(17) - 8, per element, row-major. */
+/* C3 GEMM inputs: g*2^e, all g = RandGauss first, then all e = RandLW(17) - 8, row-major. */
 void     orc_fill_gauss_exp(orc_rng* r, double* dst, int64_t count);
 
 /* ---------------- kernel family (MatrixASMStubSwitch.pas InitMathFunctions) ---------------- */
