@@ -117,6 +117,21 @@ B2M_API int32_t b2m_dev_MatrixLinEQSolve(b2m_ctx* ctx, const double* A, int64_t 
 B2M_API int32_t b2m_dev_MatrixInverseInPlace(b2m_ctx* ctx, double* A, int64_t LineWidthA, int64_t width, int32_t* status);
 B2M_API int32_t b2m_dev_MatrixDeterminant(b2m_ctx* ctx, const double* A, int64_t LineWidthA, int64_t width, double* det);
 
+/* Allocation-free solve.  No counterpart in the reference: it exists for callers that may not
+ * allocate device memory (a host program whose memory manager owns all device allocations, code
+ * running inside a stream capture, a real-time loop with a fixed budget).  Same arguments and
+ * result as b2m_dev_MatrixLinEQSolve without refinement, on the given cudaStream_t (NULL = legacy
+ * default stream) of the calling thread's current device.  All intermediates live in one static
+ * device array of about 2.5 MiB that every GPU loading the library holds until exit; orders up to
+ * 512 and up to 64 right-hand sides are accepted, larger sizes return B2M_ERR_UNSUPPORTED.  The
+ * first call on a device looks up the array's address (cudaGetSymbolAddress), so make that first
+ * call before any stream capture.  Every call shares the array and it keeps the last call's
+ * contents: calls that overlap on the GPU (other streams, other host threads) race.  *status
+ * (device int32, may be NULL) receives 0 (leOk) or 1 (leSingular). */
+B2M_API int32_t b2m_dev_MatrixLinEQSolveNoAlloc(void* stream, const double* A, int64_t LineWidthA, int64_t width,
+                                                const double* B, int64_t LineWidthB, double* X, int64_t LineWidthX,
+                                                int64_t Width2, int32_t* status);
+
 #ifdef __cplusplus
 }
 #endif

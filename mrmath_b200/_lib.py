@@ -44,6 +44,7 @@ SIGNATURES: dict[str, tuple] = {
     "b2m_dev_MatrixLinEQSolve": (i32, [vp, vp, i64, i64, vp, i64, vp, i64, i64, i64, vp]),
     "b2m_dev_MatrixInverseInPlace": (i32, [vp, vp, i64, i64, vp]),
     "b2m_dev_MatrixDeterminant": (i32, [vp, vp, i64, i64, vp]),
+    "b2m_dev_MatrixLinEQSolveNoAlloc": (i32, [vp, vp, i64, i64, vp, i64, vp, i64, i64, vp]),
 }
 
 

@@ -28,8 +28,9 @@ int32_t lu_factor_f64(Ctx* ctx, cudaStream_t st, double* A, int64_t ld, int64_t 
 
 // Solves A X = B from the factors of lu_factor_f64: B (n x nrhs, row stride ldb elements) is
 // overwritten with X.  perm is the permutation from lu_factor_f64.
+// `tmp` (n x ldb doubles) is the gather buffer; when null the context workspace is used.
 int32_t lu_solve_f64(Ctx* ctx, cudaStream_t st, const double* LU, int64_t ld, int64_t n, const int32_t* perm,
-                     double* B, int64_t ldb, int64_t nrhs);
+                     double* B, int64_t ldb, int64_t nrhs, double* tmp = nullptr);
 
 // Builds perm from ipiv on the device (used when factors come from outside: b2m_MatrixLUBackSubst).
 int32_t perm_from_ipiv(Ctx* ctx, cudaStream_t st, const int32_t* ipiv, int64_t n, int32_t* perm);

@@ -565,13 +565,16 @@ int32_t lu_factor_f64(Ctx* ctx, cudaStream_t st, double* A, int64_t ld, int64_t 
 }
 
 int32_t lu_solve_f64(Ctx* ctx, cudaStream_t st, const double* LU, int64_t ld, int64_t n, const int32_t* perm,
-                     double* B, int64_t ldb, int64_t nrhs) {
+                     double* B, int64_t ldb, int64_t nrhs, double* tmp) {
     if (n <= 0 || nrhs <= 0) return B2M_OK;
     if ((ldb & 1) || !aligned16(B)) return fail(ctx, B2M_ERR_DIM, "lu_solve_f64: ldb must be even");
     // X = P B
-    void* tmp = nullptr;
-    B2M_TRY(ws_get(ctx, kWsE, (size_t)(n * ldb * sizeof(double)), &tmp));
-    double* X = static_cast<double*>(tmp);
+    double* X = tmp;
+    if (!X) {
+        void* w = nullptr;
+        B2M_TRY(ws_get(ctx, kWsE, (size_t)(n * ldb * sizeof(double)), &w));
+        X = static_cast<double*>(w);
+    }
     B2M_CU(ctx, cudaMemcpy2DAsync(X, ldb * 8, B, ldb * 8, nrhs * 8, n, cudaMemcpyDeviceToDevice, st));
     gather_rows_kernel<<<(unsigned)ceil_div(n * nrhs, 256), 256, 0, st>>>(B, ldb, X, ldb, perm, n, nrhs);
     B2M_LAUNCHED(ctx);
