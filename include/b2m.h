@@ -60,6 +60,10 @@ B2M_API int32_t     b2m_destroy(b2m_ctx* ctx);
 B2M_API int32_t     b2m_set_stream(b2m_ctx* ctx, void* stream);
 /* Go back to the context's own (non-blocking) stream. */
 B2M_API int32_t     b2m_use_own_stream(b2m_ctx* ctx);
+/* Launch sequences whose shape depends only on sizes and buffers (factorisations, solves) are
+ * captured into CUDA graphs on first use and replayed afterwards (default on); 0 launches
+ * every kernel from the host instead. */
+B2M_API int32_t     b2m_use_graphs(b2m_ctx* ctx, int32_t enable);
 B2M_API int32_t     b2m_synchronize(b2m_ctx* ctx);
 B2M_API const char* b2m_last_error(b2m_ctx* ctx);
 B2M_API const char* b2m_status_string(int32_t status);

@@ -25,6 +25,7 @@ SIGNATURES: dict[str, tuple] = {
     "b2m_destroy": (i32, [vp]),
     "b2m_set_stream": (i32, [vp, vp]),
     "b2m_use_own_stream": (i32, [vp]),
+    "b2m_use_graphs": (i32, [vp, i32]),
     "b2m_synchronize": (i32, [vp]),
     "b2m_last_error": (C.c_char_p, [vp]),
     "b2m_status_string": (C.c_char_p, [i32]),
@@ -103,6 +104,9 @@ class Context:
     def set_stream(self, stream_handle: int | None) -> None:
         """Bind a cudaStream_t (0 / None = the legacy default stream)."""
         self.check(lib.b2m_set_stream(self.h, stream_handle or None))
+
+    def use_graphs(self, enable: bool) -> None:
+        self.check(lib.b2m_use_graphs(self.h, int(enable)))
 
     def use_own_stream(self) -> None:
         self.check(lib.b2m_use_own_stream(self.h))

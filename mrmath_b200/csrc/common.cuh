@@ -7,7 +7,10 @@
 
 #include <cstdint>
 #include <cstdio>
+#include <functional>
+#include <map>
 #include <mutex>
+#include <tuple>
 #include <string>
 #include <vector>
 
@@ -49,6 +52,15 @@ struct Prof {
     double work[kNumCls] = {};             // algorithmic flops (or bytes) recorded with the launches
 };
 
+// key of a captured launch sequence: (kind, pointers and sizes baked into the graph)
+typedef std::tuple<int, const void*, const void*, const void*, const void*, int64_t, int64_t, int64_t, int64_t>
+    GraphKey;
+struct GraphEntry {
+    cudaGraphExec_t exec = nullptr;
+    int64_t launches = 0;
+    uint64_t last_use = 0;
+};
+
 struct Ctx {
     int device = 0;
     int num_sms = 148;
@@ -63,6 +75,10 @@ struct Ctx {
     size_t h_pinned_bytes = 0;
     int64_t launches = 0;
     Prof prof;
+    bool use_graphs = true;
+    std::map<GraphKey, GraphEntry> graphs;
+    uint64_t graph_clock = 0;
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     std::string last_error;
     std::mutex mtx;
 };
@@ -97,6 +113,12 @@ int32_t fail(Ctx* ctx, int32_t status, const char* fmt, ...);
 // Event profiler: brackets one launch on stream `st` (no-ops unless enabled).
 void prof_begin(Ctx* ctx, cudaStream_t st, int cls);
 void prof_end(Ctx* ctx, cudaStream_t st, int cls, double work);
+
+// Runs `issue(stream)` -- a launch sequence whose shape depends only on `key` -- through a cached
+// CUDA graph: the first call captures and instantiates it, later calls replay it.  The legacy
+// default stream cannot be captured, so the graph then runs on the context's own stream, joined
+// to `st` with events both ways.  Falls back to eager launches while profiling.
+int32_t run_graph(Ctx* ctx, cudaStream_t st, const GraphKey& key, const std::function<int32_t(cudaStream_t)>& issue);
 
 // grows workspace slot `slot` to at least `bytes` (never shrinks); 256-byte aligned
 int32_t ws_get(Ctx* ctx, int slot, size_t bytes, void** out);

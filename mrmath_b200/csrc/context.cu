@@ -77,6 +77,61 @@ void prof_end(Ctx* ctx, cudaStream_t st, int cls, double work) {
     p.work[cls] += work;
 }
 
+int32_t run_graph(Ctx* ctx, cudaStream_t st, const GraphKey& key, const std::function<int32_t(cudaStream_t)>& issue) {
+    if (!ctx->use_graphs || ctx->prof.on) return issue(st);
+    cudaStreamCaptureStatus cs_status = cudaStreamCaptureStatusNone;
+    if (st != nullptr && st != cudaStreamLegacy) {
+        B2M_CU(ctx, cudaStreamIsCapturing(st, &cs_status));
+        if (cs_status != cudaStreamCaptureStatusNone) return issue(st);  // the caller is capturing: join it
+    }
+    const bool fork = (st == nullptr || st == cudaStreamLegacy || st == cudaStreamPerThread);
+    cudaStream_t gs = fork ? ctx->own_stream : st;
+    auto it = ctx->graphs.find(key);
+    if (it == ctx->graphs.end()) {
+        if (ctx->graphs.size() >= 32) {  // evict the least recently used graph
+            auto lru = ctx->graphs.begin();
+            for (auto g = ctx->graphs.begin(); g != ctx->graphs.end(); ++g)
+                if (g->second.last_use < lru->second.last_use) lru = g;
+            B2M_CU(ctx, cudaStreamSynchronize(gs));
+            cudaGraphExecDestroy(lru->second.exec);
+            ctx->graphs.erase(lru);
+        }
+        cudaGraph_t g = nullptr;
+        const int64_t l0 = ctx->launches;
+        B2M_CU(ctx, cudaStreamBeginCapture(gs, cudaStreamCaptureModeThreadLocal));
+        const int32_t r = issue(gs);
+        const cudaError_t ce = cudaStreamEndCapture(gs, &g);
+        if (r != B2M_OK) {
+            if (g) cudaGraphDestroy(g);
+            return r;
+        }
+        if (ce != cudaSuccess) return fail(ctx, B2M_ERR_CUDA, "stream capture failed: %s", cudaGetErrorString(ce));
+        GraphEntry e;
+        const cudaError_t ie = cudaGraphInstantiate(&e.exec, g, 0);
+        cudaGraphDestroy(g);
+        if (ie != cudaSuccess) return fail(ctx, B2M_ERR_CUDA, "graph instantiate failed: %s", cudaGetErrorString(ie));
+        e.launches = ctx->launches - l0;
+        ctx->launches = l0;
+        it = ctx->graphs.emplace(key, e).first;
+    }
+    it->second.last_use = ++ctx->graph_clock;
+    if (fork) {
+        if (!ctx->ev_fork) {
+            B2M_CU(ctx, cudaEventCreateWithFlags(&ctx->ev_fork, cudaEventDisableTiming));
+            B2M_CU(ctx, cudaEventCreateWithFlags(&ctx->ev_join, cudaEventDisableTiming));
+        }
+        B2M_CU(ctx, cudaEventRecord(ctx->ev_fork, st));
+        B2M_CU(ctx, cudaStreamWaitEvent(gs, ctx->ev_fork, 0));
+    }
+    B2M_CU(ctx, cudaGraphLaunch(it->second.exec, gs));
+    if (fork) {
+        B2M_CU(ctx, cudaEventRecord(ctx->ev_join, gs));
+        B2M_CU(ctx, cudaStreamWaitEvent(st, ctx->ev_join, 0));
+    }
+    ctx->launches += it->second.launches;
+    return B2M_OK;
+}
+
 typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
                                   const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
@@ -172,6 +227,9 @@ extern "C" int32_t b2m_destroy(b2m_ctx* h) {
     if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
     for (int c = 0; c < b2m::kNumCls; ++c)
         for (cudaEvent_t e : ctx->prof.ev[c]) cudaEventDestroy(e);
+    for (auto& g : ctx->graphs) cudaGraphExecDestroy(g.second.exec);
+    if (ctx->ev_fork) cudaEventDestroy(ctx->ev_fork);
+    if (ctx->ev_join) cudaEventDestroy(ctx->ev_join);
     delete ctx;
     return B2M_OK;
 }
@@ -215,6 +273,13 @@ extern "C" int32_t b2m_profile_read(b2m_ctx* h, int32_t cls, int64_t* launches, 
     if (launches) *launches = (int64_t)(p.used[cls] / 2);
     if (ms) *ms = tot;
     if (work) *work = p.work[cls];
+    return B2M_OK;
+}
+
+extern "C" int32_t b2m_use_graphs(b2m_ctx* h, int32_t enable) {
+    Ctx* ctx = reinterpret_cast<Ctx*>(h);
+    if (!ctx) return B2M_ERR_ARG;
+    ctx->use_graphs = enable != 0;
     return B2M_OK;
 }
 

@@ -39,6 +39,13 @@ int32_t perm_from_ipiv(Ctx* ctx, cudaStream_t st, const int32_t* ipiv, int64_t n
 int32_t lu_determinant(Ctx* ctx, cudaStream_t st, const double* LU, int64_t ld, int64_t n, const int32_t* ipiv,
                        double* d_det);
 
+// Factors one m x w panel (w <= 32, row stride ld) with partial pivoting on one thread-block
+// cluster; ipiv[col_base + j] = row_base + pivot row.  panel_max_rows: tallest panel supported.
+template <typename T>
+int32_t launch_panel(Ctx* ctx, cudaStream_t st, T* P, int64_t ld, int m, int w, int row_base, int col_base,
+                     int32_t* ipiv);
+int panel_max_rows(bool fp64, int w);
+
 // Copies a strided FP64 matrix (rows x cols, byte strides) device to device.
 int32_t copy_matrix(Ctx* ctx, cudaStream_t st, double* dst, int64_t ldd_bytes, const double* src, int64_t lds_bytes,
                     int64_t rows, int64_t cols);

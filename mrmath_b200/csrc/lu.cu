@@ -45,145 +45,7 @@ __device__ __forceinline__ void warp_argmax(T& a, int& i) {
     }
 }
 
-// ------------------------------------------------------------------------------------------
-// Panel kernel: one cluster of C CTAs factors an m x w panel (w <= 32) held in distributed
-// shared memory; CTA `rank` owns panel rows [rank*R, rank*R + R).  One cluster barrier per
-// column: candidates (|max|, row, full row) and the current diagonal row are published in
-// double-buffered slots, read remotely after the barrier, and every CTA derives the same pivot.
-// ------------------------------------------------------------------------------------------
-constexpr int kPanelThreads = 512;
-constexpr int kPanelW = 32;
-constexpr int kMaxCluster = 16;
-
-template <typename T, int RPT>
-__global__ void __launch_bounds__(kPanelThreads, 1)
-    panel_lu_kernel(T* P, int64_t ld, int m, int w, int R, int row_base, int col_base, int32_t* ipiv,
-                    int32_t* status) {
-    cg::cluster_group cluster = cg::this_cluster();
-    const int C = (int)cluster.num_blocks();
-    const int rank = (int)cluster.block_rank();
-    extern __shared__ __align__(16) unsigned char panel_smem[];
-    T* S = reinterpret_cast<T*>(panel_smem);
-    const int SS = w | 1;  // odd row stride: conflict-free column access
-
-    __shared__ T cand_abs[2];
-    __shared__ int cand_idx[2];
-    __shared__ T cand_row[2][kPanelW];
-    __shared__ T diag_row[2][kPanelW];
-    __shared__ T allrows[kMaxCluster][kPanelW];
-    __shared__ T c_abs[kMaxCluster];
-    __shared__ int c_idx[kMaxCluster];
-    __shared__ T urow[kPanelW], drow[kPanelW];
-    __shared__ T wabs[kPanelThreads / 32];
-    __shared__ int widx[kPanelThreads / 32];
-
-    if (status[kInfo] != 0) return;  // uniform over the cluster: written before this launch
-
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const int lo = rank * R;
-    const int hi = min(m, lo + R);
-    const int nr = max(0, hi - lo);
-
-    for (int e = tid; e < nr * w; e += kPanelThreads) {
-        const int r = e / w, c = e - r * w;
-        S[r * SS + c] = P[(int64_t)(lo + r) * ld + c];
-    }
-    __syncthreads();
-
-    // local argmax of column `col` over rows >= col, CTA-reduced, then published with its row
-    auto reduce_publish = [&](int col, int par) {
-        T ma = T(0);
-        int mi = -1;
-#pragma unroll
-        for (int k = 0; k < RPT; ++k) {
-            const int rl = tid + k * kPanelThreads;
-            const int r = lo + rl;
-            if (rl < nr && r >= col) {
-                const T a = fabs(S[rl * SS + col]);
-                if (a > ma) { ma = a; mi = r; }
-            }
-        }
-        warp_argmax(ma, mi);
-        if (lane == 0) { wabs[warp] = ma; widx[warp] = mi; }
-        __syncthreads();
-        if (warp == 0) {
-            T a = lane < kPanelThreads / 32 ? wabs[lane] : T(0);
-            int i = lane < kPanelThreads / 32 ? widx[lane] : -1;
-            warp_argmax(a, i);
-            if (lane == 0) { cand_abs[par] = a; cand_idx[par] = i; }
-            if (i >= 0 && lane < w) cand_row[par][lane] = S[(i - lo) * SS + lane];
-            if (col >= lo && col < hi && lane < w) diag_row[par][lane] = S[(col - lo) * SS + lane];
-        }
-    };
-
-    reduce_publish(0, 0);
-    cluster.sync();
-
-    bool singular = false;
-    const int ownj_stride = R;
-    for (int j = 0; j < w; ++j) {
-        const int par = j & 1;
-        const int ownj = j / ownj_stride;
-        // phase A: one round of remote loads (candidates, their rows, the diagonal row)
-        for (int e = tid; e < C * w + w + C; e += kPanelThreads) {
-            if (e < C * w) {
-                const int c = e / w, col = e - c * w;
-                allrows[c][col] = cluster.map_shared_rank(&cand_row[0][0], c)[par * kPanelW + col];
-            } else if (e < C * w + w) {
-                const int col = e - C * w;
-                drow[col] = cluster.map_shared_rank(&diag_row[0][0], ownj)[par * kPanelW + col];
-            } else {
-                const int c = e - C * w - w;
-                c_abs[c] = cluster.map_shared_rank(cand_abs, c)[par];
-                c_idx[c] = cluster.map_shared_rank(cand_idx, c)[par];
-            }
-        }
-        __syncthreads();
-        // phase B: every thread derives the same pivot
-        T babs = T(0);
-        int bidx = -1, bc = 0;
-        for (int c = 0; c < C; ++c)
-            if (piv_better(c_abs[c], c_idx[c], babs, bidx)) { babs = c_abs[c]; bidx = c_idx[c]; bc = c; }
-        if (bidx < 0 || !(babs > singular_threshold<T>())) {
-            singular = true;
-            if (rank == 0 && tid == 0) atomicExch(&status[kInfo], 1);
-            break;
-        }
-        const int p = bidx;
-        if (rank == 0 && tid == 0) ipiv[col_base + j] = row_base + p;
-        if (tid < w) {
-            const T u = allrows[bc][tid];
-            urow[tid] = u;
-            if (p != j && p >= lo && p < hi) S[(p - lo) * SS + tid] = drow[tid];
-            if (j >= lo && j < hi) S[(j - lo) * SS + tid] = u;
-        }
-        __syncthreads();
-        // phase C: scale the pivot column by 1/pivot, rank-1 update of the rest of the panel
-        const T rinv = T(1) / urow[j];
-#pragma unroll
-        for (int k = 0; k < RPT; ++k) {
-            const int rl = tid + k * kPanelThreads;
-            const int r = lo + rl;
-            if (rl < nr && r > j) {
-                T* row = S + rl * SS;
-                const T l = row[j] * rinv + T(0);
-                row[j] = l;
-                for (int c = j + 1; c < w; ++c) row[c] = fma(-l, urow[c], row[c]);
-            }
-        }
-        __syncthreads();
-        if (j + 1 < w) reduce_publish(j + 1, par ^ 1);
-        cluster.sync();
-    }
-    if (singular) {
-        cluster.sync();  // nobody leaves while others may still read its shared memory
-        return;
-    }
-    for (int e = tid; e < nr * w; e += kPanelThreads) {
-        const int r = e / w, c = e - r * w;
-        P[(int64_t)(lo + r) * ld + c] = S[r * SS + c];
-    }
-}
+constexpr int kPanelW = 32;  // largest leaf width
 
 // ------------------------------------------------------------------------------------------
 // Row interchanges of one leaf, applied to every column outside the leaf's own columns and to
@@ -204,8 +66,9 @@ __global__ void __launch_bounds__(kSwapThreads)
         if (lane < w) src_main[lane] = c0 + lane;
         __syncwarp();
         int my_pos = -1, my_src = -1, n_extra = 0;
+        const int qv = lane < w ? ipiv[c0 + lane] : 0;  // one load per lane, not w dependent loads
         for (int j = 0; j < w; ++j) {
-            const int q = ipiv[c0 + j];
+            const int q = __shfl_sync(0xffffffffu, qv, j);
             if (q < c0 + w) {
                 if (lane == 0 && q != c0 + j) {
                     const int t = src_main[j];
@@ -271,55 +134,57 @@ __global__ void __launch_bounds__(kSwapThreads)
 }
 
 // ------------------------------------------------------------------------------------------
-// Small triangular solves (k <= 32) on a strip of columns: one thread per column, the column
-// in registers, the triangle in shared memory.  Lower: unit diagonal, ascending j as in
-// LUBacksup / the forward sweep of MatrixLUBackSubst.  Upper: ascending j then a true
-// division by the diagonal, as the backward sweep of MatrixLUBackSubst (:362-382).
+// Small triangular solves (k <= 32) on a strip of columns.  One warp handles 4 columns; lane i
+// holds row i of the triangle (registers) and x_i of each column; at step j the final x_j is
+// broadcast with a shuffle and every later row subtracts its multiple, so the dependent chain is
+// 32 shuffle+FMA steps.  Lower: unit diagonal, contributions in ascending j (LUBacksup and the
+// forward sweep of MatrixLUBackSubst).  Upper: x_j = (b_j - sum) / U[j][j] with a true division
+// (the backward sweep, LinAlgLU.pas:362-382), contributions in descending j.
 // ------------------------------------------------------------------------------------------
 constexpr int kTrsmThreads = 128;
+constexpr int kTrsmCpw = 4;  // columns per warp
 
 template <typename T>
 __global__ void __launch_bounds__(kTrsmThreads)
     trsm_small_kernel(const T* L, int64_t ldl, T* B, int64_t ldb, int k, int ncols, int upper,
                       const int32_t* status) {
-    __shared__ T Ts[kPanelW][kPanelW + 1];
-    if (status && status[kInfo] != 0) return;
-    for (int e = threadIdx.x; e < k * k; e += kTrsmThreads) {
-        const int i = e / k, j = e - i * k;
-        Ts[i][j] = L[(int64_t)i * ldl + j];
-    }
-    __syncthreads();
-    const int c = blockIdx.x * kTrsmThreads + threadIdx.x;
-    if (c >= ncols) return;
-    T x[kPanelW];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int c0 = (blockIdx.x * (kTrsmThreads / 32) + warp) * kTrsmCpw;
+    // all global loads first: the status word, this lane's row of the triangle, its x values
+    const int32_t st = status ? status[kInfo] : 0;
+    T lrow[kPanelW];
 #pragma unroll
-    for (int i = 0; i < kPanelW; ++i)
-        if (i < k) x[i] = B[(int64_t)i * ldb + c];
+    for (int j = 0; j < kPanelW; ++j) lrow[j] = (lane < k && j < k) ? L[(int64_t)lane * ldl + j] : T(0);
+    T x[kTrsmCpw];
+#pragma unroll
+    for (int q = 0; q < kTrsmCpw; ++q)
+        x[q] = (lane < k && c0 + q < ncols) ? B[(int64_t)lane * ldb + c0 + q] : T(0);
+    if (st != 0 || c0 >= ncols) return;
     if (!upper) {
 #pragma unroll
-        for (int i = 1; i < kPanelW; ++i) {
-            if (i < k) {
-                T s = x[i];
+        for (int j = 0; j < kPanelW - 1; ++j) {
+            if (j >= k) break;
 #pragma unroll
-                for (int j = 0; j < i; ++j) s = fma(-Ts[i][j], x[j], s);
-                x[i] = s;
+            for (int q = 0; q < kTrsmCpw; ++q) {
+                const T xj = __shfl_sync(0xffffffffu, x[q], j);
+                if (lane > j) x[q] = fma(-lrow[j], xj, x[q]);
             }
         }
     } else {
 #pragma unroll
-        for (int i = kPanelW - 1; i >= 0; --i) {
-            if (i < k) {
-                T s = x[i];
+        for (int j = kPanelW - 1; j >= 0; --j) {
+            if (j >= k) continue;
 #pragma unroll
-                for (int j = i + 1; j < kPanelW; ++j)
-                    if (j < k) s = fma(-Ts[i][j], x[j], s);
-                x[i] = s / Ts[i][i];
+            for (int q = 0; q < kTrsmCpw; ++q) {
+                if (lane == j) x[q] = x[q] / lrow[j];
+                const T xj = __shfl_sync(0xffffffffu, x[q], j);
+                if (lane < j) x[q] = fma(-lrow[j], xj, x[q]);
             }
         }
     }
 #pragma unroll
-    for (int i = 0; i < kPanelW; ++i)
-        if (i < k) B[(int64_t)i * ldb + c] = x[i];
+    for (int q = 0; q < kTrsmCpw; ++q)
+        if (lane < k && c0 + q < ncols) B[(int64_t)lane * ldb + c0 + q] = x[q];
 }
 
 __global__ void iota_kernel(int32_t* v, int64_t n) {
@@ -384,94 +249,6 @@ namespace {
 
 int64_t split_cols(int64_t w) { return round_up((w + 1) / 2, kPanelW); }
 
-struct PanelCfg {
-    int C;    // cluster size
-    int R;    // rows per CTA
-    int rpt;  // rows per thread
-    size_t smem;
-};
-
-template <typename T>
-int32_t panel_config(Ctx* ctx, int m, int w, PanelCfg* cfg) {
-    const int SS = w | 1;
-    const size_t budget = std::min<size_t>(ctx->smem_optin ? ctx->smem_optin : 232448, 232448) - 16 * 1024;
-    const int rmax_smem = (int)(budget / (SS * sizeof(T)));
-    for (int rpt = 1; rpt <= 4; rpt *= 2) {
-        const int rmax = std::min(rmax_smem, rpt * kPanelThreads);
-        const int C = (int)ceil_div(m, rmax);
-        if (C <= kMaxCluster) {
-            cfg->C = std::max(1, C);
-            cfg->R = (int)ceil_div(m, cfg->C);
-            cfg->rpt = rpt;
-            cfg->smem = (size_t)cfg->R * SS * sizeof(T);
-            return B2M_OK;
-        }
-    }
-    return fail(ctx, B2M_ERR_UNSUPPORTED, "panel of %d rows x %d columns does not fit one cluster", m, w);
-}
-
-template <typename T, int RPT>
-int32_t launch_panel_rpt(Ctx* ctx, cudaStream_t st, const PanelCfg& pc, T* P, int64_t ld, int m, int w, int row_base,
-                         int col_base, int32_t* ipiv) {
-    auto kern = panel_lu_kernel<T, RPT>;
-    static bool attr = false;
-    if (!attr) {
-        B2M_CU(ctx, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 232448 - 16 * 1024));
-        B2M_CU(ctx, cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
-        attr = true;
-    }
-    // a non-portable cluster size must be schedulable with this much shared memory per CTA
-    static int checked_c[kMaxCluster + 1] = {};
-    if (pc.C > 8 && checked_c[pc.C] == 0) {
-        cudaLaunchConfig_t occ = {};
-        occ.gridDim = dim3(pc.C, 1, 1);
-        occ.blockDim = dim3(kPanelThreads, 1, 1);
-        occ.dynamicSmemBytes = 232448 - 16 * 1024;
-        cudaLaunchAttribute oat[1];
-        oat[0].id = cudaLaunchAttributeClusterDimension;
-        oat[0].val.clusterDim.x = pc.C;
-        oat[0].val.clusterDim.y = 1;
-        oat[0].val.clusterDim.z = 1;
-        occ.attrs = oat;
-        occ.numAttrs = 1;
-        int clusters = 0;
-        B2M_CU(ctx, cudaOccupancyMaxActiveClusters(&clusters, kern, &occ));
-        checked_c[pc.C] = clusters > 0 ? 1 : -1;
-    }
-    if (pc.C > 8 && checked_c[pc.C] < 0)
-        return fail(ctx, B2M_ERR_UNSUPPORTED, "panel cluster of %d CTAs cannot be scheduled", pc.C);
-    cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3(pc.C, 1, 1);
-    cfg.blockDim = dim3(kPanelThreads, 1, 1);
-    cfg.dynamicSmemBytes = pc.smem;
-    cfg.stream = st;
-    cudaLaunchAttribute at[1];
-    at[0].id = cudaLaunchAttributeClusterDimension;
-    at[0].val.clusterDim.x = pc.C;
-    at[0].val.clusterDim.y = 1;
-    at[0].val.clusterDim.z = 1;
-    cfg.attrs = at;
-    cfg.numAttrs = 1;
-    prof_begin(ctx, st, kClsPanel);
-    B2M_CU(ctx, cudaLaunchKernelEx(&cfg, kern, P, ld, m, w, pc.R, row_base, col_base, ipiv, ctx->d_status));
-    // algorithmic flops of an m x w partial-pivoting panel: sum_j 2(m-j-1)(w-j-1) + (m-j-1)
-    double fl = 0.0;
-    for (int j = 0; j < w; ++j) fl += 2.0 * (m - j - 1) * (w - j - 1) + (m - j - 1);
-    prof_end(ctx, st, kClsPanel, fl);
-    B2M_LAUNCHED(ctx);
-    return B2M_OK;
-}
-
-template <typename T>
-int32_t launch_panel(Ctx* ctx, cudaStream_t st, T* P, int64_t ld, int m, int w, int row_base, int col_base,
-                     int32_t* ipiv) {
-    PanelCfg pc;
-    B2M_TRY(panel_config<T>(ctx, m, w, &pc));
-    if (pc.rpt == 1) return launch_panel_rpt<T, 1>(ctx, st, pc, P, ld, m, w, row_base, col_base, ipiv);
-    if (pc.rpt == 2) return launch_panel_rpt<T, 2>(ctx, st, pc, P, ld, m, w, row_base, col_base, ipiv);
-    return launch_panel_rpt<T, 4>(ctx, st, pc, P, ld, m, w, row_base, col_base, ipiv);
-}
-
 template <typename T>
 int32_t launch_swaps(Ctx* ctx, cudaStream_t st, T* A, int64_t ld, int ncols, int c0, int w, const int32_t* ipiv,
                      int32_t* perm) {
@@ -488,7 +265,7 @@ template <typename T>
 int32_t launch_trsm_small(Ctx* ctx, cudaStream_t st, const T* L, int64_t ldl, T* B, int64_t ldb, int k, int ncols,
                           bool upper) {
     if (k <= 0 || ncols <= 0) return B2M_OK;
-    const int blocks = (int)ceil_div(ncols, kTrsmThreads);
+    const int blocks = (int)ceil_div(ncols, (kTrsmThreads / 32) * kTrsmCpw);
     prof_begin(ctx, st, kClsTrsm);
     trsm_small_kernel<T><<<blocks, kTrsmThreads, 0, st>>>(L, ldl, B, ldb, k, ncols, upper ? 1 : 0, ctx->d_status);
     prof_end(ctx, st, kClsTrsm, (double)k * k * ncols);
@@ -530,16 +307,16 @@ int32_t trsm_upper_rec(Ctx* ctx, cudaStream_t st, const TriSolve& t, int64_t r0,
     return trsm_upper_rec(ctx, st, t, r0, br0, k1);
 }
 
-// factor columns [c0, c0+width), rows [c0, n)
+// factor columns [c0, c0+width), rows [c0, n); leaves of at most `leaf` columns
 int32_t lu_rec(Ctx* ctx, cudaStream_t st, double* A, int64_t ld, int64_t n, int64_t c0, int64_t width,
-               int32_t* ipiv, int32_t* perm) {
-    if (width <= kPanelW) {
+               int32_t* ipiv, int32_t* perm, int64_t leaf) {
+    if (width <= leaf) {
         B2M_TRY(launch_panel<double>(ctx, st, A + c0 * ld + c0, ld, (int)(n - c0), (int)width, (int)c0, (int)c0,
                                      ipiv));
         return launch_swaps<double>(ctx, st, A, ld, (int)n, (int)c0, (int)width, ipiv, perm);
     }
-    const int64_t nleft = split_cols(width), nright = width - nleft;
-    B2M_TRY(lu_rec(ctx, st, A, ld, n, c0, nleft, ipiv, perm));
+    const int64_t nleft = round_up((width + 1) / 2, leaf), nright = width - nleft;
+    B2M_TRY(lu_rec(ctx, st, A, ld, n, c0, nleft, ipiv, perm, leaf));
     // A12 <- L11^{-1} A12
     TriSolve t{A, ld, n, A, ld, n, n, c0 + nleft, nright};
     B2M_TRY(trsm_lower_rec(ctx, st, t, c0, c0, nleft));
@@ -548,7 +325,7 @@ int32_t lu_rec(Ctx* ctx, cudaStream_t st, double* A, int64_t ld, int64_t n, int6
     DOperand a{A, ld, n, n, r1, c0, true};
     DOperand b{A, ld, n, n, c0, r1, false};
     B2M_TRY(dgemm_tiled(ctx, st, a, b, A + r1 * ld + r1, ld, n - r1, nright, nleft, B2M_DO_SUB, true));
-    return lu_rec(ctx, st, A, ld, n, r1, nright, ipiv, perm);
+    return lu_rec(ctx, st, A, ld, n, r1, nright, ipiv, perm, leaf);
 }
 
 }  // namespace
@@ -557,11 +334,16 @@ int32_t lu_factor_f64(Ctx* ctx, cudaStream_t st, double* A, int64_t ld, int64_t 
     if (n <= 0) return B2M_OK;
     if ((ld & 1) || !aligned16(A)) return fail(ctx, B2M_ERR_DIM, "lu_factor_f64: ld must be even, A 16-byte aligned");
     if (n > (1 << 30)) return fail(ctx, B2M_ERR_UNSUPPORTED, "n too large");
-    if (perm) {
-        iota_kernel<<<(unsigned)ceil_div(n, 256), 256, 0, st>>>(perm, n);
-        B2M_LAUNCHED(ctx);
-    }
-    return lu_rec(ctx, st, A, ld, n, 0, n, ipiv, perm);
+    const int64_t leaf = n <= panel_max_rows(true, 32) ? 32 : 16;
+    if (n > panel_max_rows(true, 16)) return fail(ctx, B2M_ERR_UNSUPPORTED, "FP64 LU supports n <= %d", panel_max_rows(true, 16));
+    const GraphKey key{1, A, ipiv, perm, ctx->d_status, ld, n, 0, 0};
+    return run_graph(ctx, st, key, [&](cudaStream_t s) -> int32_t {
+        if (perm) {
+            iota_kernel<<<(unsigned)ceil_div(n, 256), 256, 0, s>>>(perm, n);
+            B2M_LAUNCHED(ctx);
+        }
+        return lu_rec(ctx, s, A, ld, n, 0, n, ipiv, perm, leaf);
+    });
 }
 
 int32_t lu_solve_f64(Ctx* ctx, cudaStream_t st, const double* LU, int64_t ld, int64_t n, const int32_t* perm,
@@ -575,12 +357,15 @@ int32_t lu_solve_f64(Ctx* ctx, cudaStream_t st, const double* LU, int64_t ld, in
         B2M_TRY(ws_get(ctx, kWsE, (size_t)(n * ldb * sizeof(double)), &w));
         X = static_cast<double*>(w);
     }
-    B2M_CU(ctx, cudaMemcpy2DAsync(X, ldb * 8, B, ldb * 8, nrhs * 8, n, cudaMemcpyDeviceToDevice, st));
-    gather_rows_kernel<<<(unsigned)ceil_div(n * nrhs, 256), 256, 0, st>>>(B, ldb, X, ldb, perm, n, nrhs);
-    B2M_LAUNCHED(ctx);
-    TriSolve t{LU, ld, n, B, ldb, n, nrhs, 0, nrhs};
-    B2M_TRY(trsm_lower_rec(ctx, st, t, 0, 0, n));
-    return trsm_upper_rec(ctx, st, t, 0, 0, n);
+    const GraphKey key{2, LU, perm, B, X, ld, n, ldb, nrhs};
+    return run_graph(ctx, st, key, [&](cudaStream_t s) -> int32_t {
+        B2M_CU(ctx, cudaMemcpy2DAsync(X, ldb * 8, B, ldb * 8, nrhs * 8, n, cudaMemcpyDeviceToDevice, s));
+        gather_rows_kernel<<<(unsigned)ceil_div(n * nrhs, 256), 256, 0, s>>>(B, ldb, X, ldb, perm, n, nrhs);
+        B2M_LAUNCHED(ctx);
+        TriSolve t{LU, ld, n, B, ldb, n, nrhs, 0, nrhs};
+        B2M_TRY(trsm_lower_rec(ctx, s, t, 0, 0, n));
+        return trsm_upper_rec(ctx, s, t, 0, 0, n);
+    });
 }
 
 int32_t perm_from_ipiv(Ctx* ctx, cudaStream_t st, const int32_t* ipiv, int64_t n, int32_t* perm) {

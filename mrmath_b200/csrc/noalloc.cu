@@ -76,6 +76,7 @@ extern "C" int32_t b2m_dev_MatrixLinEQSolveNoAlloc(void* stream, const double* A
     c.stream = st;
     c.own_stream = st;
     c.d_status = words;
+    c.use_graphs = false;  // instantiating a graph may allocate; this path launches directly
     int v = 0;
     if (cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) == cudaSuccess) c.smem_optin = v;
     if (cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess) c.num_sms = v;

@@ -49,7 +49,7 @@ def test_inverse_det_singular_kats(ctx):
     assert L.MatrixDeterminant(s0, ctx=ctx) == 0.0
 
 
-@pytest.mark.parametrize("n", [1, 2, 3, 5, 7, 31, 32, 33, 47, 48, 49, 63, 64, 65, 100, 127, 129, 255, 257, 500, 1000])
+@pytest.mark.parametrize("n", [1, 2, 3, 5, 7, 31, 32, 33, 47, 48, 49, 63, 64, 65, 100, 127, 129, 255, 257, 500, 512, 513, 544, 1000, 1024, 1056, 2048])
 def test_lu_odd_sizes(ctx, n):
     r = oracle.Mersenne(seed=1000 + n)
     a = r.uniform(n, n) - 0.5
