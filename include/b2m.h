@@ -121,6 +121,30 @@ B2M_API int32_t b2m_dev_MatrixLinEQSolve(b2m_ctx* ctx, const double* A, int64_t 
 B2M_API int32_t b2m_dev_MatrixInverseInPlace(b2m_ctx* ctx, double* A, int64_t LineWidthA, int64_t width, int32_t* status);
 B2M_API int32_t b2m_dev_MatrixDeterminant(b2m_ctx* ctx, const double* A, int64_t LineWidthA, int64_t width, double* det);
 
+/* ------------------------------------------------------------------ mixed-precision solve
+ * No counterpart in the reference.  A X = B with an FP32 LU whose trailing and triangular-solve
+ * updates run on the tcgen05 tensor cores (mode B2M_MIXED_TF32: TF32; B2M_MIXED_3XTF32: hi/lo
+ * split, about FP32 accuracy), refined in FP64 (residual B - A X, update, normwise backward-error
+ * stopping test) until max_j ||b_j - A x_j||_inf / (||A||_inf ||x_j||_inf + ||b_j||_inf) <= tol
+ * (tol <= 0 means n * 2^-53; maxIter <= 0 means 30 for TF32, 10 for 3xTF32).  When refinement stalls, the plain FP64 LU solve runs instead and
+ * report->fell_back = 1.  Status as b2m_MatrixLinEQSolve. */
+#define B2M_MIXED_TF32   1
+#define B2M_MIXED_3XTF32 3
+typedef struct b2m_solve_report {
+    int32_t iterations;      /* refinement steps taken */
+    int32_t fell_back;       /* 1 if the plain FP64 solve produced X */
+    double  backward_error;  /* normwise backward error of the returned X (FP64 residual) */
+    double  refinement_backward_error;  /* the last refinement step's, before any fallback */
+} b2m_solve_report;
+B2M_API int32_t b2m_MatrixLinEQSolveMixed(b2m_ctx* ctx, const double* A, int64_t LineWidthA, int64_t width,
+                                          const double* B, int64_t LineWidthB, double* X, int64_t LineWidthX,
+                                          int64_t Width2, int32_t mode, int32_t maxIter, double tol,
+                                          b2m_solve_report* report);
+B2M_API int32_t b2m_dev_MatrixLinEQSolveMixed(b2m_ctx* ctx, const double* A, int64_t LineWidthA, int64_t width,
+                                              const double* B, int64_t LineWidthB, double* X, int64_t LineWidthX,
+                                              int64_t Width2, int32_t mode, int32_t maxIter, double tol,
+                                              b2m_solve_report* report);
+
 /* Allocation-free solve.  No counterpart in the reference: it exists for callers that may not
  * allocate device memory (a host program whose memory manager owns all device allocations, code
  * running inside a stream capture, a real-time loop with a fixed budget).  Same arguments and

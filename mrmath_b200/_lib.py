@@ -17,6 +17,13 @@ i32, i64, dbl, vp = C.c_int32, C.c_int64, C.c_double, C.c_void_p
 OK, SINGULAR = 0, 1
 ERR_DIM, ERR_CUDA, ERR_ALLOC, ERR_TIMEOUT, ERR_ARG, ERR_NOCONV, ERR_UNSUPPORTED = -1, -2, -3, -4, -5, -6, -7
 DO_NONE, DO_ADD, DO_SUB = 0, 1, 2
+MIXED_TF32, MIXED_3XTF32 = 1, 3
+
+
+class SolveReport(C.Structure):
+    """b2m_solve_report"""
+    _fields_ = [("iterations", C.c_int32), ("fell_back", C.c_int32), ("backward_error", C.c_double),
+                ("refinement_backward_error", C.c_double)]
 
 # name -> (restype, argtypes); pointers are passed as integers (c_void_p) so that numpy
 # arrays (host) and torch tensors (device) use the same signatures.
@@ -46,6 +53,8 @@ SIGNATURES: dict[str, tuple] = {
     "b2m_dev_MatrixInverseInPlace": (i32, [vp, vp, i64, i64, vp]),
     "b2m_dev_MatrixDeterminant": (i32, [vp, vp, i64, i64, vp]),
     "b2m_dev_MatrixLinEQSolveNoAlloc": (i32, [vp, vp, i64, i64, vp, i64, vp, i64, i64, vp]),
+    "b2m_MatrixLinEQSolveMixed": (i32, [vp, vp, i64, i64, vp, i64, vp, i64, i64, i32, i32, dbl, vp]),
+    "b2m_dev_MatrixLinEQSolveMixed": (i32, [vp, vp, i64, i64, vp, i64, vp, i64, i64, i32, i32, dbl, vp]),
 }
 
 

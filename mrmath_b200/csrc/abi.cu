@@ -5,6 +5,7 @@
 // the operands into library-owned device buffers whose row stride is padded for TMA, run the
 // device path on the context stream, copy the results back and return the reference's result
 // code.  Device-buffer calls (b2m_dev_*) run asynchronously on the context stream.
+#include <cmath>
 #include <cstring>
 
 #include "common.cuh"
@@ -481,4 +482,93 @@ extern "C" int32_t b2m_dev_MatrixDeterminant(b2m_ctx* h, const double* A, int64_
     B2M_TRY(reset_status(ctx));
     B2M_TRY(lu_factor_f64(ctx, ctx->stream, (double*)pa, ld, n, (int32_t*)pp, (int32_t*)pp + n));
     return lu_determinant(ctx, ctx->stream, (double*)pa, ld, n, (int32_t*)pp, det);
+}
+
+// ======================================================================================= mixed precision
+namespace {
+int32_t mixed_common(Ctx* ctx, const double* A, int64_t lda, int64_t n, const double* B, int64_t ldb, double* X,
+                     int64_t ldx, int64_t nrhs, int32_t mode, int32_t maxIter, double tol, b2m_solve_report* report) {
+    MixedReport rep{};
+    const double t = tol > 0 ? tol : (double)n * std::ldexp(1.0, -53);
+    const int defit = mode == B2M_MIXED_TF32 ? 30 : 10;  // TF32 contracts ~10x per step, 3xTF32 ~1e3x
+    const int32_t st = solve_mixed(ctx, ctx->stream, A, lda, n, B, ldb, X, ldx, nrhs, mode,
+                                   maxIter > 0 ? maxIter : defit, t, &rep);
+    if (report) {
+        report->iterations = rep.iterations;
+        report->fell_back = rep.fell_back;
+        report->backward_error = rep.backward_error;
+        report->refinement_backward_error = rep.ir_backward_error;
+    }
+    return st;
+}
+}  // namespace
+
+extern "C" int32_t b2m_dev_MatrixLinEQSolveMixed(b2m_ctx* h, const double* A, int64_t LineWidthA, int64_t width,
+                                                 const double* B, int64_t LineWidthB, double* X, int64_t LineWidthX,
+                                                 int64_t Width2, int32_t mode, int32_t maxIter, double tol,
+                                                 b2m_solve_report* report) {
+    Ctx* ctx = as_ctx(h);
+    if (!ctx) return B2M_ERR_ARG;
+    std::lock_guard<std::mutex> lk(ctx->mtx);
+    if (!A || !B || !X) return fail(ctx, B2M_ERR_ARG, "null pointer");
+    if (width <= 0 || Width2 <= 0 || !lw_ok(LineWidthA, width) || !lw_ok(LineWidthB, Width2) ||
+        !lw_ok(LineWidthX, Width2))
+        return fail(ctx, B2M_ERR_DIM, "Dimension error");
+    const int64_t n = width;
+    const double* dA = A;
+    int64_t lda = LineWidthA / 8;
+    if (!aligned16(A) || (LineWidthA & 15)) {
+        void* p;
+        lda = padded_ld(n);
+        B2M_TRY(ws_get(ctx, kWsMatA, (size_t)(n * lda * 8), &p));
+        B2M_TRY(copy_matrix(ctx, ctx->stream, (double*)p, lda * 8, A, LineWidthA, n, n));
+        dA = (const double*)p;
+    }
+    const double* dB = B;
+    int64_t ldb = LineWidthB / 8;
+    if (!aligned16(B) || (LineWidthB & 15)) {
+        void* p;
+        ldb = padded_ld(Width2);
+        B2M_TRY(ws_get(ctx, kWsMatB, (size_t)(n * ldb * 8), &p));
+        B2M_TRY(copy_matrix(ctx, ctx->stream, (double*)p, ldb * 8, B, LineWidthB, n, Width2));
+        dB = (const double*)p;
+    }
+    double* dX = X;
+    int64_t ldx = LineWidthX / 8;
+    const bool xdirect = aligned16(X) && (LineWidthX & 15) == 0;
+    if (!xdirect) {
+        void* p;
+        ldx = padded_ld(Width2);
+        B2M_TRY(ws_get(ctx, kWsG, (size_t)(n * ldx * 8), &p));
+        dX = (double*)p;
+    }
+    const int32_t st = mixed_common(ctx, dA, lda, n, dB, ldb, dX, ldx, Width2, mode, maxIter, tol, report);
+    if (st == B2M_OK && !xdirect) B2M_TRY(copy_matrix(ctx, ctx->stream, X, LineWidthX, dX, ldx * 8, n, Width2));
+    return st;
+}
+
+extern "C" int32_t b2m_MatrixLinEQSolveMixed(b2m_ctx* h, const double* A, int64_t LineWidthA, int64_t width,
+                                             const double* B, int64_t LineWidthB, double* X, int64_t LineWidthX,
+                                             int64_t Width2, int32_t mode, int32_t maxIter, double tol,
+                                             b2m_solve_report* report) {
+    Ctx* ctx = as_ctx(h);
+    if (!ctx) return B2M_ERR_ARG;
+    std::lock_guard<std::mutex> lk(ctx->mtx);
+    if (!A || !B || !X) return fail(ctx, B2M_ERR_ARG, "null pointer");
+    if (width <= 0 || Width2 <= 0 || !lw_ok(LineWidthA, width) || !lw_ok(LineWidthB, Width2) ||
+        !lw_ok(LineWidthX, Width2))
+        return fail(ctx, B2M_ERR_DIM, "Dimension error");
+    cudaSetDevice(ctx->device);
+    const int64_t n = width, lda = padded_ld(n), ldb = padded_ld(Width2);
+    void *pa, *pb, *pxx;
+    B2M_TRY(ws_get(ctx, kWsMatA, (size_t)(n * lda * 8), &pa));
+    B2M_TRY(ws_get(ctx, kWsMatB, (size_t)(n * ldb * 8), &pb));
+    B2M_TRY(ws_get(ctx, kWsG, (size_t)(n * ldb * 8), &pxx));
+    B2M_TRY(upload(ctx, (double*)pa, lda, A, LineWidthA, n, n));
+    B2M_TRY(upload(ctx, (double*)pb, ldb, B, LineWidthB, n, Width2));
+    const int32_t st = mixed_common(ctx, (double*)pa, lda, n, (double*)pb, ldb, (double*)pxx, ldb, Width2, mode,
+                                    maxIter, tol, report);
+    if (st != B2M_OK) return st;
+    B2M_TRY(download(ctx, X, LineWidthX, (double*)pxx, ldb, n, Width2));
+    return finish(ctx);
 }

@@ -39,6 +39,8 @@ enum WsSlot : int {
     kWsSmall,      // norms, small vectors
     kWsE,
     kWsF,
+    kWsG,          // the mixed solve's X when the caller's buffer cannot be used directly
+    kWsH,
     kNumWs
 };
 

@@ -62,3 +62,48 @@ int32_t set_diagonal(Ctx* ctx, cudaStream_t st, double* X, int64_t ldx, int64_t 
 int32_t copy_if_ok(Ctx* ctx, cudaStream_t st, double* dst, int64_t ldd, const double* src, int64_t lds, int64_t rows,
                    int64_t cols);
 }  // namespace b2m
+
+namespace b2m {
+// K-major FP32 operand for the tensor-core GEMM: rows x cols map of (base, ld) starting at (r0, c0)
+struct FOperand {
+    const float* base;
+    int64_t ld;
+    int64_t rows, cols;
+    int64_t r0, c0;
+};
+// C(M x N) op= A(M x K) * Bt(N x K)^T on tcgen05 (split 1 = TF32, 3 = 3xTF32 with lo operands
+// laid out exactly like the hi ones).
+int32_t sgemm_tc(Ctx* ctx, cudaStream_t st, const FOperand& Ah, const float* Al_base, const FOperand& Bh,
+                 const float* Bl_base, float* C, int64_t ldc, int64_t M, int64_t N, int64_t K, int op, int split,
+                 bool check_info);
+// hi / lo split for 3xTF32 (lo may be null: plain copy), optionally transposing.
+int32_t tf32_split(Ctx* ctx, cudaStream_t st, const float* src, int64_t lds, int64_t rows, int64_t cols, float* hi,
+                   float* lo, int64_t ldo, bool transpose);
+
+template <typename T>
+int32_t launch_swaps(Ctx* ctx, cudaStream_t st, T* A, int64_t ld, int ncols, int c0, int w, const int32_t* ipiv,
+                     int32_t* perm);
+template <typename T>
+int32_t launch_trsm_small(Ctx* ctx, cudaStream_t st, const T* L, int64_t ldl, T* B, int64_t ldb, int k, int ncols,
+                          bool upper);
+}  // namespace b2m
+
+namespace b2m {
+struct MixedReport {
+    int32_t iterations;
+    int32_t fell_back;
+    double backward_error;
+    double ir_backward_error;
+};
+int32_t lu_factor_f32(Ctx* ctx, cudaStream_t st, float* A, int64_t ld, int64_t n, int32_t* ipiv, int32_t* perm,
+                      int mode, float* scratch, int64_t scratch_cap);
+int32_t lu_solve_f32(Ctx* ctx, cudaStream_t st, const float* LU, int64_t ld, int64_t n, const int32_t* perm, float* B,
+                     int64_t ldb, int64_t nrhs, float* tmp, int mode, float* scratch, int64_t scratch_cap);
+// A X = B with an FP32 tensor-core factorisation and FP64 refinement to normwise backward error
+// <= tol; falls back to the plain FP64 solve when refinement stalls.  Device operands, even strides.
+int32_t solve_mixed(Ctx* ctx, cudaStream_t st, const double* A, int64_t lda, int64_t n, const double* B, int64_t ldb,
+                    double* X, int64_t ldx, int64_t nrhs, int mode, int max_iter, double tol, MixedReport* rep);
+// plain FP64 LU solve of device operands (factors in a workspace); fills rep->backward_error
+int32_t solve_plain_f64(Ctx* ctx, cudaStream_t st, const double* A, int64_t lda, int64_t n, const double* B,
+                        int64_t ldb, double* X, int64_t ldx, int64_t nrhs, MixedReport* rep);
+}  // namespace b2m

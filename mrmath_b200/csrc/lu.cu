@@ -250,7 +250,7 @@ namespace {
 int64_t split_cols(int64_t w) { return round_up((w + 1) / 2, kPanelW); }
 
 template <typename T>
-int32_t launch_swaps(Ctx* ctx, cudaStream_t st, T* A, int64_t ld, int ncols, int c0, int w, const int32_t* ipiv,
+int32_t launch_swaps_impl(Ctx* ctx, cudaStream_t st, T* A, int64_t ld, int ncols, int c0, int w, const int32_t* ipiv,
                      int32_t* perm) {
     const int other = ncols - w;
     const int blocks = std::max(1, (int)ceil_div(other, kSwapThreads));
@@ -262,7 +262,7 @@ int32_t launch_swaps(Ctx* ctx, cudaStream_t st, T* A, int64_t ld, int ncols, int
 }
 
 template <typename T>
-int32_t launch_trsm_small(Ctx* ctx, cudaStream_t st, const T* L, int64_t ldl, T* B, int64_t ldb, int k, int ncols,
+int32_t launch_trsm_small_impl(Ctx* ctx, cudaStream_t st, const T* L, int64_t ldl, T* B, int64_t ldb, int k, int ncols,
                           bool upper) {
     if (k <= 0 || ncols <= 0) return B2M_OK;
     const int blocks = (int)ceil_div(ncols, (kTrsmThreads / 32) * kTrsmCpw);
@@ -285,7 +285,7 @@ struct TriSolve {
 
 int32_t trsm_lower_rec(Ctx* ctx, cudaStream_t st, const TriSolve& t, int64_t r0, int64_t br0, int64_t k) {
     if (k <= kPanelW)
-        return launch_trsm_small<double>(ctx, st, t.A + r0 * t.lda + r0, t.lda, t.B + br0 * t.ldb + t.bc0, t.ldb,
+        return launch_trsm_small_impl<double>(ctx, st, t.A + r0 * t.lda + r0, t.lda, t.B + br0 * t.ldb + t.bc0, t.ldb,
                                          (int)k, (int)t.ncols, false);
     const int64_t k1 = split_cols(k), k2 = k - k1;
     B2M_TRY(trsm_lower_rec(ctx, st, t, r0, br0, k1));
@@ -297,7 +297,7 @@ int32_t trsm_lower_rec(Ctx* ctx, cudaStream_t st, const TriSolve& t, int64_t r0,
 
 int32_t trsm_upper_rec(Ctx* ctx, cudaStream_t st, const TriSolve& t, int64_t r0, int64_t br0, int64_t k) {
     if (k <= kPanelW)
-        return launch_trsm_small<double>(ctx, st, t.A + r0 * t.lda + r0, t.lda, t.B + br0 * t.ldb + t.bc0, t.ldb,
+        return launch_trsm_small_impl<double>(ctx, st, t.A + r0 * t.lda + r0, t.lda, t.B + br0 * t.ldb + t.bc0, t.ldb,
                                          (int)k, (int)t.ncols, true);
     const int64_t k1 = split_cols(k), k2 = k - k1;
     B2M_TRY(trsm_upper_rec(ctx, st, t, r0 + k1, br0 + k1, k2));
@@ -313,7 +313,7 @@ int32_t lu_rec(Ctx* ctx, cudaStream_t st, double* A, int64_t ld, int64_t n, int6
     if (width <= leaf) {
         B2M_TRY(launch_panel<double>(ctx, st, A + c0 * ld + c0, ld, (int)(n - c0), (int)width, (int)c0, (int)c0,
                                      ipiv));
-        return launch_swaps<double>(ctx, st, A, ld, (int)n, (int)c0, (int)width, ipiv, perm);
+        return launch_swaps_impl<double>(ctx, st, A, ld, (int)n, (int)c0, (int)width, ipiv, perm);
     }
     const int64_t nleft = round_up((width + 1) / 2, leaf), nright = width - nleft;
     B2M_TRY(lu_rec(ctx, st, A, ld, n, c0, nleft, ipiv, perm, leaf));
@@ -329,6 +329,22 @@ int32_t lu_rec(Ctx* ctx, cudaStream_t st, double* A, int64_t ld, int64_t n, int6
 }
 
 }  // namespace
+
+template <typename T>
+int32_t launch_swaps(Ctx* ctx, cudaStream_t st, T* A, int64_t ld, int ncols, int c0, int w, const int32_t* ipiv,
+                     int32_t* perm) {
+    return launch_swaps_impl<T>(ctx, st, A, ld, ncols, c0, w, ipiv, perm);
+}
+template <typename T>
+int32_t launch_trsm_small(Ctx* ctx, cudaStream_t st, const T* L, int64_t ldl, T* B, int64_t ldb, int k, int ncols,
+                          bool upper) {
+    return launch_trsm_small_impl<T>(ctx, st, L, ldl, B, ldb, k, ncols, upper);
+}
+template int32_t launch_swaps<float>(Ctx*, cudaStream_t, float*, int64_t, int, int, int, const int32_t*, int32_t*);
+template int32_t launch_swaps<double>(Ctx*, cudaStream_t, double*, int64_t, int, int, int, const int32_t*, int32_t*);
+template int32_t launch_trsm_small<float>(Ctx*, cudaStream_t, const float*, int64_t, float*, int64_t, int, int, bool);
+template int32_t launch_trsm_small<double>(Ctx*, cudaStream_t, const double*, int64_t, double*, int64_t, int, int,
+                                           bool);
 
 int32_t lu_factor_f64(Ctx* ctx, cudaStream_t st, double* A, int64_t ld, int64_t n, int32_t* ipiv, int32_t* perm) {
     if (n <= 0) return B2M_OK;

@@ -15,7 +15,7 @@ import ctypes as C
 
 import numpy as np
 
-from ._lib import DO_ADD, DO_NONE, DO_SUB, OK, SINGULAR, Context
+from ._lib import DO_ADD, DO_NONE, DO_SUB, MIXED_3XTF32, MIXED_TF32, OK, SINGULAR, Context, SolveReport
 
 __all__ = [
     "default_context", "MatrixMult", "MatrixMultEx", "MatrixMultT1Ex", "MatrixMultT2Ex", "MatrixLUDecompInPlace",
@@ -118,6 +118,24 @@ def MatrixLinEQSolve(A: np.ndarray, B: np.ndarray, num_refinements: int = 0, X: 
     return st, X
 
 
+def _rep(rep) -> dict:
+    return {"iterations": rep.iterations, "fell_back": rep.fell_back, "backward_error": rep.backward_error,
+            "refinement_backward_error": rep.refinement_backward_error}
+
+
+def MatrixLinEQSolveMixed(A: np.ndarray, B: np.ndarray, mode: int = MIXED_3XTF32, max_iter: int = 0,
+                          tol: float = 0.0, X: np.ndarray | None = None, ctx: Context | None = None):
+    """FP32 tensor-core factorisation + FP64 refinement; returns (status, X, report)."""
+    n = A.shape[1]
+    k = B.shape[1]
+    if X is None:
+        X = np.zeros((n, k))
+    rep = SolveReport()
+    st = _ctx_of(ctx).call("b2m_MatrixLinEQSolveMixed", _ptr(A), _lw(A), n, _ptr(B), _lw(B), _ptr(X), _lw(X), k,
+                           mode, max_iter, tol, C.addressof(rep), allow=(OK, SINGULAR))
+    return st, X, _rep(rep)
+
+
 # ----------------------------------------------------------------------------- device (torch) twins
 def _tptr(t) -> int:
     return t.data_ptr()
@@ -173,3 +191,15 @@ def dev_MatrixDeterminant(A, det, ctx=None):
     c = _ctx_of(ctx)
     _bind_stream(c, A)
     c.call("b2m_dev_MatrixDeterminant", _tptr(A), _tlw(A), A.shape[1], _tptr(det))
+
+
+def dev_MatrixLinEQSolveMixed(A, B, X, mode=MIXED_3XTF32, max_iter=0, tol=0.0, status=None, ctx=None):
+    """Device twin of MatrixLinEQSolveMixed; returns (status, report)."""
+    c = _ctx_of(ctx)
+    _bind_stream(c, A)
+    rep = SolveReport()
+    st = c.call("b2m_dev_MatrixLinEQSolveMixed", _tptr(A), _tlw(A), A.shape[1], _tptr(B), _tlw(B), _tptr(X), _tlw(X),
+                B.shape[1], mode, max_iter, tol, C.addressof(rep), allow=(OK, SINGULAR))
+    if status is not None:
+        status.fill_(st)
+    return st, _rep(rep)
