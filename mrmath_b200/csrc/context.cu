@@ -22,8 +22,12 @@ int32_t ws_get(Ctx* ctx, int slot, size_t bytes, void** out) {
     bytes = (size_t)round_up((int64_t)std::max<size_t>(bytes, 256), 256);
     if (ctx->ws_bytes[slot] < bytes) {
         if (ctx->ws[slot]) {
-            // the buffer may still be in use by queued work on this stream
+            // the buffer may still be in use by queued work, and captured graphs hold its address:
+            // drain both streams and drop every cached graph before freeing it
             B2M_CU(ctx, cudaStreamSynchronize(ctx->stream));
+            if (ctx->own_stream) B2M_CU(ctx, cudaStreamSynchronize(ctx->own_stream));
+            for (auto& g : ctx->graphs) cudaGraphExecDestroy(g.second.exec);
+            ctx->graphs.clear();
             B2M_CU(ctx, cudaFree(ctx->ws[slot]));
             ctx->ws[slot] = nullptr;
             ctx->ws_bytes[slot] = 0;

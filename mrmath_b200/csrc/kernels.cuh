@@ -95,10 +95,27 @@ struct MixedReport {
     double backward_error;
     double ir_backward_error;
 };
-int32_t lu_factor_f32(Ctx* ctx, cudaStream_t st, float* A, int64_t ld, int64_t n, int32_t* ipiv, int32_t* perm,
-                      int mode, float* scratch, int64_t scratch_cap);
-int32_t lu_solve_f32(Ctx* ctx, cudaStream_t st, const float* LU, int64_t ld, int64_t n, const int32_t* perm, float* B,
-                     int64_t ldb, int64_t nrhs, float* tmp, int mode, float* scratch, int64_t scratch_cap);
+// FP32 factorisation of the mixed solve (lu_f32.cu): tournament-pivoting panels, tcgen05
+// trailing updates (mode 1 TF32, 3 3xTF32), and the inverses of the kTrsvNB-row diagonal blocks
+// of L and U used by the refinement's blocked triangular solves.
+constexpr int kTrsvNB = 128;
+struct F32Scratch {
+    int* cand;
+    unsigned* counters;
+    size_t counters_bytes;
+    float* top;
+    float* mvals;
+    float* wmat;
+    int* moves;
+    float *bth, *btl, *ah, *al;
+    float *linv, *uinv;
+};
+size_t f32_scratch_bytes(int64_t n);
+F32Scratch f32_scratch_carve(void* base, int64_t n);
+// A (n x n, row stride ld a multiple of 32, 128-byte aligned) is factored in place as P A = L U;
+// perm[i] = original row of factor row i.  status[kInfo] != 0 on a tiny pivot.
+int32_t lu_factor_f32(Ctx* ctx, cudaStream_t st, float* A, int64_t ld, int64_t n, int32_t* perm, int mode,
+                      const F32Scratch& s);
 // A X = B with an FP32 tensor-core factorisation and FP64 refinement to normwise backward error
 // <= tol; falls back to the plain FP64 solve when refinement stalls.  Device operands, even strides.
 int32_t solve_mixed(Ctx* ctx, cudaStream_t st, const double* A, int64_t lda, int64_t n, const double* B, int64_t ldb,

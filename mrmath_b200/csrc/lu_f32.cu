@@ -1,0 +1,705 @@
+// lu_f32.cu -- FP32 LU factorisation for the mixed-precision solve.
+//
+// This factorisation only has to be good enough for iterative refinement to converge (the answer
+// is judged by its FP64 backward error), so it is free to pick its pivots differently from the
+// reference's FP64 LU.  It uses tournament pivoting (communication-avoiding LU, Grigori, Demmel
+// and Xiang 2011), which removes the per-column grid-wide reduction that bounds a classic panel:
+//
+//   * outer panels of kNB = 256 columns, blocked right-looking: after a panel is factored, the
+//     rows above the trailing matrix are solved with the panel's unit-lower block (U12) and the
+//     trailing matrix is updated by one tcgen05 GEMM (TF32 or 3xTF32, K = 256);
+//   * inside a panel, 32-column leaves.  tslu_select_kernel runs Gaussian elimination with
+//     partial pivoting on 512-row chunks in parallel; each chunk nominates 32 candidate rows, and
+//     the last CTA of every group of 16 chunks (found with an atomic counter, no spinning) runs
+//     the same elimination on the stacked candidates' original rows, up to a single root.  The
+//     root's pivots are the leaf's pivots and its eliminated rows are the leaf's L11\U11;
+//   * tslu_apply_kernel moves the chosen rows into place (a side buffer holds the rows whose
+//     slots get overwritten, so the move is race free), forms L21 = A21 U11^-1 and applies the
+//     leaf's rank-32 update to the rest of the panel; extra CTAs apply the same row moves to all
+//     columns outside the panel.
+//
+// The permutation is tracked in `perm` (row i of the factors is original row perm[i]); no LAPACK
+// style interchange vector is produced because nothing downstream of the mixed solve needs one.
+// A pivot whose magnitude is <= 10/FLT_MAX at the root sets status[kInfo] (the driver then
+// falls back to the plain FP64 factorisation).
+#include <cfloat>
+
+#include "common.cuh"
+#include "kernels.cuh"
+
+namespace b2m {
+namespace {
+
+constexpr int kTsThreads = 256;
+constexpr int kTsRpt = 2;                         // rows per thread in the elimination
+constexpr int kTsRows = kTsThreads * kTsRpt;      // rows per chunk / per merge
+constexpr int kTsFan = kTsRows / 32;              // candidate sets merged per tree node (16)
+constexpr int kTsLevels = 4;
+constexpr int kTsMaxCand = 2048;                  // nodes per level (rows <= 1M)
+constexpr int kNB = 256;                          // outer panel width
+constexpr int kApRows = 32;                       // rows per apply CTA
+
+struct TsArgs {
+    const float* A;
+    int64_t ld;
+    int n, lc0, w, oc0, pw;
+    int* cand;            // [kTsLevels][kTsMaxCand][32] candidate row ids
+    unsigned* counters;   // [kTsLevels][kTsMaxCand] arrival counters (zero between launches)
+    float* top;           // [32][kNB]: final content of the leaf's top rows over the outer panel
+    float* mvals;         // [32][kNB]: original content of the top rows that move below the leaf
+    float* wmat;          // [32][kNB]: U11^-1 in the leaf's columns, U11^-1 U12 right of them
+    int* moves;           // [0] moves, [1] moves below the top block, [2..66) dst, [66..130) src
+    int32_t* status;
+};
+
+// reciprocal: hardware approximation refined by one Newton step (a correctly rounded division
+// costs ~300 cycles of dependent latency, and this factorisation only has to feed refinement)
+__device__ __forceinline__ float rcp_nr(float x) {
+    float r;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r * fmaf(-x, r, 2.0f);
+}
+
+// Gaussian elimination with partial pivoting of up to 512 stacked rows (thread t holds stack rows
+// t and t + 256 in registers) over w <= 32 columns.  Chooses w pivot rows (largest magnitude);
+// s_win[j] = row id of pivot j (-1 if the stack ran out), s_lu[j][*] = pivot row j at the time it
+// was chosen, i.e. row j of L\U.
+//
+// The column loop is a runtime loop over steps of 4 columns (compact code: a fully unrolled
+// elimination does not fit the instruction cache).  Register indices stay compile-time because
+// the rows rotate left by 4 after each step: at step `it`, v[r][k] holds column 4 it + k for
+// k < 32 - 4 it and the multiplier of column q sits at v[r][32 - 4 it + q].  Those multiplier
+// quads are skipped by the elimination.
+//
+// One barrier per column: every warp's best lane publishes its candidate row (and key) into a
+// double-buffered slot before the barrier; afterwards all threads pick the winning warp with a
+// warp reduction over the slots and read its row directly.  A pivot's full row (with its
+// multipliers) is written to s_lu by its owner once, after the last column.
+struct GeppSmem {
+    float4 cand[2][kTsThreads / 32][8];  // candidate rows, by column parity and warp
+    unsigned key[2][kTsThreads / 32];
+    unsigned slot[2][kTsThreads / 32];
+};
+
+__device__ __forceinline__ void block_gepp(float (&v)[kTsRpt][32], const int (&rid)[kTsRpt], int w, int* s_win,
+                                           float (*s_lu)[33], GeppSmem& g) {
+    const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+    bool live[kTsRpt];
+    int my_j[kTsRpt];
+#pragma unroll
+    for (int r = 0; r < kTsRpt; ++r) { live[r] = rid[r] >= 0; my_j[r] = -1; }
+    if (t < 32) s_win[t] = -1;
+    const int nit = (w + 3) >> 2;
+#pragma unroll 1
+    for (int it = 0; it < nit; ++it) {
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+            const int j = 4 * it + c;
+            if (j >= w) break;  // uniform
+            const int b = j & 1;
+            unsigned key = 0u;
+            int rbest = 0;
+#pragma unroll
+            for (int r = 0; r < kTsRpt; ++r) {
+                const unsigned k = live[r] ? __float_as_uint(fabsf(v[r][c])) + 1u : 0u;
+                if (k > key) { key = k; rbest = r; }
+            }
+            const unsigned wk = __reduce_max_sync(0xffffffffu, key);
+            const unsigned bal = __ballot_sync(0xffffffffu, key == wk && key != 0u);
+            if (lane == (bal ? __ffs(bal) - 1 : 0)) {
+#pragma unroll
+                for (int r = 0; r < kTsRpt; ++r) {
+                    if (r == rbest) {
+#pragma unroll
+                        for (int q = 0; q < 8; ++q)
+                            if (q < 8 - it)
+                                g.cand[b][warp][q] = make_float4(v[r][4 * q], v[r][4 * q + 1], v[r][4 * q + 2], v[r][4 * q + 3]);
+                    }
+                }
+                g.key[b][warp] = wk;
+                g.slot[b][warp] = (unsigned)(rbest * kTsThreads + t);
+            }
+            __syncthreads();
+            // winning warp: largest key, lowest warp among equals
+            const unsigned kq = g.key[b][lane & (kTsThreads / 32 - 1)];
+            const unsigned pk = __reduce_max_sync(0xffffffffu, kq);
+            if (pk == 0u) continue;  // nothing left to choose from (uniform)
+            const int pwarp = __ffs(__ballot_sync(0xffffffffu, kq == pk)) - 1;
+            const unsigned ps = g.slot[b][pwarp];
+            const float4* prow = g.cand[b][pwarp];
+            const float4 f0 = prow[0];
+            const float p0[4] = {f0.x, f0.y, f0.z, f0.w};
+            const float rcp = pk > 1u ? rcp_nr(p0[c]) : 0.0f;  // a zero column eliminates nothing
+#pragma unroll
+            for (int r = 0; r < kTsRpt; ++r) {
+                if (ps == (unsigned)(r * kTsThreads + t)) {
+                    live[r] = false;
+                    my_j[r] = j;
+                    s_win[j] = rid[r];
+                }
+                if (live[r]) {
+                    const float l = v[r][c] * rcp;
+                    v[r][c] = l;
+#pragma unroll
+                    for (int e = c + 1; e < 4; ++e) v[r][e] = fmaf(-l, p0[e], v[r][e]);
+#pragma unroll
+                    for (int q = 1; q < 8; ++q) {
+                        if (q < 8 - it) {  // uniform: quads from 8 - it on hold multipliers
+                            const float4 f = prow[q];
+                            v[r][4 * q] = fmaf(-l, f.x, v[r][4 * q]);
+                            v[r][4 * q + 1] = fmaf(-l, f.y, v[r][4 * q + 1]);
+                            v[r][4 * q + 2] = fmaf(-l, f.z, v[r][4 * q + 2]);
+                            v[r][4 * q + 3] = fmaf(-l, f.w, v[r][4 * q + 3]);
+                        }
+                    }
+                }
+            }
+        }
+        // rotate left by 4: this step's multipliers go to the end
+#pragma unroll
+        for (int r = 0; r < kTsRpt; ++r) {
+            const float r0 = v[r][0], r1 = v[r][1], r2 = v[r][2], r3 = v[r][3];
+#pragma unroll
+            for (int k = 0; k < 28; ++k) v[r][k] = v[r][k + 4];
+            v[r][28] = r0; v[r][29] = r1; v[r][30] = r2; v[r][31] = r3;
+        }
+    }
+    // pivot rows: original column col now sits at register (col - 4 nit) mod 32
+#pragma unroll
+    for (int r = 0; r < kTsRpt; ++r) {
+        if (my_j[r] >= 0) {
+#pragma unroll
+            for (int k = 0; k < 32; ++k) s_lu[my_j[r]][(k + 4 * nit) & 31] = v[r][k];
+        }
+    }
+    __syncthreads();
+}
+
+// loads columns [c0, c0 + w) of row `row` (zeros past w); rows are 128-byte aligned
+__device__ __forceinline__ void load_leaf_row(const float* A, int64_t ld, int row, int c0, int w, float (&x)[32]) {
+    if (row < 0) {
+#pragma unroll
+        for (int k = 0; k < 32; ++k) x[k] = 0.f;
+        return;
+    }
+    const float4* p = reinterpret_cast<const float4*>(A + (int64_t)row * ld + c0);
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+        const float4 f = __ldg(p + q);
+        x[4 * q + 0] = f.x; x[4 * q + 1] = f.y; x[4 * q + 2] = f.z; x[4 * q + 3] = f.w;
+    }
+#pragma unroll
+    for (int k = 0; k < 32; ++k)
+        if (k >= w) x[k] = 0.f;
+}
+
+__global__ void __launch_bounds__(kTsThreads) tslu_select_kernel(TsArgs a) {
+    __shared__ __align__(16) GeppSmem s_g;
+    __shared__ int s_win[32];
+    __shared__ float s_lu[32][33];
+    __shared__ float s_rdiag[32];
+    __shared__ int s_last, s_bad;
+    __shared__ int s_flag[32], s_outpos[32], s_mdst[64], s_msrc[64], s_nm, s_nout;
+    if (a.status[kInfo] != 0) return;
+    const int t = threadIdx.x;
+    const int m = a.n - a.lc0;
+    float v[kTsRpt][32];
+    int rid[kTsRpt];
+#pragma unroll
+    for (int r = 0; r < kTsRpt; ++r) {
+        const int row = a.lc0 + blockIdx.x * kTsRows + r * kTsThreads + t;
+        rid[r] = row < a.n ? row : -1;
+        load_leaf_row(a.A, a.ld, rid[r], a.lc0, a.w, v[r]);
+    }
+    int node = blockIdx.x, count = (int)ceil_div(m, kTsRows), level = 0;
+    for (;;) {
+        block_gepp(v, rid, a.w, s_win, s_lu, s_g);
+        if (count == 1) break;
+        // publish this node's candidates; the last member of the group merges them
+        if (t < 32) a.cand[((int64_t)level * kTsMaxCand + node) * 32 + t] = s_win[t];
+        __threadfence();
+        __syncthreads();
+        const int parent = node / kTsFan;
+        const int members = min(kTsFan, count - parent * kTsFan);
+        if (t == 0) {
+            unsigned* ctr = a.counters + level * kTsMaxCand + parent;
+            const unsigned prev = atomicAdd(ctr, 1u);
+            s_last = prev == (unsigned)(members - 1);
+            if (s_last) *ctr = 0u;  // every member has arrived: ready for the next launch
+        }
+        __syncthreads();
+        if (!s_last) return;
+        __threadfence();
+#pragma unroll
+        for (int r = 0; r < kTsRpt; ++r) {
+            const int sidx = r * kTsThreads + t, mem = sidx >> 5;
+            rid[r] = mem < members
+                         ? __ldcg(a.cand + ((int64_t)level * kTsMaxCand + parent * kTsFan + mem) * 32 + (sidx & 31))
+                         : -1;
+        }
+#pragma unroll
+        for (int r = 0; r < kTsRpt; ++r) load_leaf_row(a.A, a.ld, rid[r], a.lc0, a.w, v[r]);
+        node = parent;
+        count = (int)ceil_div(count, kTsFan);
+        ++level;
+    }
+
+    // ---- root: pivots s_win[0..w), factors s_lu
+    const int lc0 = a.lc0, w = a.w;
+    if (t == 0) {
+        int bad = 0;
+        for (int j = 0; j < w; ++j)
+            if (s_win[j] < 0 || !(fabsf(s_lu[j][j]) > 10.0f / FLT_MAX)) { bad = lc0 + j + 1; break; }
+        s_bad = bad;
+        if (bad) a.status[kInfo] = bad;
+    }
+    if (t < 32) {
+        s_flag[t] = 0;
+        s_rdiag[t] = t < w ? rcp_nr(s_lu[t][t]) : 0.f;
+    }
+    __syncthreads();
+    if (s_bad) return;
+    // row moves: top slot lc0+j <- winner j; the displaced top rows fill the winners' old slots
+    if (t < 32) {
+        const int lane = t;
+        const int p = lane < w ? s_win[lane] : -1;
+        if (lane < w && p < lc0 + w) s_flag[p - lc0] = 1;
+        __syncwarp();
+        const bool disp = lane < w && !s_flag[lane];
+        const bool outw = lane < w && p >= lc0 + w;
+        const bool mtop = lane < w && p != lc0 + lane;
+        const unsigned bd = __ballot_sync(0xffffffffu, disp), bo = __ballot_sync(0xffffffffu, outw),
+                       bt = __ballot_sync(0xffffffffu, mtop);
+        const unsigned below = (1u << lane) - 1u;
+        if (outw) s_outpos[__popc(bo & below)] = p;
+        __syncwarp();
+        const int ntop = __popc(bt);
+        if (mtop) {
+            const int k = __popc(bt & below);
+            s_mdst[k] = lc0 + lane;
+            s_msrc[k] = p;
+        }
+        if (disp) {
+            const int k = __popc(bd & below);
+            s_mdst[ntop + k] = s_outpos[k];
+            s_msrc[ntop + k] = lc0 + lane;
+        }
+        if (lane == 0) { s_nm = ntop + __popc(bd); s_nout = __popc(bd); }
+    }
+    __syncthreads();
+    const int nm = s_nm, nout = s_nout;
+    if (t == 0) { a.moves[0] = nm; a.moves[1] = nout; }
+    if (t < nm) { a.moves[2 + t] = s_mdst[t]; a.moves[66 + t] = s_msrc[t]; }
+    // thread t owns column c = t of the outer panel.  It writes the top rows' final content
+    // (original rows left of the leaf, L11\U11 inside it, U12 = L11^-1 * original rows right of
+    // it), the column of M = [U11^-1 | U11^-1 U12] that the apply kernel multiplies by, and the
+    // original content of the rows that leave the top block.  All loads are issued before use.
+    const int lo = lc0 - a.oc0, pw = a.pw, c = t;
+    if (c < pw) {
+        const bool in_leaf = c >= lo && c < lo + w;
+        const float* col = a.A + a.oc0 + c;
+        float x[32], y[32];
+#pragma unroll
+        for (int j = 0; j < 32; ++j) x[j] = (j < w && !in_leaf) ? col[(int64_t)s_win[j] * a.ld] : 0.f;
+#pragma unroll
+        for (int k = 0; k < 32; ++k) y[k] = k < nout ? col[(int64_t)s_msrc[nm - nout + k] * a.ld] : 0.f;
+#pragma unroll
+        for (int k = 0; k < 32; ++k)
+            if (k < nout) a.mvals[k * kNB + c] = y[k];
+        if (in_leaf) {
+#pragma unroll
+            for (int j = 0; j < 32; ++j) x[j] = s_lu[j][c - lo];
+        } else if (c >= lo + w) {
+#pragma unroll
+            for (int j = 0; j < 32; ++j) {
+                if (j >= w) break;
+#pragma unroll
+                for (int k = j + 1; k < 32; ++k) x[k] = fmaf(-s_lu[k][j], x[j], x[k]);
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < 32; ++j)
+            if (j < w) a.top[j * kNB + c] = x[j];
+        if (c >= lo) {
+            // z = U11^-1 e_(c-lo) in the leaf, z = U11^-1 U12(:, c) right of it (back substitution)
+            float z[32];
+#pragma unroll
+            for (int i = 0; i < 32; ++i) z[i] = in_leaf ? (i == c - lo ? 1.f : 0.f) : x[i];
+#pragma unroll
+            for (int i = 31; i >= 0; --i) {
+                if (i >= w) continue;
+                z[i] *= s_rdiag[i];
+#pragma unroll
+                for (int k = 0; k < i; ++k) z[k] = fmaf(-s_lu[k][i], z[i], z[k]);
+            }
+#pragma unroll
+            for (int i = 0; i < 32; ++i)
+                if (i < w) a.wmat[i * kNB + c] = z[i];
+        }
+    }
+}
+
+struct ApArgs {
+    float* A;
+    int64_t ld;
+    int n, lc0, w, oc0, pw;
+    const float* top;
+    const float* mvals;
+    const float* wmat;
+    const int* moves;
+    int32_t* perm;
+    const int32_t* status;
+    int nR;
+};
+
+// Applies a leaf: rows of the leaf's top block get their final content; every other row r below
+// it (moved in from the side buffer or in place) becomes [v_left | l | v_right - l U12] with
+// l = v_leaf U11^-1, computed as the product v_leaf * [U11^-1 | U11^-1 U12] (thread per column).
+// Column CTAs apply the leaf's row moves to the columns outside the outer panel.
+__global__ void __launch_bounds__(256) tslu_apply_kernel(ApArgs a) {
+    __shared__ __align__(16) float s_l[kApRows][36];  // the rows' leaf values v_leaf
+    __shared__ int s_mdst[64], s_msrc[64], s_src[kApRows];
+    if (a.status[kInfo] != 0) return;
+    const int t = threadIdx.x;
+    const int nm = a.moves[0], nout = a.moves[1];
+    if (t < nm) { s_mdst[t] = a.moves[2 + t]; s_msrc[t] = a.moves[66 + t]; }
+    __syncthreads();
+    if (blockIdx.x >= a.nR) {
+        // columns outside the outer panel: the leaf's row moves (all reads before all writes)
+        const int cidx = (blockIdx.x - a.nR) * 256 + t;
+        const int col = cidx < a.oc0 ? cidx : cidx + a.pw;
+        if (col >= a.n) return;
+        float x[64];
+#pragma unroll
+        for (int k = 0; k < 64; ++k)
+            if (k < nm) x[k] = a.A[(int64_t)s_msrc[k] * a.ld + col];
+#pragma unroll
+        for (int k = 0; k < 64; ++k)
+            if (k < nm) a.A[(int64_t)s_mdst[k] * a.ld + col] = x[k];
+        return;
+    }
+    if (blockIdx.x == 0 && a.perm) {
+        int pv = 0;
+        if (t < nm) pv = a.perm[s_msrc[t]];
+        __syncthreads();
+        if (t < nm) a.perm[s_mdst[t]] = pv;
+    }
+    const int lo = a.lc0 - a.oc0, w = a.w, pw = a.pw, lc0 = a.lc0;
+    const int r0 = lc0 + blockIdx.x * kApRows;
+    const int nrows = min(kApRows, a.n - r0);
+    if (t < kApRows) {
+        const int i = r0 + t;
+        int s = -1;                   // -1 own row, -2 top row, k >= 0 mvals[k]
+        if (i < lc0 + w) {
+            s = -2;
+        } else {
+            for (int k = 0; k < nout; ++k)
+                if (s_mdst[nm - nout + k] == i) s = k;
+        }
+        s_src[t] = s;
+    }
+    __syncthreads();
+    // thread t owns column c = t of the outer panel
+    const int c = t;
+    const bool active = c < pw;
+    const bool in_leaf = c >= lo && c < lo + w;
+    float x[kApRows], m[32];
+#pragma unroll
+    for (int r = 0; r < kApRows; ++r) {
+        const int s = r < nrows ? s_src[r] : -1;
+        const float* p = s == -2 ? a.top + (r0 + r - lc0) * kNB + c
+                         : s >= 0 ? a.mvals + s * kNB + c
+                                  : a.A + (int64_t)(r0 + r) * a.ld + a.oc0 + c;
+        x[r] = (active && r < nrows && (s != -1 || c >= lo)) ? *p : 0.f;
+    }
+#pragma unroll
+    for (int k = 0; k < 32; ++k) m[k] = (active && c >= lo && k < w) ? a.wmat[k * kNB + c] : 0.f;
+    if (in_leaf) {
+#pragma unroll
+        for (int r = 0; r < kApRows; ++r) s_l[r][c - lo] = x[r];
+    }
+    if (t < kApRows * 4 && w < 32) {  // zero the unused leaf columns
+        const int r = t >> 2;
+        for (int k = w + (t & 3); k < 32; k += 4) s_l[r][k] = 0.f;
+    }
+    __syncthreads();
+    if (!active) return;
+    if (c >= lo) {
+        const float sgn = in_leaf ? 1.f : -1.f;
+#pragma unroll
+        for (int r = 0; r < kApRows; ++r) {
+            if (r >= nrows || s_src[r] == -2) continue;
+            float acc = 0.f;
+#pragma unroll
+            for (int q = 0; q < 8; ++q) {
+                const float4 lv = *reinterpret_cast<const float4*>(&s_l[r][4 * q]);
+                acc = fmaf(lv.x, m[4 * q], acc);
+                acc = fmaf(lv.y, m[4 * q + 1], acc);
+                acc = fmaf(lv.z, m[4 * q + 2], acc);
+                acc = fmaf(lv.w, m[4 * q + 3], acc);
+            }
+            x[r] = in_leaf ? acc : fmaf(sgn, acc, x[r]);
+        }
+    }
+#pragma unroll
+    for (int r = 0; r < kApRows; ++r) {
+        const int s = r < nrows ? s_src[r] : -1;
+        if (r < nrows && (s != -1 || c >= lo)) a.A[(int64_t)(r0 + r) * a.ld + a.oc0 + c] = x[r];
+    }
+}
+
+// U12 = L11^-1 A12 for the rows of the outer panel and the columns right of it (32-column strips),
+// plus the K-major copies of U12 (and for 3xTF32 of L21) that the trailing GEMM reads.
+struct OuArgs {
+    float* A;
+    int64_t ld;
+    int n, oc0, pw, mode, nU;
+    float* bth;
+    float* btl;
+    float* ah;
+    float* al;
+    const int32_t* status;
+};
+
+__device__ __forceinline__ float tf32_hi(float x) { return __uint_as_float(__float_as_uint(x) & 0xFFFFE000u); }
+
+__global__ void __launch_bounds__(256) lu_outer_kernel(OuArgs a) {
+    extern __shared__ float sm[];
+    if (a.status[kInfo] != 0) return;
+    const int t = threadIdx.x;
+    const int c_first = a.oc0 + a.pw;  // first trailing column / row
+    if (blockIdx.x >= a.nU) {
+        // L21 split for 3xTF32: rows [c_first, n) x panel columns -> (ah, al) with row stride pw
+        const int64_t e0 = ((int64_t)(blockIdx.x - a.nU) * 256 + t) * 4;
+        const int64_t total = (int64_t)(a.n - c_first) * a.pw;
+        if (e0 >= total) return;
+        const int64_t r = e0 / a.pw;
+        const int k = (int)(e0 - r * a.pw);
+        const float4 x = *reinterpret_cast<const float4*>(a.A + (c_first + r) * a.ld + a.oc0 + k);
+        const float4 h = make_float4(tf32_hi(x.x), tf32_hi(x.y), tf32_hi(x.z), tf32_hi(x.w));
+        *reinterpret_cast<float4*>(a.ah + e0) = h;
+        *reinterpret_cast<float4*>(a.al + e0) = make_float4(x.x - h.x, x.y - h.y, x.z - h.z, x.w - h.w);
+        return;
+    }
+    const int pw = a.pw;
+    const int cs = c_first + blockIdx.x * 32;
+    const int ncol = min(32, a.n - cs);
+    float* s_x = sm;               // [kNB][33] the strip
+    float* s_l = sm + kNB * 33;    // [kNB][33] one 32-column block of L (rows from the block down)
+    const int c = t & 31, rg = t >> 5;
+    {
+        float tmp[kNB / 8];
+#pragma unroll
+        for (int i = 0; i < kNB / 8; ++i) {
+            const int r = rg + 8 * i;
+            tmp[i] = (r < pw && c < ncol) ? a.A[(int64_t)(a.oc0 + r) * a.ld + cs + c] : 0.f;
+        }
+#pragma unroll
+        for (int i = 0; i < kNB / 8; ++i) s_x[(rg + 8 * i) * 33 + c] = tmp[i];
+    }
+    for (int b0 = 0; b0 < pw; b0 += 32) {
+        const int bw = min(32, pw - b0);
+        float tmp[kNB / 8];
+#pragma unroll
+        for (int i = 0; i < kNB / 8; ++i) {
+            const int r = b0 + rg + 8 * i;
+            tmp[i] = (r < pw && c < bw) ? a.A[(int64_t)(a.oc0 + r) * a.ld + a.oc0 + b0 + c] : 0.f;
+        }
+        __syncthreads();
+#pragma unroll
+        for (int i = 0; i < kNB / 8; ++i)
+            if (b0 + rg + 8 * i < pw) s_l[(rg + 8 * i) * 33 + c] = tmp[i];
+        __syncthreads();
+        if (t < 32) {
+            float x[32];
+#pragma unroll
+            for (int j = 0; j < 32; ++j) x[j] = j < bw ? s_x[(b0 + j) * 33 + c] : 0.f;
+#pragma unroll
+            for (int j = 0; j < 32; ++j)
+#pragma unroll
+                for (int k = j + 1; k < 32; ++k) x[k] = fmaf(-s_l[k * 33 + j], x[j], x[k]);
+#pragma unroll
+            for (int j = 0; j < 32; ++j)
+                if (j < bw) s_x[(b0 + j) * 33 + c] = x[j];
+        }
+        __syncthreads();
+        for (int r = b0 + bw + rg; r < pw; r += 8) {
+            float acc = s_x[r * 33 + c];
+            const float* lr = s_l + (r - b0) * 33;
+#pragma unroll
+            for (int k = 0; k < 32; ++k) acc = fmaf(-lr[k], s_x[(b0 + k) * 33 + c], acc);
+            s_x[r * 33 + c] = acc;
+        }
+    }
+    __syncthreads();
+    for (int r = rg; r < pw; r += 8)
+        if (c < ncol) a.A[(int64_t)(a.oc0 + r) * a.ld + cs + c] = s_x[r * 33 + c];
+    // Bt[col][k] = U12[k][col] (K-major), split for 3xTF32
+    for (int cc = 0; cc < ncol; ++cc) {
+        const int64_t o = (int64_t)(cs - c_first + cc) * pw;
+        for (int k = t; k < pw; k += 256) {
+            const float x = s_x[k * 33 + cc];
+            if (a.mode == 3) {
+                const float h = tf32_hi(x);
+                a.bth[o + k] = h;
+                a.btl[o + k] = x - h;
+            } else {
+                a.bth[o + k] = x;
+            }
+        }
+    }
+}
+
+__global__ void iota_f32_kernel(int32_t* v, int64_t n) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) v[i] = (int32_t)i;
+}
+
+// Inverses of the diagonal blocks (nb x nb) of the unit-lower L (which 0) and of U (which 1), used
+// by the blocked triangular solves of the refinement.  One CTA per (block, triangle), thread per
+// column of the inverse; the block and the growing inverse live in shared memory.
+__global__ void diag_inv_kernel(const float* LU, int64_t ld, int n, int nb, float* linv, float* uinv,
+                                const int32_t* status) {
+    extern __shared__ float sm[];
+    if (status[kInfo] != 0) return;
+    const int blk = blockIdx.x >> 1, upper = blockIdx.x & 1;
+    const int b0 = blk * nb, bs = min(nb, n - b0);
+    const int SP = nb + 1;
+    float* s_t = sm;             // [nb][SP] the triangle
+    float* s_x = sm + nb * SP;   // [nb][SP] the inverse, column c owned by thread c
+    const int c = threadIdx.x;
+    for (int r = 0; r < bs; ++r)
+        if (c < bs) s_t[r * SP + c] = LU[(int64_t)(b0 + r) * ld + b0 + c];
+    __syncthreads();
+    if (c < nb) {
+        if (!upper) {
+            for (int i = 0; i < nb; ++i) {
+                float acc = (i == c) ? 1.f : 0.f;
+                if (i < bs)
+                    for (int k = 0; k < i; ++k) acc = fmaf(-s_t[i * SP + k], s_x[k * SP + c], acc);
+                s_x[i * SP + c] = (i < c || i >= bs) ? 0.f : acc;
+            }
+        } else {
+            for (int i = nb - 1; i >= 0; --i) {
+                float v = 0.f;
+                if (i < bs && i <= c && c < bs) {
+                    float acc = (i == c) ? 1.f : 0.f;
+                    for (int k = i + 1; k <= c; ++k) acc = fmaf(-s_t[i * SP + k], s_x[k * SP + c], acc);
+                    v = acc / s_t[i * SP + i];
+                }
+                s_x[i * SP + c] = v;
+            }
+        }
+    }
+    __syncthreads();
+    float* out = (upper ? uinv : linv) + (int64_t)blk * nb * nb;
+    for (int r = 0; r < nb; ++r)
+        if (c < nb) out[r * nb + c] = s_x[r * SP + c];
+}
+
+}  // namespace
+
+// Scratch of the FP32 factorisation (all device memory, carved from one workspace).
+size_t f32_scratch_bytes(int64_t n) {
+    const int64_t nblk = ceil_div(n, kTrsvNB);
+    size_t b = 0;
+    b += (size_t)kTsLevels * kTsMaxCand * 32 * sizeof(int);   // cand
+    b += (size_t)kTsLevels * kTsMaxCand * sizeof(unsigned);   // counters
+    b += 3 * 32 * kNB * sizeof(float);                          // top, mvals, wmat
+    b += 256 * sizeof(int);                                     // moves
+    b += 4 * (size_t)round_up(n, 32) * kNB * sizeof(float);     // bth, btl, ah, al
+    b += 2 * (size_t)nblk * kTrsvNB * kTrsvNB * sizeof(float);  // diagonal inverses
+    return b + 16 * 256;
+}
+
+F32Scratch f32_scratch_carve(void* base, int64_t n) {
+    F32Scratch s;
+    char* p = static_cast<char*>(base);
+    auto take = [&](size_t bytes) {
+        char* q = p;
+        p += round_up((int64_t)bytes, 256);
+        return q;
+    };
+    const int64_t nblk = ceil_div(n, kTrsvNB);
+    s.cand = reinterpret_cast<int*>(take((size_t)kTsLevels * kTsMaxCand * 32 * sizeof(int)));
+    s.counters = reinterpret_cast<unsigned*>(take((size_t)kTsLevels * kTsMaxCand * sizeof(unsigned)));
+    s.counters_bytes = (size_t)kTsLevels * kTsMaxCand * sizeof(unsigned);
+    s.top = reinterpret_cast<float*>(take(32 * kNB * sizeof(float)));
+    s.mvals = reinterpret_cast<float*>(take(32 * kNB * sizeof(float)));
+    s.wmat = reinterpret_cast<float*>(take(32 * kNB * sizeof(float)));
+    s.moves = reinterpret_cast<int*>(take(256 * sizeof(int)));
+    const size_t panel = (size_t)round_up(n, 32) * kNB * sizeof(float);
+    s.bth = reinterpret_cast<float*>(take(panel));
+    s.btl = reinterpret_cast<float*>(take(panel));
+    s.ah = reinterpret_cast<float*>(take(panel));
+    s.al = reinterpret_cast<float*>(take(panel));
+    s.linv = reinterpret_cast<float*>(take((size_t)nblk * kTrsvNB * kTrsvNB * sizeof(float)));
+    s.uinv = reinterpret_cast<float*>(take((size_t)nblk * kTrsvNB * kTrsvNB * sizeof(float)));
+    return s;
+}
+
+int32_t lu_factor_f32(Ctx* ctx, cudaStream_t st, float* A, int64_t ld, int64_t n, int32_t* perm, int mode,
+                      const F32Scratch& s) {
+    if (n <= 0) return B2M_OK;
+    if ((ld & 31) || (reinterpret_cast<uintptr_t>(A) & 127))
+        return fail(ctx, B2M_ERR_DIM, "lu_factor_f32: ld must be a multiple of 32 floats, A 128-byte aligned");
+    if (n > (int64_t)kTsMaxCand * kTsRows) return fail(ctx, B2M_ERR_UNSUPPORTED, "mixed LU: n too large");
+    static bool attr = false;
+    const int ou_smem = 2 * kNB * 33 * sizeof(float);
+    const int di_smem = 2 * kTrsvNB * (kTrsvNB + 1) * sizeof(float);
+    if (!attr) {
+        B2M_CU(ctx, cudaFuncSetAttribute(lu_outer_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, ou_smem));
+        B2M_CU(ctx, cudaFuncSetAttribute(diag_inv_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, di_smem));
+        attr = true;
+    }
+    const GraphKey key{3 + mode * 10, A, perm, s.cand, s.bth, ld, n, 0, 0};
+    return run_graph(ctx, st, key, [&](cudaStream_t q) -> int32_t {
+        B2M_CU(ctx, cudaMemsetAsync(s.counters, 0, s.counters_bytes, q));
+        iota_f32_kernel<<<(unsigned)ceil_div(n, 256), 256, 0, q>>>(perm, n);
+        B2M_LAUNCHED(ctx);
+        for (int64_t oc0 = 0; oc0 < n; oc0 += kNB) {
+            const int pw = (int)std::min<int64_t>(kNB, n - oc0);
+            for (int64_t lc0 = oc0; lc0 < oc0 + pw; lc0 += 32) {
+                const int w = (int)std::min<int64_t>(32, n - lc0);
+                TsArgs ta{A, ld, (int)n, (int)lc0, w, (int)oc0, pw, s.cand, s.counters, s.top, s.mvals, s.wmat,
+                          s.moves, ctx->d_status};
+                prof_begin(ctx, q, kClsPanel);
+                tslu_select_kernel<<<(unsigned)ceil_div(n - lc0, kTsRows), kTsThreads, 0, q>>>(ta);
+                prof_end(ctx, q, kClsPanel, 2.0 * (n - lc0) * w * w);
+                B2M_LAUNCHED(ctx);
+                ApArgs aa{A, ld, (int)n, (int)lc0, w, (int)oc0, pw, s.top, s.mvals, s.wmat, s.moves, perm,
+                          ctx->d_status, 0};
+                aa.nR = (int)ceil_div(n - lc0, kApRows);
+                const int nC = (int)ceil_div(n - pw, 256);
+                prof_begin(ctx, q, kClsSwap);
+                tslu_apply_kernel<<<aa.nR + nC, 256, 0, q>>>(aa);
+                prof_end(ctx, q, kClsSwap, 2.0 * (n - lc0) * w * (pw - (lc0 - oc0)));
+                B2M_LAUNCHED(ctx);
+            }
+            const int64_t c1 = oc0 + pw;
+            if (c1 >= n) break;
+            const int64_t M = n - c1;
+            OuArgs oa{A, ld, (int)n, (int)oc0, pw, mode, (int)ceil_div(M, 32), s.bth, s.btl, s.ah, s.al, ctx->d_status};
+            const int nL = mode == 3 ? (int)ceil_div(M * pw, 1024) : 0;
+            prof_begin(ctx, q, kClsTrsm);
+            lu_outer_kernel<<<oa.nU + nL, 256, ou_smem, q>>>(oa);
+            prof_end(ctx, q, kClsTrsm, (double)pw * pw * M);
+            B2M_LAUNCHED(ctx);
+            FOperand bh{s.bth, pw, M, pw, 0, 0};
+            float* C = A + c1 * ld + c1;
+            if (mode == 3) {
+                FOperand ah{s.ah, pw, M, pw, 0, 0};
+                B2M_TRY(sgemm_tc(ctx, q, ah, s.al, bh, s.btl, C, ld, M, M, pw, B2M_DO_SUB, 3, true));
+            } else {
+                FOperand ah{A, ld, n, n, c1, oc0};
+                B2M_TRY(sgemm_tc(ctx, q, ah, nullptr, bh, nullptr, C, ld, M, M, pw, B2M_DO_SUB, 1, true));
+            }
+        }
+        const int nblk = (int)ceil_div(n, kTrsvNB);
+        diag_inv_kernel<<<2 * nblk, kTrsvNB, di_smem, q>>>(A, ld, (int)n, kTrsvNB, s.linv, s.uinv, ctx->d_status);
+        B2M_LAUNCHED(ctx);
+        return B2M_OK;
+    });
+}
+
+}  // namespace b2m

@@ -1,11 +1,20 @@
-// lu_mixed.cu -- mixed-precision LU solve: FP32 factorisation whose trailing updates and
-// triangular-solve updates run on the tcgen05 tensor cores (TF32 or 3xTF32), FP64 iterative
-// refinement (residual b - Ax, update x += d, normwise backward-error stopping test, all in FP64),
-// and a plain FP64 re-factorisation when refinement stalls or the FP32 factorisation is singular.
+// lu_mixed.cu -- mixed-precision LU solve: an FP32 factorisation whose trailing updates run on the
+// tcgen05 tensor cores (TF32 or 3xTF32, lu_f32.cu), FP64 iterative refinement (residual b - Ax,
+// update x += d, normwise backward-error stopping test, all in FP64), and a plain FP64
+// re-factorisation when refinement stalls or the FP32 factorisation meets a tiny pivot.
 //
 // There is no counterpart in the reference (MatrixLinEQSolve, LinAlgLU.pas:481-592, refines a
 // fixed number of times in FP64 around an FP64 factorisation); the result is judged against the
 // FP64 oracle through its backward error.
+//
+// One refinement step is three kinds of launch, captured once and replayed:
+//   * trsv_block_kernel, once per 128-row block and sweep: the block's diagonal CTAs (four
+//     right-hand sides each) apply the previous block's contribution and multiply by the
+//     precomputed inverse of the diagonal block; the other CTAs apply the previous block's
+//     contribution to every later row.  The backward sweep also adds d to the FP64 solution;
+//   * resid_kernel: r = b - A x in FP64 (64 rows x 16 right-hand sides per CTA), which also writes
+//     P r in FP32 for the next step and the column maxima of |r|, |x| and |b| for the test
+//     eta = max_c ||r_c||inf / (||A||inf ||x_c||inf + ||b_c||inf).
 #include <cmath>
 #include <vector>
 
@@ -15,22 +24,25 @@
 namespace b2m {
 namespace {
 
-// ------------------------------------------------------------------ small kernels
-__global__ void f64_to_f32_kernel(const double* src, int64_t lds, float* dst, int64_t ldd, int64_t rows, int64_t cols) {
-    const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (e >= rows * cols) return;
-    const int64_t r = e / cols, c = e - r * cols;
-    dst[r * ldd + c] = (float)src[r * lds + c];
+constexpr int kTrRhs = 4;      // right-hand sides per diagonal CTA
+constexpr int kTrRows = 64;    // rows per update CTA
+constexpr int kTrMaxRhs = 16;  // right-hand sides per sweep launch
+constexpr int kReRows = 64;    // rows per residual CTA
+constexpr int kReRhs = 16;     // right-hand sides per residual CTA
+constexpr int kReK = 64;       // K chunk of the residual
+constexpr int kReSplit = 4;    // K slices inside a residual CTA
+constexpr int kReStages = 3;   // cp.async pipeline depth
+constexpr int kReAS = kReK + 2;                                   // A tile row stride (doubles)
+constexpr int kReStage = kReRows * kReAS + kReK * kReRhs;         // doubles per stage
+constexpr int kReSmem = kReStages * kReStage * (int)sizeof(double);
+
+unsigned gsz(int64_t n, int b = 256) { return (unsigned)ceil_div(std::max<int64_t>(n, 1), b); }
+
+__device__ __forceinline__ void atomic_max_abs(unsigned long long* p, double v) {
+    atomicMax(p, (unsigned long long)__double_as_longlong(fabs(v)));
 }
 
-__global__ void add_f32_to_f64_kernel(double* x, int64_t ldx, const float* d, int64_t ldd, int64_t rows, int64_t cols) {
-    const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (e >= rows * cols) return;
-    const int64_t r = e / cols, c = e - r * cols;
-    x[r * ldx + c] += (double)d[r * ldd + c];
-}
-
-// ||A||_inf: max row sum of |a_ij| (one warp per row, then a global max on the bit pattern)
+// ||A||inf: max row sum of |a_ij| (one warp per row, then a global max on the bit pattern)
 __global__ void norm_inf_kernel(const double* A, int64_t lda, int64_t n, unsigned long long* out) {
     const int64_t row = (int64_t)blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5);
     const int lane = threadIdx.x & 31;
@@ -48,133 +60,383 @@ __global__ void colmax3_kernel(const double* R, int64_t ldr, const double* X, in
     const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (e >= n * k) return;
     const int64_t i = e / k, c = e - i * k;
-    atomicMax(&out[c], (unsigned long long)__double_as_longlong(fabs(R[i * ldr + c])));
-    atomicMax(&out[k + c], (unsigned long long)__double_as_longlong(fabs(X[i * ldx + c])));
-    atomicMax(&out[2 * k + c], (unsigned long long)__double_as_longlong(fabs(B[i * ldb + c])));
+    atomic_max_abs(&out[c], R[i * ldr + c]);
+    atomic_max_abs(&out[k + c], X[i * ldx + c]);
+    atomic_max_abs(&out[2 * k + c], B[i * ldb + c]);
 }
 
-// X[i][:] = B[perm[i]][:] (FP32)
-__global__ void gather_rows_f32_kernel(float* X, int64_t ldx, const float* B, int64_t ldb, const int32_t* perm,
-                                       int64_t n, int64_t nrhs) {
+__global__ void f64_to_f32_kernel(const double* src, int64_t lds, float* dst, int64_t ldd, int64_t rows, int64_t cols) {
+    const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= rows * cols) return;
+    const int64_t r = e / cols, c = e - r * cols;
+    dst[r * ldd + c] = (float)src[r * lds + c];
+}
+
+// pinv[perm[i]] = i
+__global__ void invert_perm_kernel(const int32_t* perm, int32_t* pinv, int64_t n) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) pinv[perm[i]] = (int32_t)i;
+}
+
+// start of refinement: x = 0, r32 = P b
+__global__ void ir_init_kernel(const double* B, int64_t ldb, const int32_t* perm, float* r32, int64_t ldr, double* X,
+                               int64_t ldx, int64_t n, int64_t nrhs) {
     const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (e >= n * nrhs) return;
     const int64_t i = e / nrhs, c = e - i * nrhs;
-    X[i * ldx + c] = B[(int64_t)perm[i] * ldb + c];
+    r32[i * ldr + c] = (float)B[(int64_t)perm[i] * ldb + c];
+    X[i * ldx + c] = 0.0;
 }
 
-__global__ void iota32_kernel(int32_t* v, int64_t n) {
-    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < n) v[i] = (int32_t)i;
-}
-
-unsigned gsz(int64_t n, int b = 256) { return (unsigned)ceil_div(std::max<int64_t>(n, 1), b); }
-
-// ------------------------------------------------------------------ FP32 GEMM through the tensor cores
-struct Split {
-    float* ah;
-    float* al;
-    float* bh;
-    float* bl;
-    int64_t cap;  // floats available in each buffer
-    int mode;     // 1 TF32, 3 3xTF32
+struct TrArgs {
+    const float* T;     // the FP32 factors (unit-lower L below the diagonal, U on and above)
+    int64_t ld;
+    int n;
+    const float* inv;   // inverses of the diagonal blocks, kTrsvNB x kTrsvNB each
+    float* Xr;          // right-hand sides / solution (n x ldr), columns [c0, c0 + nc)
+    int64_t ldr;
+    int c0, nc;
+    double* X64;        // backward sweep: X64 += solution
+    int64_t ldx;
+    int upper;
+    int nd;             // diagonal CTAs
+    const int32_t* status;
 };
 
-// C(M x N) op= A(M x K) * B(K x N): A is a block of a row-major FP32 matrix (K-major as stored), B a
-// row-major block (transposed into Bt for the K-major B operand, and split for 3xTF32).
-int32_t f32_gemm(Ctx* ctx, cudaStream_t st, const float* A, int64_t lda, int64_t a_rows, int64_t a_cols, int64_t ar0,
-                 int64_t ac0, const float* B, int64_t ldb, int64_t br0, int64_t bc0, float* C, int64_t ldc, int64_t M,
-                 int64_t N, int64_t K, int op, const Split& sp) {
-    if (M <= 0 || N <= 0 || K <= 0) return B2M_OK;
-    const int64_t ldk = round_up(K, 4);
-    if (N * ldk > sp.cap || (sp.mode == 3 && M * ldk > sp.cap))
-        return fail(ctx, B2M_ERR_UNSUPPORTED, "mixed GEMM scratch too small");
-    B2M_TRY(tf32_split(ctx, st, B + br0 * ldb + bc0, ldb, K, N, sp.bh, sp.mode == 3 ? sp.bl : nullptr, ldk, true));
-    FOperand bh{sp.bh, ldk, N, K, 0, 0};
-    if (sp.mode == 3) {
-        B2M_TRY(tf32_split(ctx, st, A + ar0 * lda + ac0, lda, M, K, sp.ah, sp.al, ldk, false));
-        FOperand ah{sp.ah, ldk, M, K, 0, 0};
-        return sgemm_tc(ctx, st, ah, sp.al, bh, sp.bl, C, ldc, M, N, K, op, 3, true);
-    }
-    FOperand ah{A, lda, a_rows, a_cols, ar0, ac0};
-    return sgemm_tc(ctx, st, ah, nullptr, bh, nullptr, C, ldc, M, N, K, op, 1, true);
+// One block step of a blocked triangular solve.  Block b's diagonal CTAs (kTrRhs columns each)
+// subtract block `prev`'s contribution from block b and multiply by inv(T_bb); the update CTAs
+// subtract block `prev`'s contribution from the rows still to come (below b when forward, above b
+// when backward).  Rows of T are read as float4 straight into registers (a row of the factors
+// starts 128-byte aligned), so every thread has all of its loads in flight at once.
+__device__ __forceinline__ float4 ld_row4(const float* row, int k, int kmax) {
+    if (k >= kmax) return make_float4(0.f, 0.f, 0.f, 0.f);
+    float4 v = __ldg(reinterpret_cast<const float4*>(row + k));
+    if (k + 1 >= kmax) v.y = 0.f;  // the factors' padding columns are never initialised
+    if (k + 2 >= kmax) v.z = 0.f;
+    if (k + 3 >= kmax) v.w = 0.f;
+    return v;
 }
 
-// triangle of the FP32 LU at (A, lda, n x n), right-hand sides rows of (B, ldb) at column bc0
-struct TriF {
-    const float* A;
-    int64_t lda, n;
-    float* B;
-    int64_t ldb, bc0, ncols;
+__global__ void __launch_bounds__(256) trsv_block_kernel(TrArgs a, int b) {
+    __shared__ __align__(16) float s_p[kTrsvNB][kTrMaxRhs];  // solution of block prev
+    __shared__ __align__(16) float s_y[kTrsvNB][kTrRhs];
+    __shared__ __align__(16) float s_h[kTrsvNB][kTrRhs];     // second-half partial sums
+    if (a.status[kInfo] != 0) return;
+    const int t = threadIdx.x;
+    const int NB = kTrsvNB;
+    const int nblk = (int)ceil_div(a.n, NB);
+    const int prev = a.upper ? b + 1 : b - 1;
+    const bool has_prev = prev >= 0 && prev < nblk;
+    const int p0 = prev * NB, ps = has_prev ? min(NB, a.n - p0) : 0;
+    const int b0 = b * NB, bs = min(NB, a.n - b0);
+    if (blockIdx.x < a.nd) {
+        const int g = blockIdx.x * kTrRhs;  // first column of this CTA's group, relative to c0
+        const int r = t & (NB - 1), h = t >> 7;  // row r, K half h
+        // every global load of this CTA is issued before the first barrier
+        float4 tv[16], iv[16];
+        {
+            const float* trow = a.T + (int64_t)(b0 + min(r, bs - 1)) * a.ld + p0;
+            const float* irow = a.inv + (int64_t)b * NB * NB + (int64_t)r * NB + 64 * h;
+#pragma unroll
+            for (int i = 0; i < 16; ++i) tv[i] = (r < bs && has_prev) ? ld_row4(trow, 64 * h + 4 * i, ps) : make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+            for (int i = 0; i < 16; ++i) iv[i] = __ldg(reinterpret_cast<const float4*>(irow) + i);
+        }
+        float xb[kTrRhs];
+#pragma unroll
+        for (int q = 0; q < kTrRhs; ++q)
+            xb[q] = (h == 0 && r < bs && g + q < a.nc) ? a.Xr[(int64_t)(b0 + r) * a.ldr + a.c0 + g + q] : 0.f;
+        {
+            float v[2];
+#pragma unroll
+            for (int i = 0; i < 2; ++i) {
+                const int e = t + 256 * i, k = e >> 2, q = e & 3;
+                v[i] = (k < ps && g + q < a.nc) ? a.Xr[(int64_t)(p0 + k) * a.ldr + a.c0 + g + q] : 0.f;
+            }
+#pragma unroll
+            for (int i = 0; i < 2; ++i) s_p[(t + 256 * i) >> 2][(t + 256 * i) & 3] = v[i];
+        }
+        __syncthreads();
+        // y = X_b - T_{b,prev} X_prev
+        float acc[kTrRhs] = {0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+        for (int i = 0; i < 16; ++i) {
+            const float tk[4] = {tv[i].x, tv[i].y, tv[i].z, tv[i].w};
+#pragma unroll
+            for (int e = 0; e < 4; ++e) {
+                const float4 xp = *reinterpret_cast<const float4*>(&s_p[64 * h + 4 * i + e][0]);
+                acc[0] = fmaf(tk[e], xp.x, acc[0]);
+                acc[1] = fmaf(tk[e], xp.y, acc[1]);
+                acc[2] = fmaf(tk[e], xp.z, acc[2]);
+                acc[3] = fmaf(tk[e], xp.w, acc[3]);
+            }
+        }
+        if (h == 1) *reinterpret_cast<float4*>(&s_h[r][0]) = make_float4(acc[0], acc[1], acc[2], acc[3]);
+        __syncthreads();
+        if (h == 0) {
+            const float4 o = *reinterpret_cast<const float4*>(&s_h[r][0]);
+            const float oh[4] = {o.x, o.y, o.z, o.w};
+#pragma unroll
+            for (int q = 0; q < kTrRhs; ++q) s_y[r][q] = (r < bs) ? xb[q] - acc[q] - oh[q] : 0.f;
+        }
+        __syncthreads();
+        // x_b = inv(T_bb) y (the inverse is zero outside the block's extent)
+        float x[kTrRhs] = {0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+        for (int i = 0; i < 16; ++i) {
+            const float ik[4] = {iv[i].x, iv[i].y, iv[i].z, iv[i].w};
+#pragma unroll
+            for (int e = 0; e < 4; ++e) {
+                const float4 y = *reinterpret_cast<const float4*>(&s_y[64 * h + 4 * i + e][0]);
+                x[0] = fmaf(ik[e], y.x, x[0]);
+                x[1] = fmaf(ik[e], y.y, x[1]);
+                x[2] = fmaf(ik[e], y.z, x[2]);
+                x[3] = fmaf(ik[e], y.w, x[3]);
+            }
+        }
+        if (h == 1) *reinterpret_cast<float4*>(&s_h[r][0]) = make_float4(x[0], x[1], x[2], x[3]);
+        __syncthreads();
+        if (h == 0 && r < bs) {
+            const float4 o = *reinterpret_cast<const float4*>(&s_h[r][0]);
+            const float oh[4] = {o.x, o.y, o.z, o.w};
+#pragma unroll
+            for (int q = 0; q < kTrRhs; ++q) {
+                if (g + q >= a.nc) continue;
+                const float v = x[q] + oh[q];
+                const int64_t col = a.c0 + g + q;
+                a.Xr[(int64_t)(b0 + r) * a.ldr + col] = v;
+                if (a.upper) a.X64[(int64_t)(b0 + r) * a.ldx + col] += (double)v;
+            }
+        }
+        return;
+    }
+    if (!has_prev) return;
+    // update CTA: rows [u0, u0 + kTrRows) of the remaining range; 4 lanes per row split K in
+    // quarters.  s_p rows are stored with their 16-byte chunks rotated by (k >> 5) so that the four
+    // quarter-groups of a warp read different banks.
+    const int u = blockIdx.x - a.nd;
+    const int u0 = a.upper ? u * kTrRows : b0 + bs + u * kTrRows;
+    const int uend = a.upper ? b0 : a.n;
+    if (u0 >= uend) return;
+    const int rr = t >> 2, kq = t & 3;
+    const int row = u0 + rr;
+    float4 tv[8];
+    {
+        const float* trow = a.T + (int64_t)min(row, uend - 1) * a.ld + p0;
+#pragma unroll
+        for (int i = 0; i < 8; ++i) tv[i] = row < uend ? ld_row4(trow, 32 * kq + 4 * i, ps) : make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+    {
+        float v[8];
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+            const int e = t + 256 * i, k = e >> 4, c = e & 15;
+            v[i] = (k < ps && c < a.nc) ? a.Xr[(int64_t)(p0 + k) * a.ldr + a.c0 + c] : 0.f;
+        }
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+            const int e = t + 256 * i, k = e >> 4, c = e & 15;
+            s_p[k][(((c >> 2) ^ (k >> 5)) & 3) * 4 + (c & 3)] = v[i];
+        }
+    }
+    __syncthreads();
+    float acc[kTrMaxRhs];
+#pragma unroll
+    for (int c = 0; c < kTrMaxRhs; ++c) acc[c] = 0.f;
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+        const float tk[4] = {tv[i].x, tv[i].y, tv[i].z, tv[i].w};
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+            const int k = 32 * kq + 4 * i + e;
+            const float* xp = &s_p[k][0];
+#pragma unroll
+            for (int c4 = 0; c4 < kTrMaxRhs / 4; ++c4) {
+                const float4 xv = *reinterpret_cast<const float4*>(xp + ((c4 ^ kq) & 3) * 4);
+                acc[4 * c4 + 0] = fmaf(tk[e], xv.x, acc[4 * c4 + 0]);
+                acc[4 * c4 + 1] = fmaf(tk[e], xv.y, acc[4 * c4 + 1]);
+                acc[4 * c4 + 2] = fmaf(tk[e], xv.z, acc[4 * c4 + 2]);
+                acc[4 * c4 + 3] = fmaf(tk[e], xv.w, acc[4 * c4 + 3]);
+            }
+        }
+    }
+#pragma unroll
+    for (int c = 0; c < kTrMaxRhs; ++c) {
+        acc[c] += __shfl_xor_sync(0xffffffffu, acc[c], 1);
+        acc[c] += __shfl_xor_sync(0xffffffffu, acc[c], 2);
+    }
+    if (row < uend) {
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            const int c = 4 * kq + i;
+            if (c < a.nc) a.Xr[(int64_t)row * a.ldr + a.c0 + c] -= acc[c];
+        }
+    }
+}
+
+struct ReArgs {
+    const double* A;
+    int64_t lda;
+    const double* X;
+    int64_t ldx;
+    const double* B;
+    int64_t ldb;
+    int n, nrhs;
+    float* r32;          // P r in FP32 (row pinv[i] <- r_i)
+    int64_t ldr;
+    const int32_t* pinv;
+    unsigned long long* nrm;  // [0,k) |r|, [k,2k) |x|, [2k,3k) |b|
 };
 
-int32_t trsm_lower_f32(Ctx* ctx, cudaStream_t st, const TriF& t, int64_t r0, int64_t br0, int64_t k, const Split& sp) {
-    if (k <= 32)
-        return launch_trsm_small<float>(ctx, st, t.A + r0 * t.lda + r0, t.lda, t.B + br0 * t.ldb + t.bc0, t.ldb,
-                                        (int)k, (int)t.ncols, false);
-    const int64_t k1 = round_up((k + 1) / 2, 32), k2 = k - k1;
-    B2M_TRY(trsm_lower_f32(ctx, st, t, r0, br0, k1, sp));
-    B2M_TRY(f32_gemm(ctx, st, t.A, t.lda, t.n, t.n, r0 + k1, r0, t.B, t.ldb, br0, t.bc0,
-                     t.B + (br0 + k1) * t.ldb + t.bc0, t.ldb, k2, t.ncols, k1, B2M_DO_SUB, sp));
-    return trsm_lower_f32(ctx, st, t, r0 + k1, br0 + k1, k2, sp);
+__device__ __forceinline__ void cp_async16(void* dst, const void* src, int src_bytes) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(smem_u32(dst)), "l"(src), "r"(src_bytes)
+                 : "memory");
 }
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
 
-int32_t trsm_upper_f32(Ctx* ctx, cudaStream_t st, const TriF& t, int64_t r0, int64_t br0, int64_t k, const Split& sp) {
-    if (k <= 32)
-        return launch_trsm_small<float>(ctx, st, t.A + r0 * t.lda + r0, t.lda, t.B + br0 * t.ldb + t.bc0, t.ldb,
-                                        (int)k, (int)t.ncols, true);
-    const int64_t k1 = round_up((k + 1) / 2, 32), k2 = k - k1;
-    B2M_TRY(trsm_upper_f32(ctx, st, t, r0 + k1, br0 + k1, k2, sp));
-    B2M_TRY(f32_gemm(ctx, st, t.A, t.lda, t.n, t.n, r0, r0 + k1, t.B, t.ldb, br0 + k1, t.bc0, t.B + br0 * t.ldb + t.bc0,
-                     t.ldb, k1, t.ncols, k2, B2M_DO_SUB, sp));
-    return trsm_upper_f32(ctx, st, t, r0, br0, k1, sp);
-}
-
-int32_t lu_rec_f32(Ctx* ctx, cudaStream_t st, float* A, int64_t ld, int64_t n, int64_t c0, int64_t width, int32_t* ipiv,
-                   int32_t* perm, const Split& sp) {
-    if (width <= 32) {
-        B2M_TRY(launch_panel<float>(ctx, st, A + c0 * ld + c0, ld, (int)(n - c0), (int)width, (int)c0, (int)c0, ipiv));
-        return launch_swaps<float>(ctx, st, A, ld, (int)n, (int)c0, (int)width, ipiv, perm);
+// r = b - A x for rows [64 blockIdx.x, +64) and columns [16 blockIdx.y, +16).  A and X stream
+// through a 3-stage cp.async pipeline (64 x 64 tiles of A, 64 x 16 of X); four K slices of 64
+// threads each; a thread accumulates rows rg, rg+16, rg+32, rg+48 x 4 columns (A rows 66 doubles
+// apart keep those four-row loads free of bank conflicts).
+__global__ void __launch_bounds__(256, 1) resid_kernel(ReArgs a) {
+    extern __shared__ __align__(16) double re_sm[];
+    __shared__ unsigned long long s_n[3 * kReRhs];
+    const int t = threadIdx.x;
+    const int r0 = blockIdx.x * kReRows, cb = blockIdx.y * kReRhs;
+    const int nc = min(kReRhs, a.nrhs - cb);
+    const int ks = t >> 6, u = t & 63, rg = u >> 2, q = u & 3;
+    const int nk = (int)ceil_div(a.n, kReK);
+    if (t < 3 * kReRhs) s_n[t] = 0ull;
+    auto issue = [&](int kc) {
+        double* sa = re_sm + (kc % kReStages) * kReStage;
+        double* sx = sa + kReRows * kReAS;
+        const int k0 = kc * kReK;
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {  // A: 64 rows x 32 pieces of 2 doubles
+            const int piece = t + 256 * i, row = piece >> 5, kp = (piece & 31) * 2;
+            const int grow = r0 + row, gk = k0 + kp;
+            const bool ok = grow < a.n && gk < a.n;
+            const double* src = ok ? a.A + (int64_t)grow * a.lda + gk : a.A;
+            cp_async16(sa + row * kReAS + kp, src, ok ? (gk + 1 < a.n ? 16 : 8) : 0);
+        }
+#pragma unroll
+        for (int i = 0; i < 2; ++i) {  // X: 64 k x 8 pieces of 2 doubles
+            const int piece = t + 256 * i, k = piece >> 3, cp = (piece & 7) * 2;
+            const int gk = k0 + k;
+            const bool ok = gk < a.n && cp < nc;
+            const double* src = ok ? a.X + (int64_t)gk * a.ldx + cb + cp : a.X;
+            cp_async16(sx + k * kReRhs + cp, src, ok ? (cp + 1 < nc ? 16 : 8) : 0);
+        }
+    };
+    double acc[4][4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) acc[i][j] = 0.0;
+#pragma unroll
+    for (int s = 0; s < kReStages - 1; ++s) {
+        if (s < nk) issue(s);
+        cp_async_commit();
     }
-    const int64_t nleft = round_up((width + 1) / 2, 32), nright = width - nleft;
-    B2M_TRY(lu_rec_f32(ctx, st, A, ld, n, c0, nleft, ipiv, perm, sp));
-    TriF t{A, ld, n, A, ld, c0 + nleft, nright};
-    B2M_TRY(trsm_lower_f32(ctx, st, t, c0, c0, nleft, sp));
-    const int64_t r1 = c0 + nleft;
-    B2M_TRY(f32_gemm(ctx, st, A, ld, n, n, r1, c0, A, ld, c0, r1, A + r1 * ld + r1, ld, n - r1, nright, nleft,
-                     B2M_DO_SUB, sp));
-    return lu_rec_f32(ctx, st, A, ld, n, r1, nright, ipiv, perm, sp);
+    for (int kc = 0; kc < nk; ++kc) {
+        cp_async_wait<kReStages - 2>();
+        __syncthreads();
+        if (kc + kReStages - 1 < nk) issue(kc + kReStages - 1);
+        cp_async_commit();
+        const double* sa = re_sm + (kc % kReStages) * kReStage;
+        const double* sx = sa + kReRows * kReAS;
+#pragma unroll
+        for (int kk = 0; kk < kReK / kReSplit; ++kk) {
+            const int k = ks * (kReK / kReSplit) + kk;
+            double av[4];
+#pragma unroll
+            for (int i = 0; i < 4; ++i) av[i] = sa[(rg + 16 * i) * kReAS + k];
+            const double2 x01 = *reinterpret_cast<const double2*>(sx + k * kReRhs + 4 * q);
+            const double2 x23 = *reinterpret_cast<const double2*>(sx + k * kReRhs + 4 * q + 2);
+            const double xv[4] = {x01.x, x01.y, x23.x, x23.y};
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+#pragma unroll
+                for (int j = 0; j < 4; ++j) acc[i][j] = fma(av[i], xv[j], acc[i][j]);
+        }
+    }
+    cp_async_wait<0>();
+    // reduce the K slices through shared memory
+    __syncthreads();
+    double* red = re_sm;  // [kReSplit][kReRows][kReRhs]
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) red[(ks * kReRows + rg + 16 * i) * kReRhs + 4 * q + j] = acc[i][j];
+    __syncthreads();
+#pragma unroll
+    for (int o = 0; o < 4; ++o) {
+        const int e = t + 256 * o, rl = e >> 4, c = e & 15;
+        const int row = r0 + rl;
+        if (row >= a.n || c >= nc) continue;
+        double sum = 0.0;
+#pragma unroll
+        for (int p = 0; p < kReSplit; ++p) sum += red[(p * kReRows + rl) * kReRhs + c];
+        const int64_t gc = cb + c;
+        const double bv = a.B[(int64_t)row * a.ldb + gc];
+        const double xv = a.X[(int64_t)row * a.ldx + gc];
+        const double rv = bv - sum;
+        a.r32[(int64_t)a.pinv[row] * a.ldr + gc] = (float)rv;
+        atomicMax(&s_n[c], (unsigned long long)__double_as_longlong(fabs(rv)));
+        atomicMax(&s_n[kReRhs + c], (unsigned long long)__double_as_longlong(fabs(xv)));
+        atomicMax(&s_n[2 * kReRhs + c], (unsigned long long)__double_as_longlong(fabs(bv)));
+    }
+    __syncthreads();
+    if (t < 3 * kReRhs) {
+        const int which = t / kReRhs, c = t - which * kReRhs;
+        if (c < nc) atomicMax(&a.nrm[which * a.nrhs + cb + c], s_n[t]);
+    }
+}
+
+// FP32 solve of the refinement: Xr (already permuted) <- U^-1 L^-1 Xr, X64 += Xr.
+int32_t ir_solve(Ctx* ctx, cudaStream_t st, const float* LU, int64_t ld, int64_t n, const F32Scratch& s, float* Xr,
+                 int64_t ldr, int64_t nrhs, double* X64, int64_t ldx) {
+    const int nblk = (int)ceil_div(n, kTrsvNB);
+    for (int64_t c0 = 0; c0 < nrhs; c0 += kTrMaxRhs) {
+        const int nc = (int)std::min<int64_t>(kTrMaxRhs, nrhs - c0);
+        TrArgs a{LU, ld, (int)n, s.linv, Xr, ldr, (int)c0, nc, X64, ldx, 0, (int)ceil_div(nc, kTrRhs), ctx->d_status};
+        for (int b = 0; b < nblk; ++b) {
+            const int rows = (int)(n - std::min<int64_t>(n, (int64_t)(b + 1) * kTrsvNB));
+            const int nu = b > 0 ? (int)ceil_div(rows, kTrRows) : 0;
+            prof_begin(ctx, st, kClsSolve);
+            trsv_block_kernel<<<a.nd + nu, 256, 0, st>>>(a, b);
+            prof_end(ctx, st, kClsSolve, 2.0 * kTrsvNB * (rows + kTrsvNB) * nc);
+            B2M_LAUNCHED(ctx);
+        }
+        a.upper = 1;
+        a.inv = s.uinv;
+        for (int b = nblk - 1; b >= 0; --b) {
+            const int rows = b * kTrsvNB;
+            const int nu = b < nblk - 1 ? (int)ceil_div(rows, kTrRows) : 0;
+            prof_begin(ctx, st, kClsSolve);
+            trsv_block_kernel<<<a.nd + nu, 256, 0, st>>>(a, b);
+            prof_end(ctx, st, kClsSolve, 2.0 * kTrsvNB * (rows + kTrsvNB) * nc);
+            B2M_LAUNCHED(ctx);
+        }
+    }
+    return B2M_OK;
+}
+
+double eta_from(const std::vector<unsigned long long>& h, int64_t nrhs, double normA) {
+    double eta = 0.0;
+    for (int64_t c = 0; c < nrhs; ++c) {
+        const double rn = __builtin_bit_cast(double, h[c]);
+        const double xn = __builtin_bit_cast(double, h[nrhs + c]);
+        const double bn = __builtin_bit_cast(double, h[2 * nrhs + c]);
+        const double den = normA * xn + bn;
+        eta = std::max(eta, den > 0 ? rn / den : (rn > 0 ? INFINITY : 0.0));
+    }
+    return eta;
 }
 
 }  // namespace
-
-// FP32 LU with tensor-core updates (graph-captured like the FP64 one)
-int32_t lu_factor_f32(Ctx* ctx, cudaStream_t st, float* A, int64_t ld, int64_t n, int32_t* ipiv, int32_t* perm,
-                      int mode, float* scratch, int64_t scratch_cap) {
-    if (n <= 0) return B2M_OK;
-    if ((ld & 3) || !aligned16(A)) return fail(ctx, B2M_ERR_DIM, "lu_factor_f32: ld must be a multiple of 4");
-    if (n > panel_max_rows(false, 32)) return fail(ctx, B2M_ERR_UNSUPPORTED, "mixed LU supports n <= 16384");
-    Split sp{scratch, scratch + scratch_cap, scratch + 2 * scratch_cap, scratch + 3 * scratch_cap, scratch_cap, mode};
-    const GraphKey key{3 + mode * 10, A, ipiv, perm, scratch, ld, n, scratch_cap, 0};
-    return run_graph(ctx, st, key, [&](cudaStream_t s) -> int32_t {
-        iota32_kernel<<<gsz(n), 256, 0, s>>>(perm, n);
-        B2M_LAUNCHED(ctx);
-        return lu_rec_f32(ctx, s, A, ld, n, 0, n, ipiv, perm, sp);
-    });
-}
-
-int32_t lu_solve_f32(Ctx* ctx, cudaStream_t st, const float* LU, int64_t ld, int64_t n, const int32_t* perm, float* B,
-                     int64_t ldb, int64_t nrhs, float* tmp, int mode, float* scratch, int64_t scratch_cap) {
-    Split sp{scratch, scratch + scratch_cap, scratch + 2 * scratch_cap, scratch + 3 * scratch_cap, scratch_cap, mode};
-    const GraphKey key{4 + mode * 10, LU, perm, B, tmp, ld, n, ldb, nrhs};
-    return run_graph(ctx, st, key, [&](cudaStream_t s) -> int32_t {
-        B2M_CU(ctx, cudaMemcpy2DAsync(tmp, ldb * 4, B, ldb * 4, nrhs * 4, n, cudaMemcpyDeviceToDevice, s));
-        gather_rows_f32_kernel<<<gsz(n * nrhs), 256, 0, s>>>(B, ldb, tmp, ldb, perm, n, nrhs);
-        B2M_LAUNCHED(ctx);
-        TriF t{LU, ld, n, B, ldb, 0, nrhs};
-        B2M_TRY(trsm_lower_f32(ctx, s, t, 0, 0, n, sp));
-        return trsm_upper_f32(ctx, s, t, 0, 0, n, sp);
-    });
-}
 
 // ------------------------------------------------------------------ the refinement driver
 int32_t solve_mixed(Ctx* ctx, cudaStream_t st, const double* A, int64_t lda, int64_t n, const double* B, int64_t ldb,
@@ -184,33 +446,35 @@ int32_t solve_mixed(Ctx* ctx, cudaStream_t st, const double* A, int64_t lda, int
         return fail(ctx, B2M_ERR_DIM, "solve_mixed: device operands need even strides and 16-byte alignment");
     const int64_t ld32 = round_up(n, 32);
     const int64_t ldr = round_up(nrhs, 4);
-    const int64_t cap = round_up(n, 32) * (round_up(n, 32) / 2 + 32);
-    // workspace layout: [A32 | split scratch x4] in kWsMatD, [r64] kWsF, [r32 | tmp32] kWsE, pivots kWsPiv,
+    // workspace layout: [A32 | factorisation scratch] kWsMatD, [r32] kWsE, [perm | pinv] kWsPiv,
     // norms kWsSmall
-    void *pD, *pF, *pE, *pP, *pS;
-    B2M_TRY(ws_get(ctx, kWsMatD, (size_t)(n * ld32 + 4 * cap) * sizeof(float), &pD));
-    B2M_TRY(ws_get(ctx, kWsF, (size_t)(n * ldr) * sizeof(double), &pF));
-    B2M_TRY(ws_get(ctx, kWsE, (size_t)(2 * n * ldr) * sizeof(float), &pE));
+    const size_t a32_bytes = (size_t)round_up(n * ld32 * (int64_t)sizeof(float), 256);
+    void *pD, *pE, *pP, *pS;
+    B2M_TRY(ws_get(ctx, kWsMatD, a32_bytes + f32_scratch_bytes(n), &pD));
+    B2M_TRY(ws_get(ctx, kWsE, (size_t)(n * ldr) * sizeof(float), &pE));
     B2M_TRY(ws_get(ctx, kWsPiv, (size_t)(2 * n) * sizeof(int32_t), &pP));
     B2M_TRY(ws_get(ctx, kWsSmall, (size_t)(4 + 3 * nrhs) * sizeof(unsigned long long), &pS));
     float* A32 = (float*)pD;
-    float* scratch = A32 + n * ld32;
-    double* R = (double*)pF;
+    const F32Scratch sc = f32_scratch_carve(static_cast<char*>(pD) + a32_bytes, n);
     float* r32 = (float*)pE;
-    float* t32 = r32 + n * ldr;
-    int32_t* ipiv = (int32_t*)pP;
-    int32_t* perm = ipiv + n;
+    int32_t* perm = (int32_t*)pP;
+    int32_t* pinv = perm + n;
     unsigned long long* nrm = (unsigned long long*)pS;
     std::vector<unsigned long long> h((size_t)(1 + 3 * nrhs));
 
     MixedReport local{};
     if (!rep) rep = &local;
     *rep = MixedReport{};
+    static bool attr = false;
+    if (!attr) {
+        B2M_CU(ctx, cudaFuncSetAttribute(resid_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kReSmem));
+        attr = true;
+    }
 
     B2M_CU(ctx, cudaMemsetAsync(ctx->d_status, 0, kNumStatus * sizeof(int32_t), st));
     f64_to_f32_kernel<<<gsz(n * n), 256, 0, st>>>(A, lda, A32, ld32, n, n);
     B2M_LAUNCHED(ctx);
-    B2M_TRY(lu_factor_f32(ctx, st, A32, ld32, n, ipiv, perm, mode, scratch, cap));
+    B2M_TRY(lu_factor_f32(ctx, st, A32, ld32, n, perm, mode, sc));
     B2M_CU(ctx, cudaMemsetAsync(nrm, 0, sizeof(unsigned long long), st));
     norm_inf_kernel<<<gsz(n, 8), 256, 0, st>>>(A, lda, n, nrm);
     B2M_LAUNCHED(ctx);
@@ -222,37 +486,30 @@ int32_t solve_mixed(Ctx* ctx, cudaStream_t st, const double* A, int64_t lda, int
 
     bool converged = false;
     if (ctx->h_status[kInfo] == 0) {
-        // x = 0, r = b
-        B2M_CU(ctx, cudaMemset2DAsync(X, ldx * 8, 0, nrhs * 8, n, st));
-        B2M_TRY(copy_matrix(ctx, st, R, ldr * 8, B, ldb * 8, n, nrhs));
+        invert_perm_kernel<<<gsz(n), 256, 0, st>>>(perm, pinv, n);
+        B2M_LAUNCHED(ctx);
+        ir_init_kernel<<<gsz(n * nrhs), 256, 0, st>>>(B, ldb, perm, r32, ldr, X, ldx, n, nrhs);
+        B2M_LAUNCHED(ctx);
+        // one refinement step: d = (LU)^-1 P r in FP32, x += d, r = b - A x in FP64 (and P r in FP32)
+        const GraphKey key{5 + mode * 10, A32, X, B, A, ld32, n, nrhs, lda * 1000003 + ldb * 1009 + ldx};
+        auto step = [&](cudaStream_t q) -> int32_t {
+            B2M_TRY(ir_solve(ctx, q, A32, ld32, n, sc, r32, ldr, nrhs, X, ldx));
+            B2M_CU(ctx, cudaMemsetAsync(nrm + 1, 0, 3 * nrhs * sizeof(unsigned long long), q));
+            ReArgs ra{A, lda, X, ldx, B, ldb, (int)n, (int)nrhs, r32, ldr, pinv, nrm + 1};
+            prof_begin(ctx, q, kClsGemm);
+            resid_kernel<<<dim3((unsigned)ceil_div(n, kReRows), (unsigned)ceil_div(nrhs, kReRhs)), 256, kReSmem, q>>>(ra);
+            prof_end(ctx, q, kClsGemm, 2.0 * n * n * nrhs);
+            B2M_LAUNCHED(ctx);
+            return B2M_OK;
+        };
         double prev = INFINITY;
         for (int it = 0; it < max_iter; ++it) {
-            // d = (LU)^{-1} P r in FP32, x += d
-            f64_to_f32_kernel<<<gsz(n * nrhs), 256, 0, st>>>(R, ldr, r32, ldr, n, nrhs);
-            B2M_LAUNCHED(ctx);
-            B2M_TRY(lu_solve_f32(ctx, st, A32, ld32, n, perm, r32, ldr, nrhs, t32, mode, scratch, cap));
-            add_f32_to_f64_kernel<<<gsz(n * nrhs), 256, 0, st>>>(X, ldx, r32, ldr, n, nrhs);
-            B2M_LAUNCHED(ctx);
-            // r = b - A x in FP64
-            B2M_TRY(copy_matrix(ctx, st, R, ldr * 8, B, ldb * 8, n, nrhs));
-            DOperand a{A, lda, n, n, 0, 0, true};
-            DOperand b{X, ldx, n, nrhs, 0, 0, false};
-            B2M_TRY(dgemm_tiled(ctx, st, a, b, R, ldr, n, nrhs, n, B2M_DO_SUB, false));
-            // normwise backward error per column
-            B2M_CU(ctx, cudaMemsetAsync(nrm + 1, 0, 3 * nrhs * sizeof(unsigned long long), st));
-            colmax3_kernel<<<gsz(n * nrhs), 256, 0, st>>>(R, ldr, X, ldx, B, ldb, n, nrhs, nrm + 1);
-            B2M_LAUNCHED(ctx);
+            B2M_TRY(run_graph(ctx, st, key, step));
             B2M_CU(ctx, cudaMemcpyAsync(h.data() + 1, nrm + 1, 3 * nrhs * sizeof(unsigned long long),
                                         cudaMemcpyDeviceToHost, st));
             B2M_CU(ctx, cudaStreamSynchronize(st));
-            double eta = 0.0;
-            for (int64_t c = 0; c < nrhs; ++c) {
-                const double rn = __builtin_bit_cast(double, h[1 + c]);
-                const double xn = __builtin_bit_cast(double, h[1 + nrhs + c]);
-                const double bn = __builtin_bit_cast(double, h[1 + 2 * nrhs + c]);
-                const double den = normA * xn + bn;
-                eta = std::max(eta, den > 0 ? rn / den : (rn > 0 ? INFINITY : 0.0));
-            }
+            std::vector<unsigned long long> hv(h.begin() + 1, h.end());
+            const double eta = eta_from(hv, nrhs, normA);
             rep->iterations = it + 1;
             rep->backward_error = eta;
             rep->ir_backward_error = eta;
@@ -309,14 +566,8 @@ int32_t solve_plain_f64(Ctx* ctx, cudaStream_t st, const double* A, int64_t lda,
         B2M_CU(ctx, cudaMemcpyAsync(h.data(), nrm, h.size() * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
         B2M_CU(ctx, cudaStreamSynchronize(st));
         const double normA = __builtin_bit_cast(double, h[0]);
-        double eta = 0.0;
-        for (int64_t c = 0; c < nrhs; ++c) {
-            const double den = normA * __builtin_bit_cast(double, h[1 + nrhs + c]) +
-                               __builtin_bit_cast(double, h[1 + 2 * nrhs + c]);
-            const double rn = __builtin_bit_cast(double, h[1 + c]);
-            eta = std::max(eta, den > 0 ? rn / den : 0.0);
-        }
-        rep->backward_error = eta;
+        std::vector<unsigned long long> hv(h.begin() + 1, h.end());
+        rep->backward_error = eta_from(hv, nrhs, normA);
     }
     return B2M_OK;
 }

@@ -437,13 +437,11 @@ int32_t launch_panel(Ctx* ctx, cudaStream_t st, T* P, int64_t ld, int m, int w, 
         if (C > kPMaxC) return fail(ctx, B2M_ERR_UNSUPPORTED, "FP64 panel of %d rows is too tall", m);
         return launch_push<T, 16, 4>(ctx, st, C, (int)ceil_div(m, C), P, ld, m, w, row_base, col_base, ipiv);
     } else {
-        const int C = (int)ceil_div(m, kPT * 4);
-        if (C > kPMaxC) return fail(ctx, B2M_ERR_UNSUPPORTED, "FP32 panel of %d rows is too tall", m);
-        return launch_push<T, 32, 4>(ctx, st, C, (int)ceil_div(m, C), P, ld, m, w, row_base, col_base, ipiv);
+        static_assert(sizeof(T) == 8, "the cluster panel is instantiated for FP64 only");
+        return B2M_ERR_UNSUPPORTED;
     }
 }
 
 template int32_t launch_panel<double>(Ctx*, cudaStream_t, double*, int64_t, int, int, int, int, int32_t*);
-template int32_t launch_panel<float>(Ctx*, cudaStream_t, float*, int64_t, int, int, int, int, int32_t*);
 
 }  // namespace b2m

@@ -12,7 +12,10 @@
 // CTA: 6 warps.  Warps 0-3: epilogue (warp w reads TMEM lanes 32w..32w+31), warp 4: TMA producer,
 // warp 5: TMEM allocation and the single MMA-issuing thread.  Tile 128 x 128, k-step 32 floats
 // (one 128-byte swizzle row), 4 MMAs of K = 8 per k-step; stages guarded by mbarriers, smem
-// stages released by tcgen05.commit.
+// stages released by tcgen05.commit.  Epilogue: TMEM -> registers -> 128-byte-swizzled staging
+// tiles in the (then idle) stage memory -> TMA tensor store (op none) or TMA reduce-add (op add,
+// and op sub with the accumulator negated), so C is never read by the SM and every global write
+// is a full 128-byte line.
 #include "common.cuh"
 #include "kernels.cuh"
 
@@ -25,6 +28,7 @@ constexpr int kTcThreads = 192;
 
 struct TcArgs {
     int M, N, K;
+    int c_x0, c_y0;
     int a_x0, a_y0, b_x0, b_y0;
     float* C;
     int64_t ldc;
@@ -84,7 +88,8 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&r)[16]) {
 template <int SPLIT>
 __global__ void __launch_bounds__(kTcThreads, 1)
     sgemm_tc_kernel(const __grid_constant__ CUtensorMap tmAh, const __grid_constant__ CUtensorMap tmAl,
-                    const __grid_constant__ CUtensorMap tmBh, const __grid_constant__ CUtensorMap tmBl, TcArgs p) {
+                    const __grid_constant__ CUtensorMap tmBh, const __grid_constant__ CUtensorMap tmBl,
+                    const __grid_constant__ CUtensorMap tmC, TcArgs p) {
     constexpr int NOPS = SPLIT == 3 ? 4 : 2;            // operand tiles per stage
     constexpr int STAGES = SPLIT == 3 ? 3 : 5;
     constexpr int kStage = NOPS * kTileB;
@@ -173,27 +178,48 @@ __global__ void __launch_bounds__(kTcThreads, 1)
             umma_commit(&acc_bar);  // accumulator complete
         }
     } else {
-        // epilogue warps 0-3: TMEM lanes 32w..32w+31 = tile rows
+        // epilogue warps 0-3: TMEM lanes 32w..32w+31 = tile rows.  Column group cg (32 columns) of
+        // row r goes to staging tile cg, 128-byte row r, 16-byte chunk j at position j ^ (r & 7).
         if (mbar_wait(&acc_bar, 0, &p.status[kTimeout], 303)) {
             tc_fence_after();
-            const int row = tm * TBM + warp * 32 + lane;
-            float* crow = p.C + (int64_t)row * p.ldc;
+            const int r = warp * 32 + lane;
+            const float sgn = p.op == B2M_DO_SUB ? -1.0f : 1.0f;
 #pragma unroll 1
-            for (int c0 = 0; c0 < TBN; c0 += 16) {
-                uint32_t r[16];
-                tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, r);
-                if (row < p.M) {
+            for (int cg = 0; cg < TBN / 32; ++cg) {
+                uint32_t v[32];
+                tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(cg * 32), *reinterpret_cast<uint32_t(*)[16]>(v));
+                tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(cg * 32 + 16),
+                          *reinterpret_cast<uint32_t(*)[16]>(v + 16));
+                uint8_t* tile = smem + cg * (TBM * 128);
 #pragma unroll
-                    for (int e = 0; e < 16; ++e) {
-                        const int col = tn * TBN + c0 + e;
-                        if (col < p.N) {
-                            const float v = __uint_as_float(r[e]);
-                            if (p.op == B2M_DO_NONE) crow[col] = v;
-                            else if (p.op == B2M_DO_ADD) crow[col] = crow[col] + v;
-                            else crow[col] = crow[col] - v;
-                        }
-                    }
+                for (int j = 0; j < 8; ++j) {
+                    const float4 f = make_float4(sgn * __uint_as_float(v[4 * j]), sgn * __uint_as_float(v[4 * j + 1]),
+                                                 sgn * __uint_as_float(v[4 * j + 2]), sgn * __uint_as_float(v[4 * j + 3]));
+                    *reinterpret_cast<float4*>(tile + r * 128 + ((j ^ (r & 7)) << 4)) = f;
                 }
+            }
+            fence_proxy_async();
+            asm volatile("bar.sync 1, 128;\n" ::: "memory");  // the four epilogue warps
+            if (threadIdx.x == 0) {
+                for (int cg = 0; cg < TBN / 32; ++cg) {
+                    const int x = p.c_x0 + tn * TBN + cg * 32, y = p.c_y0 + tm * TBM;
+                    if (tn * TBN + cg * 32 >= p.N) break;
+                    const uint32_t src = smem_u32(smem + cg * (TBM * 128));
+                    if (p.op == B2M_DO_NONE)
+                        asm volatile(
+                            "cp.async.bulk.tensor.2d.global.shared::cta.tile.bulk_group [%0, {%1, %2}], [%3];\n" ::"l"(
+                                reinterpret_cast<uint64_t>(&tmC)),
+                            "r"(x), "r"(y), "r"(src)
+                            : "memory");
+                    else
+                        asm volatile(
+                            "cp.reduce.async.bulk.tensor.2d.global.shared::cta.add.tile.bulk_group [%0, {%1, %2}], "
+                            "[%3];\n" ::"l"(reinterpret_cast<uint64_t>(&tmC)),
+                            "r"(x), "r"(y), "r"(src)
+                            : "memory");
+                }
+                asm volatile("cp.async.bulk.commit_group;\n" ::: "memory");
+                asm volatile("cp.async.bulk.wait_group 0;\n" ::: "memory");
             }
         }
     }
@@ -243,6 +269,7 @@ int32_t launch_tc(Ctx* ctx, cudaStream_t st, const CUtensorMap* maps, const TcAr
     constexpr int NOPS = SPLIT == 3 ? 4 : 2;
     constexpr int STAGES = SPLIT == 3 ? 3 : 5;
     constexpr int smem = STAGES * NOPS * kTileB + 1024;
+    static_assert(STAGES * NOPS * kTileB >= (TBN / 32) * TBM * 128, "epilogue staging must fit in the stages");
     static bool attr = false;
     if (!attr) {
         B2M_CU(ctx, cudaFuncSetAttribute(sgemm_tc_kernel<SPLIT>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
@@ -250,7 +277,7 @@ int32_t launch_tc(Ctx* ctx, cudaStream_t st, const CUtensorMap* maps, const TcAr
     }
     const int tiles = (int)(ceil_div(a.M, TBM) * ceil_div(a.N, TBN));
     prof_begin(ctx, st, kClsTcGemm);
-    sgemm_tc_kernel<SPLIT><<<tiles, kTcThreads, smem, st>>>(maps[0], maps[1], maps[2], maps[3], a);
+    sgemm_tc_kernel<SPLIT><<<tiles, kTcThreads, smem, st>>>(maps[0], maps[1], maps[2], maps[3], maps[4], a);
     prof_end(ctx, st, kClsTcGemm, 2.0 * a.M * a.N * a.K * SPLIT);
     B2M_LAUNCHED(ctx);
     return B2M_OK;
@@ -278,7 +305,10 @@ int32_t sgemm_tc(Ctx* ctx, cudaStream_t st, const FOperand& Ah, const float* Al_
     if ((Ah.c0 & 3) || (Bh.c0 & 3) || (Ah.ld & 3) || (Bh.ld & 3))
         return fail(ctx, B2M_ERR_DIM, "sgemm_tc: TMA origins/strides must be multiples of 4 floats");
     if (split == 3 && (!Al_base || !Bl_base)) return fail(ctx, B2M_ERR_ARG, "sgemm_tc: 3xTF32 needs lo operands");
-    CUtensorMap maps[4];
+    if (!aligned16(C) || (ldc & 3)) return fail(ctx, B2M_ERR_DIM, "sgemm_tc: C must be 16-byte aligned, ldc % 4 == 0");
+    CUtensorMap maps[5];
+    B2M_TRY(encode_tmap_2d(ctx, &maps[4], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, C, N, M, ldc * 4, 32, TBM,
+                           CU_TENSOR_MAP_SWIZZLE_128B));
     B2M_TRY(encode_tmap_2d(ctx, &maps[0], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, Ah.base, Ah.cols, Ah.rows, Ah.ld * 4,
                            TBK, TBM, CU_TENSOR_MAP_SWIZZLE_128B));
     B2M_TRY(encode_tmap_2d(ctx, &maps[2], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, Bh.base, Bh.cols, Bh.rows, Bh.ld * 4,
@@ -294,6 +324,7 @@ int32_t sgemm_tc(Ctx* ctx, cudaStream_t st, const FOperand& Ah, const float* Al_
     }
     TcArgs a;
     a.M = (int)M; a.N = (int)N; a.K = (int)K;
+    a.c_x0 = 0; a.c_y0 = 0;
     a.a_x0 = (int)Ah.c0; a.a_y0 = (int)Ah.r0;
     a.b_x0 = (int)Bh.c0; a.b_y0 = (int)Bh.r0;
     a.C = C; a.ldc = ldc; a.op = op; a.split = split;

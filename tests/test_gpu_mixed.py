@@ -26,6 +26,24 @@ def test_mixed_solve_reaches_fp64_backward_error(ctx, n, k, mode):
         assert rep["fell_back"] == 0
 
 
+@pytest.mark.parametrize("n,k", [(257, 2), (513, 5), (4100, 16), (8500, 4)])
+def test_mixed_solve_ragged_and_tall(ctx, n, k):
+    """Ragged leaves and outer panels (n not a multiple of 32 / 256) and, at n = 8500, a
+    tournament tree with two merge levels (17 chunks of 512 rows)."""
+    import torch
+    g = torch.Generator(device="cuda").manual_seed(n)
+    A = torch.rand((n, n), generator=g, device="cuda", dtype=torch.float64) - 0.5
+    A += torch.eye(n, device="cuda", dtype=torch.float64) * 2.0
+    B = torch.randn((n, k), generator=g, device="cuda", dtype=torch.float64)
+    X = torch.empty_like(B)
+    st, rep = L.dev_MatrixLinEQSolveMixed(A, B, X, mode=_lib.MIXED_3XTF32, ctx=ctx)
+    torch.cuda.synchronize()
+    assert st == 0 and rep["fell_back"] == 0, rep
+    a, b, x = A.cpu().numpy(), B.cpu().numpy(), X.cpu().numpy()
+    eta = oracle.backward_error(a, x, b)
+    assert eta <= n * 2.0 ** -53, (eta, rep)
+
+
 @pytest.mark.parametrize("kappa", [1e2, 1e4, 1e5])
 def test_mixed_solve_kappa_family(ctx, kappa):
     """The benchmark's construction A = U diag(s) V^T at n = 1024."""
