@@ -34,7 +34,7 @@ METRIC = "LU-solve GFLOP/s at n=8192 to FP64 backward error: mixed-precision IR 
 def parse():
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
-    p.add_argument("--steps", type=int, default=5)
+    p.add_argument("--steps", type=int, default=20)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", choices=["b200", "reference"], default="b200")
     p.add_argument("--form", choices=["mixed", "plain"], default=None)
@@ -43,13 +43,14 @@ def parse():
     p.add_argument("--kappa", type=float, default=KAPPA_DEFAULT)
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu", action="store_true")
+    p.add_argument("--no-plain", action="store_true", help="skip the plain FP64 comparison steps")
     p.add_argument("--cpu-n", type=int, default=4096, help="order of the CPU-baseline sample")
     return p.parse_args()
 
 
 # ----------------------------------------------------------------------------- clocks
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons, sampled every 200 ms during the timed region."""
+    """nvidia-smi clocks and throttle reasons, sampled every 100 ms during the timed region."""
 
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
@@ -64,7 +65,7 @@ class ClockSampler:
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
-                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
         except Exception:
@@ -291,31 +292,50 @@ def run_b200(args, world, rank, local):
                "backward_error": eta_e2e, "api": "b2m_MatrixLinEQSolve" + ("Mixed" if form == "mixed" else "")}
         del hA, hB, hX
 
-    # ---- roofline of the dominant kernel class (by device time in the timed region)
-    dom = max(prof.items(), key=lambda kv: kv[1]["ms"])
-    dom_name, d = dom
-    peak_f64 = fp64_peak_tflops()
+    # ---- plain FP64 drop-in on the same system (the comparison the metric names)
+    plain = None
+    if form == "mixed" and not args.no_plain:
+        for _ in range(2):
+            L.dev_MatrixLinEQSolve(A, B, X, status=status, ctx=ctx)
+        torch.cuda.synchronize()
+        p0, p1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        p0.record()
+        for _ in range(args.steps):
+            L.dev_MatrixLinEQSolve(A, B, X, status=status, ctx=ctx)
+        p1.record()
+        torch.cuda.synchronize()
+        pms = max_over_ranks(world, p0.elapsed_time(p1))
+        pv = args.steps * world * flops / (pms / 1e3) / 1e9
+        plain = {"value": pv, "unit": "GFLOP/s", "ms_per_step": pms / args.steps,
+                 "backward_error": backward_error_torch(A, X, B), "mixed_over_plain": value / pv}
+
+    # ---- roofline of the dominant kernel class (by device time in the profiled pass).  The profiler
+    # records FLOPs for the tensor-core GEMM classes and HBM bytes for every other class.
+    dom_name, d = max(prof.items(), key=lambda kv: kv[1]["ms"])
     peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))) if os.path.exists(
         os.path.join(ROOT, "MEASURED_PEAKS.json")) else {}
-    if dom_name in ("gemm_f64", "panel", "trsm"):
-        achieved = d["work"] / (d["ms"] / 1e3) / 1e12 if d["ms"] > 0 else 0.0
-        roof = {"kernel_class": dom_name, "bound": "tensor", "achieved": achieved, "peak": peak_f64,
-                "unit": "TFLOP/s", "frac": achieved / peak_f64, "traffic": None,
-                "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (MEASURED_PEAKS.json has no FP64 figure)",
-                "launches": d["launches"], "share": d["ms"] / max(1e-9, sum(v["ms"] for v in prof.values()))}
+    avg_s = d["ms"] / 1e3 / max(1, d["launches"])
+    per_launch = d["work"] / max(1, d["launches"])
+    share = d["ms"] / max(1e-9, sum(v["ms"] for v in prof.values()))
+    if dom_name == "gemm_f64":
+        pk = fp64_peak_tflops()
+        achieved = per_launch / avg_s / 1e12
+        roof = {"bound": "tensor", "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (of measured)"}
+        unit = "TFLOP/s"
     elif dom_name == "gemm_tc":
         pk = peaks.get("bf16_tflops", 1590.0) / 2.0
-        achieved = d["work"] / (d["ms"] / 1e3) / 1e12 if d["ms"] > 0 else 0.0
-        roof = {"kernel_class": dom_name, "bound": "tensor", "achieved": achieved, "peak": pk, "unit": "TFLOP/s",
-                "frac": achieved / pk, "traffic": None,
-                "peak_source": "TF32 dense = half of measured bf16_tflops (MEASURED_PEAKS.json)",
-                "launches": d["launches"]}
+        achieved = per_launch / avg_s / 1e12
+        roof = {"bound": "tensor", "peak_source": "TF32 dense = half of measured bf16_tflops (of measured)"}
+        unit = "TFLOP/s"
     else:
-        bw = peaks.get("hbm_gbs", 6650.0)
-        achieved = d["work"] / (d["ms"] / 1e3) / 1e9 if d["ms"] > 0 else 0.0
-        roof = {"kernel_class": dom_name, "bound": "hbm", "achieved": achieved, "peak": bw, "unit": "GB/s",
-                "frac": achieved / bw, "traffic": None, "peak_source": "MEASURED_PEAKS.json hbm_gbs",
-                "launches": d["launches"]}
+        pk = peaks.get("hbm_gbs", 6650.0)
+        achieved = per_launch / avg_s / 1e9
+        roof = {"bound": "hbm", "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if "hbm_gbs" in peaks
+                else "fallback 6650 GB/s (of fallback)"}
+        unit = "GB/s"
+    roof.update({"kernel_class": dom_name, "achieved": achieved, "peak": pk, "unit": unit, "frac": achieved / pk,
+                 "traffic": None, "launches": d["launches"], "avg_launch_us": avg_s * 1e6,
+                 "work_per_launch": per_launch, "share_of_device_time": share})
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -335,7 +355,7 @@ def run_b200(args, world, rank, local):
                        "kappa": args.kappa, "form": form, "parallelism": f"replicas x{world}",
                        "l2": "A (512 MiB) exceeds L2; no flush needed"},
             "backward_error": eta, "backward_error_bound": n * 2.0 ** -53,
-            "e2e": e2e, "gpu_launches": launches, "roofline": roof, "cpu_baseline": cpu,
+            "e2e": e2e, "gpu_launches": launches, "roofline": roof, "cpu_baseline": cpu, "plain_fp64": plain,
             "kernel_classes": {kname: {"launches": v["launches"], "ms": round(v["ms"], 4)}
                                for kname, v in prof.items() if v["launches"]},
             "clocks": clk.summary(),

@@ -71,7 +71,8 @@ B2M_API const char* b2m_status_string(int32_t status);
 B2M_API int64_t     b2m_kernel_launches(b2m_ctx* ctx);
 /* Event profiler: when enabled, every launch is bracketed by CUDA events on its own stream and
  * its algorithmic work is recorded per kernel class (0 FP64 GEMM, 1 panel, 2 row swaps,
- * 3 triangular solve, 4 tensor-core GEMM, 5 solve/refinement kernels, 6 other).  Enabling (or
+ * 3 triangular solve, 4 tensor-core GEMM, 5 solve/refinement kernels, 6 other, e.g. the FP64
+ * residual).  Work is FLOPs for classes 0 and 4 and HBM bytes for the others.  Enabling (or
  * disabling) resets the counters.  Reading synchronizes the device. */
 B2M_API int32_t     b2m_profile(b2m_ctx* ctx, int32_t enable);
 B2M_API int32_t     b2m_profile_read(b2m_ctx* ctx, int32_t kernel_class, int64_t* launches, double* ms,

@@ -44,7 +44,10 @@ enum WsSlot : int {
     kNumWs
 };
 
-// kernel classes for the optional event profiler (b2m_profile / b2m_profile_read)
+// kernel classes for the optional event profiler (b2m_profile / b2m_profile_read).  The work
+// recorded with each launch is algorithmic: FLOPs for the tensor-core GEMM classes (gemm_f64,
+// gemm_tc -- for gemm_tc the MMA passes of a split mode are counted), bytes that must cross HBM for
+// every other class (panel, row moves, triangular solves, the residual under `other`).
 enum KernelClass : int { kClsGemm = 0, kClsPanel, kClsSwap, kClsTrsm, kClsTcGemm, kClsSolve, kClsOther, kNumCls };
 
 struct Prof {

@@ -268,7 +268,7 @@ int32_t launch_trsm_small_impl(Ctx* ctx, cudaStream_t st, const T* L, int64_t ld
     const int blocks = (int)ceil_div(ncols, (kTrsmThreads / 32) * kTrsmCpw);
     prof_begin(ctx, st, kClsTrsm);
     trsm_small_kernel<T><<<blocks, kTrsmThreads, 0, st>>>(L, ldl, B, ldb, k, ncols, upper ? 1 : 0, ctx->d_status);
-    prof_end(ctx, st, kClsTrsm, (double)k * k * ncols);
+    prof_end(ctx, st, kClsTrsm, (double)sizeof(T) * (k * k + 2.0 * k * ncols));  // bytes
     B2M_LAUNCHED(ctx);
     return B2M_OK;
 }

@@ -665,7 +665,7 @@ int32_t lu_factor_f32(Ctx* ctx, cudaStream_t st, float* A, int64_t ld, int64_t n
                           s.moves, ctx->d_status};
                 prof_begin(ctx, q, kClsPanel);
                 tslu_select_kernel<<<(unsigned)ceil_div(n - lc0, kTsRows), kTsThreads, 0, q>>>(ta);
-                prof_end(ctx, q, kClsPanel, 2.0 * (n - lc0) * w * w);
+                prof_end(ctx, q, kClsPanel, 4.0 * (n - lc0) * 32);  // bytes: the leaf's columns, read once
                 B2M_LAUNCHED(ctx);
                 ApArgs aa{A, ld, (int)n, (int)lc0, w, (int)oc0, pw, s.top, s.mvals, s.wmat, s.moves, perm,
                           ctx->d_status, 0};
@@ -673,7 +673,8 @@ int32_t lu_factor_f32(Ctx* ctx, cudaStream_t st, float* A, int64_t ld, int64_t n
                 const int nC = (int)ceil_div(n - pw, 256);
                 prof_begin(ctx, q, kClsSwap);
                 tslu_apply_kernel<<<aa.nR + nC, 256, 0, q>>>(aa);
-                prof_end(ctx, q, kClsSwap, 2.0 * (n - lc0) * w * (pw - (lc0 - oc0)));
+                // bytes: the panel rows read and written, plus <= 64 row moves outside the panel
+                prof_end(ctx, q, kClsSwap, 8.0 * (n - lc0) * (pw - (lc0 - oc0)) + 8.0 * 64 * (n - pw));
                 B2M_LAUNCHED(ctx);
             }
             const int64_t c1 = oc0 + pw;
@@ -683,7 +684,8 @@ int32_t lu_factor_f32(Ctx* ctx, cudaStream_t st, float* A, int64_t ld, int64_t n
             const int nL = mode == 3 ? (int)ceil_div(M * pw, 1024) : 0;
             prof_begin(ctx, q, kClsTrsm);
             lu_outer_kernel<<<oa.nU + nL, 256, ou_smem, q>>>(oa);
-            prof_end(ctx, q, kClsTrsm, (double)pw * pw * M);
+            // bytes: U12 read and written, the GEMM copies of U12 (and of L21 for 3xTF32) written
+            prof_end(ctx, q, kClsTrsm, 8.0 * pw * M + 4.0 * M * pw * (mode == 3 ? 5 : 1));
             B2M_LAUNCHED(ctx);
             FOperand bh{s.bth, pw, M, pw, 0, 0};
             float* C = A + c1 * ld + c1;

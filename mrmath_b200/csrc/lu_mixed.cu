@@ -407,7 +407,7 @@ int32_t ir_solve(Ctx* ctx, cudaStream_t st, const float* LU, int64_t ld, int64_t
             const int nu = b > 0 ? (int)ceil_div(rows, kTrRows) : 0;
             prof_begin(ctx, st, kClsSolve);
             trsv_block_kernel<<<a.nd + nu, 256, 0, st>>>(a, b);
-            prof_end(ctx, st, kClsSolve, 2.0 * kTrsvNB * (rows + kTrsvNB) * nc);
+            prof_end(ctx, st, kClsSolve, 4.0 * kTrsvNB * (rows + kTrsvNB) + 8.0 * (rows + kTrsvNB) * nc);
             B2M_LAUNCHED(ctx);
         }
         a.upper = 1;
@@ -417,7 +417,7 @@ int32_t ir_solve(Ctx* ctx, cudaStream_t st, const float* LU, int64_t ld, int64_t
             const int nu = b < nblk - 1 ? (int)ceil_div(rows, kTrRows) : 0;
             prof_begin(ctx, st, kClsSolve);
             trsv_block_kernel<<<a.nd + nu, 256, 0, st>>>(a, b);
-            prof_end(ctx, st, kClsSolve, 2.0 * kTrsvNB * (rows + kTrsvNB) * nc);
+            prof_end(ctx, st, kClsSolve, 4.0 * kTrsvNB * (rows + kTrsvNB) + 8.0 * (rows + kTrsvNB) * nc);
             B2M_LAUNCHED(ctx);
         }
     }
@@ -496,9 +496,9 @@ int32_t solve_mixed(Ctx* ctx, cudaStream_t st, const double* A, int64_t lda, int
             B2M_TRY(ir_solve(ctx, q, A32, ld32, n, sc, r32, ldr, nrhs, X, ldx));
             B2M_CU(ctx, cudaMemsetAsync(nrm + 1, 0, 3 * nrhs * sizeof(unsigned long long), q));
             ReArgs ra{A, lda, X, ldx, B, ldb, (int)n, (int)nrhs, r32, ldr, pinv, nrm + 1};
-            prof_begin(ctx, q, kClsGemm);
+            prof_begin(ctx, q, kClsOther);
             resid_kernel<<<dim3((unsigned)ceil_div(n, kReRows), (unsigned)ceil_div(nrhs, kReRhs)), 256, kReSmem, q>>>(ra);
-            prof_end(ctx, q, kClsGemm, 2.0 * n * n * nrhs);
+            prof_end(ctx, q, kClsOther, 8.0 * n * n + 8.0 * 3 * n * nrhs);  // bytes: A once, B, X, r
             B2M_LAUNCHED(ctx);
             return B2M_OK;
         };

@@ -409,9 +409,7 @@ int32_t launch_push(Ctx* ctx, cudaStream_t st, int C, int R, T* P, int64_t ld, i
         return fail(ctx, B2M_ERR_UNSUPPORTED, "panel cluster of %d CTAs cannot be scheduled", C);
     prof_begin(ctx, st, kClsPanel);
     B2M_CU(ctx, cudaLaunchKernelEx(&cfg, kern, P, ld, m, w, R, row_base, col_base, ipiv, ctx->d_status));
-    double fl = 0.0;
-    for (int j = 0; j < w; ++j) fl += 2.0 * (m - j - 1) * (w - j - 1) + (m - j - 1);
-    prof_end(ctx, st, kClsPanel, fl);
+    prof_end(ctx, st, kClsPanel, 2.0 * m * w * sizeof(T));  // bytes: the panel read and written once
     B2M_LAUNCHED(ctx);
     return B2M_OK;
 }
