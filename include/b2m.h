@@ -146,6 +146,23 @@ B2M_API int32_t b2m_dev_MatrixLinEQSolveMixed(b2m_ctx* ctx, const double* A, int
                                               int64_t Width2, int32_t mode, int32_t maxIter, double tol,
                                               b2m_solve_report* report);
 
+/* SolveLinEQAdjoint.  No counterpart in the reference: the adjoint (reverse-mode derivative) of
+ * MatrixLinEQSolve (LinAlgLU.pas:481-592).  From the factors of b2m_MatrixLUDecomp (LUDecomp and the
+ * reference-format interchange vector indx), the solution X (width x nrhs) of A X = B and a seed
+ * G = dLoss/dX, computes Lambda = A^{-T} G (= dLoss/dB) and, when dA is not NULL, the rank-nrhs
+ * update dA = -Lambda X^T (op B2M_DO_NONE) or dA -= Lambda X^T (op B2M_DO_ADD, to accumulate).
+ * Strides in bytes. */
+B2M_API int32_t b2m_MatrixLinEQSolveAdjoint(b2m_ctx* ctx, const double* LUDecomp, int64_t LineWidthLU, int64_t width,
+                                    const int32_t* indx, const double* X, int64_t LineWidthX, const double* G,
+                                    int64_t LineWidthG, int64_t nrhs, double* Lambda, int64_t LineWidthLambda,
+                                    double* dA, int64_t LineWidthdA, int32_t op);
+/* Device twin: every pointer is device memory (indx as produced by b2m_dev_MatrixLUDecompInPlace);
+ * asynchronous on the context's stream. */
+B2M_API int32_t b2m_dev_MatrixLinEQSolveAdjoint(b2m_ctx* ctx, const double* LUDecomp, int64_t LineWidthLU,
+                                        int64_t width, const int32_t* indx, const double* X, int64_t LineWidthX,
+                                        const double* G, int64_t LineWidthG, int64_t nrhs, double* Lambda,
+                                        int64_t LineWidthLambda, double* dA, int64_t LineWidthdA, int32_t op);
+
 /* Allocation-free solve.  No counterpart in the reference: it exists for callers that may not
  * allocate device memory (a host program whose memory manager owns all device allocations, code
  * running inside a stream capture, a real-time loop with a fixed budget).  Same arguments and

@@ -572,3 +572,70 @@ extern "C" int32_t b2m_MatrixLinEQSolveMixed(b2m_ctx* h, const double* A, int64_
     B2M_TRY(download(ctx, X, LineWidthX, (double*)pxx, ldb, n, Width2));
     return finish(ctx);
 }
+
+// ------------------------------------------------------------------ adjoint solve (SolveLinEQAdjoint)
+extern "C" int32_t b2m_dev_MatrixLinEQSolveAdjoint(b2m_ctx* h, const double* LUDecomp, int64_t LineWidthLU,
+                                                   int64_t width, const int32_t* indx, const double* X,
+                                                   int64_t LineWidthX, const double* G, int64_t LineWidthG,
+                                                   int64_t nrhs, double* Lambda, int64_t LineWidthLambda, double* dA,
+                                                   int64_t LineWidthdA, int32_t op) {
+    Ctx* ctx = as_ctx(h);
+    if (!ctx) return B2M_ERR_ARG;
+    std::lock_guard<std::mutex> lk(ctx->mtx);
+    if (!LUDecomp || !indx || !X || !G || !Lambda) return fail(ctx, B2M_ERR_ARG, "null pointer");
+    if (op != B2M_DO_NONE && op != B2M_DO_ADD) return fail(ctx, B2M_ERR_ARG, "op must be B2M_DO_NONE or B2M_DO_ADD");
+    const int64_t n = width;
+    if (n <= 0 || nrhs <= 0 || !lw_ok(LineWidthLU, n) || !lw_ok(LineWidthX, nrhs) || !lw_ok(LineWidthG, nrhs) ||
+        !lw_ok(LineWidthLambda, nrhs) || (dA && !lw_ok(LineWidthdA, n)))
+        return fail(ctx, B2M_ERR_DIM, "Dimension Error");
+    const int64_t ldy = padded_ld(nrhs);
+    void *py, *pp;
+    B2M_TRY(ws_get(ctx, kWsG, (size_t)(n * ldy * 8), &py));
+    B2M_TRY(ws_get(ctx, kWsPiv, (size_t)(2 * n * 4), &pp));
+    int32_t* dperm = (int32_t*)pp + n;
+    B2M_TRY(reset_status(ctx));
+    B2M_TRY(perm_from_ipiv(ctx, ctx->stream, indx, n, dperm));
+    B2M_TRY(solve_adjoint_f64(ctx, ctx->stream, LUDecomp, LineWidthLU / 8, n, dperm, X, LineWidthX / 8, G,
+                              LineWidthG / 8, nrhs, Lambda, LineWidthLambda / 8, dA, LineWidthdA / 8, op, (double*)py,
+                              ldy));
+    return B2M_OK;
+}
+
+extern "C" int32_t b2m_MatrixLinEQSolveAdjoint(b2m_ctx* h, const double* LUDecomp, int64_t LineWidthLU, int64_t width,
+                                               const int32_t* indx, const double* X, int64_t LineWidthX,
+                                               const double* G, int64_t LineWidthG, int64_t nrhs, double* Lambda,
+                                               int64_t LineWidthLambda, double* dA, int64_t LineWidthdA, int32_t op) {
+    Ctx* ctx = as_ctx(h);
+    if (!ctx) return B2M_ERR_ARG;
+    std::lock_guard<std::mutex> lk(ctx->mtx);
+    if (!LUDecomp || !indx || !X || !G || !Lambda) return fail(ctx, B2M_ERR_ARG, "null pointer");
+    if (op != B2M_DO_NONE && op != B2M_DO_ADD) return fail(ctx, B2M_ERR_ARG, "op must be B2M_DO_NONE or B2M_DO_ADD");
+    const int64_t n = width;
+    if (n <= 0 || nrhs <= 0 || !lw_ok(LineWidthLU, n) || !lw_ok(LineWidthX, nrhs) || !lw_ok(LineWidthG, nrhs) ||
+        !lw_ok(LineWidthLambda, nrhs) || (dA && !lw_ok(LineWidthdA, n)))
+        return fail(ctx, B2M_ERR_DIM, "Dimension Error");
+    cudaSetDevice(ctx->device);
+    const int64_t ld = padded_ld(n), ldk = padded_ld(nrhs);
+    void *pa, *px, *pg, *py, *pl, *pd = nullptr, *pp;
+    B2M_TRY(ws_get(ctx, kWsMatA, (size_t)(n * ld * 8), &pa));
+    B2M_TRY(ws_get(ctx, kWsMatB, (size_t)(n * ldk * 8), &px));
+    B2M_TRY(ws_get(ctx, kWsE, (size_t)(n * ldk * 8), &pg));
+    B2M_TRY(ws_get(ctx, kWsF, (size_t)(n * ldk * 8), &pl));
+    B2M_TRY(ws_get(ctx, kWsG, (size_t)(n * ldk * 8), &py));
+    if (dA) B2M_TRY(ws_get(ctx, kWsMatC, (size_t)(n * ld * 8), &pd));
+    B2M_TRY(ws_get(ctx, kWsPiv, (size_t)(2 * n * 4), &pp));
+    int32_t* dpiv = (int32_t*)pp;
+    int32_t* dperm = dpiv + n;
+    B2M_TRY(upload(ctx, (double*)pa, ld, LUDecomp, LineWidthLU, n, n));
+    B2M_TRY(upload(ctx, (double*)px, ldk, X, LineWidthX, n, nrhs));
+    B2M_TRY(upload(ctx, (double*)pg, ldk, G, LineWidthG, n, nrhs));
+    if (dA && op == B2M_DO_ADD) B2M_TRY(upload(ctx, (double*)pd, ld, dA, LineWidthdA, n, n));
+    B2M_CU(ctx, cudaMemcpyAsync(dpiv, indx, (size_t)n * 4, cudaMemcpyHostToDevice, ctx->stream));
+    B2M_TRY(reset_status(ctx));
+    B2M_TRY(perm_from_ipiv(ctx, ctx->stream, dpiv, n, dperm));
+    B2M_TRY(solve_adjoint_f64(ctx, ctx->stream, (double*)pa, ld, n, dperm, (double*)px, ldk, (double*)pg, ldk, nrhs,
+                              (double*)pl, ldk, (double*)pd, ld, op, (double*)py, ldk));
+    B2M_TRY(download(ctx, Lambda, LineWidthLambda, (double*)pl, ldk, n, nrhs));
+    if (dA) B2M_TRY(download(ctx, dA, LineWidthdA, (double*)pd, ld, n, n));
+    return finish(ctx);
+}

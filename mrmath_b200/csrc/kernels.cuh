@@ -32,6 +32,19 @@ int32_t lu_factor_f64(Ctx* ctx, cudaStream_t st, double* A, int64_t ld, int64_t 
 int32_t lu_solve_f64(Ctx* ctx, cudaStream_t st, const double* LU, int64_t ld, int64_t n, const int32_t* perm,
                      double* B, int64_t ldb, int64_t nrhs, double* tmp = nullptr);
 
+// Blocked FP64 triangular solve of X (n x nrhs, row stride ldx) in place with a triangle of the FP64
+// LU factors: kTriL unit-lower L, kTriU upper U, kTriUt = U^T (lower), kTriLt = L^T (unit upper).
+enum TriMode : int { kTriL = 0, kTriU = 1, kTriUt = 2, kTriLt = 3 };
+int32_t tri_solve_f64(Ctx* ctx, cudaStream_t st, const double* LU, int64_t ld, int64_t n, int mode, double* X,
+                      int64_t ldx, int64_t nrhs);
+
+// Adjoint of the LU solve from the FP64 factors (adjoint.cu): Lambda = A^{-T} G and, when dA is
+// non-null, dA = -Lambda X^T (op B2M_DO_NONE) or dA -= Lambda X^T (op B2M_DO_ADD).  Y (n x ldy) is
+// scratch for the two triangular sweeps.
+int32_t solve_adjoint_f64(Ctx* ctx, cudaStream_t st, const double* LU, int64_t ld, int64_t n, const int32_t* perm,
+                          const double* X, int64_t ldx, const double* G, int64_t ldg, int64_t nrhs, double* Lam,
+                          int64_t ldl, double* dA, int64_t ldd, int op, double* Y, int64_t ldy);
+
 // Builds perm from ipiv on the device (used when factors come from outside: b2m_MatrixLUBackSubst).
 int32_t perm_from_ipiv(Ctx* ctx, cudaStream_t st, const int32_t* ipiv, int64_t n, int32_t* perm);
 

@@ -378,6 +378,10 @@ int32_t lu_solve_f64(Ctx* ctx, cudaStream_t st, const double* LU, int64_t ld, in
         B2M_CU(ctx, cudaMemcpy2DAsync(X, ldb * 8, B, ldb * 8, nrhs * 8, n, cudaMemcpyDeviceToDevice, s));
         gather_rows_kernel<<<(unsigned)ceil_div(n * nrhs, 256), 256, 0, s>>>(B, ldb, X, ldb, perm, n, nrhs);
         B2M_LAUNCHED(ctx);
+        if (nrhs <= 64) {  // few right-hand sides: block-row sweeps (dtrsv.cu)
+            B2M_TRY(tri_solve_f64(ctx, s, LU, ld, n, kTriL, B, ldb, nrhs));
+            return tri_solve_f64(ctx, s, LU, ld, n, kTriU, B, ldb, nrhs);
+        }
         TriSolve t{LU, ld, n, B, ldb, n, nrhs, 0, nrhs};
         B2M_TRY(trsm_lower_rec(ctx, s, t, 0, 0, n));
         return trsm_upper_rec(ctx, s, t, 0, 0, n);

@@ -20,7 +20,7 @@ from ._lib import DO_ADD, DO_NONE, DO_SUB, MIXED_3XTF32, MIXED_TF32, OK, SINGULA
 __all__ = [
     "default_context", "MatrixMult", "MatrixMultEx", "MatrixMultT1Ex", "MatrixMultT2Ex", "MatrixLUDecompInPlace",
     "MatrixLUDecomp", "MatrixLUBackSubst", "MatrixInverseInPlace", "MatrixDeterminant", "MatrixLinEQSolve",
-    "DO_NONE", "DO_ADD", "DO_SUB",
+    "MatrixLinEQSolveMixed", "MatrixLinEQSolveAdjoint", "DO_NONE", "DO_ADD", "DO_SUB",
 ]
 
 _ctx: dict[int, Context] = {}
@@ -136,6 +136,20 @@ def MatrixLinEQSolveMixed(A: np.ndarray, B: np.ndarray, mode: int = MIXED_3XTF32
     return st, X, _rep(rep)
 
 
+def MatrixLinEQSolveAdjoint(LU: np.ndarray, indx: np.ndarray, X: np.ndarray, G: np.ndarray,
+                            dA: np.ndarray | None = None, op: int = DO_NONE, ctx: Context | None = None):
+    """Adjoint of MatrixLinEQSolve from the factors of MatrixLUDecomp: returns Lambda = A^-T G and
+    fills dA with -Lambda X^T (op DO_NONE) or subtracts Lambda X^T from it (op DO_ADD)."""
+    n = LU.shape[1]
+    k = X.shape[1]
+    assert indx.dtype == np.int32
+    lam = np.empty((n, k))
+    _ctx_of(ctx).call("b2m_MatrixLinEQSolveAdjoint", _ptr(LU), _lw(LU), n, indx.ctypes.data, _ptr(X), _lw(X),
+                      _ptr(G), _lw(G), k, _ptr(lam), _lw(lam), _ptr(dA) if dA is not None else None,
+                      _lw(dA) if dA is not None else 0, op)
+    return lam
+
+
 # ----------------------------------------------------------------------------- device (torch) twins
 def _tptr(t) -> int:
     return t.data_ptr()
@@ -203,3 +217,13 @@ def dev_MatrixLinEQSolveMixed(A, B, X, mode=MIXED_3XTF32, max_iter=0, tol=0.0, s
     if status is not None:
         status.fill_(st)
     return st, _rep(rep)
+
+
+def dev_MatrixLinEQSolveAdjoint(LU, indx, X, G, Lam, dA=None, op=DO_NONE, ctx=None):
+    """Device twin of MatrixLinEQSolveAdjoint (torch CUDA tensors, indx int32 as produced by
+    dev_MatrixLUDecompInPlace); Lam receives A^-T G, dA (optional) -Lam X^T."""
+    c = _ctx_of(ctx)
+    _bind_stream(c, LU)
+    c.call("b2m_dev_MatrixLinEQSolveAdjoint", _tptr(LU), _tlw(LU), LU.shape[1], _tptr(indx), _tptr(X), _tlw(X),
+           _tptr(G), _tlw(G), X.shape[1], _tptr(Lam), _tlw(Lam), _tptr(dA) if dA is not None else None,
+           _tlw(dA) if dA is not None else 0, op)
