@@ -163,6 +163,28 @@ B2M_API int32_t b2m_dev_MatrixLinEQSolveAdjoint(b2m_ctx* ctx, const double* LUDe
                                         const double* G, int64_t LineWidthG, int64_t nrhs, double* Lambda,
                                         int64_t LineWidthLambda, double* dA, int64_t LineWidthdA, int32_t op);
 
+/* Batched solves of many independent systems of uneven order in one persistent launch.  No
+ * counterpart in the reference, which solves one system per MatrixLinEQSolve call
+ * (LinAlgLU.pas:481-592); each system follows that routine's pivoting, singularity test and
+ * substitution.  System i has order n[i] (1..256) and nrhs[i] (1..8) right-hand sides; A_i is
+ * row-major n_i x n_i at A + a_off[i], B_i and X_i are row-major n_i x nrhs_i at B + b_off[i] and
+ * X + b_off[i] (offsets in doubles).  The plan arrays n, nrhs, a_off, b_off are host memory.
+ * mode 0: FP64 LU with partial pivoting; mode 1: FP32 factorisation + FP64 refinement to
+ * backward error <= n_i 2^-53, refactored in FP64 when refinement stalls.  info[i] = 0 (leOk) or
+ * 1 (leSingular); iters[i] (may be NULL) = refinement steps in mode 1, -1 when FP64 was needed.
+ * The first call with a new plan runs the autotuner (it times the candidate tile shapes). */
+B2M_API int32_t b2m_BatchLinEQSolve(b2m_ctx* ctx, int64_t count, const int32_t* n, const int32_t* nrhs,
+                                    const int64_t* a_off, const int64_t* b_off, const double* A, const double* B,
+                                    double* X, int32_t mode, int32_t* info, int32_t* iters);
+/* Device twin: A, B, X, info, iters are device memory (the plan arrays stay on the host);
+ * asynchronous on the context's stream, replayed from a CUDA graph after the first call. */
+B2M_API int32_t b2m_dev_BatchLinEQSolve(b2m_ctx* ctx, int64_t count, const int32_t* n, const int32_t* nrhs,
+                                        const int64_t* a_off, const int64_t* b_off, const double* A,
+                                        const double* B, double* X, int32_t mode, int32_t* info, int32_t* iters);
+/* The tile shape the autotuner chose for the last batch plan. */
+B2M_API int32_t b2m_batch_tune_read(b2m_ctx* ctx, int32_t* small_n, int32_t* group_warps, int32_t* pw_large,
+                                    int32_t* pw_small, float* ms);
+
 /* Allocation-free solve.  No counterpart in the reference: it exists for callers that may not
  * allocate device memory (a host program whose memory manager owns all device allocations, code
  * running inside a stream capture, a real-time loop with a fixed budget).  Same arguments and

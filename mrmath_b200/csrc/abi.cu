@@ -639,3 +639,81 @@ extern "C" int32_t b2m_MatrixLinEQSolveAdjoint(b2m_ctx* h, const double* LUDecom
     if (dA) B2M_TRY(download(ctx, dA, LineWidthdA, (double*)pd, ld, n, n));
     return finish(ctx);
 }
+
+// ------------------------------------------------------------------ batched uneven solves
+namespace {
+int32_t batch_check(Ctx* ctx, int64_t count, const int32_t* n, const int32_t* nrhs, const int64_t* a_off,
+                    const int64_t* b_off, int64_t* a_elems, int64_t* b_elems) {
+    if (count < 0) return fail(ctx, B2M_ERR_DIM, "count < 0");
+    if (count > 0 && (!n || !nrhs || !a_off || !b_off)) return fail(ctx, B2M_ERR_ARG, "null plan array");
+    int64_t ae = 0, be = 0;
+    for (int64_t i = 0; i < count; ++i) {
+        if (a_off[i] < 0 || b_off[i] < 0) return fail(ctx, B2M_ERR_DIM, "negative offset");
+        ae = std::max(ae, a_off[i] + (int64_t)n[i] * n[i]);
+        be = std::max(be, b_off[i] + (int64_t)n[i] * nrhs[i]);
+    }
+    *a_elems = ae;
+    *b_elems = be;
+    return B2M_OK;
+}
+}  // namespace
+
+extern "C" int32_t b2m_dev_BatchLinEQSolve(b2m_ctx* h, int64_t count, const int32_t* n, const int32_t* nrhs,
+                                           const int64_t* a_off, const int64_t* b_off, const double* A,
+                                           const double* B, double* X, int32_t mode, int32_t* info, int32_t* iters) {
+    Ctx* ctx = as_ctx(h);
+    if (!ctx) return B2M_ERR_ARG;
+    std::lock_guard<std::mutex> lk(ctx->mtx);
+    int64_t ae, be;
+    B2M_TRY(batch_check(ctx, count, n, nrhs, a_off, b_off, &ae, &be));
+    if (count == 0) return B2M_OK;
+    if (!A || !B || !X || !info) return fail(ctx, B2M_ERR_ARG, "null pointer");
+    return batch_solve(ctx, ctx->stream, count, n, nrhs, a_off, b_off, A, B, X, mode, info, iters, nullptr);
+}
+
+extern "C" int32_t b2m_BatchLinEQSolve(b2m_ctx* h, int64_t count, const int32_t* n, const int32_t* nrhs,
+                                       const int64_t* a_off, const int64_t* b_off, const double* A, const double* B,
+                                       double* X, int32_t mode, int32_t* info, int32_t* iters) {
+    Ctx* ctx = as_ctx(h);
+    if (!ctx) return B2M_ERR_ARG;
+    std::lock_guard<std::mutex> lk(ctx->mtx);
+    int64_t ae, be;
+    B2M_TRY(batch_check(ctx, count, n, nrhs, a_off, b_off, &ae, &be));
+    if (count == 0) return B2M_OK;
+    if (!A || !B || !X || !info) return fail(ctx, B2M_ERR_ARG, "null pointer");
+    cudaSetDevice(ctx->device);
+    void *pa, *pb, *px, *pi;
+    B2M_TRY(ws_get(ctx, kWsMatA, (size_t)ae * 8, &pa));
+    B2M_TRY(ws_get(ctx, kWsMatB, (size_t)be * 8, &pb));
+    B2M_TRY(ws_get(ctx, kWsMatC, (size_t)be * 8, &px));
+    B2M_TRY(ws_get(ctx, kWsE, (size_t)count * 8, &pi));
+    int32_t* dinfo = (int32_t*)pi;
+    int32_t* diters = dinfo + count;
+    B2M_CU(ctx, cudaMemcpyAsync(pa, A, (size_t)ae * 8, cudaMemcpyHostToDevice, ctx->stream));
+    B2M_CU(ctx, cudaMemcpyAsync(pb, B, (size_t)be * 8, cudaMemcpyHostToDevice, ctx->stream));
+    B2M_TRY(reset_status(ctx));
+    B2M_TRY(batch_solve(ctx, ctx->stream, count, n, nrhs, a_off, b_off, (const double*)pa, (const double*)pb,
+                        (double*)px, mode, dinfo, diters, nullptr));
+    B2M_CU(ctx, cudaMemcpyAsync(X, px, (size_t)be * 8, cudaMemcpyDeviceToHost, ctx->stream));
+    B2M_CU(ctx, cudaMemcpyAsync(info, dinfo, (size_t)count * 4, cudaMemcpyDeviceToHost, ctx->stream));
+    if (iters) B2M_CU(ctx, cudaMemcpyAsync(iters, diters, (size_t)count * 4, cudaMemcpyDeviceToHost, ctx->stream));
+    B2M_CU(ctx, cudaStreamSynchronize(ctx->stream));
+    return B2M_OK;
+}
+
+extern "C" int32_t b2m_batch_tune_read(b2m_ctx* h, int32_t* small_n, int32_t* group_warps, int32_t* pw_large,
+                                       int32_t* pw_small, float* ms) {
+    Ctx* ctx = as_ctx(h);
+    if (!ctx) return B2M_ERR_ARG;
+    std::lock_guard<std::mutex> lk(ctx->mtx);
+    if (ctx->batch_tunes.empty()) return fail(ctx, B2M_ERR_ARG, "no batch has been tuned yet");
+    const BatchTune& t = ctx->batch_tunes.find(ctx->batch_plan_sig) != ctx->batch_tunes.end()
+                             ? ctx->batch_tunes[ctx->batch_plan_sig]
+                             : ctx->batch_tunes.begin()->second;
+    if (small_n) *small_n = t.small_n;
+    if (group_warps) *group_warps = t.group_warps;
+    if (pw_large) *pw_large = t.pw_large;
+    if (pw_small) *pw_small = t.pw_small;
+    if (ms) *ms = t.ms;
+    return B2M_OK;
+}

@@ -1,0 +1,541 @@
+// batched.cu -- many independent LU solves of uneven order in one persistent launch.
+//
+// There is no counterpart in the reference, which solves one system per MatrixLinEQSolve call
+// (LinAlgLU.pas:481-592); every system here follows that routine's semantics: partial pivoting with
+// the first maximum winning, the pivot column scaled by the reciprocal of the pivot, a pivot of
+// magnitude <= 10/MaxDouble reporting the system singular (:246-268), forward substitution with the
+// unit-lower factor and back substitution dividing by U's diagonal (:315-385).
+//
+// Scheduling: the host sorts the systems largest first; resident CTAs pull them from an atomic work
+// queue (longest-processing-time first, no tail of big systems).  Systems of order > small_n take
+// a whole CTA; smaller ones are handed out in batches, one per group of G warps, each group with its
+// own named barrier.  The panel width of both size buckets and G are chosen by the autotuner at the
+// bottom of this file, which times the candidate shapes on the caller's batch.
+//
+// Per system: A is copied into the CTA's private scratch slice (<= 256 x 256, L2 resident), where
+// a blocked right-looking LU runs with the current panel and the block row of U in shared memory.
+// Rows are never moved: a permutation maps factor rows to storage rows, so a pivot interchange swaps
+// two integers (the factors and the reference's interchange order are the same as with physical
+// swaps).  The solve is blocked by 32 rows: one warp per right-hand side substitutes a diagonal
+// block with shuffles, then the group folds it into the remaining rows.
+//
+// Mode 1 factors in FP32 and refines in FP64: r = b - A x from the caller's FP64 A, d from the FP32
+// factors, x += d, until the normwise backward error max_q ||r_q|| / (||A|| ||x_q|| + ||b_q||) is
+// <= n 2^-53; a stall or an FP32 pivot <= 10/FLT_MAX refactors that system in FP64.
+#include <algorithm>
+#include <cfloat>
+#include <chrono>
+#include <cstring>
+#include <numeric>
+#include <vector>
+
+#include "common.cuh"
+#include "kernels.cuh"
+
+namespace b2m {
+namespace {
+
+constexpr int kBThreads = 256;
+constexpr int kBMaxN = 256;
+constexpr int kBMaxK = 8;
+constexpr int kBMaxPW = 32;
+
+struct BatchArgs {
+    int count;
+    const int32_t* n;
+    const int32_t* k;
+    const int64_t* a_off;
+    const int64_t* b_off;
+    const double* A;
+    const double* B;
+    double* X;
+    double* scratch;  // kBMaxN^2 doubles per CTA
+    const int32_t* order;
+    int32_t* counter;
+    int32_t* info;
+    int32_t* iters;
+    int mode;
+    int small_n;
+    int group_warps;
+    int pw_large, pw_small;
+    int max_iter;
+};
+
+// a group of threads working on one system, with its own named barrier
+struct Grp {
+    int tid, nt, bar;
+    __device__ __forceinline__ void sync() const { asm volatile("bar.sync %0, %1;\n" ::"r"(bar), "r"(nt) : "memory"); }
+};
+
+// shared-memory slice of one group
+struct Slice {
+    double* pan;   // [nmax][pw + 1] panel (factor rows c0.., panel columns)
+    double* u;     // [pw][nmax + 1] block row of U right of the panel
+    double* y;     // [nmax][kBMaxK] right-hand sides / solution in factor order
+    double* red;   // [8] reduction values
+    int* redi;     // [8] reduction indices
+    int* perm;     // [nmax] storage row of factor row i
+    int* flag;     // [4]
+    int us;        // row stride of u
+};
+
+__host__ __device__ inline size_t slice_doubles(int nmax, int pw) {
+    return (size_t)nmax * (pw + 1) + (size_t)pw * (nmax + 1) + (size_t)nmax * kBMaxK + 8 + (nmax + 8 + 4 + 1) / 2 + 1;
+}
+
+__device__ Slice carve(double* base, int nmax, int pw) {
+    Slice s;
+    s.pan = base;
+    s.u = s.pan + (size_t)nmax * (pw + 1);
+    s.y = s.u + (size_t)pw * (nmax + 1);
+    s.red = s.y + (size_t)nmax * kBMaxK;
+    s.redi = reinterpret_cast<int*>(s.red + 8);
+    s.perm = s.redi + 8;
+    s.flag = s.perm + nmax;
+    s.us = nmax + 1;
+    return s;
+}
+
+template <typename T> __device__ __forceinline__ T sing_thresh();
+template <> __device__ __forceinline__ double sing_thresh<double>() { return 10.0 / DBL_MAX; }
+template <> __device__ __forceinline__ float sing_thresh<float>() { return 10.0f / FLT_MAX; }
+
+// argmax of |v| over the group (first maximum wins: lowest index among equals); all threads get it
+__device__ __forceinline__ void grp_argmax(const Grp& g, const Slice& s, double v, int i, double& bv, int& bi) {
+    const int lane = g.tid & 31, w = g.tid >> 5, nw = g.nt >> 5;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        const double v2 = __shfl_xor_sync(0xffffffffu, v, o);
+        const int i2 = __shfl_xor_sync(0xffffffffu, i, o);
+        if (i2 >= 0 && (i < 0 || v2 > v || (v2 == v && i2 < i))) { v = v2; i = i2; }
+    }
+    if (nw == 1) {
+        bv = v;
+        bi = i;
+        return;
+    }
+    if (lane == 0) { s.red[w] = v; s.redi[w] = i; }
+    g.sync();
+    bv = -1.0;
+    bi = -1;
+    for (int q = 0; q < nw; ++q) {
+        const double v2 = s.red[q];
+        const int i2 = s.redi[q];
+        if (i2 >= 0 && (bi < 0 || v2 > bv || (v2 == bv && i2 < bi))) { bv = v2; bi = i2; }
+    }
+    g.sync();
+}
+
+// Blocked LU of the n x n matrix W (row-major, ld n, element type T) with row permutation perm.
+// Returns 0, or 1 when a pivot is <= the singular threshold (uniform across the group).
+template <typename T>
+__device__ int grp_lu(const Grp& g, const Slice& s, T* W, int n, int PW) {
+    for (int i = g.tid; i < n; i += g.nt) s.perm[i] = i;
+    g.sync();
+    const int pwp = PW + 1;
+    for (int c0 = 0; c0 < n; c0 += PW) {
+        const int pw = min(PW, n - c0), m = n - c0;
+        for (int e = g.tid; e < m * pw; e += g.nt) {
+            const int r = e / pw, c = e - r * pw;
+            s.pan[r * pwp + c] = (double)W[(int64_t)s.perm[c0 + r] * n + c0 + c];
+        }
+        g.sync();
+        for (int j = 0; j < pw; ++j) {
+            double v = -1.0;
+            int vi = -1;
+            for (int r = j + g.tid; r < m; r += g.nt) {
+                const double a = fabs(s.pan[r * pwp + j]);
+                if (vi < 0 || a > v) { v = a; vi = r; }
+            }
+            double bv;
+            int pr;
+            grp_argmax(g, s, v, vi, bv, pr);
+            if (!(bv > (double)sing_thresh<T>())) return 1;
+            if (pr != j) {
+                for (int c = g.tid; c < pw; c += g.nt) {
+                    const double t0 = s.pan[j * pwp + c];
+                    s.pan[j * pwp + c] = s.pan[pr * pwp + c];
+                    s.pan[pr * pwp + c] = t0;
+                }
+                if (g.tid == 0) {
+                    const int t1 = s.perm[c0 + j];
+                    s.perm[c0 + j] = s.perm[c0 + pr];
+                    s.perm[c0 + pr] = t1;
+                }
+            }
+            g.sync();
+            // reference scaling: the column is multiplied by 1/pivot, in the element type
+            const T rinv = (T)1 / (T)s.pan[j * pwp + j];
+            for (int r = j + 1 + g.tid; r < m; r += g.nt) {
+                const T l = (T)s.pan[r * pwp + j] * rinv;
+                s.pan[r * pwp + j] = (double)l;
+                for (int c = j + 1; c < pw; ++c)
+                    s.pan[r * pwp + c] = (double)((T)s.pan[r * pwp + c] - l * (T)s.pan[j * pwp + c]);
+            }
+            g.sync();
+        }
+        for (int e = g.tid; e < m * pw; e += g.nt) {
+            const int r = e / pw, c = e - r * pw;
+            W[(int64_t)s.perm[c0 + r] * n + c0 + c] = (T)s.pan[r * pwp + c];
+        }
+        const int c1 = c0 + pw, nr = n - c1;
+        if (nr > 0) {
+            // block row of U: u = L11^-1 A12 (thread per column, in shared memory)
+            for (int c = g.tid; c < nr; c += g.nt) {
+                for (int r = 0; r < pw; ++r) s.u[r * s.us + c] = (double)W[(int64_t)s.perm[c0 + r] * n + c1 + c];
+                for (int r = 1; r < pw; ++r) {
+                    T acc = (T)s.u[r * s.us + c];
+                    for (int q = 0; q < r; ++q) acc -= (T)s.pan[r * pwp + q] * (T)s.u[q * s.us + c];
+                    s.u[r * s.us + c] = (double)acc;
+                    W[(int64_t)s.perm[c0 + r] * n + c1 + c] = acc;
+                }
+            }
+            g.sync();
+            // trailing update: A22 -= L21 U12
+            for (int e = g.tid; e < nr * nr; e += g.nt) {
+                const int r = e / nr, c = e - r * nr;
+                T* p = W + (int64_t)s.perm[c1 + r] * n + c1 + c;
+                T acc = *p;
+                const double* lr = s.pan + (pw + r) * pwp;
+                for (int q = 0; q < pw; ++q) acc -= (T)lr[q] * (T)s.u[q * s.us + c];
+                *p = acc;
+            }
+            g.sync();
+        }
+    }
+    return 0;
+}
+
+// y (factor order, kk columns) <- U^-1 L^-1 y with the factors in W (element type T)
+template <typename T>
+__device__ void grp_solve(const Grp& g, const Slice& s, const T* W, int n, int kk) {
+    const int lane = g.tid & 31, w = g.tid >> 5, nw = g.nt >> 5;
+    const int nb = (n + 31) / 32;
+    for (int pass = 0; pass < 2; ++pass) {
+        const bool lower = pass == 0;
+        for (int bi = 0; bi < nb; ++bi) {
+            const int b = lower ? bi : nb - 1 - bi;
+            const int b0 = 32 * b, bs = min(32, n - b0);
+            for (int q = w; q < kk; q += nw) {
+                double tr[32];
+                const int row = b0 + lane;
+#pragma unroll
+                for (int j = 0; j < 32; ++j)
+                    tr[j] = (lane < bs && j < bs) ? (double)W[(int64_t)s.perm[row] * n + b0 + j] : 0.0;
+                double yv = lane < bs ? s.y[row * kBMaxK + q] : 0.0;
+                if (lower) {
+#pragma unroll
+                    for (int j = 0; j < 32; ++j) {
+                        if (j >= bs) break;
+                        const double xj = __shfl_sync(0xffffffffu, yv, j);
+                        if (lane > j) yv = (double)((T)yv - (T)tr[j] * (T)xj);
+                    }
+                } else {
+#pragma unroll
+                    for (int j = 31; j >= 0; --j) {
+                        if (j >= bs) continue;
+                        if (lane == j) yv = (double)((T)yv / (T)tr[j]);
+                        const double xj = __shfl_sync(0xffffffffu, yv, j);
+                        if (lane < j) yv = (double)((T)yv - (T)tr[j] * (T)xj);
+                    }
+                }
+                if (lane < bs) s.y[row * kBMaxK + q] = yv;
+            }
+            g.sync();
+            const int rlo = lower ? b0 + bs : 0, rhi = lower ? n : b0;
+            for (int e = g.tid; e < (rhi - rlo) * kk; e += g.nt) {
+                const int r = rlo + e / kk, q = e % kk;
+                const T* lr = W + (int64_t)s.perm[r] * n + b0;
+                T acc = (T)s.y[r * kBMaxK + q];
+                for (int j = 0; j < bs; ++j) acc -= lr[j] * (T)s.y[(b0 + j) * kBMaxK + q];
+                s.y[r * kBMaxK + q] = (double)acc;
+            }
+            g.sync();
+        }
+    }
+}
+
+// plain FP64 solve of one system
+__device__ int solve_plain(const Grp& g, const Slice& s, const BatchArgs& a, int sys, double* W) {
+    const int n = a.n[sys], kk = a.k[sys];
+    const double* A = a.A + a.a_off[sys];
+    for (int e = g.tid; e < n * n; e += g.nt) W[e] = A[e];
+    g.sync();
+    if (grp_lu<double>(g, s, W, n, g.nt == kBThreads ? a.pw_large : a.pw_small)) return 1;
+    const double* B = a.B + a.b_off[sys];
+    for (int e = g.tid; e < n * kk; e += g.nt) {
+        const int i = e / kk, q = e - i * kk;
+        s.y[i * kBMaxK + q] = B[(int64_t)s.perm[i] * kk + q];
+    }
+    g.sync();
+    grp_solve<double>(g, s, W, n, kk);
+    double* X = a.X + a.b_off[sys];
+    for (int e = g.tid; e < n * kk; e += g.nt) {
+        const int i = e / kk, q = e - i * kk;
+        X[e] = s.y[i * kBMaxK + q];
+    }
+    g.sync();
+    return 0;
+}
+
+// FP32 factorisation + FP64 refinement; returns refinement steps, or -1 when FP64 is needed
+__device__ int solve_mixed(const Grp& g, const Slice& s, const BatchArgs& a, int sys, double* Wd) {
+    const int n = a.n[sys], kk = a.k[sys];
+    float* W = reinterpret_cast<float*>(Wd);
+    const double* A = a.A + a.a_off[sys];
+    const double* B = a.B + a.b_off[sys];
+    double* X = a.X + a.b_off[sys];
+    for (int e = g.tid; e < n * n; e += g.nt) W[e] = (float)A[e];
+    g.sync();
+    if (grp_lu<float>(g, s, W, n, g.nt == kBThreads ? a.pw_large : a.pw_small)) return -1;
+    // ||A||inf (kept in s.red[7] after the reduction below) and ||b_q||inf
+    double an = 0.0;
+    for (int i = g.tid; i < n; i += g.nt) {
+        double rs = 0.0;
+        for (int j = 0; j < n; ++j) rs += fabs(A[(int64_t)i * n + j]);
+        an = fmax(an, rs);
+    }
+    double bv;
+    int bi;
+    grp_argmax(g, s, an, g.tid < n ? 0 : -1, bv, bi);
+    const double normA = bv;
+    for (int e = g.tid; e < n * kk; e += g.nt) X[e] = 0.0;
+    // r = b in factor order
+    for (int e = g.tid; e < n * kk; e += g.nt) {
+        const int i = e / kk, q = e - i * kk;
+        s.y[i * kBMaxK + q] = B[(int64_t)s.perm[i] * kk + q];
+    }
+    g.sync();
+    const double tol = (double)n * 0x1.0p-53;
+    double prev = INFINITY;
+    for (int it = 1; it <= a.max_iter; ++it) {
+        grp_solve<float>(g, s, W, n, kk);
+        for (int e = g.tid; e < n * kk; e += g.nt) X[e] += s.y[(e / kk) * kBMaxK + (e % kk)];
+        g.sync();
+        // r = b - A x (FP64), written in factor order; eta over the columns
+        double eta = 0.0;
+        for (int q = 0; q < kk; ++q) {
+            double rmax = 0.0, xmax = 0.0, bmax = 0.0;
+            for (int i = g.tid; i < n; i += g.nt) {
+                double acc = B[(int64_t)i * kk + q];
+                for (int j = 0; j < n; ++j) acc = fma(-A[(int64_t)i * n + j], X[(int64_t)j * kk + q], acc);
+                s.pan[i] = acc;  // residual in natural order (the panel buffer is free now)
+                rmax = fmax(rmax, fabs(acc));
+                xmax = fmax(xmax, fabs(X[(int64_t)i * kk + q]));
+                bmax = fmax(bmax, fabs(B[(int64_t)i * kk + q]));
+            }
+            g.sync();
+            double r1, x1, b1;
+            int d;
+            grp_argmax(g, s, rmax, g.tid < n ? 0 : -1, r1, d);
+            grp_argmax(g, s, xmax, g.tid < n ? 0 : -1, x1, d);
+            grp_argmax(g, s, bmax, g.tid < n ? 0 : -1, b1, d);
+            const double den = normA * x1 + b1;
+            eta = fmax(eta, den > 0.0 ? r1 / den : (r1 > 0.0 ? INFINITY : 0.0));
+            for (int i = g.tid; i < n; i += g.nt) s.y[i * kBMaxK + q] = s.pan[s.perm[i]];
+            g.sync();
+        }
+        if (eta <= tol) return it;
+        if (!(eta < INFINITY) || (it >= 2 && eta > 0.5 * prev)) return -1;
+        prev = eta;
+    }
+    return -1;
+}
+
+__global__ void __launch_bounds__(kBThreads, 1) batch_solve_kernel(BatchArgs a) {
+    extern __shared__ __align__(16) double bsm[];
+    __shared__ int s_sys[8];
+    const int t = threadIdx.x;
+    double* W = a.scratch + (size_t)blockIdx.x * kBMaxN * kBMaxN;
+    const int G = a.group_warps, ngroups = (kBThreads / 32) / G;
+    for (;;) {
+        if (t == 0) s_sys[0] = atomicAdd(a.counter, 1);
+        __syncthreads();
+        const int idx = s_sys[0];
+        __syncthreads();
+        if (idx >= a.count) return;
+        const int sys = a.order[idx];
+        if (a.n[sys] > a.small_n) {
+            const Grp g{t, kBThreads, 1};
+            const Slice s = carve(bsm, kBMaxN, a.pw_large);
+            int st, iters = 0;
+            if (a.mode == 1) {
+                iters = solve_mixed(g, s, a, sys, W);
+                st = iters < 0 ? solve_plain(g, s, a, sys, W) : 0;
+            } else {
+                st = solve_plain(g, s, a, sys, W);
+            }
+            if (t == 0) {
+                a.info[sys] = st;
+                if (a.iters) a.iters[sys] = iters;
+            }
+            __syncthreads();
+            continue;
+        }
+        // small systems: this one plus up to ngroups - 1 more from the queue, one per group
+        if (t == 0) {
+            s_sys[0] = idx;
+            for (int q = 1; q < ngroups; ++q) {
+                const int j = atomicAdd(a.counter, 1);
+                s_sys[q] = j < a.count ? j : -1;
+            }
+        }
+        __syncthreads();
+        const int gi = t / (32 * G);
+        const int myidx = s_sys[gi];
+        if (myidx >= 0) {
+            const int msys = a.order[myidx];
+            const Grp g{t - gi * 32 * G, 32 * G, 2 + gi};
+            const Slice s = carve(bsm + (size_t)gi * slice_doubles(a.small_n, a.pw_small), a.small_n, a.pw_small);
+            double* Wg = W + (size_t)gi * a.small_n * a.small_n;
+            int st, iters = 0;
+            if (a.mode == 1) {
+                iters = solve_mixed(g, s, a, msys, Wg);
+                st = iters < 0 ? solve_plain(g, s, a, msys, Wg) : 0;
+            } else {
+                st = solve_plain(g, s, a, msys, Wg);
+            }
+            if (g.tid == 0) {
+                a.info[msys] = st;
+                if (a.iters) a.iters[msys] = iters;
+            }
+        }
+        __syncthreads();
+    }
+}
+
+size_t batch_smem_bytes(int small_n, int G, int pw_large, int pw_small) {
+    const size_t big = slice_doubles(kBMaxN, pw_large);
+    const size_t small = slice_doubles(small_n, pw_small) * ((kBThreads / 32) / G);
+    return std::max(big, small) * sizeof(double);
+}
+
+}  // namespace
+
+// ------------------------------------------------------------------ host side
+struct BatchPlanCache {
+    std::vector<int32_t> n, k;
+    std::vector<int64_t> a_off, b_off;
+    int64_t count = -1;
+};
+
+int32_t batch_solve(Ctx* ctx, cudaStream_t st, int64_t count, const int32_t* hn, const int32_t* hk,
+                    const int64_t* ha_off, const int64_t* hb_off, const double* A, const double* B, double* X,
+                    int mode, int32_t* info, int32_t* iters, BatchTune* tune_out) {
+    if (count <= 0) return B2M_OK;
+    if (mode != 0 && mode != 1) return fail(ctx, B2M_ERR_ARG, "batch: mode must be 0 (FP64) or 1 (FP32 + FP64 IR)");
+    for (int64_t i = 0; i < count; ++i) {
+        if (hn[i] < 1 || hn[i] > kBMaxN) return fail(ctx, B2M_ERR_UNSUPPORTED, "batch: system %lld order %d not in [1, 256]", (long long)i, hn[i]);
+        if (hk[i] < 1 || hk[i] > kBMaxK) return fail(ctx, B2M_ERR_UNSUPPORTED, "batch: system %lld has %d right-hand sides (1..8)", (long long)i, hk[i]);
+    }
+    // device copies of the plan: n, k, offsets, order (largest first), queue head
+    std::vector<int32_t> order((size_t)count);
+    std::iota(order.begin(), order.end(), 0);
+    std::stable_sort(order.begin(), order.end(), [&](int32_t x, int32_t y) { return hn[x] > hn[y]; });
+    const size_t bytes_i = (size_t)count * 4, bytes_l = (size_t)count * 8;
+    const size_t plan_bytes = 3 * bytes_i + 2 * bytes_l + 256;
+    void* pplan;
+    B2M_TRY(ws_get(ctx, kWsH, plan_bytes + 256, &pplan));
+    char* pp = static_cast<char*>(pplan);
+    int32_t* dn = reinterpret_cast<int32_t*>(pp);
+    int32_t* dk = dn + count;
+    int32_t* dord = dk + count;
+    int64_t* dao = reinterpret_cast<int64_t*>(pp + round_up((int64_t)(3 * bytes_i), 256));
+    int64_t* dbo = dao + count;
+    int32_t* dctr = reinterpret_cast<int32_t*>(dbo + count);
+    uint64_t sig = 1469598103934665603ull ^ (uint64_t)mode;
+    for (int64_t i = 0; i < count; ++i)
+        sig = (sig ^ (uint64_t)(hn[i] * 16 + hk[i]) ^ ((uint64_t)ha_off[i] << 20) ^ ((uint64_t)hb_off[i] << 40)) *
+              1099511628211ull;
+    const bool same_plan = ctx->batch_plan_sig == sig && ctx->batch_plan_dev == pplan;
+    void* ph = nullptr;
+    if (!same_plan) {
+        // the pinned staging buffer may still feed an earlier asynchronous copy
+        B2M_CU(ctx, cudaStreamSynchronize(st));
+        B2M_TRY(pinned_get(ctx, plan_bytes + 256, &ph));
+    }
+    if (!same_plan) {
+        char* hp = static_cast<char*>(ph);
+        std::memcpy(hp, hn, bytes_i);
+        std::memcpy(hp + bytes_i, hk, bytes_i);
+        std::memcpy(hp + 2 * bytes_i, order.data(), bytes_i);
+        std::memcpy(hp + round_up((int64_t)(3 * bytes_i), 256), ha_off, bytes_l);
+        std::memcpy(hp + round_up((int64_t)(3 * bytes_i), 256) + bytes_l, hb_off, bytes_l);
+        B2M_CU(ctx, cudaMemcpyAsync(pp, hp, round_up((int64_t)(3 * bytes_i), 256) + 2 * bytes_l,
+                                    cudaMemcpyHostToDevice, st));
+        ctx->batch_plan_sig = sig;
+        ctx->batch_plan_dev = pplan;
+    }
+
+    int occ_sms = ctx->num_sms;
+    BatchArgs a{};
+    a.count = (int)count;
+    a.n = dn; a.k = dk; a.a_off = dao; a.b_off = dbo;
+    a.A = A; a.B = B; a.X = X;
+    a.order = dord; a.counter = dctr; a.info = info; a.iters = iters;
+    a.mode = mode;
+    a.max_iter = 10;
+
+    auto launch = [&](const BatchTune& tc, cudaStream_t q) -> int32_t {
+        const size_t smem = batch_smem_bytes(tc.small_n, tc.group_warps, tc.pw_large, tc.pw_small);
+        B2M_CU(ctx, cudaFuncSetAttribute(batch_solve_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        int per_sm = 0;
+        B2M_CU(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_solve_kernel, kBThreads, smem));
+        if (per_sm < 1) return fail(ctx, B2M_ERR_UNSUPPORTED, "batch: tile shape does not fit one SM");
+        const int grid = occ_sms * per_sm;
+        void* pscr;
+        B2M_TRY(ws_get(ctx, kWsMatD, (size_t)grid * kBMaxN * kBMaxN * sizeof(double), &pscr));
+        BatchArgs b = a;
+        b.scratch = static_cast<double*>(pscr);
+        b.small_n = tc.small_n;
+        b.group_warps = tc.group_warps;
+        b.pw_large = tc.pw_large;
+        b.pw_small = tc.pw_small;
+        B2M_CU(ctx, cudaMemsetAsync(dctr, 0, sizeof(int32_t), q));
+        prof_begin(ctx, q, kClsSolve);
+        batch_solve_kernel<<<grid, kBThreads, smem, q>>>(b);
+        prof_end(ctx, q, kClsSolve, 0.0);
+        B2M_LAUNCHED(ctx);
+        return B2M_OK;
+    };
+
+    // autotune once per plan (mode, sizes, layout): time each candidate shape on this batch
+    BatchTune best;
+    auto it = ctx->batch_tunes.find(sig);
+    if (it != ctx->batch_tunes.end()) {
+        best = it->second;
+    } else {
+        std::vector<BatchTune> cands;
+        for (int pwl : {8, 16, 32})
+            for (int G : {1, 2, 4})
+                for (int pws : {8, 16}) cands.push_back(BatchTune{64, G, pwl, pws, 0.0f});
+        cudaEvent_t e0, e1;
+        B2M_CU(ctx, cudaEventCreate(&e0));
+        B2M_CU(ctx, cudaEventCreate(&e1));
+        float best_ms = 1e30f;
+        for (auto& c : cands) {
+            const size_t smem = batch_smem_bytes(c.small_n, c.group_warps, c.pw_large, c.pw_small);
+            if (smem > ctx->smem_optin) continue;
+            B2M_TRY(launch(c, st));  // warm
+            B2M_CU(ctx, cudaEventRecord(e0, st));
+            B2M_TRY(launch(c, st));
+            B2M_CU(ctx, cudaEventRecord(e1, st));
+            B2M_CU(ctx, cudaEventSynchronize(e1));
+            float ms = 0.f;
+            B2M_CU(ctx, cudaEventElapsedTime(&ms, e0, e1));
+            c.ms = ms;
+            if (ms < best_ms) { best_ms = ms; best = c; }
+        }
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        if (best_ms >= 1e30f) return fail(ctx, B2M_ERR_UNSUPPORTED, "batch: no tile shape fits");
+        ctx->batch_tunes[sig] = best;
+    }
+    if (tune_out) *tune_out = best;
+    const GraphKey key{7 + mode * 10, A, B, X, info, count, (int64_t)sig,
+                       best.pw_large * 10000 + best.pw_small * 100 + best.group_warps,
+                       (int64_t)reinterpret_cast<intptr_t>(iters)};
+    return run_graph(ctx, st, key, [&](cudaStream_t q) { return launch(best, q); });
+}
+
+}  // namespace b2m

@@ -66,6 +66,15 @@ struct GraphEntry {
     uint64_t last_use = 0;
 };
 
+// tile shape of the batched solve, chosen by its autotuner (batched.cu)
+struct BatchTune {
+    int small_n;      // systems of order <= small_n run on groups of group_warps warps
+    int group_warps;
+    int pw_large;     // panel widths of the two size buckets
+    int pw_small;
+    float ms;         // measured time of the whole batch with this shape
+};
+
 struct Ctx {
     int device = 0;
     int num_sms = 148;
@@ -86,6 +95,9 @@ struct Ctx {
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     std::string last_error;
     std::mutex mtx;
+    std::map<uint64_t, BatchTune> batch_tunes;  // per batch plan
+    uint64_t batch_plan_sig = 0;                 // plan whose metadata is on the device now
+    void* batch_plan_dev = nullptr;
 };
 
 // records a message and returns the status (for `return fail(ctx, ...)`)

@@ -102,6 +102,14 @@ int32_t launch_trsm_small(Ctx* ctx, cudaStream_t st, const T* L, int64_t ldl, T*
 }  // namespace b2m
 
 namespace b2m {
+// Batched solves of `count` independent systems (batched.cu); metadata arrays are host memory,
+// A/B/X/info/iters device memory.  tune_out (may be null) receives the tile shape used.
+int32_t batch_solve(Ctx* ctx, cudaStream_t st, int64_t count, const int32_t* n, const int32_t* k,
+                    const int64_t* a_off, const int64_t* b_off, const double* A, const double* B, double* X,
+                    int mode, int32_t* info, int32_t* iters, BatchTune* tune_out);
+}  // namespace b2m
+
+namespace b2m {
 struct MixedReport {
     int32_t iterations;
     int32_t fell_back;

@@ -227,3 +227,51 @@ def dev_MatrixLinEQSolveAdjoint(LU, indx, X, G, Lam, dA=None, op=DO_NONE, ctx=No
     c.call("b2m_dev_MatrixLinEQSolveAdjoint", _tptr(LU), _tlw(LU), LU.shape[1], _tptr(indx), _tptr(X), _tlw(X),
            _tptr(G), _tlw(G), X.shape[1], _tptr(Lam), _tlw(Lam), _tptr(dA) if dA is not None else None,
            _tlw(dA) if dA is not None else 0, op)
+
+
+# ----------------------------------------------------------------------------- batched uneven solves
+def pack_batch(mats, rhss):
+    """Packs lists of square A_i and B_i (n_i x k_i) into the flat layout of b2m_BatchLinEQSolve:
+    returns (n, nrhs, a_off, b_off, A, B) with int32 orders / RHS counts and int64 offsets."""
+    n = np.array([m.shape[0] for m in mats], dtype=np.int32)
+    k = np.array([b.shape[1] for b in rhss], dtype=np.int32)
+    a_sz = n.astype(np.int64) ** 2
+    b_sz = n.astype(np.int64) * k
+    a_off = np.concatenate([[0], np.cumsum(a_sz)[:-1]]).astype(np.int64)
+    b_off = np.concatenate([[0], np.cumsum(b_sz)[:-1]]).astype(np.int64)
+    A = np.concatenate([np.ascontiguousarray(m, dtype=np.float64).ravel() for m in mats])
+    B = np.concatenate([np.ascontiguousarray(b, dtype=np.float64).ravel() for b in rhss])
+    return n, k, a_off, b_off, A, B
+
+
+def unpack_batch(X: np.ndarray, n, k, b_off):
+    return [X[o:o + ni * ki].reshape(ni, ki) for ni, ki, o in zip(n, k, b_off)]
+
+
+def BatchLinEQSolve(mats, rhss, mode: int = 0, ctx: Context | None = None):
+    """Solves every A_i X_i = B_i in one batched launch; returns (list of X_i, info, iters)."""
+    n, k, a_off, b_off, A, B = pack_batch(mats, rhss)
+    X = np.zeros_like(B)
+    info = np.zeros(len(n), dtype=np.int32)
+    iters = np.zeros(len(n), dtype=np.int32)
+    _ctx_of(ctx).call("b2m_BatchLinEQSolve", len(n), n.ctypes.data, k.ctypes.data, a_off.ctypes.data,
+                      b_off.ctypes.data, _ptr(A), _ptr(B), _ptr(X), mode, info.ctypes.data, iters.ctypes.data)
+    return unpack_batch(X, n, k, b_off), info, iters
+
+
+def dev_BatchLinEQSolve(n, k, a_off, b_off, A, B, X, info, iters=None, mode: int = 0, ctx=None):
+    """Device twin: plan arrays (numpy int32 / int64) on the host, A/B/X (flat float64) and
+    info/iters (int32) torch CUDA tensors; asynchronous on torch's current stream."""
+    c = _ctx_of(ctx)
+    _bind_stream(c, A)
+    c.call("b2m_dev_BatchLinEQSolve", len(n), n.ctypes.data, k.ctypes.data, a_off.ctypes.data, b_off.ctypes.data,
+           _tptr(A), _tptr(B), _tptr(X), mode, _tptr(info), _tptr(iters) if iters is not None else None)
+
+
+def batch_tune(ctx=None) -> dict:
+    """The tile shape the batched solve's autotuner chose for the last plan."""
+    vals = [C.c_int32(0) for _ in range(4)]
+    ms = C.c_float(0.0)
+    _ctx_of(ctx).call("b2m_batch_tune_read", *[C.addressof(v) for v in vals], C.addressof(ms))
+    return {"small_n": vals[0].value, "group_warps": vals[1].value, "pw_large": vals[2].value,
+            "pw_small": vals[3].value, "ms": ms.value}
