@@ -27,6 +27,7 @@
 #include <chrono>
 #include <cstring>
 #include <numeric>
+#include <type_traits>
 #include <vector>
 
 #include "common.cuh"
@@ -126,18 +127,34 @@ __device__ __forceinline__ void grp_argmax(const Grp& g, const Slice& s, double 
     g.sync();
 }
 
-// Blocked LU of the n x n matrix W (row-major, ld n, element type T) with row permutation perm.
+// Blocked LU of the n x n matrix A0 (FP64, row-major, ld n) into W (element type T, same layout)
+// with row permutation perm.  The first panel reads A0 directly and its updates write every entry
+// of W, so A0 is never copied separately.  Global loads are issued in groups before they are used
+// (a loop that loads, computes and stores one element at a time pays one L2 latency per element).
 // Returns 0, or 1 when a pivot is <= the singular threshold (uniform across the group).
 template <typename T>
-__device__ int grp_lu(const Grp& g, const Slice& s, T* W, int n, int PW) {
+__device__ int grp_lu(const Grp& g, const Slice& s, const double* A0, T* W, int n, int PW) {
     for (int i = g.tid; i < n; i += g.nt) s.perm[i] = i;
     g.sync();
     const int pwp = PW + 1;
     for (int c0 = 0; c0 < n; c0 += PW) {
+        const bool first = c0 == 0;
+        auto at = [&](int row, int col) -> T {
+            return first ? (T)A0[(int64_t)row * n + col] : W[(int64_t)row * n + col];
+        };
         const int pw = min(PW, n - c0), m = n - c0;
-        for (int e = g.tid; e < m * pw; e += g.nt) {
-            const int r = e / pw, c = e - r * pw;
-            s.pan[r * pwp + c] = (double)W[(int64_t)s.perm[c0 + r] * n + c0 + c];
+        // panel: one factor row per thread, all of its loads in flight
+        for (int r = g.tid; r < m; r += g.nt) {
+            const int row = s.perm[c0 + r];
+            for (int cb = 0; cb < pw; cb += 8) {
+                T v[8];
+#pragma unroll
+                for (int c = 0; c < 8; ++c)
+                    if (cb + c < pw) v[c] = at(row, c0 + cb + c);
+#pragma unroll
+                for (int c = 0; c < 8; ++c)
+                    if (cb + c < pw) s.pan[r * pwp + cb + c] = (double)v[c];
+            }
         }
         g.sync();
         for (int j = 0; j < pw; ++j) {
@@ -174,15 +191,24 @@ __device__ int grp_lu(const Grp& g, const Slice& s, T* W, int n, int PW) {
             }
             g.sync();
         }
-        for (int e = g.tid; e < m * pw; e += g.nt) {
-            const int r = e / pw, c = e - r * pw;
-            W[(int64_t)s.perm[c0 + r] * n + c0 + c] = (T)s.pan[r * pwp + c];
+        for (int r = g.tid; r < m; r += g.nt) {
+            T* dst = W + (int64_t)s.perm[c0 + r] * n + c0;
+            for (int c = 0; c < pw; ++c) dst[c] = (T)s.pan[r * pwp + c];
         }
         const int c1 = c0 + pw, nr = n - c1;
         if (nr > 0) {
-            // block row of U: u = L11^-1 A12 (thread per column, in shared memory)
+            // block row of U: u = L11^-1 A12 (thread per column, loads in groups of 8)
             for (int c = g.tid; c < nr; c += g.nt) {
-                for (int r = 0; r < pw; ++r) s.u[r * s.us + c] = (double)W[(int64_t)s.perm[c0 + r] * n + c1 + c];
+                for (int r0 = 0; r0 < pw; r0 += 8) {
+                    T v[8];
+#pragma unroll
+                    for (int e = 0; e < 8; ++e)
+                        if (r0 + e < pw) v[e] = at(s.perm[c0 + r0 + e], c1 + c);
+#pragma unroll
+                    for (int e = 0; e < 8; ++e)
+                        if (r0 + e < pw) s.u[(r0 + e) * s.us + c] = (double)v[e];
+                }
+                W[(int64_t)s.perm[c0] * n + c1 + c] = (T)s.u[c];
                 for (int r = 1; r < pw; ++r) {
                     T acc = (T)s.u[r * s.us + c];
                     for (int q = 0; q < r; ++q) acc -= (T)s.pan[r * pwp + q] * (T)s.u[q * s.us + c];
@@ -191,14 +217,58 @@ __device__ int grp_lu(const Grp& g, const Slice& s, T* W, int n, int PW) {
                 }
             }
             g.sync();
-            // trailing update: A22 -= L21 U12
-            for (int e = g.tid; e < nr * nr; e += g.nt) {
-                const int r = e / nr, c = e - r * nr;
-                T* p = W + (int64_t)s.perm[c1 + r] * n + c1 + c;
-                T acc = *p;
-                const double* lr = s.pan + (pw + r) * pwp;
-                for (int q = 0; q < pw; ++q) acc -= (T)lr[q] * (T)s.u[q * s.us + c];
-                *p = acc;
+            if constexpr (std::is_same<T, double>::value) {
+                // trailing update A22 -= L21 U12 on the FP64 tensor cores: warps walk 16 x 8 tiles;
+                // m16n8k4 fragments (g = lane / 4, t = lane % 4): a = (L21[g][k+t], L21[g+8][k+t]),
+                // b = U12[k+t][g], c = C[g][2t..2t+1], C[g+8][2t..2t+1]
+                const int lane = g.tid & 31, nw = g.nt >> 5, gq = lane >> 2, tq = lane & 3;
+                const int tm = (nr + 15) / 16, tn = (nr + 7) / 8;
+                for (int tile = g.tid >> 5; tile < tm * tn; tile += nw) {
+                    const int r0 = (tile / tn) * 16, q0 = (tile % tn) * 8;
+                    const int ra = r0 + gq, rb = r0 + gq + 8, cc = q0 + 2 * tq;
+                    const bool oka = ra < nr, okb = rb < nr;
+                    const int64_t rowa = oka ? (int64_t)s.perm[c1 + ra] * n : 0, rowb = okb ? (int64_t)s.perm[c1 + rb] * n : 0;
+                    double d[4];
+                    d[0] = (oka && cc < nr) ? (double)at(rowa / n, c1 + cc) : 0.0;
+                    d[1] = (oka && cc + 1 < nr) ? (double)at(rowa / n, c1 + cc + 1) : 0.0;
+                    d[2] = (okb && cc < nr) ? (double)at(rowb / n, c1 + cc) : 0.0;
+                    d[3] = (okb && cc + 1 < nr) ? (double)at(rowb / n, c1 + cc + 1) : 0.0;
+                    const double* la = s.pan + (pw + min(ra, nr - 1)) * pwp;
+                    const double* lb = s.pan + (pw + min(rb, nr - 1)) * pwp;
+                    const int cb = min(q0 + gq, nr - 1);
+                    for (int k = 0; k < pw; k += 4) {
+                        const int kk = k + tq;
+                        const double a0 = kk < pw ? -la[kk] : 0.0;
+                        const double a1 = kk < pw ? -lb[kk] : 0.0;
+                        const double b0 = kk < pw ? s.u[kk * s.us + cb] : 0.0;
+                        asm volatile(
+                            "mma.sync.aligned.m16n8k4.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5}, {%6}, "
+                            "{%0,%1,%2,%3};\n"
+                            : "+d"(d[0]), "+d"(d[1]), "+d"(d[2]), "+d"(d[3])
+                            : "d"(a0), "d"(a1), "d"(b0));
+                    }
+                    if (oka && cc < nr) W[rowa + c1 + cc] = (T)d[0];
+                    if (oka && cc + 1 < nr) W[rowa + c1 + cc + 1] = (T)d[1];
+                    if (okb && cc < nr) W[rowb + c1 + cc] = (T)d[2];
+                    if (okb && cc + 1 < nr) W[rowb + c1 + cc + 1] = (T)d[3];
+                }
+            } else {
+            // trailing update A22 -= L21 U12: thread per column, 8 rows per step, loads first
+            for (int c = g.tid; c < nr; c += g.nt) {
+                for (int r0 = 0; r0 < nr; r0 += 8) {
+                    T v[8];
+#pragma unroll
+                    for (int e = 0; e < 8; ++e) v[e] = r0 + e < nr ? at(s.perm[c1 + r0 + e], c1 + c) : (T)0;
+                    for (int q = 0; q < pw; ++q) {
+                        const T uq = (T)s.u[q * s.us + c];
+#pragma unroll
+                        for (int e = 0; e < 8; ++e) v[e] -= (T)s.pan[min(pw + r0 + e, m - 1) * pwp + q] * uq;
+                    }
+#pragma unroll
+                    for (int e = 0; e < 8; ++e)
+                        if (r0 + e < nr) W[(int64_t)s.perm[c1 + r0 + e] * n + c1 + c] = v[e];
+                }
+            }
             }
             g.sync();
         }
@@ -206,34 +276,35 @@ __device__ int grp_lu(const Grp& g, const Slice& s, T* W, int n, int PW) {
     return 0;
 }
 
-// y (factor order, kk columns) <- U^-1 L^-1 y with the factors in W (element type T)
+// y (factor order, kk columns) <- U^-1 L^-1 y with the factors in W (element type T).  Each
+// 32-row diagonal block is staged in shared memory (over the then idle panel / U buffers); one warp
+// per right-hand side substitutes it with shuffles, then the group folds it into the other rows.
 template <typename T>
 __device__ void grp_solve(const Grp& g, const Slice& s, const T* W, int n, int kk) {
     const int lane = g.tid & 31, w = g.tid >> 5, nw = g.nt >> 5;
     const int nb = (n + 31) / 32;
+    double* blk = s.pan;  // [32][33], spans into the U buffer for narrow panels
     for (int pass = 0; pass < 2; ++pass) {
         const bool lower = pass == 0;
         for (int bi = 0; bi < nb; ++bi) {
             const int b = lower ? bi : nb - 1 - bi;
             const int b0 = 32 * b, bs = min(32, n - b0);
+            for (int e = g.tid; e < 32 * 32; e += g.nt) {
+                const int r = e >> 5, j = e & 31;
+                blk[r * 33 + j] = (r < bs && j < bs) ? (double)W[(int64_t)s.perm[b0 + r] * n + b0 + j] : 0.0;
+            }
+            g.sync();
             for (int q = w; q < kk; q += nw) {
-                double tr[32];
                 const int row = b0 + lane;
-#pragma unroll
-                for (int j = 0; j < 32; ++j)
-                    tr[j] = (lane < bs && j < bs) ? (double)W[(int64_t)s.perm[row] * n + b0 + j] : 0.0;
+                const double* tr = blk + lane * 33;
                 double yv = lane < bs ? s.y[row * kBMaxK + q] : 0.0;
                 if (lower) {
-#pragma unroll
-                    for (int j = 0; j < 32; ++j) {
-                        if (j >= bs) break;
+                    for (int j = 0; j < bs; ++j) {
                         const double xj = __shfl_sync(0xffffffffu, yv, j);
                         if (lane > j) yv = (double)((T)yv - (T)tr[j] * (T)xj);
                     }
                 } else {
-#pragma unroll
-                    for (int j = 31; j >= 0; --j) {
-                        if (j >= bs) continue;
+                    for (int j = bs - 1; j >= 0; --j) {
                         if (lane == j) yv = (double)((T)yv / (T)tr[j]);
                         const double xj = __shfl_sync(0xffffffffu, yv, j);
                         if (lane < j) yv = (double)((T)yv - (T)tr[j] * (T)xj);
@@ -247,7 +318,14 @@ __device__ void grp_solve(const Grp& g, const Slice& s, const T* W, int n, int k
                 const int r = rlo + e / kk, q = e % kk;
                 const T* lr = W + (int64_t)s.perm[r] * n + b0;
                 T acc = (T)s.y[r * kBMaxK + q];
-                for (int j = 0; j < bs; ++j) acc -= lr[j] * (T)s.y[(b0 + j) * kBMaxK + q];
+                for (int j0 = 0; j0 < bs; j0 += 8) {
+                    T v[8];
+#pragma unroll
+                    for (int e2 = 0; e2 < 8; ++e2) v[e2] = j0 + e2 < bs ? lr[j0 + e2] : (T)0;
+#pragma unroll
+                    for (int e2 = 0; e2 < 8; ++e2)
+                        if (j0 + e2 < bs) acc -= v[e2] * (T)s.y[(b0 + j0 + e2) * kBMaxK + q];
+                }
                 s.y[r * kBMaxK + q] = (double)acc;
             }
             g.sync();
@@ -259,9 +337,7 @@ __device__ void grp_solve(const Grp& g, const Slice& s, const T* W, int n, int k
 __device__ int solve_plain(const Grp& g, const Slice& s, const BatchArgs& a, int sys, double* W) {
     const int n = a.n[sys], kk = a.k[sys];
     const double* A = a.A + a.a_off[sys];
-    for (int e = g.tid; e < n * n; e += g.nt) W[e] = A[e];
-    g.sync();
-    if (grp_lu<double>(g, s, W, n, g.nt == kBThreads ? a.pw_large : a.pw_small)) return 1;
+    if (grp_lu<double>(g, s, A, W, n, g.nt == kBThreads ? a.pw_large : a.pw_small)) return 1;
     const double* B = a.B + a.b_off[sys];
     for (int e = g.tid; e < n * kk; e += g.nt) {
         const int i = e / kk, q = e - i * kk;
@@ -285,19 +361,20 @@ __device__ int solve_mixed(const Grp& g, const Slice& s, const BatchArgs& a, int
     const double* A = a.A + a.a_off[sys];
     const double* B = a.B + a.b_off[sys];
     double* X = a.X + a.b_off[sys];
-    for (int e = g.tid; e < n * n; e += g.nt) W[e] = (float)A[e];
-    g.sync();
-    if (grp_lu<float>(g, s, W, n, g.nt == kBThreads ? a.pw_large : a.pw_small)) return -1;
-    // ||A||inf (kept in s.red[7] after the reduction below) and ||b_q||inf
+    if (grp_lu<float>(g, s, A, W, n, g.nt == kBThreads ? a.pw_large : a.pw_small)) return -1;
+    // ||A||inf: a warp per row
+    const int lane = g.tid & 31, wp = g.tid >> 5, nw = g.nt >> 5;
     double an = 0.0;
-    for (int i = g.tid; i < n; i += g.nt) {
+    for (int i = wp; i < n; i += nw) {
         double rs = 0.0;
-        for (int j = 0; j < n; ++j) rs += fabs(A[(int64_t)i * n + j]);
+        for (int j = lane; j < n; j += 32) rs += fabs(A[(int64_t)i * n + j]);
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) rs += __shfl_xor_sync(0xffffffffu, rs, o);
         an = fmax(an, rs);
     }
     double bv;
     int bi;
-    grp_argmax(g, s, an, g.tid < n ? 0 : -1, bv, bi);
+    grp_argmax(g, s, an, 0, bv, bi);
     const double normA = bv;
     for (int e = g.tid; e < n * kk; e += g.nt) X[e] = 0.0;
     // r = b in factor order
@@ -307,34 +384,60 @@ __device__ int solve_mixed(const Grp& g, const Slice& s, const BatchArgs& a, int
     }
     g.sync();
     const double tol = (double)n * 0x1.0p-53;
+    const int nmax = s.us - 1;
+    double* res = s.pan;  // [n][kBMaxK] residual, natural order (the panel buffer is free now)
+    unsigned long long* mx = reinterpret_cast<unsigned long long*>(s.pan + (size_t)nmax * kBMaxK);  // [3][8]
     double prev = INFINITY;
     for (int it = 1; it <= a.max_iter; ++it) {
         grp_solve<float>(g, s, W, n, kk);
-        for (int e = g.tid; e < n * kk; e += g.nt) X[e] += s.y[(e / kk) * kBMaxK + (e % kk)];
+        for (int e = g.tid; e < n * kk; e += g.nt) {
+            const int i = e / kk, q = e - i * kk;
+            const double xv = X[e] + s.y[i * kBMaxK + q];
+            X[e] = xv;
+            s.y[i * kBMaxK + q] = xv;  // x in natural order for the residual below
+        }
+        if (g.tid < 3 * kBMaxK) mx[g.tid] = 0ull;
         g.sync();
-        // r = b - A x (FP64), written in factor order; eta over the columns
+        // r = b - A x in FP64, a warp per row (coalesced rows of A), with the column maxima
+        for (int i = wp; i < n; i += nw) {
+            double acc[kBMaxK];
+#pragma unroll
+            for (int q = 0; q < kBMaxK; ++q) acc[q] = 0.0;
+            for (int j = lane; j < n; j += 32) {
+                const double aij = A[(int64_t)i * n + j];
+#pragma unroll
+                for (int q = 0; q < kBMaxK; ++q)
+                    if (q < kk) acc[q] = fma(aij, s.y[j * kBMaxK + q], acc[q]);
+            }
+#pragma unroll
+            for (int q = 0; q < kBMaxK; ++q) {
+                double v = acc[q];
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+                if (lane == q && q < kk) {
+                    const double bq = B[(int64_t)i * kk + q], xq = s.y[i * kBMaxK + q];
+                    const double rq = bq - v;
+                    res[i * kBMaxK + q] = rq;
+                    atomicMax(&mx[q], (unsigned long long)__double_as_longlong(fabs(rq)));
+                    atomicMax(&mx[kBMaxK + q], (unsigned long long)__double_as_longlong(fabs(xq)));
+                    atomicMax(&mx[2 * kBMaxK + q], (unsigned long long)__double_as_longlong(fabs(bq)));
+                }
+            }
+        }
+        g.sync();
         double eta = 0.0;
         for (int q = 0; q < kk; ++q) {
-            double rmax = 0.0, xmax = 0.0, bmax = 0.0;
-            for (int i = g.tid; i < n; i += g.nt) {
-                double acc = B[(int64_t)i * kk + q];
-                for (int j = 0; j < n; ++j) acc = fma(-A[(int64_t)i * n + j], X[(int64_t)j * kk + q], acc);
-                s.pan[i] = acc;  // residual in natural order (the panel buffer is free now)
-                rmax = fmax(rmax, fabs(acc));
-                xmax = fmax(xmax, fabs(X[(int64_t)i * kk + q]));
-                bmax = fmax(bmax, fabs(B[(int64_t)i * kk + q]));
-            }
-            g.sync();
-            double r1, x1, b1;
-            int d;
-            grp_argmax(g, s, rmax, g.tid < n ? 0 : -1, r1, d);
-            grp_argmax(g, s, xmax, g.tid < n ? 0 : -1, x1, d);
-            grp_argmax(g, s, bmax, g.tid < n ? 0 : -1, b1, d);
+            const double r1 = __longlong_as_double((long long)mx[q]);
+            const double x1 = __longlong_as_double((long long)mx[kBMaxK + q]);
+            const double b1 = __longlong_as_double((long long)mx[2 * kBMaxK + q]);
             const double den = normA * x1 + b1;
             eta = fmax(eta, den > 0.0 ? r1 / den : (r1 > 0.0 ? INFINITY : 0.0));
-            for (int i = g.tid; i < n; i += g.nt) s.y[i * kBMaxK + q] = s.pan[s.perm[i]];
-            g.sync();
         }
+        for (int e = g.tid; e < n * kk; e += g.nt) {
+            const int i = e / kk, q = e - i * kk;
+            s.y[i * kBMaxK + q] = res[s.perm[i] * kBMaxK + q];
+        }
+        g.sync();
         if (eta <= tol) return it;
         if (!(eta < INFINITY) || (it >= 2 && eta > 0.5 * prev)) return -1;
         prev = eta;
