@@ -91,6 +91,18 @@ B2M_API int32_t b2m_MatrixMultEx(b2m_ctx* ctx, double* dest, int64_t destLineWid
 B2M_API int32_t b2m_dev_MatrixMultEx(b2m_ctx* ctx, double* dest, int64_t destLineWidth, const double* mt1,
                              const double* mt2, int64_t width1, int64_t height1, int64_t width2, int64_t height2,
                              int64_t LineWidth1, int64_t LineWidth2, int32_t op, int32_t trans);
+/* MatrixMultEx (trans 0) emulated on the INT8 tensor cores (Ozaki scheme).  No counterpart in the
+ * reference: an alternative engine for MatrixMult / MatrixMultEx (MatrixASMStubSwitch.pas:769-782),
+ * same arguments plus `slices` (2..10, 0 = 8): every row of mt1 and column of mt2 is scaled by a
+ * power of two and cut into `slices` signed 7-bit pieces, and the pairwise products are summed
+ * exactly in int32 and scaled in FP64.  The error is below about 2^-7(slices+1) times
+ * |row max of mt1| |column max of mt2| times the inner dimension. */
+B2M_API int32_t b2m_MatrixMultOzaki(b2m_ctx* ctx, double* dest, int64_t destLineWidth, const double* mt1,
+                            const double* mt2, int64_t width1, int64_t height1, int64_t width2, int64_t height2,
+                            int64_t LineWidth1, int64_t LineWidth2, int32_t op, int32_t slices);
+B2M_API int32_t b2m_dev_MatrixMultOzaki(b2m_ctx* ctx, double* dest, int64_t destLineWidth, const double* mt1,
+                                const double* mt2, int64_t width1, int64_t height1, int64_t width2,
+                                int64_t height2, int64_t LineWidth1, int64_t LineWidth2, int32_t op, int32_t slices);
 
 /* ------------------------------------------------------------------ LU (src/LinAlgLU.pas) */
 /* MatrixLUDecompInPlace LinAlgLU.pas:283-295 */

@@ -55,6 +55,8 @@ SIGNATURES: dict[str, tuple] = {
     "b2m_dev_MatrixLinEQSolveNoAlloc": (i32, [vp, vp, i64, i64, vp, i64, vp, i64, i64, vp]),
     "b2m_MatrixLinEQSolveMixed": (i32, [vp, vp, i64, i64, vp, i64, vp, i64, i64, i32, i32, dbl, vp]),
     "b2m_dev_MatrixLinEQSolveMixed": (i32, [vp, vp, i64, i64, vp, i64, vp, i64, i64, i32, i32, dbl, vp]),
+    "b2m_MatrixMultOzaki": (i32, [vp, vp, i64, vp, vp, i64, i64, i64, i64, i64, i64, i32, i32]),
+    "b2m_dev_MatrixMultOzaki": (i32, [vp, vp, i64, vp, vp, i64, i64, i64, i64, i64, i64, i32, i32]),
     "b2m_BatchLinEQSolve": (i32, [vp, i64, vp, vp, vp, vp, vp, vp, vp, i32, vp, vp]),
     "b2m_dev_BatchLinEQSolve": (i32, [vp, i64, vp, vp, vp, vp, vp, vp, vp, i32, vp, vp]),
     "b2m_batch_tune_read": (i32, [vp, vp, vp, vp, vp, vp]),

@@ -717,3 +717,54 @@ extern "C" int32_t b2m_batch_tune_read(b2m_ctx* h, int32_t* small_n, int32_t* gr
     if (ms) *ms = t.ms;
     return B2M_OK;
 }
+
+// ------------------------------------------------------------------ Ozaki split-precision GEMM
+extern "C" int32_t b2m_dev_MatrixMultOzaki(b2m_ctx* h, double* dest, int64_t destLineWidth, const double* mt1,
+                                           const double* mt2, int64_t width1, int64_t height1, int64_t width2,
+                                           int64_t height2, int64_t LineWidth1, int64_t LineWidth2, int32_t op,
+                                           int32_t slices) {
+    Ctx* ctx = as_ctx(h);
+    if (!ctx) return B2M_ERR_ARG;
+    std::lock_guard<std::mutex> lk(ctx->mtx);
+    if (!dest || !mt1 || !mt2) return fail(ctx, B2M_ERR_ARG, "null pointer");
+    if (op < 0 || op > 2) return fail(ctx, B2M_ERR_ARG, "invalid op");
+    if (width1 != height2 || width1 < 0 || height1 < 0 || width2 < 0)
+        return fail(ctx, B2M_ERR_DIM, "Dimension error");
+    if (!lw_ok(LineWidth1, width1) || !lw_ok(LineWidth2, width2) || !lw_ok(destLineWidth, width2))
+        return fail(ctx, B2M_ERR_DIM, "Line widths do not match");
+    return ozaki_gemm(ctx, ctx->stream, mt1, LineWidth1 / 8, mt2, LineWidth2 / 8, dest, destLineWidth / 8, height1,
+                      width2, width1, op, slices <= 0 ? 8 : slices);
+}
+
+extern "C" int32_t b2m_MatrixMultOzaki(b2m_ctx* h, double* dest, int64_t destLineWidth, const double* mt1,
+                                       const double* mt2, int64_t width1, int64_t height1, int64_t width2,
+                                       int64_t height2, int64_t LineWidth1, int64_t LineWidth2, int32_t op,
+                                       int32_t slices) {
+    Ctx* ctx = as_ctx(h);
+    if (!ctx) return B2M_ERR_ARG;
+    std::lock_guard<std::mutex> lk(ctx->mtx);
+    if (!dest || !mt1 || !mt2) return fail(ctx, B2M_ERR_ARG, "null pointer");
+    if (op < 0 || op > 2) return fail(ctx, B2M_ERR_ARG, "invalid op");
+    if (width1 != height2 || width1 < 0 || height1 < 0 || width2 < 0)
+        return fail(ctx, B2M_ERR_DIM, "Dimension error");
+    if (!lw_ok(LineWidth1, width1) || !lw_ok(LineWidth2, width2) || !lw_ok(destLineWidth, width2))
+        return fail(ctx, B2M_ERR_DIM, "Line widths do not match");
+    if (height1 == 0 || width2 == 0) return B2M_OK;
+    cudaSetDevice(ctx->device);
+    const int64_t M = height1, N = width2, K = width1;
+    const int64_t lda = padded_ld(K), ldb = padded_ld(N);
+    void *pa, *pb, *pc;
+    B2M_TRY(ws_get(ctx, kWsMatA, (size_t)(std::max<int64_t>(M, 1) * lda * 8), &pa));
+    B2M_TRY(ws_get(ctx, kWsMatB, (size_t)(std::max<int64_t>(K, 1) * ldb * 8), &pb));
+    B2M_TRY(ws_get(ctx, kWsMatC, (size_t)(M * ldb * 8), &pc));
+    if (K > 0) {
+        B2M_TRY(upload(ctx, (double*)pa, lda, mt1, LineWidth1, M, K));
+        B2M_TRY(upload(ctx, (double*)pb, ldb, mt2, LineWidth2, K, N));
+    }
+    if (op != B2M_DO_NONE) B2M_TRY(upload(ctx, (double*)pc, ldb, dest, destLineWidth, M, N));
+    B2M_TRY(reset_status(ctx));
+    B2M_TRY(ozaki_gemm(ctx, ctx->stream, (double*)pa, lda, (double*)pb, ldb, (double*)pc, ldb, M, N, K, op,
+                       slices <= 0 ? 8 : slices));
+    B2M_TRY(download(ctx, dest, destLineWidth, (double*)pc, ldb, M, N));
+    return finish(ctx);
+}

@@ -45,6 +45,10 @@ int32_t solve_adjoint_f64(Ctx* ctx, cudaStream_t st, const double* LU, int64_t l
                           const double* X, int64_t ldx, const double* G, int64_t ldg, int64_t nrhs, double* Lam,
                           int64_t ldl, double* dA, int64_t ldd, int op, double* Y, int64_t ldy);
 
+// C (M x N) op= A (M x K) B (K x N) in FP64 emulated with int8 slices on tcgen05 (ozaki.cu)
+int32_t ozaki_gemm(Ctx* ctx, cudaStream_t st, const double* A, int64_t lda, const double* B, int64_t ldb, double* C,
+                   int64_t ldc, int64_t M, int64_t N, int64_t K, int op, int s);
+
 // Builds perm from ipiv on the device (used when factors come from outside: b2m_MatrixLUBackSubst).
 int32_t perm_from_ipiv(Ctx* ctx, cudaStream_t st, const int32_t* ipiv, int64_t n, int32_t* perm);
 

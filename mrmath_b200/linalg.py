@@ -58,6 +58,18 @@ def MatrixMultEx(dest: np.ndarray, mt1: np.ndarray, mt2: np.ndarray, op: int = D
            op, trans)
 
 
+def MatrixMultOzaki(mt1: np.ndarray, mt2: np.ndarray, slices: int = 8, dest: np.ndarray | None = None,
+                    op: int = DO_NONE, ctx: Context | None = None) -> np.ndarray:
+    """mt1 * mt2 in FP64 emulated on the INT8 tensor cores with `slices` 7-bit slices per operand."""
+    h1, w1 = mt1.shape
+    h2, w2 = mt2.shape
+    if dest is None:
+        dest = np.zeros((h1, w2))
+    _ctx_of(ctx).call("b2m_MatrixMultOzaki", _ptr(dest), _lw(dest), _ptr(mt1), _ptr(mt2), w1, h1, w2, h2, _lw(mt1),
+                      _lw(mt2), op, slices)
+    return dest
+
+
 def MatrixMult(mt1: np.ndarray, mt2: np.ndarray, ctx: Context | None = None) -> np.ndarray:
     dest = np.empty((mt1.shape[0], mt2.shape[1]))
     MatrixMultEx(dest, mt1, mt2, DO_NONE, 0, ctx)
@@ -275,3 +287,12 @@ def batch_tune(ctx=None) -> dict:
     _ctx_of(ctx).call("b2m_batch_tune_read", *[C.addressof(v) for v in vals], C.addressof(ms))
     return {"small_n": vals[0].value, "group_warps": vals[1].value, "pw_large": vals[2].value,
             "pw_small": vals[3].value, "ms": ms.value}
+
+
+def dev_MatrixMultOzaki(dest, mt1, mt2, slices=8, op=DO_NONE, ctx=None):
+    c = _ctx_of(ctx)
+    _bind_stream(c, dest)
+    h1, w1 = mt1.shape
+    h2, w2 = mt2.shape
+    c.call("b2m_dev_MatrixMultOzaki", _tptr(dest), _tlw(dest), _tptr(mt1), _tptr(mt2), w1, h1, w2, h2, _tlw(mt1),
+           _tlw(mt2), op, slices)
