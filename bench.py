@@ -44,6 +44,10 @@ def parse():
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--no-plain", action="store_true", help="skip the plain FP64 comparison steps")
+    p.add_argument("--workload", choices=["solve", "gemm", "ozaki", "batched", "adjoint"], default="solve",
+                   help="solve: the headline (default); gemm / ozaki: m=n=k=8192 FP64 product with the "
+                        "g*2^e distribution; batched: 20,000 uneven systems; adjoint: n=4096 gradient step")
+    p.add_argument("--mode", type=int, default=0, help="batched: 0 plain FP64, 1 FP32 + FP64 refinement")
     p.add_argument("--cpu-n", type=int, default=4096, help="order of the CPU-baseline sample")
     return p.parse_args()
 
@@ -365,12 +369,121 @@ def run_b200(args, world, rank, local):
     return 0
 
 
+# ----------------------------------------------------------------------------- secondary workloads
+def _timed(fn, steps, warmup):
+    import torch
+    for _ in range(warmup):
+        fn()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(steps):
+        fn()
+    e1.record()
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / steps
+
+
+def run_secondary(args, world, rank, local):
+    """The other scope rows, one JSON line each: replicas per rank like the headline."""
+    import numpy as np
+    import torch
+
+    import mrmath_b200
+    from mrmath_b200 import inputs, linalg as L
+
+    torch.cuda.set_device(local)
+    ctx = mrmath_b200.Context(local)
+    dev = f"cuda:{local}"
+    extra = {}
+    with ClockSampler(local) as clk:
+        if args.workload in ("gemm", "ozaki"):
+            n = 8192
+            a, b = inputs.c3_gauss_exp(n, n, n, seed=15 + rank)
+            A, B = torch.from_numpy(a).to(dev), torch.from_numpy(b).to(dev)
+            C = torch.empty((n, n), dtype=torch.float64, device=dev)
+            if args.workload == "gemm":
+                fn = lambda: L.dev_MatrixMultEx(C, A, B, ctx=ctx)
+            else:
+                fn = lambda: L.dev_MatrixMultOzaki(C, A, B, slices=8, ctx=ctx)
+            ms = _timed(fn, args.steps, args.warmup)
+            work, unit = 2.0 * n ** 3, "GFLOP/s"
+            metric = f"FP64 {'DGEMM (DMMA)' if args.workload == 'gemm' else 'Ozaki int8 GEMM, 8 slices'} GFLOP/s at 8192^3"
+            if args.workload == "ozaki":
+                ref = torch.empty_like(C)
+                L.dev_MatrixMultEx(ref, A, B, ctx=ctx)
+                torch.cuda.synchronize()
+                scale = (A.abs() @ B.abs()).max()
+                extra["max_abs_diff_vs_native_dgemm_over_max_absAabsB"] = float(((C - ref).abs().max() / scale).item())
+            config = {"workload": f"C = A B, m=n=k=8192, entries g*2^e (g Gaussian, e uniform in [-8, 8])", "n": n}
+            dtype = "f64" if args.workload == "gemm" else "int8 slices -> f64"
+        elif args.workload == "batched":
+            sizes, nrhs, mats, rhss = inputs.c5_batched(20000, seed=15 + rank)
+            nn, kk, a_off, b_off, Ah, Bh = L.pack_batch(mats, rhss)
+            dA, dB = torch.from_numpy(Ah).to(dev), torch.from_numpy(Bh).to(dev)
+            dX = torch.zeros_like(dB)
+            info = torch.zeros(len(nn), dtype=torch.int32, device=dev)
+            iters = torch.zeros_like(info)
+            fn = lambda: L.dev_BatchLinEQSolve(nn, kk, a_off, b_off, dA, dB, dX, info, iters, mode=args.mode, ctx=ctx)
+            fn()  # the first call with a plan runs the autotuner
+            ms = _timed(fn, args.steps, args.warmup)
+            work = sum(inputs.lu_solve_flops(int(x), int(y)) for x, y in zip(nn, kk))
+            unit = "GFLOP/s"
+            metric = "batched uneven LU solves GFLOP/s (20,000 systems, n in [8, 256])"
+            extra.update({"solves_per_s": len(nn) / (ms / 1e3), "singular": int((info != 0).sum().item()),
+                          "tile_shape": L.batch_tune(ctx)})
+            if args.mode == 1:
+                it = iters.cpu().numpy()
+                extra.update({"mean_refinement_steps": float(it[it > 0].mean()), "fp64_fallbacks": int((it < 0).sum())})
+            config = {"workload": f"20,000 systems A = R + n I, 1-4 RHS, {'FP64' if args.mode == 0 else 'FP32 + FP64 IR'}",
+                      "count": len(nn), "mode": args.mode}
+            dtype = "f64" if args.mode == 0 else "f32 factor + f64 refinement"
+        else:  # adjoint
+            n = 4096
+            r = inputs.rng(4096 + rank)
+            a = r.random_sample((n, n)) * 2.0 - 1.0 + n * np.eye(n)
+            A = torch.from_numpy(a).to(dev)
+            bvec = torch.from_numpy(r.standard_normal((n, 1))).to(dev)
+            G = torch.from_numpy(r.standard_normal((n, 1))).to(dev)
+            LU = A.clone()
+            indx = torch.zeros(n, dtype=torch.int32, device=dev)
+            X = torch.empty_like(bvec)
+            Lam, dAt = torch.empty_like(bvec), torch.empty_like(A)
+
+            def fn():
+                LU.copy_(A)
+                L.dev_MatrixLUDecompInPlace(LU, indx, ctx=ctx)
+                X.copy_(bvec)
+                L.dev_MatrixLUBackSubst(LU, indx, X, ctx=ctx)
+                L.dev_MatrixLinEQSolveAdjoint(LU, indx, X, G, Lam, dAt, ctx=ctx)
+            ms = _timed(fn, args.steps, args.warmup)
+            ms_adj = _timed(lambda: L.dev_MatrixLinEQSolveAdjoint(LU, indx, X, G, Lam, dAt, ctx=ctx), args.steps,
+                            args.warmup)
+            work = 2.0 / 3.0 * n ** 3 + 4.0 * n * n
+            unit = "GFLOP/s"
+            metric = "differentiated solve (factor + solve + adjoint with dA) GFLOP/s at n=4096"
+            extra.update({"adjoint_only_ms": ms_adj, "adjoint_dA_write_GBs": 8.0 * n * n / (ms_adj / 1e3) / 1e9})
+            config = {"workload": "loss = w^T A^-1 b, A = R + 4096 I, dA = -lambda x^T, db = lambda", "n": n}
+            dtype = "f64"
+    ms_max = max_over_ranks(world, ms)
+    if rank == 0:
+        line = {"metric": metric, "value": world * work / (ms_max / 1e3) / 1e9, "unit": unit, "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": dtype, "data": "synthetic, MT19937-seeded",
+                "config": config, "clocks": clk.summary(), **extra}
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    return 0
+
+
 def main():
     args = parse()
     world, rank, local = dist_setup()
     try:
         if args.impl == "reference":
             return run_reference(args, world, rank)
+        if args.workload != "solve":
+            return run_secondary(args, world, rank, local)
         return run_b200(args, world, rank, local)
     finally:
         if world > 1:
