@@ -78,6 +78,7 @@ struct BatchTune {
 struct Ctx {
     int device = 0;
     int num_sms = 148;
+    int sweep_ctas = -1;  // co-resident CTAs of the persistent refinement sweep (-1: not queried yet)
     size_t smem_optin = 0;
     cudaStream_t own_stream = nullptr;
     cudaStream_t stream = nullptr;

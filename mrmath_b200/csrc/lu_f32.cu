@@ -597,6 +597,56 @@ __global__ void diag_inv_kernel(const float* LU, int64_t ld, int n, int nb, floa
         if (c < nb) out[r * nb + c] = s_x[r * SP + c];
 }
 
+// Coupling blocks of the persistent triangular sweeps: W_b = L_bb^-1 L_{b,b-1} (which 0, b >= 1) and
+// W_b = U_bb^-1 U_{b,b+1} (which 1, b <= nblk - 2), 128 x 128 each, zero padded past the matrix.
+// One CTA per (block, triangle); thread t owns rows 8 (t / 16) + [0, 8) and columns t % 16 + 16 [0, 8).
+constexpr int kCpPitch = kTrsvNB + 1;
+constexpr int kCpSmem = 2 * kTrsvNB * kCpPitch * (int)sizeof(float);
+__global__ void __launch_bounds__(256) coupling_kernel(const float* LU, int64_t ld, int n, const float* linv,
+                                                       const float* uinv, float* wl, float* wu, const int32_t* status) {
+    extern __shared__ float sm[];
+    if (status[kInfo] != 0) return;
+    const int NB = kTrsvNB;
+    const int nblk = (n + NB - 1) / NB;
+    const int blk = blockIdx.x >> 1, upper = blockIdx.x & 1;
+    if (upper ? blk >= nblk - 1 : blk == 0) return;
+    const int b0 = blk * NB, bs = min(NB, n - b0);
+    const int p0 = upper ? b0 + NB : b0 - NB, ps = min(NB, n - p0);
+    float* s_i = sm;                 // [128][kCpPitch] T_bb^-1
+    float* s_t = sm + NB * kCpPitch; // [128][kCpPitch] T_{b,p}
+    const float* inv = (upper ? uinv : linv) + (int64_t)blk * NB * NB;
+    const int t = threadIdx.x;
+    for (int e = t; e < NB * NB; e += 256) {
+        const int r = e >> 7, c = e & (NB - 1);
+        s_i[r * kCpPitch + c] = inv[e];
+        s_t[r * kCpPitch + c] = (r < bs && c < ps) ? LU[(int64_t)(b0 + r) * ld + p0 + c] : 0.f;
+    }
+    __syncthreads();
+    const int r0 = 8 * (t >> 4), c0 = t & 15;
+    float acc[8][8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i)
+#pragma unroll
+        for (int j = 0; j < 8; ++j) acc[i][j] = 0.f;
+#pragma unroll 2
+    for (int k = 0; k < NB; ++k) {
+        float iv[8], tv[8];
+#pragma unroll
+        for (int i = 0; i < 8; ++i) iv[i] = s_i[(r0 + i) * kCpPitch + k];
+#pragma unroll
+        for (int j = 0; j < 8; ++j) tv[j] = s_t[k * kCpPitch + c0 + 16 * j];
+#pragma unroll
+        for (int i = 0; i < 8; ++i)
+#pragma unroll
+            for (int j = 0; j < 8; ++j) acc[i][j] = fmaf(iv[i], tv[j], acc[i][j]);
+    }
+    float* out = (upper ? wu : wl) + (int64_t)blk * NB * NB;
+#pragma unroll
+    for (int i = 0; i < 8; ++i)
+#pragma unroll
+        for (int j = 0; j < 8; ++j) out[(r0 + i) * NB + c0 + 16 * j] = acc[i][j];
+}
+
 }  // namespace
 
 // Scratch of the FP32 factorisation (all device memory, carved from one workspace).
@@ -608,7 +658,8 @@ size_t f32_scratch_bytes(int64_t n) {
     b += 3 * 32 * kNB * sizeof(float);                          // top, mvals, wmat
     b += 256 * sizeof(int);                                     // moves
     b += 4 * (size_t)round_up(n, 32) * kNB * sizeof(float);     // bth, btl, ah, al
-    b += 2 * (size_t)nblk * kTrsvNB * kTrsvNB * sizeof(float);  // diagonal inverses
+    b += 4 * (size_t)nblk * kTrsvNB * kTrsvNB * sizeof(float);  // diagonal inverses, coupling blocks
+    b += kSweepFlags * sizeof(int);                             // sweep flags
     return b + 16 * 256;
 }
 
@@ -635,6 +686,9 @@ F32Scratch f32_scratch_carve(void* base, int64_t n) {
     s.al = reinterpret_cast<float*>(take(panel));
     s.linv = reinterpret_cast<float*>(take((size_t)nblk * kTrsvNB * kTrsvNB * sizeof(float)));
     s.uinv = reinterpret_cast<float*>(take((size_t)nblk * kTrsvNB * kTrsvNB * sizeof(float)));
+    s.wl = reinterpret_cast<float*>(take((size_t)nblk * kTrsvNB * kTrsvNB * sizeof(float)));
+    s.wu = reinterpret_cast<float*>(take((size_t)nblk * kTrsvNB * kTrsvNB * sizeof(float)));
+    s.flags = reinterpret_cast<int*>(take(kSweepFlags * sizeof(int)));
     return s;
 }
 
@@ -650,6 +704,7 @@ int32_t lu_factor_f32(Ctx* ctx, cudaStream_t st, float* A, int64_t ld, int64_t n
     if (!attr) {
         B2M_CU(ctx, cudaFuncSetAttribute(lu_outer_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, ou_smem));
         B2M_CU(ctx, cudaFuncSetAttribute(diag_inv_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, di_smem));
+        B2M_CU(ctx, cudaFuncSetAttribute(coupling_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kCpSmem));
         attr = true;
     }
     const GraphKey key{3 + mode * 10, A, perm, s.cand, s.bth, ld, n, 0, 0};
@@ -699,6 +754,8 @@ int32_t lu_factor_f32(Ctx* ctx, cudaStream_t st, float* A, int64_t ld, int64_t n
         }
         const int nblk = (int)ceil_div(n, kTrsvNB);
         diag_inv_kernel<<<2 * nblk, kTrsvNB, di_smem, q>>>(A, ld, (int)n, kTrsvNB, s.linv, s.uinv, ctx->d_status);
+        B2M_LAUNCHED(ctx);
+        coupling_kernel<<<2 * nblk, 256, kCpSmem, q>>>(A, ld, (int)n, s.linv, s.uinv, s.wl, s.wu, ctx->d_status);
         B2M_LAUNCHED(ctx);
         return B2M_OK;
     });

@@ -274,6 +274,224 @@ __global__ void __launch_bounds__(256) trsv_block_kernel(TrArgs a, int b) {
     }
 }
 
+__device__ __forceinline__ void cp_async16(void* dst, const void* src, int src_bytes) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(smem_u32(dst)), "l"(src), "r"(src_bytes)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+
+// ------------------------------------------------------------------ persistent sweep
+// One cooperative launch per sweep: CTA (block b, group g) owns rows [128 b, +128) and right-hand
+// sides [8 g, +8).  With T_bb^-1 and the coupling block W_b = T_bb^-1 T_{b,p} (p the block solved
+// just before b) precomputed, the block's solution is
+//     x_b = T_bb^-1 (X_b - sum_{j before p} T_bj x_j)  -  W_b x_p,
+// so everything but the last product is done while block p is still being solved, and the chain
+// of 128-row blocks advances by one 128 x 128 x 8 product, a flag and an L2 round trip per step.
+// T_bb^-1 and W_b are staged in shared memory at kernel start, the rows of the other T_bj are
+// loaded into registers before each wait.  All CTAs are resident (cooperative launch); every wait
+// is bounded and reports a timeout through the status words, and a CTA that gives up sets its flag
+// to -1 so that the CTAs after it give up without waiting again.
+constexpr int kSwRhs = 8;
+constexpr uint32_t kSwSpin = 1u << 22;
+constexpr int kSwSmem = 2 * kTrsvNB * kTrsvNB * (int)sizeof(float);  // T_bb^-1 and W_b
+
+struct SwArgs {
+    const float* T;
+    int64_t ld;
+    int n;
+    const float* inv;  // T_bb^-1 per block (128 x 128, zero padded)
+    const float* w;    // W_b per block (128 x 128, zero padded; unused for the first block)
+    float* Xr;
+    int64_t ldr;
+    int c0, nc;
+    double* X64;
+    int64_t ldx;
+    int upper;
+    int* flags;
+    int32_t* status;
+};
+
+__device__ __forceinline__ int ld_acquire(const int* p) {
+    int v;
+    asm volatile("ld.acquire.gpu.global.b32 %0, [%1];\n" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_release(int* p, int v) {
+    asm volatile("st.release.gpu.global.b32 [%0], %1;\n" ::"l"(p), "r"(v) : "memory");
+}
+
+// acc[q] += sum over this thread's 64 k of M[r][k] * P[k][q], M staged as float4 [k/4][row].
+__device__ __forceinline__ void sw_smem_product(const float4* sM, int r, int h, const float (*P)[kSwRhs],
+                                                float (&acc)[kSwRhs]) {
+#pragma unroll
+    for (int i = 0; i < 16; ++i) {
+        const float4 m = sM[(16 * h + i) * kTrsvNB + r];
+        const float mk[4] = {m.x, m.y, m.z, m.w};
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+            const int k = 64 * h + 4 * i + e;
+            const float4 x0 = *reinterpret_cast<const float4*>(&P[k][0]);
+            const float4 x1 = *reinterpret_cast<const float4*>(&P[k][4]);
+            acc[0] = fmaf(mk[e], x0.x, acc[0]);
+            acc[1] = fmaf(mk[e], x0.y, acc[1]);
+            acc[2] = fmaf(mk[e], x0.z, acc[2]);
+            acc[3] = fmaf(mk[e], x0.w, acc[3]);
+            acc[4] = fmaf(mk[e], x1.x, acc[4]);
+            acc[5] = fmaf(mk[e], x1.y, acc[5]);
+            acc[6] = fmaf(mk[e], x1.z, acc[6]);
+            acc[7] = fmaf(mk[e], x1.w, acc[7]);
+        }
+    }
+}
+
+__global__ void __launch_bounds__(256, 1) trsv_sweep_kernel(SwArgs a) {
+    extern __shared__ __align__(16) float4 sw_dyn[];
+    __shared__ __align__(16) float s_p[kTrsvNB][kSwRhs];  // x of the block being folded in
+    __shared__ __align__(16) float s_y[kTrsvNB][kSwRhs];
+    __shared__ __align__(16) float s_h[kTrsvNB][kSwRhs];
+    __shared__ int s_abort;
+    float4* s_inv = sw_dyn;                        // [32][128]: s_inv[kq][r] = inv[r][4kq .. 4kq+3]
+    float4* s_w = sw_dyn + kTrsvNB * kTrsvNB / 4;  // same layout for W_b
+    const int t = threadIdx.x;
+    if (a.status[kInfo] != 0) return;
+    const int NB = kTrsvNB;
+    const int nblk = (int)ceil_div(a.n, NB);
+    const int ng = (int)ceil_div(a.nc, kSwRhs);
+    const int bi = blockIdx.x / ng, g = blockIdx.x - bi * ng;
+    const int b = a.upper ? nblk - 1 - bi : bi;
+    const int b0 = b * NB, bs = min(NB, a.n - b0);
+    const int r = t & (NB - 1), h = t >> 7;
+    const int cg = a.c0 + g * kSwRhs;
+    const int ncg = min(kSwRhs, a.nc - g * kSwRhs);
+    if (t == 0) s_abort = 0;
+    {
+        const float* inv = a.inv + (int64_t)b * NB * NB;
+        const float* w = a.w + (int64_t)b * NB * NB;
+#pragma unroll 4
+        for (int i = 0; i < 16; ++i) {
+            const int e = t + 256 * i, rr = e & (NB - 1), kq = e >> 7;
+            cp_async16(s_inv + kq * NB + rr, inv + rr * NB + 4 * kq, 16);
+            if (bi > 0) cp_async16(s_w + kq * NB + rr, w + rr * NB + 4 * kq, 16);
+        }
+        cp_async_commit();
+    }
+    float xb[kSwRhs];  // own right-hand side (h == 0 threads)
+#pragma unroll
+    for (int q = 0; q < kSwRhs; ++q)
+        xb[q] = (h == 0 && r < bs && q < ncg) ? a.Xr[(int64_t)(b0 + r) * a.ldr + cg + q] : 0.f;
+    float acc[kSwRhs];
+#pragma unroll
+    for (int q = 0; q < kSwRhs; ++q) acc[q] = 0.f;
+
+    // wait for block j of the sweep and stage its solution in s_p; false if the sweep is abandoned
+    auto wait_and_stage = [&](int j) -> bool {
+        if (t == 0) {
+            const int* f = a.flags + j * ng + g;
+            uint32_t it = 0;
+            int v;
+            while ((v = ld_acquire(f)) == 0 && ++it < kSwSpin) {
+            }
+            if (v == 0) atomicExch(&a.status[kTimeout], 501);
+            if (v <= 0) {
+                s_abort = 1;
+                st_release(a.flags + b * ng + g, -1);
+            }
+        }
+        __syncthreads();
+        if (s_abort) return false;
+        const int p0 = j * NB, ps = min(NB, a.n - p0);
+        const int k = t >> 1, q0 = (t & 1) * 4;  // 128 rows x 8 columns, one float4 per thread
+        float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (k < ps && q0 < ncg) v = __ldcg(reinterpret_cast<const float4*>(a.Xr + (int64_t)(p0 + k) * a.ldr + cg + q0));
+        if (q0 + 1 >= ncg) v.y = 0.f;
+        if (q0 + 2 >= ncg) v.z = 0.f;
+        if (q0 + 3 >= ncg) v.w = 0.f;
+        *reinterpret_cast<float4*>(&s_p[k][q0]) = v;
+        __syncthreads();
+        return true;
+    };
+
+    // all blocks before the last one: contributions with T_bj rows from registers
+    for (int jj = 0; jj + 1 < bi; ++jj) {
+        const int j = a.upper ? nblk - 1 - jj : jj;
+        const int p0 = j * NB, ps = min(NB, a.n - p0);
+        float4 tv[16];
+        {
+            const float* trow = a.T + (int64_t)(b0 + min(r, bs - 1)) * a.ld + p0;
+#pragma unroll
+            for (int i = 0; i < 16; ++i)
+                tv[i] = r < bs ? ld_row4(trow, 64 * h + 4 * i, ps) : make_float4(0.f, 0.f, 0.f, 0.f);
+        }
+        if (!wait_and_stage(j)) return;
+#pragma unroll
+        for (int i = 0; i < 16; ++i) {
+            const float tk[4] = {tv[i].x, tv[i].y, tv[i].z, tv[i].w};
+#pragma unroll
+            for (int e = 0; e < 4; ++e) {
+                const int k = 64 * h + 4 * i + e;
+                const float4 x0 = *reinterpret_cast<const float4*>(&s_p[k][0]);
+                const float4 x1 = *reinterpret_cast<const float4*>(&s_p[k][4]);
+                acc[0] = fmaf(tk[e], x0.x, acc[0]);
+                acc[1] = fmaf(tk[e], x0.y, acc[1]);
+                acc[2] = fmaf(tk[e], x0.z, acc[2]);
+                acc[3] = fmaf(tk[e], x0.w, acc[3]);
+                acc[4] = fmaf(tk[e], x1.x, acc[4]);
+                acc[5] = fmaf(tk[e], x1.y, acc[5]);
+                acc[6] = fmaf(tk[e], x1.z, acc[6]);
+                acc[7] = fmaf(tk[e], x1.w, acc[7]);
+            }
+        }
+        __syncthreads();  // s_p is rewritten by the next block
+    }
+    // y = X_b - sum_{j before p} T_bj x_j ;  z = T_bb^-1 y
+    if (h == 1) {
+#pragma unroll
+        for (int q = 0; q < kSwRhs; ++q) s_h[r][q] = acc[q];
+    }
+    cp_async_wait<0>();
+    __syncthreads();
+    if (h == 0) {
+#pragma unroll
+        for (int q = 0; q < kSwRhs; ++q) s_y[r][q] = xb[q] - acc[q] - s_h[r][q];
+    }
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < kSwRhs; ++q) acc[q] = 0.f;
+    sw_smem_product(s_inv, r, h, s_y, acc);
+    if (bi > 0) {  // x_b = z - W_b x_p
+        const int p = a.upper ? b + 1 : b - 1;
+        if (!wait_and_stage(p)) return;
+#pragma unroll
+        for (int q = 0; q < kSwRhs; ++q) acc[q] = -acc[q];
+        sw_smem_product(s_w, r, h, s_p, acc);
+#pragma unroll
+        for (int q = 0; q < kSwRhs; ++q) acc[q] = -acc[q];
+    }
+    if (h == 1) {
+#pragma unroll
+        for (int q = 0; q < kSwRhs; ++q) s_h[r][q] = acc[q];
+    }
+    __syncthreads();
+    float xv[kSwRhs];
+    if (h == 0 && r < bs) {
+#pragma unroll
+        for (int q = 0; q < kSwRhs; ++q) {
+            xv[q] = acc[q] + s_h[r][q];
+            if (q < ncg) a.Xr[(int64_t)(b0 + r) * a.ldr + cg + q] = xv[q];
+        }
+    }
+    __threadfence();
+    __syncthreads();
+    if (t == 0) st_release(a.flags + b * ng + g, 1);
+    if (a.upper && h == 0 && r < bs) {  // the FP64 accumulation is off the chain
+#pragma unroll
+        for (int q = 0; q < kSwRhs; ++q)
+            if (q < ncg) a.X64[(int64_t)(b0 + r) * a.ldx + cg + q] += (double)xv[q];
+    }
+}
+
 struct ReArgs {
     const double* A;
     int64_t lda;
@@ -287,14 +505,6 @@ struct ReArgs {
     const int32_t* pinv;
     unsigned long long* nrm;  // [0,k) |r|, [k,2k) |x|, [2k,3k) |b|
 };
-
-__device__ __forceinline__ void cp_async16(void* dst, const void* src, int src_bytes) {
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(smem_u32(dst)), "l"(src), "r"(src_bytes)
-                 : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-template <int N>
-__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
 
 // r = b - A x for rows [64 blockIdx.x, +64) and columns [16 blockIdx.y, +16).  A and X stream
 // through a 3-stage cp.async pipeline (64 x 64 tiles of A, 64 x 16 of X); four K slices of 64
@@ -399,8 +609,41 @@ __global__ void __launch_bounds__(256, 1) resid_kernel(ReArgs a) {
 int32_t ir_solve(Ctx* ctx, cudaStream_t st, const float* LU, int64_t ld, int64_t n, const F32Scratch& s, float* Xr,
                  int64_t ldr, int64_t nrhs, double* X64, int64_t ldx) {
     const int nblk = (int)ceil_div(n, kTrsvNB);
+    if (ctx->sweep_ctas < 0) {
+        int per_sm = 0, coop = 0;
+        B2M_CU(ctx, cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, ctx->device));
+        B2M_CU(ctx, cudaFuncSetAttribute(trsv_sweep_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSwSmem));
+        B2M_CU(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, trsv_sweep_kernel, 256, kSwSmem));
+        ctx->sweep_ctas = coop ? per_sm * ctx->num_sms : 0;
+    }
+    const int coop_ctas = ctx->sweep_ctas;
     for (int64_t c0 = 0; c0 < nrhs; c0 += kTrMaxRhs) {
         const int nc = (int)std::min<int64_t>(kTrMaxRhs, nrhs - c0);
+        const int ng = (int)ceil_div(nc, kSwRhs);
+        if (nblk * ng <= coop_ctas && 2 * nblk * ng <= kSweepFlags) {
+            // persistent sweeps: one cooperative launch each
+            for (int up = 0; up < 2; ++up) {
+                int* flags = s.flags + up * nblk * ng;
+                B2M_CU(ctx, cudaMemsetAsync(flags, 0, (size_t)nblk * ng * sizeof(int), st));
+                SwArgs sa{LU,  ld, (int)n, up ? s.uinv : s.linv, up ? s.wu : s.wl, Xr, ldr, (int)c0, nc, X64, ldx, up,
+                          flags, ctx->d_status};
+                cudaLaunchConfig_t cfg{};
+                cudaLaunchAttribute at[1];
+                at[0].id = cudaLaunchAttributeCooperative;
+                at[0].val.cooperative = 1;
+                cfg.gridDim = dim3((unsigned)(nblk * ng));
+                cfg.blockDim = dim3(256);
+                cfg.dynamicSmemBytes = kSwSmem;
+                cfg.stream = st;
+                cfg.attrs = at;
+                cfg.numAttrs = 1;
+                prof_begin(ctx, st, kClsSolve);
+                B2M_CU(ctx, cudaLaunchKernelEx(&cfg, trsv_sweep_kernel, sa));
+                prof_end(ctx, st, kClsSolve, 4.0 * (double)n * n / 2 + 4.0 * nblk * kTrsvNB * kTrsvNB + 8.0 * n * nc);
+                B2M_LAUNCHED(ctx);
+            }
+            continue;
+        }
         TrArgs a{LU, ld, (int)n, s.linv, Xr, ldr, (int)c0, nc, X64, ldx, 0, (int)ceil_div(nc, kTrRhs), ctx->d_status};
         for (int b = 0; b < nblk; ++b) {
             const int rows = (int)(n - std::min<int64_t>(n, (int64_t)(b + 1) * kTrsvNB));
