@@ -94,6 +94,9 @@ struct Ctx {
     std::map<GraphKey, GraphEntry> graphs;
     uint64_t graph_clock = 0;
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+    cudaStream_t side_stream = nullptr;                  // look-ahead trailing updates of the FP32 LU
+    cudaEvent_t ev_side_fork = nullptr, ev_side_join = nullptr;
+    int chain_priority = 0;                               // stream priority of the panel kernels
     std::string last_error;
     std::mutex mtx;
     std::map<uint64_t, BatchTune> batch_tunes;  // per batch plan

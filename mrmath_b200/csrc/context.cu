@@ -26,6 +26,7 @@ int32_t ws_get(Ctx* ctx, int slot, size_t bytes, void** out) {
             // drain both streams and drop every cached graph before freeing it
             B2M_CU(ctx, cudaStreamSynchronize(ctx->stream));
             if (ctx->own_stream) B2M_CU(ctx, cudaStreamSynchronize(ctx->own_stream));
+            if (ctx->side_stream) B2M_CU(ctx, cudaStreamSynchronize(ctx->side_stream));
             for (auto& g : ctx->graphs) cudaGraphExecDestroy(g.second.exec);
             ctx->graphs.clear();
             B2M_CU(ctx, cudaFree(ctx->ws[slot]));
@@ -111,7 +112,9 @@ int32_t run_graph(Ctx* ctx, cudaStream_t st, const GraphKey& key, const std::fun
         }
         if (ce != cudaSuccess) return fail(ctx, B2M_ERR_CUDA, "stream capture failed: %s", cudaGetErrorString(ce));
         GraphEntry e;
-        const cudaError_t ie = cudaGraphInstantiate(&e.exec, g, 0);
+        // per-node priorities: the LU's panel kernels are launched with the highest priority so that
+        // they take SMs ahead of a concurrent trailing GEMM (a graph otherwise ignores them)
+        const cudaError_t ie = cudaGraphInstantiateWithFlags(&e.exec, g, cudaGraphInstantiateFlagUseNodePriority);
         cudaGraphDestroy(g);
         if (ie != cudaSuccess) return fail(ctx, B2M_ERR_CUDA, "graph instantiate failed: %s", cudaGetErrorString(ie));
         e.launches = ctx->launches - l0;
@@ -228,6 +231,9 @@ extern "C" int32_t b2m_destroy(b2m_ctx* h) {
     if (ctx->h_pinned) cudaFreeHost(ctx->h_pinned);
     if (ctx->d_status) cudaFree(ctx->d_status);
     if (ctx->h_status) cudaFreeHost(ctx->h_status);
+    if (ctx->side_stream) cudaStreamDestroy(ctx->side_stream);
+    if (ctx->ev_side_fork) cudaEventDestroy(ctx->ev_side_fork);
+    if (ctx->ev_side_join) cudaEventDestroy(ctx->ev_side_join);
     if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
     for (int c = 0; c < b2m::kNumCls; ++c)
         for (cudaEvent_t e : ctx->prof.ev[c]) cudaEventDestroy(e);

@@ -132,6 +132,8 @@ struct F32Scratch {
     float* mvals;
     float* wmat;
     int* moves;
+    float* lmul;
+    int32_t* pmap;
     float *bth, *btl, *ah, *al;
     float *linv, *uinv;
     float *wl, *wu;  // coupling blocks T_bb^-1 T_{b,b-1} (L) and T_bb^-1 T_{b,b+1} (U)

@@ -49,6 +49,8 @@ struct TsArgs {
     float* mvals;         // [32][kNB]: original content of the top rows that move below the leaf
     float* wmat;          // [32][kNB]: U11^-1 in the leaf's columns, U11^-1 U12 right of them
     int* moves;           // [0] moves, [1] moves below the top block, [2..66) dst, [66..130) src
+    float* lmul;          // [32][kTsRows] the root elimination's multipliers
+    int32_t* pmap;        // first leaf of a panel: pmap[i] = i for the panel's rows (identity)
     int32_t* status;
 };
 
@@ -62,114 +64,82 @@ __device__ __forceinline__ float rcp_nr(float x) {
 
 // Gaussian elimination with partial pivoting of up to 512 stacked rows (thread t holds stack rows
 // t and t + 256 in registers) over w <= 32 columns.  Chooses w pivot rows (largest magnitude);
-// s_win[j] = row id of pivot j (-1 if the stack ran out), s_lu[j][*] = pivot row j at the time it
-// was chosen, i.e. row j of L\U.
+// s_win[j] = row id of pivot j and s_loc[j] = its stack index (-1 if the stack ran out).
 //
-// The column loop is a runtime loop over steps of 4 columns (compact code: a fully unrolled
-// elimination does not fit the instruction cache).  Register indices stay compile-time because
-// the rows rotate left by 4 after each step: at step `it`, v[r][k] holds column 4 it + k for
-// k < 32 - 4 it and the multiplier of column q sits at v[r][32 - 4 it + q].  Those multiplier
-// quads are skipped by the elimination.
-//
-// One barrier per column: every warp's best lane publishes its candidate row (and key) into a
-// double-buffered slot before the barrier; afterwards all threads pick the winning warp with a
-// warp reduction over the slots and read its row directly.  A pivot's full row (with its
-// multipliers) is written to s_lu by its owner once, after the last column.
+// One column per iteration of a runtime loop (a compact body: unrolled multi-column steps spill
+// out of the instruction cache).  Register indices stay compile-time because every row shifts
+// left by one as its column is eliminated (the update writes v[k - 1]), so the current column is
+// always v[0].  One barrier per column: every warp's best lane publishes its candidate row (and
+// key) before the barrier (double-buffered by column parity); afterwards all threads pick the
+// winning warp with a warp reduction over the keys and read its row directly.  For the root
+// (lm given) the winner of column j is copied to s_u[j] (row j of U, from column j on) and every
+// row's multiplier of column j goes to lm[j][stack index] (global scratch), which gives the rows
+// of L; keeping them out of shared memory lets the CTA share an SM with a tensor-core GEMM.
 struct GeppSmem {
-    float4 cand[2][kTsThreads / 32][8];  // candidate rows, by column parity and warp
+    float4 cand[2][kTsThreads / 32][8];  // candidate rows by column parity and warp (column j first)
     unsigned key[2][kTsThreads / 32];
     unsigned slot[2][kTsThreads / 32];
+    float4 u[32][8];                     // root: pivot rows as chosen
 };
 
 __device__ __forceinline__ void block_gepp(float (&v)[kTsRpt][32], const int (&rid)[kTsRpt], int w, int* s_win,
-                                           float (*s_lu)[33], GeppSmem& g) {
+                                           int* s_loc, GeppSmem& g, float* lm) {
     const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
     bool live[kTsRpt];
-    int my_j[kTsRpt];
 #pragma unroll
-    for (int r = 0; r < kTsRpt; ++r) { live[r] = rid[r] >= 0; my_j[r] = -1; }
-    if (t < 32) s_win[t] = -1;
-    const int nit = (w + 3) >> 2;
+    for (int r = 0; r < kTsRpt; ++r) live[r] = rid[r] >= 0;
+    if (t < 32) { s_win[t] = -1; s_loc[t] = -1; }
 #pragma unroll 1
-    for (int it = 0; it < nit; ++it) {
-#pragma unroll
-        for (int c = 0; c < 4; ++c) {
-            const int j = 4 * it + c;
-            if (j >= w) break;  // uniform
-            const int b = j & 1;
-            unsigned key = 0u;
-            int rbest = 0;
-#pragma unroll
-            for (int r = 0; r < kTsRpt; ++r) {
-                const unsigned k = live[r] ? __float_as_uint(fabsf(v[r][c])) + 1u : 0u;
-                if (k > key) { key = k; rbest = r; }
-            }
-            const unsigned wk = __reduce_max_sync(0xffffffffu, key);
-            const unsigned bal = __ballot_sync(0xffffffffu, key == wk && key != 0u);
-            if (lane == (bal ? __ffs(bal) - 1 : 0)) {
-#pragma unroll
-                for (int r = 0; r < kTsRpt; ++r) {
-                    if (r == rbest) {
-#pragma unroll
-                        for (int q = 0; q < 8; ++q)
-                            if (q < 8 - it)
-                                g.cand[b][warp][q] = make_float4(v[r][4 * q], v[r][4 * q + 1], v[r][4 * q + 2], v[r][4 * q + 3]);
-                    }
-                }
-                g.key[b][warp] = wk;
-                g.slot[b][warp] = (unsigned)(rbest * kTsThreads + t);
-            }
-            __syncthreads();
-            // winning warp: largest key, lowest warp among equals
-            const unsigned kq = g.key[b][lane & (kTsThreads / 32 - 1)];
-            const unsigned pk = __reduce_max_sync(0xffffffffu, kq);
-            if (pk == 0u) continue;  // nothing left to choose from (uniform)
-            const int pwarp = __ffs(__ballot_sync(0xffffffffu, kq == pk)) - 1;
-            const unsigned ps = g.slot[b][pwarp];
-            const float4* prow = g.cand[b][pwarp];
-            const float4 f0 = prow[0];
-            const float p0[4] = {f0.x, f0.y, f0.z, f0.w};
-            const float rcp = pk > 1u ? rcp_nr(p0[c]) : 0.0f;  // a zero column eliminates nothing
-#pragma unroll
-            for (int r = 0; r < kTsRpt; ++r) {
-                if (ps == (unsigned)(r * kTsThreads + t)) {
-                    live[r] = false;
-                    my_j[r] = j;
-                    s_win[j] = rid[r];
-                }
-                if (live[r]) {
-                    const float l = v[r][c] * rcp;
-                    v[r][c] = l;
-#pragma unroll
-                    for (int e = c + 1; e < 4; ++e) v[r][e] = fmaf(-l, p0[e], v[r][e]);
-#pragma unroll
-                    for (int q = 1; q < 8; ++q) {
-                        if (q < 8 - it) {  // uniform: quads from 8 - it on hold multipliers
-                            const float4 f = prow[q];
-                            v[r][4 * q] = fmaf(-l, f.x, v[r][4 * q]);
-                            v[r][4 * q + 1] = fmaf(-l, f.y, v[r][4 * q + 1]);
-                            v[r][4 * q + 2] = fmaf(-l, f.z, v[r][4 * q + 2]);
-                            v[r][4 * q + 3] = fmaf(-l, f.w, v[r][4 * q + 3]);
-                        }
-                    }
-                }
-            }
-        }
-        // rotate left by 4: this step's multipliers go to the end
+    for (int j = 0; j < w; ++j) {
+        const int b = j & 1;
+        unsigned key = 0u;
+        int rbest = 0;
 #pragma unroll
         for (int r = 0; r < kTsRpt; ++r) {
-            const float r0 = v[r][0], r1 = v[r][1], r2 = v[r][2], r3 = v[r][3];
-#pragma unroll
-            for (int k = 0; k < 28; ++k) v[r][k] = v[r][k + 4];
-            v[r][28] = r0; v[r][29] = r1; v[r][30] = r2; v[r][31] = r3;
+            const unsigned k = live[r] ? __float_as_uint(fabsf(v[r][0])) + 1u : 0u;
+            if (k > key) { key = k; rbest = r; }
         }
-    }
-    // pivot rows: original column col now sits at register (col - 4 nit) mod 32
+        const unsigned wk = __reduce_max_sync(0xffffffffu, key);
+        const unsigned bal = __ballot_sync(0xffffffffu, key == wk && key != 0u);
+        if (lane == (bal ? __ffs(bal) - 1 : 0)) {
 #pragma unroll
-    for (int r = 0; r < kTsRpt; ++r) {
-        if (my_j[r] >= 0) {
+            for (int r = 0; r < kTsRpt; ++r) {
+                if (r == rbest) {
 #pragma unroll
-            for (int k = 0; k < 32; ++k) s_lu[my_j[r]][(k + 4 * nit) & 31] = v[r][k];
+                    for (int q = 0; q < 8; ++q)
+                        g.cand[b][warp][q] = make_float4(v[r][4 * q], v[r][4 * q + 1], v[r][4 * q + 2], v[r][4 * q + 3]);
+                }
+            }
+            g.key[b][warp] = wk;
+            g.slot[b][warp] = (unsigned)(rbest * kTsThreads + t);
+        }
+        __syncthreads();
+        // winning warp: largest key, lowest warp among equals
+        const unsigned kq = g.key[b][lane & (kTsThreads / 32 - 1)];
+        const unsigned pk = __reduce_max_sync(0xffffffffu, kq);
+        if (pk == 0u) break;  // no live row left anywhere (uniform)
+        const int pwarp = __ffs(__ballot_sync(0xffffffffu, kq == pk)) - 1;
+        const unsigned ps = g.slot[b][pwarp];
+        float pr[32];
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+            const float4 f = g.cand[b][pwarp][q];
+            pr[4 * q] = f.x; pr[4 * q + 1] = f.y; pr[4 * q + 2] = f.z; pr[4 * q + 3] = f.w;
+        }
+        if (lm && t < 8) g.u[j][t] = g.cand[b][pwarp][t];
+        const float rcp = pk > 1u ? rcp_nr(pr[0]) : 0.0f;  // a zero column eliminates nothing
+#pragma unroll
+        for (int r = 0; r < kTsRpt; ++r) {
+            if (ps == (unsigned)(r * kTsThreads + t)) {
+                live[r] = false;
+                s_win[j] = rid[r];
+                s_loc[j] = r * kTsThreads + t;
+            }
+            const float l = live[r] ? v[r][0] * rcp : 0.f;
+            if (lm) lm[j * kTsRows + r * kTsThreads + t] = l;
+#pragma unroll
+            for (int k = 1; k < 32; ++k) v[r][k - 1] = fmaf(-l, pr[k], v[r][k]);
+            v[r][31] = 0.f;
         }
     }
     __syncthreads();
@@ -195,8 +165,10 @@ __device__ __forceinline__ void load_leaf_row(const float* A, int64_t ld, int ro
 
 __global__ void __launch_bounds__(kTsThreads) tslu_select_kernel(TsArgs a) {
     __shared__ __align__(16) GeppSmem s_g;
-    __shared__ int s_win[32];
+    __shared__ int s_win[32], s_loc[32];
     __shared__ float s_lu[32][33];
+    __shared__ __align__(16) float s_lt[32][32];  // s_lt[j][k] = L(k, j) for k > j, else 0
+    __shared__ __align__(16) float s_ut[32][32];  // s_ut[i][k] = U(k, i) for k < i, else 0
     __shared__ float s_rdiag[32];
     __shared__ int s_last, s_bad;
     __shared__ int s_flag[32], s_outpos[32], s_mdst[64], s_msrc[64], s_nm, s_nout;
@@ -210,10 +182,11 @@ __global__ void __launch_bounds__(kTsThreads) tslu_select_kernel(TsArgs a) {
         const int row = a.lc0 + blockIdx.x * kTsRows + r * kTsThreads + t;
         rid[r] = row < a.n ? row : -1;
         load_leaf_row(a.A, a.ld, rid[r], a.lc0, a.w, v[r]);
+        if (a.pmap && row < a.n) a.pmap[row] = row;
     }
     int node = blockIdx.x, count = (int)ceil_div(m, kTsRows), level = 0;
     for (;;) {
-        block_gepp(v, rid, a.w, s_win, s_lu, s_g);
+        block_gepp(v, rid, a.w, s_win, s_loc, s_g, count == 1 ? a.lmul : nullptr);
         if (count == 1) break;
         // publish this node's candidates; the last member of the group merges them
         if (t < 32) a.cand[((int64_t)level * kTsMaxCand + node) * 32 + t] = s_win[t];
@@ -244,18 +217,38 @@ __global__ void __launch_bounds__(kTsThreads) tslu_select_kernel(TsArgs a) {
         ++level;
     }
 
-    // ---- root: pivots s_win[0..w), factors s_lu
+    // ---- root: pivots s_win[0..w); rows of L\U from the multipliers and the published pivot rows
     const int lc0 = a.lc0, w = a.w;
-    if (t == 0) {
-        int bad = 0;
-        for (int j = 0; j < w; ++j)
-            if (s_win[j] < 0 || !(fabsf(s_lu[j][j]) > 10.0f / FLT_MAX)) { bad = lc0 + j + 1; break; }
-        s_bad = bad;
-        if (bad) a.status[kInfo] = bad;
+    for (int e = t; e < 32 * 32; e += kTsThreads) {
+        const int j = e >> 5, k = e & 31;
+        const int l = s_loc[j];
+        float x = 0.f;
+        if (j < w && l >= 0 && k < w) {
+            if (k < j) {
+                x = __ldcg(a.lmul + k * kTsRows + l);
+            } else {
+                const float4 f = s_g.u[j][(k - j) >> 2];
+                const int e4 = (k - j) & 3;
+                x = e4 == 0 ? f.x : e4 == 1 ? f.y : e4 == 2 ? f.z : f.w;
+            }
+        }
+        s_lu[j][k] = x;
     }
+    __syncthreads();
     if (t < 32) {
+        const bool bad = t < w && (s_win[t] < 0 || !(fabsf(s_lu[t][t]) > 10.0f / FLT_MAX));
+        const unsigned bb = __ballot_sync(0xffffffffu, bad);
+        if (t == 0) {
+            s_bad = bb ? lc0 + __ffs(bb) : 0;
+            if (bb) a.status[kInfo] = s_bad;
+        }
         s_flag[t] = 0;
         s_rdiag[t] = t < w ? rcp_nr(s_lu[t][t]) : 0.f;
+    }
+    for (int e = t; e < 32 * 32; e += kTsThreads) {  // transposed triangles for the substitutions
+        const int i = e >> 5, k = e & 31;
+        s_lt[i][k] = (k > i && k < w && i < w) ? s_lu[k][i] : 0.f;
+        s_ut[i][k] = (k < i && i < w) ? s_lu[k][i] : 0.f;
     }
     __syncthreads();
     if (s_bad) return;
@@ -310,11 +303,17 @@ __global__ void __launch_bounds__(kTsThreads) tslu_select_kernel(TsArgs a) {
 #pragma unroll
             for (int j = 0; j < 32; ++j) x[j] = s_lu[j][c - lo];
         } else if (c >= lo + w) {
+            // x <- L11^-1 x: column j of L read as float4s of its transposed copy
 #pragma unroll
-            for (int j = 0; j < 32; ++j) {
-                if (j >= w) break;
+            for (int j = 0; j < 31; ++j) {
 #pragma unroll
-                for (int k = j + 1; k < 32; ++k) x[k] = fmaf(-s_lu[k][j], x[j], x[k]);
+                for (int q = (j + 1) >> 2; q < 8; ++q) {
+                    const float4 l4 = *reinterpret_cast<const float4*>(&s_lt[j][4 * q]);
+                    const float lk[4] = {l4.x, l4.y, l4.z, l4.w};
+#pragma unroll
+                    for (int e = 0; e < 4; ++e)
+                        if (4 * q + e > j) x[4 * q + e] = fmaf(-lk[e], x[j], x[4 * q + e]);
+                }
             }
         }
 #pragma unroll
@@ -327,10 +326,15 @@ __global__ void __launch_bounds__(kTsThreads) tslu_select_kernel(TsArgs a) {
             for (int i = 0; i < 32; ++i) z[i] = in_leaf ? (i == c - lo ? 1.f : 0.f) : x[i];
 #pragma unroll
             for (int i = 31; i >= 0; --i) {
-                if (i >= w) continue;
                 z[i] *= s_rdiag[i];
 #pragma unroll
-                for (int k = 0; k < i; ++k) z[k] = fmaf(-s_lu[k][i], z[i], z[k]);
+                for (int q = 0; q < (i + 3) / 4; ++q) {
+                    const float4 u4 = *reinterpret_cast<const float4*>(&s_ut[i][4 * q]);
+                    const float uk[4] = {u4.x, u4.y, u4.z, u4.w};
+#pragma unroll
+                    for (int e = 0; e < 4; ++e)
+                        if (4 * q + e < i) z[4 * q + e] = fmaf(-uk[e], z[i], z[4 * q + e]);
+                }
             }
 #pragma unroll
             for (int i = 0; i < 32; ++i)
@@ -348,6 +352,7 @@ struct ApArgs {
     const float* wmat;
     const int* moves;
     int32_t* perm;
+    int32_t* pmap;  // the panel's row map: row i now holds what row pmap[i] held at the panel's start
     const int32_t* status;
     int nR;
 };
@@ -355,7 +360,9 @@ struct ApArgs {
 // Applies a leaf: rows of the leaf's top block get their final content; every other row r below
 // it (moved in from the side buffer or in place) becomes [v_left | l | v_right - l U12] with
 // l = v_leaf U11^-1, computed as the product v_leaf * [U11^-1 | U11^-1 U12] (thread per column).
-// Column CTAs apply the leaf's row moves to the columns outside the outer panel.
+// The row moves are recorded in perm and in the panel's row map; the columns outside the outer
+// panel are permuted once per panel (panel_permute_kernel).  Column CTAs (blockIdx >= nR, not
+// launched by the factorisation) apply the leaf's row moves to the columns outside the panel.
 __global__ void __launch_bounds__(256) tslu_apply_kernel(ApArgs a) {
     __shared__ __align__(16) float s_l[kApRows][36];  // the rows' leaf values v_leaf
     __shared__ int s_mdst[64], s_msrc[64], s_src[kApRows];
@@ -379,10 +386,10 @@ __global__ void __launch_bounds__(256) tslu_apply_kernel(ApArgs a) {
         return;
     }
     if (blockIdx.x == 0 && a.perm) {
-        int pv = 0;
-        if (t < nm) pv = a.perm[s_msrc[t]];
+        int pv = 0, qv = 0;
+        if (t < nm) { pv = a.perm[s_msrc[t]]; qv = a.pmap[s_msrc[t]]; }
         __syncthreads();
-        if (t < nm) a.perm[s_mdst[t]] = pv;
+        if (t < nm) { a.perm[s_mdst[t]] = pv; a.pmap[s_mdst[t]] = qv; }
     }
     const int lo = a.lc0 - a.oc0, w = a.w, pw = a.pw, lc0 = a.lc0;
     const int r0 = lc0 + blockIdx.x * kApRows;
@@ -454,6 +461,7 @@ struct OuArgs {
     float* A;
     int64_t ld;
     int n, oc0, pw, mode, nU;
+    int cs0, ncols;  // trailing columns [oc0 + pw + cs0, + ncols) of U12 (the L21 split covers all rows)
     float* bth;
     float* btl;
     float* ah;
@@ -482,8 +490,8 @@ __global__ void __launch_bounds__(256) lu_outer_kernel(OuArgs a) {
         return;
     }
     const int pw = a.pw;
-    const int cs = c_first + blockIdx.x * 32;
-    const int ncol = min(32, a.n - cs);
+    const int cs = c_first + a.cs0 + blockIdx.x * 32;
+    const int ncol = min(32, min(a.n, c_first + a.cs0 + a.ncols) - cs);
     float* s_x = sm;               // [kNB][33] the strip
     float* s_l = sm + kNB * 33;    // [kNB][33] one 32-column block of L (rows from the block down)
     const int c = t & 31, rg = t >> 5;
@@ -647,6 +655,42 @@ __global__ void __launch_bounds__(256) coupling_kernel(const float* LU, int64_t 
         for (int j = 0; j < 8; ++j) out[(r0 + i) * NB + c0 + 16 * j] = acc[i][j];
 }
 
+// The outer panel's net row permutation applied to every column outside it: row i (of the panel's
+// rows [oc0, n)) receives what row pmap[i] held when the panel started.  CTA per 32 columns; each
+// CTA lists the moved rows (at most 64 per leaf) and reads all their sources before writing.
+constexpr int kPmMax = 64 * (kNB / 32);
+constexpr int kPmSmem = kPmMax * 32 * (int)sizeof(float);
+__global__ void __launch_bounds__(256) panel_permute_kernel(float* A, int64_t ld, int n, int oc0, int pw,
+                                                            const int32_t* pmap, int32_t* status) {
+    extern __shared__ float pm_buf[];  // [kPmMax][32]
+    __shared__ int s_dst[kPmMax], s_src[kPmMax], s_cnt;
+    if (status[kInfo] != 0) return;
+    const int t = threadIdx.x;
+    if (t == 0) s_cnt = 0;
+    __syncthreads();
+    for (int i = oc0 + t; i < n; i += 256) {
+        const int src = pmap[i];
+        if (src != i) {
+            const int k = atomicAdd(&s_cnt, 1);
+            if (k < kPmMax) { s_dst[k] = i; s_src[k] = src; }
+        }
+    }
+    __syncthreads();
+    const int cnt = s_cnt;
+    if (cnt > kPmMax) {  // cannot happen: each leaf moves at most 64 rows
+        if (t == 0) atomicExch(&status[kTimeout], 401);
+        return;
+    }
+    const int cb = blockIdx.x, left = oc0 / 32;
+    const int col0 = cb < left ? cb * 32 : oc0 + pw + (cb - left) * 32;
+    const int c = t & 31, rg = t >> 5;
+    const bool ok = col0 + c < n;
+    for (int k = rg; k < cnt; k += 8) pm_buf[k * 32 + c] = ok ? A[(int64_t)s_src[k] * ld + col0 + c] : 0.f;
+    __syncthreads();
+    if (ok)
+        for (int k = rg; k < cnt; k += 8) A[(int64_t)s_dst[k] * ld + col0 + c] = pm_buf[k * 32 + c];
+}
+
 }  // namespace
 
 // Scratch of the FP32 factorisation (all device memory, carved from one workspace).
@@ -657,6 +701,8 @@ size_t f32_scratch_bytes(int64_t n) {
     b += (size_t)kTsLevels * kTsMaxCand * sizeof(unsigned);   // counters
     b += 3 * 32 * kNB * sizeof(float);                          // top, mvals, wmat
     b += 256 * sizeof(int);                                     // moves
+    b += 32 * (size_t)kTsRows * sizeof(float);                  // root multipliers
+    b += (size_t)round_up(n, 64) * sizeof(int32_t);              // panel row map
     b += 4 * (size_t)round_up(n, 32) * kNB * sizeof(float);     // bth, btl, ah, al
     b += 4 * (size_t)nblk * kTrsvNB * kTrsvNB * sizeof(float);  // diagonal inverses, coupling blocks
     b += kSweepFlags * sizeof(int);                             // sweep flags
@@ -679,6 +725,8 @@ F32Scratch f32_scratch_carve(void* base, int64_t n) {
     s.mvals = reinterpret_cast<float*>(take(32 * kNB * sizeof(float)));
     s.wmat = reinterpret_cast<float*>(take(32 * kNB * sizeof(float)));
     s.moves = reinterpret_cast<int*>(take(256 * sizeof(int)));
+    s.lmul = reinterpret_cast<float*>(take(32 * (size_t)kTsRows * sizeof(float)));
+    s.pmap = reinterpret_cast<int32_t*>(take((size_t)round_up(n, 64) * sizeof(int32_t)));
     const size_t panel = (size_t)round_up(n, 32) * kNB * sizeof(float);
     s.bth = reinterpret_cast<float*>(take(panel));
     s.btl = reinterpret_cast<float*>(take(panel));
@@ -705,10 +753,45 @@ int32_t lu_factor_f32(Ctx* ctx, cudaStream_t st, float* A, int64_t ld, int64_t n
         B2M_CU(ctx, cudaFuncSetAttribute(lu_outer_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, ou_smem));
         B2M_CU(ctx, cudaFuncSetAttribute(diag_inv_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, di_smem));
         B2M_CU(ctx, cudaFuncSetAttribute(coupling_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kCpSmem));
+        B2M_CU(ctx, cudaFuncSetAttribute(panel_permute_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kPmSmem));
+        // one shared-memory carveout for every kernel of the factorisation, so that the panel kernels
+        // can share SMs with the tiles of a concurrent trailing GEMM (which needs the maximum)
+        for (const void* f : {(const void*)tslu_select_kernel, (const void*)tslu_apply_kernel,
+                              (const void*)panel_permute_kernel, (const void*)lu_outer_kernel})
+            B2M_CU(ctx, cudaFuncSetAttribute(f, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                             (int)cudaSharedmemCarveoutMaxShared));
         attr = true;
+    }
+    if (!ctx->side_stream) {
+        int least = 0, greatest = 0;
+        B2M_CU(ctx, cudaDeviceGetStreamPriorityRange(&least, &greatest));
+        B2M_CU(ctx, cudaStreamCreateWithPriority(&ctx->side_stream, cudaStreamNonBlocking, least));
+        B2M_CU(ctx, cudaEventCreateWithFlags(&ctx->ev_side_fork, cudaEventDisableTiming));
+        B2M_CU(ctx, cudaEventCreateWithFlags(&ctx->ev_side_join, cudaEventDisableTiming));
+        ctx->chain_priority = greatest;
     }
     const GraphKey key{3 + mode * 10, A, perm, s.cand, s.bth, ld, n, 0, 0};
     return run_graph(ctx, st, key, [&](cudaStream_t q) -> int32_t {
+        // Look-ahead: after a panel, only the next panel's columns are updated on this stream; the
+        // rest of the trailing update runs on the side stream, overlapping the next panel's leaves
+        // (which touch neither those columns nor the previous panel's L21), and is joined before
+        // the next panel's out-of-panel row permutation.  The leaf kernels carry the highest
+        // priority so that they take SMs ahead of the wide GEMM's tiles.
+        cudaStream_t q2 = ctx->side_stream;
+        bool side_busy = false;
+        cudaLaunchAttribute pri[1];
+        pri[0].id = cudaLaunchAttributePriority;
+        pri[0].val.priority = ctx->chain_priority;
+        auto cfg_of = [&](unsigned grid, unsigned block, size_t smem) {
+            cudaLaunchConfig_t c{};
+            c.gridDim = dim3(grid);
+            c.blockDim = dim3(block);
+            c.dynamicSmemBytes = smem;
+            c.stream = q;
+            c.attrs = pri;
+            c.numAttrs = 1;
+            return c;
+        };
         B2M_CU(ctx, cudaMemsetAsync(s.counters, 0, s.counters_bytes, q));
         iota_f32_kernel<<<(unsigned)ceil_div(n, 256), 256, 0, q>>>(perm, n);
         B2M_LAUNCHED(ctx);
@@ -717,40 +800,81 @@ int32_t lu_factor_f32(Ctx* ctx, cudaStream_t st, float* A, int64_t ld, int64_t n
             for (int64_t lc0 = oc0; lc0 < oc0 + pw; lc0 += 32) {
                 const int w = (int)std::min<int64_t>(32, n - lc0);
                 TsArgs ta{A, ld, (int)n, (int)lc0, w, (int)oc0, pw, s.cand, s.counters, s.top, s.mvals, s.wmat,
-                          s.moves, ctx->d_status};
+                          s.moves, s.lmul, lc0 == oc0 ? s.pmap : nullptr, ctx->d_status};
                 prof_begin(ctx, q, kClsPanel);
-                tslu_select_kernel<<<(unsigned)ceil_div(n - lc0, kTsRows), kTsThreads, 0, q>>>(ta);
+                {
+                    const cudaLaunchConfig_t c = cfg_of((unsigned)ceil_div(n - lc0, kTsRows), kTsThreads, 0);
+                    B2M_CU(ctx, cudaLaunchKernelEx(&c, tslu_select_kernel, ta));
+                }
                 prof_end(ctx, q, kClsPanel, 4.0 * (n - lc0) * 32);  // bytes: the leaf's columns, read once
                 B2M_LAUNCHED(ctx);
-                ApArgs aa{A, ld, (int)n, (int)lc0, w, (int)oc0, pw, s.top, s.mvals, s.wmat, s.moves, perm,
+                ApArgs aa{A, ld, (int)n, (int)lc0, w, (int)oc0, pw, s.top, s.mvals, s.wmat, s.moves, perm, s.pmap,
                           ctx->d_status, 0};
                 aa.nR = (int)ceil_div(n - lc0, kApRows);
-                const int nC = (int)ceil_div(n - pw, 256);
                 prof_begin(ctx, q, kClsSwap);
-                tslu_apply_kernel<<<aa.nR + nC, 256, 0, q>>>(aa);
-                // bytes: the panel rows read and written, plus <= 64 row moves outside the panel
-                prof_end(ctx, q, kClsSwap, 8.0 * (n - lc0) * (pw - (lc0 - oc0)) + 8.0 * 64 * (n - pw));
+                {
+                    const cudaLaunchConfig_t c = cfg_of((unsigned)aa.nR, 256, 0);
+                    B2M_CU(ctx, cudaLaunchKernelEx(&c, tslu_apply_kernel, aa));
+                }
+                // bytes: the panel rows read and written
+                prof_end(ctx, q, kClsSwap, 8.0 * (n - lc0) * (pw - (lc0 - oc0)));
                 B2M_LAUNCHED(ctx);
             }
+            if (side_busy) {  // the previous panel's wide update must be done before rows move under it
+                B2M_CU(ctx, cudaEventRecord(ctx->ev_side_join, q2));
+                B2M_CU(ctx, cudaStreamWaitEvent(q, ctx->ev_side_join, 0));
+                side_busy = false;
+            }
             const int64_t c1 = oc0 + pw;
+            const int ncb = (int)(oc0 / 32 + ceil_div(n - c1, 32));
+            if (ncb > 0) {
+                prof_begin(ctx, q, kClsSwap);
+                {
+                    const cudaLaunchConfig_t c = cfg_of((unsigned)ncb, 256, kPmSmem);
+                    B2M_CU(ctx, cudaLaunchKernelEx(&c, panel_permute_kernel, A, ld, (int)n, (int)oc0, pw,
+                                                   (const int32_t*)s.pmap, ctx->d_status));
+                }
+                // bytes: at most 64 moved rows per leaf, read and written outside the panel
+                prof_end(ctx, q, kClsSwap, 8.0 * 64 * (pw / 32) * (double)(n - pw));
+                B2M_LAUNCHED(ctx);
+            }
             if (c1 >= n) break;
             const int64_t M = n - c1;
-            OuArgs oa{A, ld, (int)n, (int)oc0, pw, mode, (int)ceil_div(M, 32), s.bth, s.btl, s.ah, s.al, ctx->d_status};
+            const int64_t nw = std::min<int64_t>(kNB, M);  // the next panel's columns
             const int nL = mode == 3 ? (int)ceil_div(M * pw, 1024) : 0;
-            prof_begin(ctx, q, kClsTrsm);
-            lu_outer_kernel<<<oa.nU + nL, 256, ou_smem, q>>>(oa);
-            // bytes: U12 read and written, the GEMM copies of U12 (and of L21 for 3xTF32) written
-            prof_end(ctx, q, kClsTrsm, 8.0 * pw * M + 4.0 * M * pw * (mode == 3 ? 5 : 1));
-            B2M_LAUNCHED(ctx);
-            FOperand bh{s.bth, pw, M, pw, 0, 0};
-            float* C = A + c1 * ld + c1;
-            if (mode == 3) {
-                FOperand ah{s.ah, pw, M, pw, 0, 0};
-                B2M_TRY(sgemm_tc(ctx, q, ah, s.al, bh, s.btl, C, ld, M, M, pw, B2M_DO_SUB, 3, true));
-            } else {
+            auto outer = [&](cudaStream_t qs, int64_t cs0, int64_t ncols, int nl) -> int32_t {
+                OuArgs oa{A, ld, (int)n, (int)oc0, pw, mode, (int)ceil_div(ncols, 32), (int)cs0, (int)ncols,
+                          s.bth, s.btl, s.ah, s.al, ctx->d_status};
+                prof_begin(ctx, qs, kClsTrsm);
+                lu_outer_kernel<<<oa.nU + nl, 256, ou_smem, qs>>>(oa);
+                // bytes: U12 read and written, its GEMM copies written, L21 read and split (3xTF32)
+                prof_end(ctx, qs, kClsTrsm,
+                         8.0 * pw * ncols + 4.0 * ncols * pw * (mode == 3 ? 2 : 1) + (nl ? 12.0 * M * pw : 0.0));
+                B2M_LAUNCHED(ctx);
+                return B2M_OK;
+            };
+            auto gemm = [&](cudaStream_t qs, int64_t cs0, int64_t ncols) -> int32_t {
+                FOperand bh{s.bth, pw, M, pw, cs0, 0};
+                float* C = A + c1 * ld + c1 + cs0;
+                if (mode == 3) {
+                    FOperand ah{s.ah, pw, M, pw, 0, 0};
+                    return sgemm_tc(ctx, qs, ah, s.al, bh, s.btl, C, ld, M, ncols, pw, B2M_DO_SUB, 3, true);
+                }
                 FOperand ah{A, ld, n, n, c1, oc0};
-                B2M_TRY(sgemm_tc(ctx, q, ah, nullptr, bh, nullptr, C, ld, M, M, pw, B2M_DO_SUB, 1, true));
+                return sgemm_tc(ctx, qs, ah, nullptr, bh, nullptr, C, ld, M, ncols, pw, B2M_DO_SUB, 1, true);
+            };
+            B2M_TRY(outer(q, 0, M, nL));
+            B2M_TRY(gemm(q, 0, nw));
+            if (M > nw) {
+                B2M_CU(ctx, cudaEventRecord(ctx->ev_side_fork, q));
+                B2M_CU(ctx, cudaStreamWaitEvent(q2, ctx->ev_side_fork, 0));
+                B2M_TRY(gemm(q2, nw, M - nw));
+                side_busy = true;
             }
+        }
+        if (side_busy) {
+            B2M_CU(ctx, cudaEventRecord(ctx->ev_side_join, q2));
+            B2M_CU(ctx, cudaStreamWaitEvent(q, ctx->ev_side_join, 0));
         }
         const int nblk = (int)ceil_div(n, kTrsvNB);
         diag_inv_kernel<<<2 * nblk, kTrsvNB, di_smem, q>>>(A, ld, (int)n, kTrsvNB, s.linv, s.uinv, ctx->d_status);

@@ -273,6 +273,10 @@ int32_t launch_tc(Ctx* ctx, cudaStream_t st, const CUtensorMap* maps, const TcAr
     static bool attr = false;
     if (!attr) {
         B2M_CU(ctx, cudaFuncSetAttribute(sgemm_tc_kernel<SPLIT>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+        // the largest carveout, so that an SM running a tile still has shared memory for the
+        // (small) panel kernels of the LU that may run beside this GEMM
+        B2M_CU(ctx, cudaFuncSetAttribute(sgemm_tc_kernel<SPLIT>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                         (int)cudaSharedmemCarveoutMaxShared));
         attr = true;
     }
     const int tiles = (int)(ceil_div(a.M, TBM) * ceil_div(a.N, TBN));
