@@ -134,6 +134,7 @@ struct F32Scratch {
     int* moves;
     float* lmul;
     int32_t* pmap;
+    float* lpinv;
     float *bth, *btl, *ah, *al;
     float *linv, *uinv;
     float *wl, *wu;  // coupling blocks T_bb^-1 T_{b,b-1} (L) and T_bb^-1 T_{b,b+1} (U)

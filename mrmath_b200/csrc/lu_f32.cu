@@ -51,6 +51,7 @@ struct TsArgs {
     int* moves;           // [0] moves, [1] moves below the top block, [2..66) dst, [66..130) src
     float* lmul;          // [32][kTsRows] the root elimination's multipliers
     int32_t* pmap;        // first leaf of a panel: pmap[i] = i for the panel's rows (identity)
+    float* lpinv;         // [kNB / 32][32][32]: L11^-1 of each leaf of the outer panel
     int32_t* status;
 };
 
@@ -299,10 +300,14 @@ __global__ void __launch_bounds__(kTsThreads) tslu_select_kernel(TsArgs a) {
 #pragma unroll
         for (int k = 0; k < 32; ++k)
             if (k < nout) a.mvals[k * kNB + c] = y[k];
-        if (in_leaf) {
+        if (in_leaf) {  // the top rows get L11\U11; x becomes e_(c-lo), for column c-lo of L11^-1
 #pragma unroll
-            for (int j = 0; j < 32; ++j) x[j] = s_lu[j][c - lo];
-        } else if (c >= lo + w) {
+            for (int j = 0; j < 32; ++j)
+                if (j < w) a.top[j * kNB + c] = s_lu[j][c - lo];
+#pragma unroll
+            for (int j = 0; j < 32; ++j) x[j] = j == c - lo ? 1.f : 0.f;
+        }
+        if (c >= lo) {
             // x <- L11^-1 x: column j of L read as float4s of its transposed copy
 #pragma unroll
             for (int j = 0; j < 31; ++j) {
@@ -316,9 +321,14 @@ __global__ void __launch_bounds__(kTsThreads) tslu_select_kernel(TsArgs a) {
                 }
             }
         }
+        if (in_leaf) {  // L11^-1 of the leaf, for the panel's triangular solve (lu_outer_kernel)
 #pragma unroll
-        for (int j = 0; j < 32; ++j)
-            if (j < w) a.top[j * kNB + c] = x[j];
+            for (int j = 0; j < 32; ++j) a.lpinv[((lo >> 5) * 32 + j) * 32 + (c - lo)] = j < w ? x[j] : 0.f;
+        } else {
+#pragma unroll
+            for (int j = 0; j < 32; ++j)
+                if (j < w) a.top[j * kNB + c] = x[j];
+        }
         if (c >= lo) {
             // z = U11^-1 e_(c-lo) in the leaf, z = U11^-1 U12(:, c) right of it (back substitution)
             float z[32];
@@ -466,6 +476,7 @@ struct OuArgs {
     float* btl;
     float* ah;
     float* al;
+    const float* lpinv;  // [kNB / 32][32][32] inverses of the panel's diagonal 32 x 32 blocks of L
     const int32_t* status;
 };
 
@@ -492,8 +503,9 @@ __global__ void __launch_bounds__(256) lu_outer_kernel(OuArgs a) {
     const int pw = a.pw;
     const int cs = c_first + a.cs0 + blockIdx.x * 32;
     const int ncol = min(32, min(a.n, c_first + a.cs0 + a.ncols) - cs);
-    float* s_x = sm;               // [kNB][33] the strip
-    float* s_l = sm + kNB * 33;    // [kNB][33] one 32-column block of L (rows from the block down)
+    float* s_x = sm;                 // [kNB][33] the strip
+    float* s_l = sm + kNB * 33;      // [kNB][33] one 32-column block of L (rows from the block down)
+    float* s_li = sm + 2 * kNB * 33; // [32][33] the inverse of its diagonal block
     const int c = t & 31, rg = t >> 5;
     {
         float tmp[kNB / 8];
@@ -505,31 +517,41 @@ __global__ void __launch_bounds__(256) lu_outer_kernel(OuArgs a) {
 #pragma unroll
         for (int i = 0; i < kNB / 8; ++i) s_x[(rg + 8 * i) * 33 + c] = tmp[i];
     }
-    for (int b0 = 0; b0 < pw; b0 += 32) {
+    // the next L block is loaded into registers while the current one is used
+    float nl[kNB / 8], ni[4];
+    auto load_block = [&](int b0) {
         const int bw = min(32, pw - b0);
-        float tmp[kNB / 8];
 #pragma unroll
         for (int i = 0; i < kNB / 8; ++i) {
             const int r = b0 + rg + 8 * i;
-            tmp[i] = (r < pw && c < bw) ? a.A[(int64_t)(a.oc0 + r) * a.ld + a.oc0 + b0 + c] : 0.f;
+            nl[i] = (r < pw && c < bw) ? a.A[(int64_t)(a.oc0 + r) * a.ld + a.oc0 + b0 + c] : 0.f;
         }
-        __syncthreads();
+#pragma unroll
+        for (int i = 0; i < 4; ++i) ni[i] = a.lpinv[(b0 >> 5) * 1024 + (rg + 8 * i) * 32 + c];
+    };
+    load_block(0);
+    for (int b0 = 0; b0 < pw; b0 += 32) {
+        const int bw = min(32, pw - b0);
+        __syncthreads();  // the previous block is no longer read
 #pragma unroll
         for (int i = 0; i < kNB / 8; ++i)
-            if (b0 + rg + 8 * i < pw) s_l[(rg + 8 * i) * 33 + c] = tmp[i];
+            if (b0 + rg + 8 * i < pw) s_l[(rg + 8 * i) * 33 + c] = nl[i];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) s_li[(rg + 8 * i) * 33 + c] = ni[i];
         __syncthreads();
-        if (t < 32) {
-            float x[32];
+        if (b0 + 32 < pw) load_block(b0 + 32);
+        // x_b <- L_bb^-1 x_b: thread (c, rg) forms rows rg + 8 q of the block
+        float y[4] = {0.f, 0.f, 0.f, 0.f};
 #pragma unroll
-            for (int j = 0; j < 32; ++j) x[j] = j < bw ? s_x[(b0 + j) * 33 + c] : 0.f;
+        for (int k = 0; k < 32; ++k) {
+            const float xk = s_x[(b0 + k) * 33 + c];
 #pragma unroll
-            for (int j = 0; j < 32; ++j)
-#pragma unroll
-                for (int k = j + 1; k < 32; ++k) x[k] = fmaf(-s_l[k * 33 + j], x[j], x[k]);
-#pragma unroll
-            for (int j = 0; j < 32; ++j)
-                if (j < bw) s_x[(b0 + j) * 33 + c] = x[j];
+            for (int q = 0; q < 4; ++q) y[q] = fmaf(s_li[(rg + 8 * q) * 33 + k], xk, y[q]);
         }
+        __syncthreads();
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+            if (rg + 8 * q < bw) s_x[(b0 + rg + 8 * q) * 33 + c] = y[q];
         __syncthreads();
         for (int r = b0 + bw + rg; r < pw; r += 8) {
             float acc = s_x[r * 33 + c];
@@ -655,23 +677,28 @@ __global__ void __launch_bounds__(256) coupling_kernel(const float* LU, int64_t 
         for (int j = 0; j < 8; ++j) out[(r0 + i) * NB + c0 + 16 * j] = acc[i][j];
 }
 
-// The outer panel's net row permutation applied to every column outside it: row i (of the panel's
-// rows [oc0, n)) receives what row pmap[i] held when the panel started.  CTA per 32 columns; each
-// CTA lists the moved rows (at most 64 per leaf) and reads all their sources before writing.
+// The outer panel's net row permutation applied to the columns [col_begin, col_end) (outside the
+// panel): row i of the panel's rows [oc0, n) receives what row pmap[i] held when the panel started.
+// CTA per 32 columns.  Each CTA lists the moved rows (at most 64 per leaf; warp-aggregated appends)
+// and loads all of their sources into registers before any write.
 constexpr int kPmMax = 64 * (kNB / 32);
-constexpr int kPmSmem = kPmMax * 32 * (int)sizeof(float);
-__global__ void __launch_bounds__(256) panel_permute_kernel(float* A, int64_t ld, int n, int oc0, int pw,
-                                                            const int32_t* pmap, int32_t* status) {
-    extern __shared__ float pm_buf[];  // [kPmMax][32]
+__global__ void __launch_bounds__(256) panel_permute_kernel(float* A, int64_t ld, int n, int oc0, int col_begin,
+                                                            int col_end, const int32_t* pmap, int32_t* status) {
     __shared__ int s_dst[kPmMax], s_src[kPmMax], s_cnt;
     if (status[kInfo] != 0) return;
-    const int t = threadIdx.x;
+    const int t = threadIdx.x, lane = t & 31;
     if (t == 0) s_cnt = 0;
     __syncthreads();
-    for (int i = oc0 + t; i < n; i += 256) {
-        const int src = pmap[i];
-        if (src != i) {
-            const int k = atomicAdd(&s_cnt, 1);
+    for (int i0 = oc0 + (t & ~31); i0 < n; i0 += 256) {
+        const int i = i0 + lane;
+        const int src = i < n ? pmap[i] : i;
+        const bool mv = src != i;
+        const unsigned bal = __ballot_sync(0xffffffffu, mv);
+        int base = 0;
+        if (lane == 0 && bal) base = atomicAdd(&s_cnt, __popc(bal));
+        base = __shfl_sync(0xffffffffu, base, 0);
+        if (mv) {
+            const int k = base + __popc(bal & ((1u << lane) - 1u));
             if (k < kPmMax) { s_dst[k] = i; s_src[k] = src; }
         }
     }
@@ -681,14 +708,20 @@ __global__ void __launch_bounds__(256) panel_permute_kernel(float* A, int64_t ld
         if (t == 0) atomicExch(&status[kTimeout], 401);
         return;
     }
-    const int cb = blockIdx.x, left = oc0 / 32;
-    const int col0 = cb < left ? cb * 32 : oc0 + pw + (cb - left) * 32;
-    const int c = t & 31, rg = t >> 5;
-    const bool ok = col0 + c < n;
-    for (int k = rg; k < cnt; k += 8) pm_buf[k * 32 + c] = ok ? A[(int64_t)s_src[k] * ld + col0 + c] : 0.f;
-    __syncthreads();
-    if (ok)
-        for (int k = rg; k < cnt; k += 8) A[(int64_t)s_dst[k] * ld + col0 + c] = pm_buf[k * 32 + c];
+    const int col = col_begin + blockIdx.x * 32 + (t & 31), rg = t >> 5;
+    const bool ok = col < col_end && col < n;
+    float x[kPmMax / 8];
+#pragma unroll
+    for (int q = 0; q < kPmMax / 8; ++q) {
+        const int k = rg + 8 * q;
+        x[q] = (ok && k < cnt) ? A[(int64_t)s_src[k] * ld + col] : 0.f;
+    }
+    __syncthreads();  // every source of this CTA's columns is read before any row is written
+#pragma unroll
+    for (int q = 0; q < kPmMax / 8; ++q) {
+        const int k = rg + 8 * q;
+        if (ok && k < cnt) A[(int64_t)s_dst[k] * ld + col] = x[q];
+    }
 }
 
 }  // namespace
@@ -703,6 +736,7 @@ size_t f32_scratch_bytes(int64_t n) {
     b += 256 * sizeof(int);                                     // moves
     b += 32 * (size_t)kTsRows * sizeof(float);                  // root multipliers
     b += (size_t)round_up(n, 64) * sizeof(int32_t);              // panel row map
+    b += (size_t)kNB * 32 * sizeof(float);                      // leaf L11^-1 blocks
     b += 4 * (size_t)round_up(n, 32) * kNB * sizeof(float);     // bth, btl, ah, al
     b += 4 * (size_t)nblk * kTrsvNB * kTrsvNB * sizeof(float);  // diagonal inverses, coupling blocks
     b += kSweepFlags * sizeof(int);                             // sweep flags
@@ -727,6 +761,7 @@ F32Scratch f32_scratch_carve(void* base, int64_t n) {
     s.moves = reinterpret_cast<int*>(take(256 * sizeof(int)));
     s.lmul = reinterpret_cast<float*>(take(32 * (size_t)kTsRows * sizeof(float)));
     s.pmap = reinterpret_cast<int32_t*>(take((size_t)round_up(n, 64) * sizeof(int32_t)));
+    s.lpinv = reinterpret_cast<float*>(take((size_t)kNB * 32 * sizeof(float)));
     const size_t panel = (size_t)round_up(n, 32) * kNB * sizeof(float);
     s.bth = reinterpret_cast<float*>(take(panel));
     s.btl = reinterpret_cast<float*>(take(panel));
@@ -747,13 +782,12 @@ int32_t lu_factor_f32(Ctx* ctx, cudaStream_t st, float* A, int64_t ld, int64_t n
         return fail(ctx, B2M_ERR_DIM, "lu_factor_f32: ld must be a multiple of 32 floats, A 128-byte aligned");
     if (n > (int64_t)kTsMaxCand * kTsRows) return fail(ctx, B2M_ERR_UNSUPPORTED, "mixed LU: n too large");
     static bool attr = false;
-    const int ou_smem = 2 * kNB * 33 * sizeof(float);
+    const int ou_smem = (2 * kNB + 32) * 33 * sizeof(float);
     const int di_smem = 2 * kTrsvNB * (kTrsvNB + 1) * sizeof(float);
     if (!attr) {
         B2M_CU(ctx, cudaFuncSetAttribute(lu_outer_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, ou_smem));
         B2M_CU(ctx, cudaFuncSetAttribute(diag_inv_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, di_smem));
         B2M_CU(ctx, cudaFuncSetAttribute(coupling_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kCpSmem));
-        B2M_CU(ctx, cudaFuncSetAttribute(panel_permute_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kPmSmem));
         // one shared-memory carveout for every kernel of the factorisation, so that the panel kernels
         // can share SMs with the tiles of a concurrent trailing GEMM (which needs the maximum)
         for (const void* f : {(const void*)tslu_select_kernel, (const void*)tslu_apply_kernel,
@@ -800,7 +834,7 @@ int32_t lu_factor_f32(Ctx* ctx, cudaStream_t st, float* A, int64_t ld, int64_t n
             for (int64_t lc0 = oc0; lc0 < oc0 + pw; lc0 += 32) {
                 const int w = (int)std::min<int64_t>(32, n - lc0);
                 TsArgs ta{A, ld, (int)n, (int)lc0, w, (int)oc0, pw, s.cand, s.counters, s.top, s.mvals, s.wmat,
-                          s.moves, s.lmul, lc0 == oc0 ? s.pmap : nullptr, ctx->d_status};
+                          s.moves, s.lmul, lc0 == oc0 ? s.pmap : nullptr, s.lpinv, ctx->d_status};
                 prof_begin(ctx, q, kClsPanel);
                 {
                     const cudaLaunchConfig_t c = cfg_of((unsigned)ceil_div(n - lc0, kTsRows), kTsThreads, 0);
@@ -826,17 +860,26 @@ int32_t lu_factor_f32(Ctx* ctx, cudaStream_t st, float* A, int64_t ld, int64_t n
                 side_busy = false;
             }
             const int64_t c1 = oc0 + pw;
-            const int ncb = (int)(oc0 / 32 + ceil_div(n - c1, 32));
-            if (ncb > 0) {
-                prof_begin(ctx, q, kClsSwap);
-                {
-                    const cudaLaunchConfig_t c = cfg_of((unsigned)ncb, 256, kPmSmem);
-                    B2M_CU(ctx, cudaLaunchKernelEx(&c, panel_permute_kernel, A, ld, (int)n, (int)oc0, pw,
-                                                   (const int32_t*)s.pmap, ctx->d_status));
-                }
-                // bytes: at most 64 moved rows per leaf, read and written outside the panel
-                prof_end(ctx, q, kClsSwap, 8.0 * 64 * (pw / 32) * (double)(n - pw));
+            auto permute = [&](cudaStream_t qs, int64_t c_begin, int64_t c_end) -> int32_t {
+                if (c_end <= c_begin) return B2M_OK;
+                cudaLaunchConfig_t c = cfg_of((unsigned)ceil_div(c_end - c_begin, 32), 256, 0);
+                c.stream = qs;
+                prof_begin(ctx, qs, kClsSwap);
+                B2M_CU(ctx, cudaLaunchKernelEx(&c, panel_permute_kernel, A, ld, (int)n, (int)oc0, (int)c_begin,
+                                               (int)c_end, (const int32_t*)s.pmap, ctx->d_status));
+                // bytes: at most 64 moved rows per leaf, read and written
+                prof_end(ctx, qs, kClsSwap, 8.0 * 64 * (pw / 32) * (double)(c_end - c_begin));
                 B2M_LAUNCHED(ctx);
+                return B2M_OK;
+            };
+            // columns right of the panel now (the next step reads them); the factored columns on
+            // the left on the side stream, ordered before the next panel's permutation by the join
+            B2M_TRY(permute(q, c1, n));
+            if (oc0 > 0) {
+                B2M_CU(ctx, cudaEventRecord(ctx->ev_side_fork, q));
+                B2M_CU(ctx, cudaStreamWaitEvent(q2, ctx->ev_side_fork, 0));
+                B2M_TRY(permute(q2, 0, oc0));
+                side_busy = true;
             }
             if (c1 >= n) break;
             const int64_t M = n - c1;
@@ -844,7 +887,7 @@ int32_t lu_factor_f32(Ctx* ctx, cudaStream_t st, float* A, int64_t ld, int64_t n
             const int nL = mode == 3 ? (int)ceil_div(M * pw, 1024) : 0;
             auto outer = [&](cudaStream_t qs, int64_t cs0, int64_t ncols, int nl) -> int32_t {
                 OuArgs oa{A, ld, (int)n, (int)oc0, pw, mode, (int)ceil_div(ncols, 32), (int)cs0, (int)ncols,
-                          s.bth, s.btl, s.ah, s.al, ctx->d_status};
+                          s.bth, s.btl, s.ah, s.al, s.lpinv, ctx->d_status};
                 prof_begin(ctx, qs, kClsTrsm);
                 lu_outer_kernel<<<oa.nU + nl, 256, ou_smem, qs>>>(oa);
                 // bytes: U12 read and written, its GEMM copies written, L21 read and split (3xTF32)
