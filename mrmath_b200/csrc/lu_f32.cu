@@ -503,9 +503,9 @@ __global__ void __launch_bounds__(256) lu_outer_kernel(OuArgs a) {
     const int pw = a.pw;
     const int cs = c_first + a.cs0 + blockIdx.x * 32;
     const int ncol = min(32, min(a.n, c_first + a.cs0 + a.ncols) - cs);
-    float* s_x = sm;                 // [kNB][33] the strip
-    float* s_l = sm + kNB * 33;      // [kNB][33] one 32-column block of L (rows from the block down)
-    float* s_li = sm + 2 * kNB * 33; // [32][33] the inverse of its diagonal block
+    float* s_x = sm;                  // [kNB][33] the strip (thread c owns column c)
+    float* s_l = sm + kNB * 33;       // [kNB][36] one 32-column block of L (rows from the block down)
+    float* s_li = s_l + kNB * 36;     // [32][36] the inverse of its diagonal block
     const int c = t & 31, rg = t >> 5;
     {
         float tmp[kNB / 8];
@@ -535,29 +535,50 @@ __global__ void __launch_bounds__(256) lu_outer_kernel(OuArgs a) {
         __syncthreads();  // the previous block is no longer read
 #pragma unroll
         for (int i = 0; i < kNB / 8; ++i)
-            if (b0 + rg + 8 * i < pw) s_l[(rg + 8 * i) * 33 + c] = nl[i];
+            if (b0 + rg + 8 * i < pw) s_l[(rg + 8 * i) * 36 + c] = nl[i];
 #pragma unroll
-        for (int i = 0; i < 4; ++i) s_li[(rg + 8 * i) * 33 + c] = ni[i];
+        for (int i = 0; i < 4; ++i) s_li[(rg + 8 * i) * 36 + c] = ni[i];
         __syncthreads();
         if (b0 + 32 < pw) load_block(b0 + 32);
-        // x_b <- L_bb^-1 x_b: thread (c, rg) forms rows rg + 8 q of the block
-        float y[4] = {0.f, 0.f, 0.f, 0.f};
+        // x_b <- L_bb^-1 x_b: the block's 32 values of column c in registers, thread (c, rg) forms
+        // rows rg + 8 q; the inverse's rows are read as float4 broadcasts
+        float xb[32];
 #pragma unroll
-        for (int k = 0; k < 32; ++k) {
-            const float xk = s_x[(b0 + k) * 33 + c];
+        for (int k = 0; k < 32; ++k) xb[k] = s_x[(b0 + k) * 33 + c];
+        float y[4];
 #pragma unroll
-            for (int q = 0; q < 4; ++q) y[q] = fmaf(s_li[(rg + 8 * q) * 33 + k], xk, y[q]);
+        for (int q = 0; q < 4; ++q) {
+            const float4* li = reinterpret_cast<const float4*>(s_li + (rg + 8 * q) * 36);
+            float acc = 0.f;
+#pragma unroll
+            for (int kq = 0; kq < 8; ++kq) {
+                const float4 l4 = li[kq];
+                acc = fmaf(l4.x, xb[4 * kq], acc);
+                acc = fmaf(l4.y, xb[4 * kq + 1], acc);
+                acc = fmaf(l4.z, xb[4 * kq + 2], acc);
+                acc = fmaf(l4.w, xb[4 * kq + 3], acc);
+            }
+            y[q] = acc;
         }
         __syncthreads();
 #pragma unroll
         for (int q = 0; q < 4; ++q)
             if (rg + 8 * q < bw) s_x[(b0 + rg + 8 * q) * 33 + c] = y[q];
         __syncthreads();
-        for (int r = b0 + bw + rg; r < pw; r += 8) {
-            float acc = s_x[r * 33 + c];
-            const float* lr = s_l + (r - b0) * 33;
 #pragma unroll
-            for (int k = 0; k < 32; ++k) acc = fmaf(-lr[k], s_x[(b0 + k) * 33 + c], acc);
+        for (int k = 0; k < 32; ++k) xb[k] = s_x[(b0 + k) * 33 + c];
+        // rows below the block: x_r -= L(r, block) x_b, one float4 broadcast per 4 multipliers
+        for (int r = b0 + bw + rg; r < pw; r += 8) {
+            const float4* lr = reinterpret_cast<const float4*>(s_l + (r - b0) * 36);
+            float acc = s_x[r * 33 + c];
+#pragma unroll
+            for (int kq = 0; kq < 8; ++kq) {
+                const float4 l4 = lr[kq];
+                acc = fmaf(-l4.x, xb[4 * kq], acc);
+                acc = fmaf(-l4.y, xb[4 * kq + 1], acc);
+                acc = fmaf(-l4.z, xb[4 * kq + 2], acc);
+                acc = fmaf(-l4.w, xb[4 * kq + 3], acc);
+            }
             s_x[r * 33 + c] = acc;
         }
     }
@@ -782,7 +803,7 @@ int32_t lu_factor_f32(Ctx* ctx, cudaStream_t st, float* A, int64_t ld, int64_t n
         return fail(ctx, B2M_ERR_DIM, "lu_factor_f32: ld must be a multiple of 32 floats, A 128-byte aligned");
     if (n > (int64_t)kTsMaxCand * kTsRows) return fail(ctx, B2M_ERR_UNSUPPORTED, "mixed LU: n too large");
     static bool attr = false;
-    const int ou_smem = (2 * kNB + 32) * 33 * sizeof(float);
+    const int ou_smem = (kNB * 33 + (kNB + 32) * 36) * sizeof(float);
     const int di_smem = 2 * kTrsvNB * (kTrsvNB + 1) * sizeof(float);
     if (!attr) {
         B2M_CU(ctx, cudaFuncSetAttribute(lu_outer_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, ou_smem));
