@@ -37,7 +37,7 @@ constexpr int kTsFan = kTsRows / 32;              // candidate sets merged per t
 constexpr int kTsLevels = 4;
 constexpr int kTsMaxCand = 2048;                  // nodes per level (rows <= 1M)
 constexpr int kNB = 256;                          // outer panel width
-constexpr int kApRows = 32;                       // rows per apply CTA
+constexpr int kApRows = 16;                       // rows per apply CTA
 
 struct TsArgs {
     const float* A;
@@ -371,9 +371,8 @@ struct ApArgs {
 // it (moved in from the side buffer or in place) becomes [v_left | l | v_right - l U12] with
 // l = v_leaf U11^-1, computed as the product v_leaf * [U11^-1 | U11^-1 U12] (thread per column).
 // The row moves are recorded in perm and in the panel's row map; the columns outside the outer
-// panel are permuted once per panel (panel_permute_kernel).  Column CTAs (blockIdx >= nR, not
-// launched by the factorisation) apply the leaf's row moves to the columns outside the panel.
-__global__ void __launch_bounds__(256) tslu_apply_kernel(ApArgs a) {
+// panel are permuted once per panel (panel_permute_kernel).
+__global__ void __launch_bounds__(256, 2) tslu_apply_kernel(ApArgs a) {
     __shared__ __align__(16) float s_l[kApRows][36];  // the rows' leaf values v_leaf
     __shared__ int s_mdst[64], s_msrc[64], s_src[kApRows];
     if (a.status[kInfo] != 0) return;
@@ -381,20 +380,6 @@ __global__ void __launch_bounds__(256) tslu_apply_kernel(ApArgs a) {
     const int nm = a.moves[0], nout = a.moves[1];
     if (t < nm) { s_mdst[t] = a.moves[2 + t]; s_msrc[t] = a.moves[66 + t]; }
     __syncthreads();
-    if (blockIdx.x >= a.nR) {
-        // columns outside the outer panel: the leaf's row moves (all reads before all writes)
-        const int cidx = (blockIdx.x - a.nR) * 256 + t;
-        const int col = cidx < a.oc0 ? cidx : cidx + a.pw;
-        if (col >= a.n) return;
-        float x[64];
-#pragma unroll
-        for (int k = 0; k < 64; ++k)
-            if (k < nm) x[k] = a.A[(int64_t)s_msrc[k] * a.ld + col];
-#pragma unroll
-        for (int k = 0; k < 64; ++k)
-            if (k < nm) a.A[(int64_t)s_mdst[k] * a.ld + col] = x[k];
-        return;
-    }
     if (blockIdx.x == 0 && a.perm) {
         int pv = 0, qv = 0;
         if (t < nm) { pv = a.perm[s_msrc[t]]; qv = a.pmap[s_msrc[t]]; }
@@ -710,17 +695,27 @@ __global__ void __launch_bounds__(256) panel_permute_kernel(float* A, int64_t ld
     const int t = threadIdx.x, lane = t & 31;
     if (t == 0) s_cnt = 0;
     __syncthreads();
-    for (int i0 = oc0 + (t & ~31); i0 < n; i0 += 256) {
-        const int i = i0 + lane;
-        const int src = i < n ? pmap[i] : i;
-        const bool mv = src != i;
-        const unsigned bal = __ballot_sync(0xffffffffu, mv);
-        int base = 0;
-        if (lane == 0 && bal) base = atomicAdd(&s_cnt, __popc(bal));
-        base = __shfl_sync(0xffffffffu, base, 0);
-        if (mv) {
-            const int k = base + __popc(bal & ((1u << lane) - 1u));
-            if (k < kPmMax) { s_dst[k] = i; s_src[k] = src; }
+    constexpr int kScan = 16;  // row-map entries per thread per pass, all loaded before use
+    for (int p0 = oc0; p0 < n; p0 += 256 * kScan) {
+        int src[kScan];
+#pragma unroll
+        for (int u = 0; u < kScan; ++u) {
+            const int i = p0 + 256 * u + t;
+            src[u] = i < n ? pmap[i] : i;
+        }
+#pragma unroll
+        for (int u = 0; u < kScan; ++u) {
+            const int i = p0 + 256 * u + t;
+            const bool mv = src[u] != i;
+            const unsigned bal = __ballot_sync(0xffffffffu, mv);
+            if (!bal) continue;  // warp-uniform
+            int base = 0;
+            if (lane == 0) base = atomicAdd(&s_cnt, __popc(bal));
+            base = __shfl_sync(0xffffffffu, base, 0);
+            if (mv) {
+                const int k = base + __popc(bal & ((1u << lane) - 1u));
+                if (k < kPmMax) { s_dst[k] = i; s_src[k] = src[u]; }
+            }
         }
     }
     __syncthreads();
