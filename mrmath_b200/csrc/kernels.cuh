@@ -138,9 +138,9 @@ struct F32Scratch {
     float *bth, *btl, *ah, *al;
     float *linv, *uinv;
     float *wl, *wu;  // coupling blocks T_bb^-1 T_{b,b-1} (L) and T_bb^-1 T_{b,b+1} (U)
-    int* flags;  // block-done flags of the persistent refinement sweeps (kSweepFlags ints)
+    unsigned long long* ll;  // published block solutions of the persistent refinement sweeps
 };
-constexpr int kSweepFlags = 4096;
+constexpr int kSweepGroups = 2;  // right-hand-side groups of 8 in one persistent sweep (16 columns)
 size_t f32_scratch_bytes(int64_t n);
 F32Scratch f32_scratch_carve(void* base, int64_t n);
 // A (n x n, row stride ld a multiple of 32, 128-byte aligned) is factored in place as P A = L U;

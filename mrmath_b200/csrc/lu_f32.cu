@@ -755,7 +755,7 @@ size_t f32_scratch_bytes(int64_t n) {
     b += (size_t)kNB * 32 * sizeof(float);                      // leaf L11^-1 blocks
     b += 4 * (size_t)round_up(n, 32) * kNB * sizeof(float);     // bth, btl, ah, al
     b += 4 * (size_t)nblk * kTrsvNB * kTrsvNB * sizeof(float);  // diagonal inverses, coupling blocks
-    b += kSweepFlags * sizeof(int);                             // sweep flags
+    b += 2 * (size_t)nblk * kSweepGroups * kTrsvNB * 8 * sizeof(unsigned long long);  // sweep words
     return b + 16 * 256;
 }
 
@@ -787,7 +787,8 @@ F32Scratch f32_scratch_carve(void* base, int64_t n) {
     s.uinv = reinterpret_cast<float*>(take((size_t)nblk * kTrsvNB * kTrsvNB * sizeof(float)));
     s.wl = reinterpret_cast<float*>(take((size_t)nblk * kTrsvNB * kTrsvNB * sizeof(float)));
     s.wu = reinterpret_cast<float*>(take((size_t)nblk * kTrsvNB * kTrsvNB * sizeof(float)));
-    s.flags = reinterpret_cast<int*>(take(kSweepFlags * sizeof(int)));
+    s.ll = reinterpret_cast<unsigned long long*>(
+        take(2 * (size_t)nblk * kSweepGroups * kTrsvNB * 8 * sizeof(unsigned long long)));
     return s;
 }
 

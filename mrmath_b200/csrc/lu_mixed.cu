@@ -288,13 +288,16 @@ __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_gr
 // just before b) precomputed, the block's solution is
 //     x_b = T_bb^-1 (X_b - sum_{j before p} T_bj x_j)  -  W_b x_p,
 // so everything but the last product is done while block p is still being solved, and the chain
-// of 128-row blocks advances by one 128 x 128 x 8 product, a flag and an L2 round trip per step.
+// of 128-row blocks advances by one 128 x 128 x 8 product and one L2 round trip per step: a block's
+// solution is published as 64-bit words {value, flag} (written and polled with single 64-bit
+// accesses, so a word whose flag is set carries its value; no fence, no separate flag read).
 // T_bb^-1 and W_b are staged in shared memory at kernel start, the rows of the other T_bj are
 // loaded into registers before each wait.  All CTAs are resident (cooperative launch); every wait
-// is bounded and reports a timeout through the status words, and a CTA that gives up sets its flag
-// to -1 so that the CTAs after it give up without waiting again.
+// is bounded and reports a timeout through the status words, and a CTA that gives up marks its
+// words with the flag kSwAbort so that the CTAs after it give up without waiting again.
 constexpr int kSwRhs = 8;
 constexpr uint32_t kSwSpin = 1u << 22;
+constexpr uint32_t kSwAbort = 0xFFFFFFFFu;
 constexpr int kSwSmem = 2 * kTrsvNB * kTrsvNB * (int)sizeof(float);  // T_bb^-1 and W_b
 
 struct SwArgs {
@@ -309,17 +312,17 @@ struct SwArgs {
     double* X64;
     int64_t ldx;
     int upper;
-    int* flags;
+    unsigned long long* ll;  // [nblk][ng][128][8] published solutions {value bits, flag}, zeroed before the launch
     int32_t* status;
 };
 
-__device__ __forceinline__ int ld_acquire(const int* p) {
-    int v;
-    asm volatile("ld.acquire.gpu.global.b32 %0, [%1];\n" : "=r"(v) : "l"(p) : "memory");
+__device__ __forceinline__ unsigned long long ld_relaxed64(const unsigned long long* p) {
+    unsigned long long v;
+    asm volatile("ld.relaxed.gpu.global.b64 %0, [%1];\n" : "=l"(v) : "l"(p) : "memory");
     return v;
 }
-__device__ __forceinline__ void st_release(int* p, int v) {
-    asm volatile("st.release.gpu.global.b32 [%0], %1;\n" ::"l"(p), "r"(v) : "memory");
+__device__ __forceinline__ void st_relaxed64(unsigned long long* p, unsigned long long v) {
+    asm volatile("st.relaxed.gpu.global.b64 [%0], %1;\n" ::"l"(p), "l"(v) : "memory");
 }
 
 // acc[q] += sum over this thread's 64 k of M[r][k] * P[k][q], M staged as float4 [k/4][row].
@@ -366,6 +369,7 @@ __global__ void __launch_bounds__(256, 1) trsv_sweep_kernel(SwArgs a) {
     const int cg = a.c0 + g * kSwRhs;
     const int ncg = min(kSwRhs, a.nc - g * kSwRhs);
     if (t == 0) s_abort = 0;
+    __syncthreads();
     {
         const float* inv = a.inv + (int64_t)b * NB * NB;
         const float* w = a.w + (int64_t)b * NB * NB;
@@ -385,31 +389,41 @@ __global__ void __launch_bounds__(256, 1) trsv_sweep_kernel(SwArgs a) {
 #pragma unroll
     for (int q = 0; q < kSwRhs; ++q) acc[q] = 0.f;
 
+    // this CTA's published words; thread t polls rows t / 2, columns 4 (t % 2) .. + 3 of a block
+    unsigned long long* ll_own = a.ll + (size_t)(b * ng + g) * (kTrsvNB * kSwRhs);
+    auto abandon = [&]() {  // mark every word of this CTA so that its dependants stop at once
+#pragma unroll
+        for (int e = 0; e < 4; ++e) st_relaxed64(ll_own + 4 * t + e, (unsigned long long)kSwAbort << 32);
+    };
     // wait for block j of the sweep and stage its solution in s_p; false if the sweep is abandoned
     auto wait_and_stage = [&](int j) -> bool {
-        if (t == 0) {
-            const int* f = a.flags + j * ng + g;
-            uint32_t it = 0;
-            int v;
-            while ((v = ld_acquire(f)) == 0 && ++it < kSwSpin) {
+        const int k = t >> 1, q0 = (t & 1) * 4;
+        const unsigned long long* src = a.ll + (size_t)(j * ng + g) * (kTrsvNB * kSwRhs) + k * kSwRhs + q0;
+        unsigned long long w[4];
+        uint32_t it = 0;
+        bool ready, bad;
+        do {
+#pragma unroll
+            for (int e = 0; e < 4; ++e) w[e] = ld_relaxed64(src + e);
+            ready = true;
+            bad = false;
+#pragma unroll
+            for (int e = 0; e < 4; ++e) {
+                const uint32_t f = (uint32_t)(w[e] >> 32);
+                ready = ready && f == 1u;
+                bad = bad || f == kSwAbort;
             }
-            if (v == 0) atomicExch(&a.status[kTimeout], 501);
-            if (v <= 0) {
-                s_abort = 1;
-                st_release(a.flags + b * ng + g, -1);
-            }
-        }
-        __syncthreads();
-        if (s_abort) return false;
-        const int p0 = j * NB, ps = min(NB, a.n - p0);
-        const int k = t >> 1, q0 = (t & 1) * 4;  // 128 rows x 8 columns, one float4 per thread
-        float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
-        if (k < ps && q0 < ncg) v = __ldcg(reinterpret_cast<const float4*>(a.Xr + (int64_t)(p0 + k) * a.ldr + cg + q0));
-        if (q0 + 1 >= ncg) v.y = 0.f;
-        if (q0 + 2 >= ncg) v.z = 0.f;
-        if (q0 + 3 >= ncg) v.w = 0.f;
+        } while (!ready && !bad && ++it < kSwSpin);
+        if (!ready && !bad) atomicExch(&a.status[kTimeout], 501);
+        if (!ready) s_abort = 1;
+        const float4 v = make_float4(__uint_as_float((uint32_t)w[0]), __uint_as_float((uint32_t)w[1]),
+                                     __uint_as_float((uint32_t)w[2]), __uint_as_float((uint32_t)w[3]));
         *reinterpret_cast<float4*>(&s_p[k][q0]) = v;
         __syncthreads();
+        if (s_abort) {
+            abandon();
+            return false;
+        }
         return true;
     };
 
@@ -475,16 +489,18 @@ __global__ void __launch_bounds__(256, 1) trsv_sweep_kernel(SwArgs a) {
     }
     __syncthreads();
     float xv[kSwRhs];
-    if (h == 0 && r < bs) {
+    if (h == 0) {  // publish every word of the block (zeros past the matrix and past the right-hand sides)
 #pragma unroll
         for (int q = 0; q < kSwRhs; ++q) {
-            xv[q] = acc[q] + s_h[r][q];
-            if (q < ncg) a.Xr[(int64_t)(b0 + r) * a.ldr + cg + q] = xv[q];
+            xv[q] = (r < bs && q < ncg) ? acc[q] + s_h[r][q] : 0.f;
+            st_relaxed64(ll_own + r * kSwRhs + q, (1ull << 32) | __float_as_uint(xv[q]));
+        }
+        if (r < bs) {
+#pragma unroll
+            for (int q = 0; q < kSwRhs; ++q)
+                if (q < ncg) a.Xr[(int64_t)(b0 + r) * a.ldr + cg + q] = xv[q];
         }
     }
-    __threadfence();
-    __syncthreads();
-    if (t == 0) st_release(a.flags + b * ng + g, 1);
     if (a.upper && h == 0 && r < bs) {  // the FP64 accumulation is off the chain
 #pragma unroll
         for (int q = 0; q < kSwRhs; ++q)
@@ -620,13 +636,14 @@ int32_t ir_solve(Ctx* ctx, cudaStream_t st, const float* LU, int64_t ld, int64_t
     for (int64_t c0 = 0; c0 < nrhs; c0 += kTrMaxRhs) {
         const int nc = (int)std::min<int64_t>(kTrMaxRhs, nrhs - c0);
         const int ng = (int)ceil_div(nc, kSwRhs);
-        if (nblk * ng <= coop_ctas && 2 * nblk * ng <= kSweepFlags) {
+        if (nblk * ng <= coop_ctas && ng <= kSweepGroups) {
             // persistent sweeps: one cooperative launch each
             for (int up = 0; up < 2; ++up) {
-                int* flags = s.flags + up * nblk * ng;
-                B2M_CU(ctx, cudaMemsetAsync(flags, 0, (size_t)nblk * ng * sizeof(int), st));
+                const size_t ll_words = (size_t)nblk * ng * kTrsvNB * kSwRhs;
+                unsigned long long* ll = s.ll + up * (size_t)nblk * kSweepGroups * kTrsvNB * kSwRhs;
+                B2M_CU(ctx, cudaMemsetAsync(ll, 0, ll_words * sizeof(unsigned long long), st));
                 SwArgs sa{LU,  ld, (int)n, up ? s.uinv : s.linv, up ? s.wu : s.wl, Xr, ldr, (int)c0, nc, X64, ldx, up,
-                          flags, ctx->d_status};
+                          ll, ctx->d_status};
                 cudaLaunchConfig_t cfg{};
                 cudaLaunchAttribute at[1];
                 at[0].id = cudaLaunchAttributeCooperative;
