@@ -5,9 +5,12 @@
 // reference's FP64 LU.  It uses tournament pivoting (communication-avoiding LU, Grigori, Demmel
 // and Xiang 2011), which removes the per-column grid-wide reduction that bounds a classic panel:
 //
-//   * outer panels of kNB = 256 columns, blocked right-looking: after a panel is factored, the
-//     rows above the trailing matrix are solved with the panel's unit-lower block (U12) and the
-//     trailing matrix is updated by one tcgen05 GEMM (TF32 or 3xTF32, K = 256);
+//   * outer panels of kNB = 256 columns, blocked right-looking: after a panel is factored, its
+//     net row permutation is applied to the columns outside it (panel_permute_kernel), the rows
+//     above the trailing matrix are solved with the panel's unit-lower block (U12, through the
+//     leaves' L11^-1) and the trailing matrix is updated by tcgen05 GEMMs (TF32 or 3xTF32,
+//     K = 256): the next panel's columns first, the rest on a side stream under the next panel's
+//     leaves (look-ahead);
 //   * inside a panel, 32-column leaves.  tslu_select_kernel runs Gaussian elimination with
 //     partial pivoting on 512-row chunks in parallel; each chunk nominates 32 candidate rows, and
 //     the last CTA of every group of 16 chunks (found with an atomic counter, no spinning) runs
@@ -15,8 +18,8 @@
 //     root's pivots are the leaf's pivots and its eliminated rows are the leaf's L11\U11;
 //   * tslu_apply_kernel moves the chosen rows into place (a side buffer holds the rows whose
 //     slots get overwritten, so the move is race free), forms L21 = A21 U11^-1 and applies the
-//     leaf's rank-32 update to the rest of the panel; extra CTAs apply the same row moves to all
-//     columns outside the panel.
+//     leaf's rank-32 update to the rest of the panel; it records the moves in `perm` and in the
+//     panel's row map, which the panel permutation applies to the other columns.
 //
 // The permutation is tracked in `perm` (row i of the factors is original row perm[i]); no LAPACK
 // style interchange vector is produced because nothing downstream of the mixed solve needs one.
