@@ -30,10 +30,11 @@ constexpr int kTrMaxRhs = 16;  // right-hand sides per sweep launch
 constexpr int kReRows = 64;    // rows per residual CTA
 constexpr int kReRhs = 16;     // right-hand sides per residual CTA
 constexpr int kReK = 64;       // K chunk of the residual
-constexpr int kReSplit = 4;    // K slices inside a residual CTA
+constexpr int kReSplit = 2;    // K halves inside a residual CTA (four warps each)
 constexpr int kReStages = 3;   // cp.async pipeline depth
 constexpr int kReAS = kReK + 2;                                   // A tile row stride (doubles)
-constexpr int kReStage = kReRows * kReAS + kReK * kReRhs;         // doubles per stage
+constexpr int kReXS = kReRhs + 4;                                 // X tile row stride (doubles)
+constexpr int kReStage = kReRows * kReAS + kReK * kReXS;          // doubles per stage
 constexpr int kReSmem = kReStages * kReStage * (int)sizeof(double);
 
 unsigned gsz(int64_t n, int b = 256) { return (unsigned)ceil_div(std::max<int64_t>(n, 1), b); }
@@ -523,16 +524,19 @@ struct ReArgs {
 };
 
 // r = b - A x for rows [64 blockIdx.x, +64) and columns [16 blockIdx.y, +16).  A and X stream
-// through a 3-stage cp.async pipeline (64 x 64 tiles of A, 64 x 16 of X); four K slices of 64
-// threads each; a thread accumulates rows rg, rg+16, rg+32, rg+48 x 4 columns (A rows 66 doubles
-// apart keep those four-row loads free of bank conflicts).
+// through a 3-stage cp.async pipeline (64 x 64 tiles of A, 64 x 16 of X).  The products run on the
+// FP64 tensor cores (mma.sync m16n8k4): warp w owns rows 16 (w % 4) .. +16 and the K half w / 4 of
+// every chunk, and both 8-column tiles, so each A fragment feeds two MMAs.  Fragments
+// (g = lane / 4, t = lane % 4): a = (A[g][k+t], A[g+8][k+t]), b = X[k+t][g],
+// c = (C[g][2t], C[g][2t+1], C[g+8][2t], C[g+8][2t+1]).  Row strides of 66 (A) and 20 (X) doubles
+// keep both fragment loads at two shared-memory wavefronts per warp.
 __global__ void __launch_bounds__(256, 1) resid_kernel(ReArgs a) {
     extern __shared__ __align__(16) double re_sm[];
     __shared__ unsigned long long s_n[3 * kReRhs];
     const int t = threadIdx.x;
     const int r0 = blockIdx.x * kReRows, cb = blockIdx.y * kReRhs;
     const int nc = min(kReRhs, a.nrhs - cb);
-    const int ks = t >> 6, u = t & 63, rg = u >> 2, q = u & 3;
+    const int lane = t & 31, wp = t >> 5, mt = wp & 3, kh = wp >> 2, gq = lane >> 2, tq = lane & 3;
     const int nk = (int)ceil_div(a.n, kReK);
     if (t < 3 * kReRhs) s_n[t] = 0ull;
     auto issue = [&](int kc) {
@@ -553,14 +557,10 @@ __global__ void __launch_bounds__(256, 1) resid_kernel(ReArgs a) {
             const int gk = k0 + k;
             const bool ok = gk < a.n && cp < nc;
             const double* src = ok ? a.X + (int64_t)gk * a.ldx + cb + cp : a.X;
-            cp_async16(sx + k * kReRhs + cp, src, ok ? (cp + 1 < nc ? 16 : 8) : 0);
+            cp_async16(sx + k * kReXS + cp, src, ok ? (cp + 1 < nc ? 16 : 8) : 0);
         }
     };
-    double acc[4][4];
-#pragma unroll
-    for (int i = 0; i < 4; ++i)
-#pragma unroll
-        for (int j = 0; j < 4; ++j) acc[i][j] = 0.0;
+    double d0[4] = {0.0, 0.0, 0.0, 0.0}, d1[4] = {0.0, 0.0, 0.0, 0.0};  // column tiles 0-7 and 8-15
 #pragma unroll
     for (int s = 0; s < kReStages - 1; ++s) {
         if (s < nk) issue(s);
@@ -573,29 +573,38 @@ __global__ void __launch_bounds__(256, 1) resid_kernel(ReArgs a) {
         cp_async_commit();
         const double* sa = re_sm + (kc % kReStages) * kReStage;
         const double* sx = sa + kReRows * kReAS;
+        const double* ra = sa + (16 * mt + gq) * kReAS + tq;
+        const double* xb = sx + tq * kReXS + gq;
 #pragma unroll
-        for (int kk = 0; kk < kReK / kReSplit; ++kk) {
-            const int k = ks * (kReK / kReSplit) + kk;
-            double av[4];
-#pragma unroll
-            for (int i = 0; i < 4; ++i) av[i] = sa[(rg + 16 * i) * kReAS + k];
-            const double2 x01 = *reinterpret_cast<const double2*>(sx + k * kReRhs + 4 * q);
-            const double2 x23 = *reinterpret_cast<const double2*>(sx + k * kReRhs + 4 * q + 2);
-            const double xv[4] = {x01.x, x01.y, x23.x, x23.y};
-#pragma unroll
-            for (int i = 0; i < 4; ++i)
-#pragma unroll
-                for (int j = 0; j < 4; ++j) acc[i][j] = fma(av[i], xv[j], acc[i][j]);
+        for (int kk = 0; kk < kReK / kReSplit; kk += 4) {
+            const int k = kh * (kReK / kReSplit) + kk;
+            const double a0 = ra[k], a1 = ra[8 * kReAS + k];
+            const double b0 = xb[k * kReXS], b1 = xb[k * kReXS + 8];
+            asm volatile(
+                "mma.sync.aligned.m16n8k4.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5}, {%6}, {%0,%1,%2,%3};\n"
+                : "+d"(d0[0]), "+d"(d0[1]), "+d"(d0[2]), "+d"(d0[3])
+                : "d"(a0), "d"(a1), "d"(b0));
+            asm volatile(
+                "mma.sync.aligned.m16n8k4.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5}, {%6}, {%0,%1,%2,%3};\n"
+                : "+d"(d1[0]), "+d"(d1[1]), "+d"(d1[2]), "+d"(d1[3])
+                : "d"(a0), "d"(a1), "d"(b1));
         }
     }
     cp_async_wait<0>();
-    // reduce the K slices through shared memory
+    // reduce the K halves through shared memory
     __syncthreads();
     double* red = re_sm;  // [kReSplit][kReRows][kReRhs]
-#pragma unroll
-    for (int i = 0; i < 4; ++i)
-#pragma unroll
-        for (int j = 0; j < 4; ++j) red[(ks * kReRows + rg + 16 * i) * kReRhs + 4 * q + j] = acc[i][j];
+    {
+        double* ra = red + (kh * kReRows + 16 * mt + gq) * kReRhs + 2 * tq;
+        ra[0] = d0[0];
+        ra[1] = d0[1];
+        ra[8 * kReRhs] = d0[2];
+        ra[8 * kReRhs + 1] = d0[3];
+        ra[8] = d1[0];
+        ra[9] = d1[1];
+        ra[8 * kReRhs + 8] = d1[2];
+        ra[8 * kReRhs + 9] = d1[3];
+    }
     __syncthreads();
 #pragma unroll
     for (int o = 0; o < 4; ++o) {
