@@ -7,13 +7,14 @@
 // fixed number of times in FP64 around an FP64 factorisation); the result is judged against the
 // FP64 oracle through its backward error.
 //
-// One refinement step is three kinds of launch, captured once and replayed:
-//   * trsv_block_kernel, once per 128-row block and sweep: the block's diagonal CTAs (four
-//     right-hand sides each) apply the previous block's contribution and multiply by the
-//     precomputed inverse of the diagonal block; the other CTAs apply the previous block's
-//     contribution to every later row.  The backward sweep also adds d to the FP64 solution;
-//   * resid_kernel: r = b - A x in FP64 (64 rows x 16 right-hand sides per CTA), which also writes
-//     P r in FP32 for the next step and the column maxima of |r|, |x| and |b| for the test
+// One refinement step is a handful of launches, captured once and replayed:
+//   * trsv_sweep_kernel, one persistent cooperative launch per triangular sweep (forward with L,
+//     backward with U): a CTA per (128-row block, 8 right-hand sides) folds in the earlier blocks
+//     as they are published and multiplies by the precomputed inverse and coupling blocks; the
+//     backward sweep also adds d to the FP64 solution.  trsv_block_kernel (one launch per block)
+//     replaces it when the sweep's CTAs cannot all be resident;
+//   * resid_kernel: r = b - A x in FP64 on DMMA (64 rows x 16 right-hand sides per CTA), which also
+//     writes P r in FP32 for the next step and the column maxima of |r|, |x| and |b| for the test
 //     eta = max_c ||r_c||inf / (||A||inf ||x_c||inf + ||b_c||inf).
 #include <cmath>
 #include <vector>
