@@ -48,7 +48,7 @@ def parse():
                    help="solve: the headline (default); gemm / ozaki: m=n=k=8192 FP64 product with the "
                         "g*2^e distribution; batched: 20,000 uneven systems; adjoint: n=4096 gradient step")
     p.add_argument("--mode", type=int, default=0, help="batched: 0 plain FP64, 1 FP32 + FP64 refinement")
-    p.add_argument("--cpu-n", type=int, default=4096, help="order of the CPU-baseline sample")
+    p.add_argument("--cpu-runs", type=int, default=3, help="solves in the CPU-baseline sample (median)")
     return p.parse_args()
 
 
@@ -140,51 +140,79 @@ def max_over_ranks(world, value: float) -> float:
 
 
 # ----------------------------------------------------------------------------- CPU baseline (oracle)
-def cpu_baseline(n: int, nrhs: int, seconds: float = 10.0, reps_max: int = 50) -> dict:
-    """The reference's threaded solve (ThrMatrixLinEQSolve, LinAlgLU.pas:986-1128) restated in C++,
-    on all host cores, on an n x n Gaussian system with nrhs right-hand sides."""
-    import numpy as np
+def headline_system_host(n: int, kappa: float, nrhs: int, seed: int):
+    """The headline system A = U diag(s) V^T and its right-hand sides as host numpy arrays.  Input
+    generation only (torch QR, on the GPU when there is one); it loads nothing of libb2m."""
+    import torch
 
+    from mrmath_b200 import inputs  # numpy / torch only
+    dev = "cuda" if torch.cuda.is_available() else "cpu"
+    A, B = inputs.c2_kappa(n, kappa, nrhs, seed=seed, device=dev)
+    a, b = A.cpu().numpy(), B.cpu().numpy()
+    del A, B
+    if dev == "cuda":
+        torch.cuda.empty_cache()
+    return a, b
+
+
+def cpu_solves(a, b, runs: int, warmup: int):
+    """The reference's threaded solve (ThrMatrixLinEQSolve, LinAlgLU.pas:986-1128) restated in C++
+    (the oracle), on every host core: `warmup` untimed then `runs` timed solves of a x = b."""
     import oracle
-    from mrmath_b200 import inputs
     oracle.set_num_threads(os.cpu_count() or 1)
-    r = inputs.rng(15)
-    a = r.standard_normal((n, n))
-    b = r.standard_normal((n, nrhs))
-    fl = inputs.lu_solve_flops(n, nrhs)
-    times = []
-    t_end = time.perf_counter() + seconds
-    while len(times) < reps_max and (not times or time.perf_counter() < t_end):
+    times, x, rc = [], None, 0
+    for i in range(warmup + runs):
         t0 = time.perf_counter()
         rc, x = oracle.thr_lineq_solve(a, b)
-        times.append(time.perf_counter() - t0)
-    best = min(times)
-    return {"value": fl / best / 1e9, "unit": "GFLOP/s", "cores": oracle.num_threads(), "kind": "port",
-            "sample": f"oracle ThrMatrixLinEQSolve restatement, n={n}, {nrhs} RHS, best of {len(times)} runs "
-                      f"({sum(times):.1f} s of CPU work); rate at this order stands in for n=8192",
-            "backward_error": float(oracle.backward_error(a, x, b))}
+        dt = time.perf_counter() - t0
+        if i >= warmup:
+            times.append(dt)
+    return times, x, rc
+
+
+def cpu_baseline(a, b, runs: int = 3) -> dict:
+    """Bounded sample of the headline workload on the host cores: `runs` solves of the same
+    n = 8192 system (about 10 s each on 16 cores), median rate."""
+    import oracle
+    from mrmath_b200 import inputs
+    n, k = a.shape[0], b.shape[1]
+    times, x, rc = cpu_solves(a, b, runs, 0)
+    med = statistics.median(times)
+    return {"value": inputs.lu_solve_flops(n, k) / med / 1e9, "unit": "GFLOP/s", "cores": oracle.num_threads(),
+            "kind": "port",
+            "sample": f"oracle ThrMatrixLinEQSolve restatement on the benchmark system itself (n={n}, {k} RHS), "
+                      f"median of {len(times)} solves ({sum(times):.1f} s of CPU work)",
+            "backward_error": float(oracle.backward_error(a, x, b)), "status": rc}
 
 
 def run_reference(args, world, rank):
+    """The reference arm: the reference's own CPU algorithm (the oracle's restatement of
+    ThrMatrixLinEQSolve; the Object Pascal reference cannot be compiled in this image) on the same
+    n = 8192 system as the B200 arm, median of 5 solves after 1 warm-up.  Nothing of libb2m is loaded."""
     if rank != 0:
         return 0
-    n = min(args.cpu_n, args.n)
     import oracle  # noqa: F401  (fails loudly if the oracle is not built)
-    vals = []
-    for i in range(args.warmup + args.steps):
-        cb = cpu_baseline(n, args.nrhs, seconds=0.0, reps_max=1)
-        if i >= args.warmup:
-            vals.append(cb["value"])
-    v = statistics.median(vals)
-    fl = __import__("mrmath_b200.inputs", fromlist=["x"]).lu_solve_flops(n, args.nrhs)
+    from mrmath_b200 import inputs
+    n, k = args.n, args.nrhs
+    runs, warm = min(args.steps, 5), min(args.warmup, 1)
+    a, b = headline_system_host(n, args.kappa, k, seed=15)
+    times, x, rc = cpu_solves(a, b, runs, warm)
+    med = statistics.median(times)
+    fl = inputs.lu_solve_flops(n, k)
+    v = fl / med / 1e9
+    sample = (f"oracle ThrMatrixLinEQSolve restatement, n={n}, {k} RHS, kappa={args.kappa:g}: median of {runs} "
+              f"solves after {warm} warm-up ({sum(times):.1f} s timed)")
     line = {
         "impl": "reference", "metric": METRIC, "value": v, "unit": "GFLOP/s", "n_gpus": args.gpus,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": fl / v / 1e6, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (MT19937 seed 15, Gaussian)",
-        "config": {"workload": f"FP64 LU solve, n={n} (bounded CPU sample of n={args.n}), {args.nrhs} RHS",
-                   "n": n, "nrhs": args.nrhs, "parallelism": "host threads"},
-        "cpu_baseline": {"value": v, "unit": "GFLOP/s", "cores": cb["cores"], "kind": "port",
-                         "sample": cb["sample"]},
+        "steps": runs, "warmup": warm, "requested_steps": args.steps, "requested_warmup": args.warmup,
+        "ms_per_step": med * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic: A = U diag(s) V^T from MT19937-seeded Gaussians (seed 15), 16 Gaussian RHS",
+        "config": {"workload": f"plain FP64 LU solve, n={n}, {k} RHS, kappa={args.kappa:g}", "n": n, "nrhs": k,
+                   "kappa": args.kappa, "parallelism": "host threads"},
+        "backward_error": float(oracle.backward_error(a, x, b)), "backward_error_bound": n * 2.0 ** -53,
+        "status": rc,
+        "cpu_baseline": {"value": v, "unit": "GFLOP/s", "cores": oracle.num_threads(), "kind": "port",
+                         "sample": sample},
         "e2e": {"value": v, "unit": "GFLOP/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -344,7 +372,7 @@ def run_b200(args, world, rank, local):
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         try:
-            cpu = cpu_baseline(min(args.cpu_n, n), k, seconds=10.0)
+            cpu = cpu_baseline(A.cpu().numpy(), B.cpu().numpy(), runs=args.cpu_runs)
         except Exception as exc:  # the oracle is test infrastructure; report why it is missing
             cpu = {"value": None, "unit": "GFLOP/s", "cores": 0, "kind": "port", "sample": f"unavailable: {exc}"}
 

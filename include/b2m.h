@@ -65,6 +65,11 @@ B2M_API int32_t     b2m_use_own_stream(b2m_ctx* ctx);
  * every kernel from the host instead. */
 B2M_API int32_t     b2m_use_graphs(b2m_ctx* ctx, int32_t enable);
 B2M_API int32_t     b2m_synchronize(b2m_ctx* ctx);
+/* Number of polls after which a bounded wait of the mixed solve's refinement sweeps gives up
+ * (polls < 0 restores the built-in limit, about a second of spinning).  No counterpart in the
+ * reference: a lower limit exists to exercise the timeout path -- with 0 polls every dependent
+ * wait gives up at once, the call returns B2M_ERR_TIMEOUT and the context stays usable. */
+B2M_API int32_t     b2m_set_wait_limit(b2m_ctx* ctx, int64_t polls);
 B2M_API const char* b2m_last_error(b2m_ctx* ctx);
 B2M_API const char* b2m_status_string(int32_t status);
 /* Number of kernels this context has launched so far (device work accounting). */
@@ -123,7 +128,9 @@ B2M_API int32_t b2m_MatrixLinEQSolve(b2m_ctx* ctx, const double* A, int64_t Line
                              int64_t LineWidthB, double* X, int64_t LineWidthX, int64_t Width2,
                              int64_t NumRefinements);
 
-/* device-resident twins (device pointers; indx / det / status are device pointers too) */
+/* device-resident twins (device pointers; indx / det / status are device pointers too).  The
+ * device result word *status (may be NULL) receives 0 (leOk), 1 (leSingular) or B2M_ERR_TIMEOUT
+ * when a bounded in-kernel wait gave up and the outputs are unfinished. */
 B2M_API int32_t b2m_dev_MatrixLUDecompInPlace(b2m_ctx* ctx, double* A, int64_t LineWidthA, int64_t width, int32_t* indx,
                                       int32_t* status);
 B2M_API int32_t b2m_dev_MatrixLUBackSubst(b2m_ctx* ctx, const double* LUDecomp, int64_t LineWidthLU, int64_t width,
@@ -148,6 +155,9 @@ typedef struct b2m_solve_report {
     int32_t fell_back;       /* 1 if the plain FP64 solve produced X */
     double  backward_error;  /* normwise backward error of the returned X (FP64 residual) */
     double  refinement_backward_error;  /* the last refinement step's, before any fallback */
+    double  forward_error;   /* normwise forward-error estimate max_j ||d_j||inf / ||x_j||inf, d the last
+                                correction applied (refinement) or one extra correction computed with
+                                the FP64 factors (fallback); an upper-side estimate of ||x - x*|| / ||x*|| */
 } b2m_solve_report;
 B2M_API int32_t b2m_MatrixLinEQSolveMixed(b2m_ctx* ctx, const double* A, int64_t LineWidthA, int64_t width,
                                           const double* B, int64_t LineWidthB, double* X, int64_t LineWidthX,
@@ -198,8 +208,8 @@ B2M_API int32_t b2m_batch_tune_read(b2m_ctx* ctx, int32_t* small_n, int32_t* gro
                                     int32_t* pw_small, float* ms);
 
 /* Allocation-free solve.  No counterpart in the reference: it exists for callers that may not
- * allocate device memory (a host program whose memory manager owns all device allocations, code
- * running inside a stream capture, a real-time loop with a fixed budget).  Same arguments and
+ * allocate device memory (a host program whose memory manager owns all device allocations and
+ * forbids any other cudaMalloc, a real-time loop with a fixed memory budget).  Same arguments and
  * result as b2m_dev_MatrixLinEQSolve without refinement, on the given cudaStream_t (NULL = legacy
  * default stream) of the calling thread's current device.  All intermediates live in one static
  * device array of about 2.5 MiB that every GPU loading the library holds until exit; orders up to
@@ -207,7 +217,9 @@ B2M_API int32_t b2m_batch_tune_read(b2m_ctx* ctx, int32_t* small_n, int32_t* gro
  * first call on a device looks up the array's address (cudaGetSymbolAddress), so make that first
  * call before any stream capture.  Every call shares the array and it keeps the last call's
  * contents: calls that overlap on the GPU (other streams, other host threads) race.  *status
- * (device int32, may be NULL) receives 0 (leOk) or 1 (leSingular). */
+ * (device int32, may be NULL) receives 0 (leOk), 1 (leSingular) or B2M_ERR_TIMEOUT when a bounded
+ * wait in the factorisation gave up (X is then unfinished).  The array's address is looked up once
+ * per device ordinal and kept: do not use this entry point across a cudaDeviceReset. */
 B2M_API int32_t b2m_dev_MatrixLinEQSolveNoAlloc(void* stream, const double* A, int64_t LineWidthA, int64_t width,
                                                 const double* B, int64_t LineWidthB, double* X, int64_t LineWidthX,
                                                 int64_t Width2, int32_t* status);

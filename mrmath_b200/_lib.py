@@ -23,7 +23,7 @@ MIXED_TF32, MIXED_3XTF32 = 1, 3
 class SolveReport(C.Structure):
     """b2m_solve_report"""
     _fields_ = [("iterations", C.c_int32), ("fell_back", C.c_int32), ("backward_error", C.c_double),
-                ("refinement_backward_error", C.c_double)]
+                ("refinement_backward_error", C.c_double), ("forward_error", C.c_double)]
 
 # name -> (restype, argtypes); pointers are passed as integers (c_void_p) so that numpy
 # arrays (host) and torch tensors (device) use the same signatures.
@@ -34,6 +34,7 @@ SIGNATURES: dict[str, tuple] = {
     "b2m_use_own_stream": (i32, [vp]),
     "b2m_use_graphs": (i32, [vp, i32]),
     "b2m_synchronize": (i32, [vp]),
+    "b2m_set_wait_limit": (i32, [vp, i64]),
     "b2m_last_error": (C.c_char_p, [vp]),
     "b2m_status_string": (C.c_char_p, [i32]),
     "b2m_kernel_launches": (i64, [vp]),
@@ -129,6 +130,10 @@ class Context:
 
     def synchronize(self) -> None:
         self.check(lib.b2m_synchronize(self.h))
+
+    def set_wait_limit(self, polls: int) -> None:
+        """Poll limit of the refinement sweeps' bounded waits (< 0: the built-in limit)."""
+        self.check(lib.b2m_set_wait_limit(self.h, polls))
 
     def kernel_launches(self) -> int:
         return lib.b2m_kernel_launches(self.h)

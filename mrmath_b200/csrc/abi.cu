@@ -358,8 +358,7 @@ extern "C" int32_t b2m_dev_MatrixLUDecompInPlace(b2m_ctx* h, double* A, int64_t 
     B2M_TRY(reset_status(ctx));
     B2M_TRY(lu_factor_f64(ctx, ctx->stream, dA, ld, n, indx, (int32_t*)pp + n));
     if (!direct) B2M_TRY(copy_matrix(ctx, ctx->stream, A, LineWidthA, dA, ld * 8, n, n));
-    if (status)
-        B2M_CU(ctx, cudaMemcpyAsync(status, ctx->d_status + kInfo, 4, cudaMemcpyDeviceToDevice, ctx->stream));
+    if (status) B2M_TRY(publish_status(ctx, ctx->stream, ctx->d_status, status));
     return B2M_OK;
 }
 
@@ -434,8 +433,7 @@ extern "C" int32_t b2m_dev_MatrixLinEQSolve(b2m_ctx* h, const double* A, int64_t
     B2M_TRY(solve_device(ctx, (double*)pa, ld, n, Ao, ldAo, (double*)pb, ldb, (double*)px, ldb, Width2,
                          NumRefinements, dpiv, dpiv + n));
     B2M_TRY(copy_matrix(ctx, ctx->stream, X, LineWidthX, (double*)px, ldb * 8, n, Width2));
-    if (status)
-        B2M_CU(ctx, cudaMemcpyAsync(status, ctx->d_status + kInfo, 4, cudaMemcpyDeviceToDevice, ctx->stream));
+    if (status) B2M_TRY(publish_status(ctx, ctx->stream, ctx->d_status, status));
     return B2M_OK;
 }
 
@@ -462,8 +460,7 @@ extern "C" int32_t b2m_dev_MatrixInverseInPlace(b2m_ctx* h, double* A, int64_t L
     B2M_TRY(lu_solve_f64(ctx, ctx->stream, dLU, ld, n, dpiv + n, X, ld, n));
     // the inverse replaces A only when the factorisation succeeded
     B2M_TRY(copy_if_ok(ctx, ctx->stream, A, LineWidthA / 8, X, ld, n, n));
-    if (status)
-        B2M_CU(ctx, cudaMemcpyAsync(status, ctx->d_status + kInfo, 4, cudaMemcpyDeviceToDevice, ctx->stream));
+    if (status) B2M_TRY(publish_status(ctx, ctx->stream, ctx->d_status, status));
     return B2M_OK;
 }
 
@@ -498,6 +495,7 @@ int32_t mixed_common(Ctx* ctx, const double* A, int64_t lda, int64_t n, const do
         report->fell_back = rep.fell_back;
         report->backward_error = rep.backward_error;
         report->refinement_backward_error = rep.ir_backward_error;
+        report->forward_error = rep.forward_error;
     }
     return st;
 }

@@ -5,6 +5,7 @@
 #include <cuda.h>
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <cstdint>
 #include <cstdio>
 #include <functional>
@@ -79,6 +80,7 @@ struct Ctx {
     int device = 0;
     int num_sms = 148;
     int sweep_ctas = -1;  // co-resident CTAs of the persistent refinement sweep (-1: not queried yet)
+    int64_t wait_limit = -1;  // polls of the refinement sweeps' bounded waits (-1: the built-in limit)
     size_t smem_optin = 0;
     cudaStream_t own_stream = nullptr;
     cudaStream_t stream = nullptr;
@@ -140,6 +142,12 @@ void prof_end(Ctx* ctx, cudaStream_t st, int cls, double work);
 // default stream cannot be captured, so the graph then runs on the context's own stream, joined
 // to `st` with events both ways.  Falls back to eager launches while profiling.
 int32_t run_graph(Ctx* ctx, cudaStream_t st, const GraphKey& key, const std::function<int32_t(cudaStream_t)>& issue);
+
+// Per-device flag for one-time launch set-up (cudaFuncSetAttribute applies to the current device
+// only, and a process may drive several devices).  `key` is the kernel's address, `tag` tells apart
+// several flags of one kernel (e.g. a cluster size).  The returned atomic starts at 0 and lives until
+// exit; setting an attribute twice is harmless, so callers test, set the attributes, then store 1.
+std::atomic<int>& device_flag(const void* key, int tag, int device);
 
 // grows workspace slot `slot` to at least `bytes` (never shrinks); 256-byte aligned
 int32_t ws_get(Ctx* ctx, int slot, size_t bytes, void** out);

@@ -18,6 +18,13 @@ int32_t fail(Ctx* ctx, int32_t status, const char* fmt, ...) {
     return status;
 }
 
+std::atomic<int>& device_flag(const void* key, int tag, int device) {
+    static std::mutex m;
+    static std::map<std::tuple<const void*, int, int>, std::atomic<int>> flags;  // nodes never move
+    std::lock_guard<std::mutex> lk(m);
+    return flags[std::make_tuple(key, tag, device)];
+}
+
 int32_t ws_get(Ctx* ctx, int slot, size_t bytes, void** out) {
     bytes = (size_t)round_up((int64_t)std::max<size_t>(bytes, 256), 256);
     if (ctx->ws_bytes[slot] < bytes) {
@@ -290,6 +297,21 @@ extern "C" int32_t b2m_use_graphs(b2m_ctx* h, int32_t enable) {
     Ctx* ctx = reinterpret_cast<Ctx*>(h);
     if (!ctx) return B2M_ERR_ARG;
     ctx->use_graphs = enable != 0;
+    return B2M_OK;
+}
+
+extern "C" int32_t b2m_set_wait_limit(b2m_ctx* h, int64_t polls) {
+    Ctx* ctx = reinterpret_cast<Ctx*>(h);
+    if (!ctx) return B2M_ERR_ARG;
+    std::lock_guard<std::mutex> lk(ctx->mtx);
+    if (polls > 0xFFFFFFFFll) return b2m::fail(ctx, B2M_ERR_ARG, "wait limit above 2^32 - 1 polls");
+    cudaSetDevice(ctx->device);
+    // the limit is a kernel argument, so captured graphs that hold the old one are dropped
+    B2M_CU(ctx, cudaStreamSynchronize(ctx->stream));
+    if (ctx->own_stream) B2M_CU(ctx, cudaStreamSynchronize(ctx->own_stream));
+    for (auto& g : ctx->graphs) cudaGraphExecDestroy(g.second.exec);
+    ctx->graphs.clear();
+    ctx->wait_limit = polls < 0 ? -1 : polls;
     return B2M_OK;
 }
 

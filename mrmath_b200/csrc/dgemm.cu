@@ -186,11 +186,11 @@ __global__ void __launch_bounds__(kThreads, 1)
 
 template <bool AK, bool BKM>
 int32_t launch_variant(Ctx* ctx, cudaStream_t st, const CUtensorMap& ta, const CUtensorMap& tb, const DgemmArgs& a) {
-    static bool attr_set = false;
-    if (!attr_set) {
+    std::atomic<int>& attr_set = device_flag((const void*)dgemm_tma_kernel<AK, BKM>, 0, ctx->device);
+    if (!attr_set.load()) {
         B2M_CU(ctx, cudaFuncSetAttribute(dgemm_tma_kernel<AK, BKM>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          kSmemBytes));
-        attr_set = true;
+        attr_set.store(1);
     }
     const int tiles = (int)(ceil_div(a.M, BM) * ceil_div(a.N, BN));
     prof_begin(ctx, st, kClsGemm);

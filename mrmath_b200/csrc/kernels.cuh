@@ -73,6 +73,9 @@ namespace b2m {
 // X += R elementwise (rows x cols, strides in elements)
 int32_t axpy_matrix(Ctx* ctx, cudaStream_t st, double* X, int64_t ldx, const double* R, int64_t ldr, int64_t rows,
                     int64_t cols);
+// *out = B2M_ERR_TIMEOUT if words[kTimeout] != 0, else words[kInfo] (0 leOk, 1 leSingular): the
+// result word of the asynchronous device-pointer entry points
+int32_t publish_status(Ctx* ctx, cudaStream_t st, const int32_t* words, int32_t* out);
 // X[i][i] = v for i < n
 int32_t set_diagonal(Ctx* ctx, cudaStream_t st, double* X, int64_t ldx, int64_t n, double v);
 // dst = src when status[kInfo] == 0 (strides in elements)
@@ -119,6 +122,7 @@ struct MixedReport {
     int32_t fell_back;
     double backward_error;
     double ir_backward_error;
+    double forward_error;  // estimate: last correction over the solution, normwise (inf-norms)
 };
 // FP32 factorisation of the mixed solve (lu_f32.cu): tournament-pivoting panels, tcgen05
 // trailing updates (mode 1 TF32, 3 3xTF32), and the inverses of the kTrsvNB-row diagonal blocks

@@ -444,6 +444,16 @@ __global__ void copy_if_ok_kernel(double* dst, int64_t ldd, const double* src, i
     dst[i * ldd + c] = src[i * lds + c];
 }
 
+__global__ void publish_status_kernel(const int32_t* words, int32_t* out) {
+    *out = words[kTimeout] != 0 ? B2M_ERR_TIMEOUT : words[kInfo];
+}
+
+int32_t publish_status(Ctx* ctx, cudaStream_t st, const int32_t* words, int32_t* out) {
+    publish_status_kernel<<<1, 1, 0, st>>>(words, out);
+    B2M_LAUNCHED(ctx);
+    return B2M_OK;
+}
+
 int32_t axpy_matrix(Ctx* ctx, cudaStream_t st, double* X, int64_t ldx, const double* R, int64_t ldr, int64_t rows,
                     int64_t cols) {
     if (rows <= 0 || cols <= 0) return B2M_OK;

@@ -801,10 +801,10 @@ int32_t lu_factor_f32(Ctx* ctx, cudaStream_t st, float* A, int64_t ld, int64_t n
     if ((ld & 31) || (reinterpret_cast<uintptr_t>(A) & 127))
         return fail(ctx, B2M_ERR_DIM, "lu_factor_f32: ld must be a multiple of 32 floats, A 128-byte aligned");
     if (n > (int64_t)kTsMaxCand * kTsRows) return fail(ctx, B2M_ERR_UNSUPPORTED, "mixed LU: n too large");
-    static bool attr = false;
+    std::atomic<int>& attr = device_flag((const void*)lu_outer_kernel, 0, ctx->device);
     const int ou_smem = (kNB * 33 + (kNB + 32) * 36) * sizeof(float);
     const int di_smem = 2 * kTrsvNB * (kTrsvNB + 1) * sizeof(float);
-    if (!attr) {
+    if (!attr.load()) {
         B2M_CU(ctx, cudaFuncSetAttribute(lu_outer_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, ou_smem));
         B2M_CU(ctx, cudaFuncSetAttribute(diag_inv_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, di_smem));
         B2M_CU(ctx, cudaFuncSetAttribute(coupling_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kCpSmem));
@@ -814,7 +814,7 @@ int32_t lu_factor_f32(Ctx* ctx, cudaStream_t st, float* A, int64_t ld, int64_t n
                               (const void*)panel_permute_kernel, (const void*)lu_outer_kernel})
             B2M_CU(ctx, cudaFuncSetAttribute(f, cudaFuncAttributePreferredSharedMemoryCarveout,
                                              (int)cudaSharedmemCarveoutMaxShared));
-        attr = true;
+        attr.store(1);
     }
     if (!ctx->side_stream) {
         int least = 0, greatest = 0;

@@ -67,6 +67,14 @@ __global__ void colmax3_kernel(const double* R, int64_t ldr, const double* X, in
     atomic_max_abs(&out[2 * k + c], B[i * ldb + c]);
 }
 
+// column-wise max |r| of R (n x k) into out[0..k) (bit patterns)
+__global__ void colmax_kernel(const double* R, int64_t ldr, int64_t n, int64_t k, unsigned long long* out) {
+    const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= n * k) return;
+    const int64_t i = e / k, c = e - i * k;
+    atomic_max_abs(&out[c], R[i * ldr + c]);
+}
+
 __global__ void f64_to_f32_kernel(const double* src, int64_t lds, float* dst, int64_t ldd, int64_t rows, int64_t cols) {
     const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (e >= rows * cols) return;
@@ -316,6 +324,7 @@ struct SwArgs {
     int upper;
     unsigned long long* ll;  // [nblk][ng][128][8] published solutions {value bits, flag}, zeroed before the launch
     int32_t* status;
+    uint32_t spin;  // polls before a wait gives up (kSwSpin unless a test lowered it)
 };
 
 __device__ __forceinline__ unsigned long long ld_relaxed64(const unsigned long long* p) {
@@ -401,21 +410,19 @@ __global__ void __launch_bounds__(256, 1) trsv_sweep_kernel(SwArgs a) {
     auto wait_and_stage = [&](int j) -> bool {
         const int k = t >> 1, q0 = (t & 1) * 4;
         const unsigned long long* src = a.ll + (size_t)(j * ng + g) * (kTrsvNB * kSwRhs) + k * kSwRhs + q0;
-        unsigned long long w[4];
-        uint32_t it = 0;
-        bool ready, bad;
-        do {
+        unsigned long long w[4] = {0ull, 0ull, 0ull, 0ull};
+        bool ready = false, bad = false;
+        for (uint32_t it = 0; it < a.spin && !ready && !bad; ++it) {
 #pragma unroll
             for (int e = 0; e < 4; ++e) w[e] = ld_relaxed64(src + e);
             ready = true;
-            bad = false;
 #pragma unroll
             for (int e = 0; e < 4; ++e) {
                 const uint32_t f = (uint32_t)(w[e] >> 32);
                 ready = ready && f == 1u;
                 bad = bad || f == kSwAbort;
             }
-        } while (!ready && !bad && ++it < kSwSpin);
+        }
         if (!ready && !bad) atomicExch(&a.status[kTimeout], 501);
         if (!ready) s_abort = 1;
         const float4 v = make_float4(__uint_as_float((uint32_t)w[0]), __uint_as_float((uint32_t)w[1]),
@@ -521,7 +528,7 @@ struct ReArgs {
     float* r32;          // P r in FP32 (row pinv[i] <- r_i)
     int64_t ldr;
     const int32_t* pinv;
-    unsigned long long* nrm;  // [0,k) |r|, [k,2k) |x|, [2k,3k) |b|
+    unsigned long long* nrm;  // [0,k) |r|, [k,2k) |x|, [2k,3k) |b|, [3k,4k) |d| (the correction just applied)
 };
 
 // r = b - A x for rows [64 blockIdx.x, +64) and columns [16 blockIdx.y, +16).  A and X stream
@@ -533,13 +540,13 @@ struct ReArgs {
 // keep both fragment loads at two shared-memory wavefronts per warp.
 __global__ void __launch_bounds__(256, 1) resid_kernel(ReArgs a) {
     extern __shared__ __align__(16) double re_sm[];
-    __shared__ unsigned long long s_n[3 * kReRhs];
+    __shared__ unsigned long long s_n[4 * kReRhs];
     const int t = threadIdx.x;
     const int r0 = blockIdx.x * kReRows, cb = blockIdx.y * kReRhs;
     const int nc = min(kReRhs, a.nrhs - cb);
     const int lane = t & 31, wp = t >> 5, mt = wp & 3, kh = wp >> 2, gq = lane >> 2, tq = lane & 3;
     const int nk = (int)ceil_div(a.n, kReK);
-    if (t < 3 * kReRhs) s_n[t] = 0ull;
+    if (t < 4 * kReRhs) s_n[t] = 0ull;
     auto issue = [&](int kc) {
         double* sa = re_sm + (kc % kReStages) * kReStage;
         double* sx = sa + kReRows * kReAS;
@@ -619,13 +626,18 @@ __global__ void __launch_bounds__(256, 1) resid_kernel(ReArgs a) {
         const double bv = a.B[(int64_t)row * a.ldb + gc];
         const double xv = a.X[(int64_t)row * a.ldx + gc];
         const double rv = bv - sum;
-        a.r32[(int64_t)a.pinv[row] * a.ldr + gc] = (float)rv;
+        // the slot still holds the correction d of the sweeps that produced X (d[pinv[row]]: every
+        // element of d is read once over the grid), which becomes the forward-error estimate
+        float* slot = &a.r32[(int64_t)a.pinv[row] * a.ldr + gc];
+        const float dv = *slot;
+        *slot = (float)rv;
+        atomicMax(&s_n[3 * kReRhs + c], (unsigned long long)__double_as_longlong(fabs((double)dv)));
         atomicMax(&s_n[c], (unsigned long long)__double_as_longlong(fabs(rv)));
         atomicMax(&s_n[kReRhs + c], (unsigned long long)__double_as_longlong(fabs(xv)));
         atomicMax(&s_n[2 * kReRhs + c], (unsigned long long)__double_as_longlong(fabs(bv)));
     }
     __syncthreads();
-    if (t < 3 * kReRhs) {
+    if (t < 4 * kReRhs) {
         const int which = t / kReRhs, c = t - which * kReRhs;
         if (c < nc) atomicMax(&a.nrm[which * a.nrhs + cb + c], s_n[t]);
     }
@@ -653,7 +665,7 @@ int32_t ir_solve(Ctx* ctx, cudaStream_t st, const float* LU, int64_t ld, int64_t
                 unsigned long long* ll = s.ll + up * (size_t)nblk * kSweepGroups * kTrsvNB * kSwRhs;
                 B2M_CU(ctx, cudaMemsetAsync(ll, 0, ll_words * sizeof(unsigned long long), st));
                 SwArgs sa{LU,  ld, (int)n, up ? s.uinv : s.linv, up ? s.wu : s.wl, Xr, ldr, (int)c0, nc, X64, ldx, up,
-                          ll, ctx->d_status};
+                          ll, ctx->d_status, ctx->wait_limit >= 0 ? (uint32_t)ctx->wait_limit : kSwSpin};
                 cudaLaunchConfig_t cfg{};
                 cudaLaunchAttribute at[1];
                 at[0].id = cudaLaunchAttributeCooperative;
@@ -706,6 +718,18 @@ double eta_from(const std::vector<unsigned long long>& h, int64_t nrhs, double n
     return eta;
 }
 
+// forward-error estimate max_c ||d_c||inf / ||x_c||inf from the column maxima [k,2k) |x| and
+// [3k,4k) |d|, d being the last correction (an upper estimate once refinement contracts)
+double fwd_from(const std::vector<unsigned long long>& h, int64_t nrhs) {
+    double f = 0.0;
+    for (int64_t c = 0; c < nrhs; ++c) {
+        const double xn = __builtin_bit_cast(double, h[nrhs + c]);
+        const double dn = __builtin_bit_cast(double, h[3 * nrhs + c]);
+        f = std::max(f, xn > 0 ? dn / xn : (dn > 0 ? INFINITY : 0.0));
+    }
+    return f;
+}
+
 }  // namespace
 
 // ------------------------------------------------------------------ the refinement driver
@@ -723,22 +747,22 @@ int32_t solve_mixed(Ctx* ctx, cudaStream_t st, const double* A, int64_t lda, int
     B2M_TRY(ws_get(ctx, kWsMatD, a32_bytes + f32_scratch_bytes(n), &pD));
     B2M_TRY(ws_get(ctx, kWsE, (size_t)(n * ldr) * sizeof(float), &pE));
     B2M_TRY(ws_get(ctx, kWsPiv, (size_t)(2 * n) * sizeof(int32_t), &pP));
-    B2M_TRY(ws_get(ctx, kWsSmall, (size_t)(4 + 3 * nrhs) * sizeof(unsigned long long), &pS));
+    B2M_TRY(ws_get(ctx, kWsSmall, (size_t)(4 + 4 * nrhs) * sizeof(unsigned long long), &pS));
     float* A32 = (float*)pD;
     const F32Scratch sc = f32_scratch_carve(static_cast<char*>(pD) + a32_bytes, n);
     float* r32 = (float*)pE;
     int32_t* perm = (int32_t*)pP;
     int32_t* pinv = perm + n;
     unsigned long long* nrm = (unsigned long long*)pS;
-    std::vector<unsigned long long> h((size_t)(1 + 3 * nrhs));
+    std::vector<unsigned long long> h((size_t)(1 + 4 * nrhs));
 
     MixedReport local{};
     if (!rep) rep = &local;
     *rep = MixedReport{};
-    static bool attr = false;
-    if (!attr) {
+    std::atomic<int>& attr = device_flag((const void*)resid_kernel, 0, ctx->device);
+    if (!attr.load()) {
         B2M_CU(ctx, cudaFuncSetAttribute(resid_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kReSmem));
-        attr = true;
+        attr.store(1);
     }
 
     B2M_CU(ctx, cudaMemsetAsync(ctx->d_status, 0, kNumStatus * sizeof(int32_t), st));
@@ -764,7 +788,7 @@ int32_t solve_mixed(Ctx* ctx, cudaStream_t st, const double* A, int64_t lda, int
         const GraphKey key{5 + mode * 10, A32, X, B, A, ld32, n, nrhs, lda * 1000003 + ldb * 1009 + ldx};
         auto step = [&](cudaStream_t q) -> int32_t {
             B2M_TRY(ir_solve(ctx, q, A32, ld32, n, sc, r32, ldr, nrhs, X, ldx));
-            B2M_CU(ctx, cudaMemsetAsync(nrm + 1, 0, 3 * nrhs * sizeof(unsigned long long), q));
+            B2M_CU(ctx, cudaMemsetAsync(nrm + 1, 0, 4 * nrhs * sizeof(unsigned long long), q));
             ReArgs ra{A, lda, X, ldx, B, ldb, (int)n, (int)nrhs, r32, ldr, pinv, nrm + 1};
             prof_begin(ctx, q, kClsOther);
             resid_kernel<<<dim3((unsigned)ceil_div(n, kReRows), (unsigned)ceil_div(nrhs, kReRhs)), 256, kReSmem, q>>>(ra);
@@ -775,14 +799,22 @@ int32_t solve_mixed(Ctx* ctx, cudaStream_t st, const double* A, int64_t lda, int
         double prev = INFINITY;
         for (int it = 0; it < max_iter; ++it) {
             B2M_TRY(run_graph(ctx, st, key, step));
-            B2M_CU(ctx, cudaMemcpyAsync(h.data() + 1, nrm + 1, 3 * nrhs * sizeof(unsigned long long),
+            B2M_CU(ctx, cudaMemcpyAsync(h.data() + 1, nrm + 1, 4 * nrhs * sizeof(unsigned long long),
+                                        cudaMemcpyDeviceToHost, st));
+            B2M_CU(ctx, cudaMemcpyAsync(ctx->h_status, ctx->d_status, kNumStatus * sizeof(int32_t),
                                         cudaMemcpyDeviceToHost, st));
             B2M_CU(ctx, cudaStreamSynchronize(st));
+            // a sweep wait that gave up leaves X unfinished: that is an error, not a stall, and the
+            // fallback below (which clears the status words) must not hide it
+            if (ctx->h_status[kTimeout])
+                return fail(ctx, B2M_ERR_TIMEOUT, "bounded wait gave up in refinement step %d (site %d)", it + 1,
+                            ctx->h_status[kTimeout]);
             std::vector<unsigned long long> hv(h.begin() + 1, h.end());
             const double eta = eta_from(hv, nrhs, normA);
             rep->iterations = it + 1;
             rep->backward_error = eta;
             rep->ir_backward_error = eta;
+            rep->forward_error = fwd_from(hv, nrhs);
             if (std::isfinite(eta) && eta <= tol) {
                 converged = true;
                 break;
@@ -804,7 +836,7 @@ int32_t solve_plain_f64(Ctx* ctx, cudaStream_t st, const double* A, int64_t lda,
     void *pC, *pP, *pS;
     B2M_TRY(ws_get(ctx, kWsMatC, (size_t)(n * ld) * sizeof(double), &pC));
     B2M_TRY(ws_get(ctx, kWsPiv, (size_t)(2 * n) * sizeof(int32_t), &pP));
-    B2M_TRY(ws_get(ctx, kWsSmall, (size_t)(4 + 3 * nrhs) * sizeof(unsigned long long), &pS));
+    B2M_TRY(ws_get(ctx, kWsSmall, (size_t)(4 + 4 * nrhs) * sizeof(unsigned long long), &pS));
     double* LU = (double*)pC;
     int32_t* ipiv = (int32_t*)pP;
     B2M_TRY(copy_matrix(ctx, st, LU, ld * 8, A, lda * 8, n, n));
@@ -827,17 +859,22 @@ int32_t solve_plain_f64(Ctx* ctx, cudaStream_t st, const double* A, int64_t lda,
         DOperand a{A, lda, n, n, 0, 0, true};
         DOperand b{X, ldx, n, nrhs, 0, 0, false};
         B2M_TRY(dgemm_tiled(ctx, st, a, b, R, ldr, n, nrhs, n, B2M_DO_SUB, false));
-        B2M_CU(ctx, cudaMemsetAsync(nrm, 0, (1 + 3 * nrhs) * sizeof(unsigned long long), st));
+        B2M_CU(ctx, cudaMemsetAsync(nrm, 0, (1 + 4 * nrhs) * sizeof(unsigned long long), st));
         norm_inf_kernel<<<gsz(n, 8), 256, 0, st>>>(A, lda, n, nrm);
         B2M_LAUNCHED(ctx);
         colmax3_kernel<<<gsz(n * nrhs), 256, 0, st>>>(R, ldr, X, ldx, B, ldb, n, nrhs, nrm + 1);
         B2M_LAUNCHED(ctx);
-        std::vector<unsigned long long> h((size_t)(1 + 3 * nrhs));
+        // forward-error estimate: one more correction d = (LU)^-1 r with the FP64 factors
+        B2M_TRY(lu_solve_f64(ctx, st, LU, ld, n, ipiv + n, R, ldr, nrhs));
+        colmax_kernel<<<gsz(n * nrhs), 256, 0, st>>>(R, ldr, n, nrhs, nrm + 1 + 3 * nrhs);
+        B2M_LAUNCHED(ctx);
+        std::vector<unsigned long long> h((size_t)(1 + 4 * nrhs));
         B2M_CU(ctx, cudaMemcpyAsync(h.data(), nrm, h.size() * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
         B2M_CU(ctx, cudaStreamSynchronize(st));
         const double normA = __builtin_bit_cast(double, h[0]);
         std::vector<unsigned long long> hv(h.begin() + 1, h.end());
         rep->backward_error = eta_from(hv, nrhs, normA);
+        rep->forward_error = fwd_from(hv, nrhs);
     }
     return B2M_OK;
 }

@@ -1,8 +1,8 @@
 // noalloc.cu -- an LU solve for callers that cannot allocate device memory.
 //
 // Some callers must not allocate: a host program whose memory manager owns every device
-// allocation, code that runs between the start and the end of a stream capture, or a real-time
-// loop with a fixed memory budget.  b2m_dev_MatrixLinEQSolveNoAlloc serves them: the caller
+// allocation and forbids any other, or a real-time loop with a fixed memory budget that may not
+// grow.  b2m_dev_MatrixLinEQSolveNoAlloc serves them: the caller
 // passes device inputs and outputs, and every intermediate (the LU factors, pivots, permutation,
 // right-hand-side buffers and status words) lives in one file-scope device array of fixed size.
 // The call makes no cudaMalloc / cudaFree and uses no context workspace.
@@ -90,7 +90,8 @@ extern "C" int32_t b2m_dev_MatrixLinEQSolveNoAlloc(void* stream, const double* A
     B2M_TRY(copy_matrix(&c, st, Xs, kNaLdx * 8, B, LineWidthB, n, k));
     B2M_TRY(lu_solve_f64(&c, st, LU, kNaLd, n, perm, Xs, kNaLdx, k, T));
     B2M_TRY(copy_matrix(&c, st, X, LineWidthX, Xs, kNaLdx * 8, n, k));
-    if (status && cudaMemcpyAsync(status, words + kInfo, sizeof(int32_t), cudaMemcpyDeviceToDevice, st) != cudaSuccess)
-        return B2M_ERR_CUDA;
+    // the caller's result word: leOk, leSingular, or B2M_ERR_TIMEOUT when a bounded wait in the panel
+    // or the GEMM gave up (X is then unfinished)
+    if (status) B2M_TRY(publish_status(&c, st, words, status));
     return B2M_OK;
 }

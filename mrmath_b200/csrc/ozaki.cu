@@ -348,10 +348,10 @@ int32_t ozaki_gemm(Ctx* ctx, cudaStream_t st, const double* A, int64_t lda, cons
     B2M_TRY(encode_tmap_2d(ctx, &mb, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, B8, (uint64_t)K, (uint64_t)s * N, (uint64_t)Kp,
                            OBK, OBN, CU_TENSOR_MAP_SWIZZLE_128B));
     constexpr int smem = kOzStages * 2 * kOzTile + 1024;
-    static bool attr = false;
-    if (!attr) {
+    std::atomic<int>& attr = device_flag((const void*)ozaki_gemm_kernel, 0, ctx->device);
+    if (!attr.load()) {
         B2M_CU(ctx, cudaFuncSetAttribute(ozaki_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-        attr = true;
+        attr.store(1);
     }
     OzArgs a{(int)M, (int)N, (int)K, s, kchunk, ea, eb, C, ldc, op, ctx->d_status};
     const int tiles = (int)(ceil_div(M, OBM) * ceil_div(N, OBN));

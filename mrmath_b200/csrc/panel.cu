@@ -28,6 +28,7 @@ namespace {
 constexpr int kPT = 256;              // threads per CTA
 constexpr int kPWarps = kPT / 32;
 constexpr int kPMaxC = 16;            // largest cluster
+constexpr int kPanelSmemMax = 200 * 1024;  // dynamic shared memory a panel CTA may use
 
 template <typename T> __device__ __forceinline__ T sing_thresh();
 template <> __device__ __forceinline__ double sing_thresh<double>() { return 10.0 / DBL_MAX; }
@@ -380,14 +381,15 @@ template <typename T, int W, int RPT>
 int32_t launch_push(Ctx* ctx, cudaStream_t st, int C, int R, T* P, int64_t ld, int m, int w, int row_base,
                     int col_base, int32_t* ipiv) {
     auto kern = panel_push_kernel<T, W, RPT>;
-    static bool attr = false;
-    static int sched[kPMaxC + 1] = {};
     const size_t smem = (size_t)W * (R | 1) * sizeof(T);
-    if (!attr) {
+    std::atomic<int>& attr = device_flag((const void*)kern, 0, ctx->device);
+    if (!attr.load()) {
         B2M_CU(ctx, cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
-        B2M_CU(ctx, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
-        attr = true;
+        B2M_CU(ctx, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, kPanelSmemMax));
+        attr.store(1);
     }
+    // whether a cluster of C CTAs fits on this device: 1 yes, -1 no, 0 not asked yet
+    std::atomic<int>& sched = device_flag((const void*)kern, 1 + C, ctx->device);
     cudaLaunchAttribute at[1];
     at[0].id = cudaLaunchAttributeClusterDimension;
     at[0].val.clusterDim.x = C;
@@ -400,12 +402,12 @@ int32_t launch_push(Ctx* ctx, cudaStream_t st, int C, int R, T* P, int64_t ld, i
     cfg.stream = st;
     cfg.attrs = at;
     cfg.numAttrs = 1;
-    if (C > 8 && sched[C] == 0) {
+    if (C > 8 && sched.load() == 0) {
         int clusters = 0;
         B2M_CU(ctx, cudaOccupancyMaxActiveClusters(&clusters, kern, &cfg));
-        sched[C] = clusters > 0 ? 1 : -1;
+        sched.store(clusters > 0 ? 1 : -1);
     }
-    if (C > 8 && sched[C] < 0)
+    if (C > 8 && sched.load() < 0)
         return fail(ctx, B2M_ERR_UNSUPPORTED, "panel cluster of %d CTAs cannot be scheduled", C);
     prof_begin(ctx, st, kClsPanel);
     B2M_CU(ctx, cudaLaunchKernelEx(&cfg, kern, P, ld, m, w, R, row_base, col_base, ipiv, ctx->d_status));

@@ -270,14 +270,14 @@ int32_t launch_tc(Ctx* ctx, cudaStream_t st, const CUtensorMap* maps, const TcAr
     constexpr int STAGES = SPLIT == 3 ? 3 : 5;
     constexpr int smem = STAGES * NOPS * kTileB + 1024;
     static_assert(STAGES * NOPS * kTileB >= (TBN / 32) * TBM * 128, "epilogue staging must fit in the stages");
-    static bool attr = false;
-    if (!attr) {
+    std::atomic<int>& attr = device_flag((const void*)sgemm_tc_kernel<SPLIT>, 0, ctx->device);
+    if (!attr.load()) {
         B2M_CU(ctx, cudaFuncSetAttribute(sgemm_tc_kernel<SPLIT>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
         // the largest carveout, so that an SM running a tile still has shared memory for the
         // (small) panel kernels of the LU that may run beside this GEMM
         B2M_CU(ctx, cudaFuncSetAttribute(sgemm_tc_kernel<SPLIT>, cudaFuncAttributePreferredSharedMemoryCarveout,
                                          (int)cudaSharedmemCarveoutMaxShared));
-        attr = true;
+        attr.store(1);
     }
     const int tiles = (int)(ceil_div(a.M, TBM) * ceil_div(a.N, TBN));
     prof_begin(ctx, st, kClsTcGemm);

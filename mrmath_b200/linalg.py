@@ -132,7 +132,7 @@ def MatrixLinEQSolve(A: np.ndarray, B: np.ndarray, num_refinements: int = 0, X: 
 
 def _rep(rep) -> dict:
     return {"iterations": rep.iterations, "fell_back": rep.fell_back, "backward_error": rep.backward_error,
-            "refinement_backward_error": rep.refinement_backward_error}
+            "refinement_backward_error": rep.refinement_backward_error, "forward_error": rep.forward_error}
 
 
 def MatrixLinEQSolveMixed(A: np.ndarray, B: np.ndarray, mode: int = MIXED_3XTF32, max_iter: int = 0,

@@ -968,20 +968,30 @@ inline void two_prod(double a, double b, double& p, double& e) {
 
 extern "C" void orc_residual_dot2(const double* A, int64_t lwA, int64_t n, const double* X, int64_t lwX,
                                   const double* B, int64_t lwB, int64_t nrhs, double* R, int64_t lwR) {
-    for (int64_t c = 0; c < nrhs; ++c) {
-        for (int64_t i = 0; i < n; ++i) {
-            const double* a = rowp(A, i, lwA);
-            double s = rowp(B, i, lwB)[c], comp = 0.0;
-            for (int64_t j = 0; j < n; ++j) {
-                double p, ep, t, et;
-                two_prod(-a[j], rowp(X, j, lwX)[c], p, ep);
-                two_sum(s, p, t, et);
-                s = t;
-                comp = comp + (et + ep);
+    // rows are independent: split them over the pool (each entry is one sequential Dot2 sum)
+    std::vector<std::function<void()>> tasks;
+    const int nt = pool()->size();
+    const int64_t per = std::max<int64_t>(1, (n + nt - 1) / nt);
+    for (int64_t i0 = 0; i0 < n; i0 += per) {
+        const int64_t i1 = std::min(n, i0 + per);
+        tasks.push_back([=] {
+            for (int64_t i = i0; i < i1; ++i) {
+                const double* a = rowp(A, i, lwA);
+                for (int64_t c = 0; c < nrhs; ++c) {
+                    double s = rowp(B, i, lwB)[c], comp = 0.0;
+                    for (int64_t j = 0; j < n; ++j) {
+                        double p, ep, t, et;
+                        two_prod(-a[j], rowp(X, j, lwX)[c], p, ep);
+                        two_sum(s, p, t, et);
+                        s = t;
+                        comp = comp + (et + ep);
+                    }
+                    rowp(R, i, lwR)[c] = s + comp;
+                }
             }
-            rowp(R, i, lwR)[c] = s + comp;
-        }
+        });
     }
+    pool()->run(tasks);
 }
 
 extern "C" double orc_backward_error(const double* A, int64_t lwA, int64_t n, const double* X, int64_t lwX,

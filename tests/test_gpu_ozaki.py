@@ -82,3 +82,5 @@ def test_ozaki_c3_8192(ctx):
     torch.cuda.synchronize()
     err_dgemm = _fwd_err(C.cpu().numpy(), a, b, rows)
     assert err < 8e-15 and err <= max(4 * err_dgemm, 2e-15), (err, err_dgemm)
+    # the native DGEMM (MatrixMult's drop-in) against the a-priori bound K u and the observed floor
+    assert err_dgemm <= 8192 * 2.0 ** -53 and err_dgemm < 8e-15, err_dgemm

@@ -1,17 +1,18 @@
-"""The allocation-free solve, b2m_dev_MatrixLinEQSolveNoAlloc, against the allocating entry point.
+"""The allocation-free solve, b2m_dev_MatrixLinEQSolveNoAlloc, against the allocating entry point
+and the oracle.
 
-It is meant for callers that may not allocate device memory -- a host program whose memory
-manager owns every device allocation, code running inside a stream capture, a real-time loop with
-a fixed budget.  Its scratch is one static device array shared by all calls, so the test makes two
-calls in a row (the second at the maximum size) to check that nothing from the first call leaks
-into the second, and compares each with b2m_dev_MatrixLinEQSolve through the C ABI.
+It serves callers that may not allocate device memory -- a host program whose memory manager owns
+every device allocation, or a real-time loop with a fixed memory budget.  Its scratch is one static
+device array shared by all calls, so the test makes two calls in a row (the second at the maximum
+size) to check that nothing from the first call leaks into the second, compares each with
+b2m_dev_MatrixLinEQSolve through the C ABI and with the oracle's MatrixLinEQSolve restatement,
+and checks that a singular system is reported through the device result word.
 This file is collected last so a run that stops at the first failure has run every other test.
 """
-import ctypes as C
-
 import numpy as np
 import pytest
 
+import oracle
 from mrmath_b200 import _lib, inputs, linalg as L
 
 pytestmark = pytest.mark.gpu
@@ -30,8 +31,8 @@ def test_noalloc_solve_matches_allocating_solve_twice(ctx):
     stream = torch.cuda.current_stream().cuda_stream
     for n, k, seed in ((300, 5, 1), (512, 64, 2)):
         r = inputs.rng(seed)
-        a = torch.from_numpy(r.random_sample((n, n)) - 0.5).cuda()
-        b = torch.from_numpy(r.standard_normal((n, k))).cuda()
+        a_np, b_np = r.random_sample((n, n)) - 0.5, r.standard_normal((n, k))
+        a, b = torch.from_numpy(a_np).cuda(), torch.from_numpy(b_np).cuda()
         x_ref = torch.empty_like(b)
         st_ref = torch.zeros(1, dtype=torch.int32, device="cuda")
         L.dev_MatrixLinEQSolve(a, b, x_ref, status=st_ref, ctx=ctx)
@@ -40,8 +41,29 @@ def test_noalloc_solve_matches_allocating_solve_twice(ctx):
         assert _noalloc(stream, a, b, x, st) == _lib.OK
         torch.cuda.synchronize()
         assert int(st.item()) == 0 and int(st_ref.item()) == 0
+        xg = x.cpu().numpy()
         xr = x_ref.cpu().numpy()
-        assert np.linalg.norm(x.cpu().numpy() - xr) <= RTOL * np.linalg.norm(xr)
+        assert np.linalg.norm(xg - xr) <= RTOL * np.linalg.norm(xr)
+        rc, xo = oracle.lineq_solve(a_np, b_np, row_quirk=False)
+        assert rc == 0 and np.linalg.norm(xg - xo) <= RTOL * np.linalg.norm(xo)
+
+
+def test_noalloc_reports_singular(ctx):
+    import torch
+    stream = torch.cuda.current_stream().cuda_stream
+    a = torch.eye(50, dtype=torch.float64, device="cuda")
+    a[:, 17] = 0.0
+    b = torch.ones(50, 2, dtype=torch.float64, device="cuda")
+    x = torch.empty_like(b)
+    st = torch.full((1,), 7, dtype=torch.int32, device="cuda")
+    assert _noalloc(stream, a, b, x, st) == _lib.OK
+    torch.cuda.synchronize()
+    assert int(st.item()) == _lib.SINGULAR
+    # the next call on the shared scratch starts clean
+    a2 = torch.eye(50, dtype=torch.float64, device="cuda") * 2.0
+    assert _noalloc(stream, a2, b, x, st) == _lib.OK
+    torch.cuda.synchronize()
+    assert int(st.item()) == 0 and torch.equal(x, b / 2.0)
 
 
 def test_noalloc_rejects_sizes_beyond_its_scratch(ctx):
