@@ -65,6 +65,31 @@ B2M_API int32_t     b2m_use_own_stream(b2m_ctx* ctx);
  * every kernel from the host instead. */
 B2M_API int32_t     b2m_use_graphs(b2m_ctx* ctx, int32_t enable);
 B2M_API int32_t     b2m_synchronize(b2m_ctx* ctx);
+/* Progress callback of the LU-based routines, the counterpart of TLinEquProgress
+ * (MatrixConst.pas:31, called with numCalc*100 div numCols at LinAlgLU.pas:272-276): `fn(percent,
+ * user)` runs on a CUDA host thread after every factored panel of the FP64 LU (every 32, 16 or 8
+ * columns), with percent = columns factored * 100 div n, in order.  It must not call CUDA or this
+ * library.  While a callback is set, factorisations run without graph replay and a call first
+ * waits for the context's previous work.  NULL removes it. */
+typedef void (*b2m_progress_fn)(int32_t percent, void* user);
+B2M_API int32_t     b2m_set_progress(b2m_ctx* ctx, b2m_progress_fn fn, void* user);
+/* ------------------------------------------------------------------ resident matrices
+ * Device-resident storage for a matrix class that keeps its data on the GPU across chained calls
+ * (Mult, SolveLinEQ, Invert ... on the b2m_dev_* entry points), so that only the first upload and
+ * the final download cross PCIe.  No counterpart in the reference, whose TDoubleMatrix owns host
+ * memory (Matrix.pas).  A sub-matrix view (SetSubMatrix, Matrix.pas:70) is a pointer into the
+ * parent, p + row * (LineWidth / 8) + col, with the parent's LineWidth: every b2m_dev_* entry point
+ * takes arbitrary byte strides.
+ *   b2m_alloc     rows x cols doubles on the context's device; *LineWidth receives the row stride
+ *                 in bytes (padded to 128 bytes).  Free with b2m_free.
+ *   b2m_upload / b2m_download  host <-> device copies of rows x cols with byte strides on both
+ *                 sides, synchronous (they wait for the context's stream). */
+B2M_API int32_t     b2m_alloc(b2m_ctx* ctx, int64_t rows, int64_t cols, double** out, int64_t* LineWidth);
+B2M_API int32_t     b2m_free(b2m_ctx* ctx, double* p);
+B2M_API int32_t     b2m_upload(b2m_ctx* ctx, double* dst, int64_t dstLineWidth, const double* src,
+                               int64_t srcLineWidth, int64_t rows, int64_t cols);
+B2M_API int32_t     b2m_download(b2m_ctx* ctx, double* dst, int64_t dstLineWidth, const double* src,
+                                 int64_t srcLineWidth, int64_t rows, int64_t cols);
 /* Number of polls after which a bounded wait of the mixed solve's refinement sweeps gives up
  * (polls < 0 restores the built-in limit, about a second of spinning).  No counterpart in the
  * reference: a lower limit exists to exercise the timeout path -- with 0 polls every dependent
@@ -109,6 +134,29 @@ B2M_API int32_t b2m_dev_MatrixMultOzaki(b2m_ctx* ctx, double* dest, int64_t dest
                                 const double* mt2, int64_t width1, int64_t height1, int64_t width2,
                                 int64_t height2, int64_t LineWidth1, int64_t LineWidth2, int32_t op, int32_t slices);
 
+/* Error report of a product.  No counterpart in the reference (MatrixMult returns only the product):
+ * `sample_rows` rows of dest (spread evenly; <= 0 means 16) are compared with op(mt1) op(mt2)
+ * computed with the compensated dot product Dot2 (Ogita, Rump, Oishi 2005; as accurate as twice
+ * the working precision).  dest must hold a B2M_DO_NONE result of b2m_MatrixMultEx (any trans) or
+ * b2m_MatrixMultOzaki (trans 0); arguments as b2m_MatrixMultEx. */
+typedef struct b2m_gemm_report {
+    int32_t rows_checked;
+    int32_t reserved;
+    double  forward_error;   /* max |C - C*| / max (|A||B|) over the sampled rows, C* the Dot2 product */
+    double  relative_error;  /* ||C - C*||_F / ||C*||_F over the sampled rows */
+    double  bound;           /* K 2^-53: the a-priori bound of an FP64 product on the forward_error scale */
+} b2m_gemm_report;
+B2M_API int32_t b2m_MatrixMultErrorReport(b2m_ctx* ctx, const double* dest, int64_t destLineWidth, const double* mt1,
+                                          const double* mt2, int64_t width1, int64_t height1, int64_t width2,
+                                          int64_t height2, int64_t LineWidth1, int64_t LineWidth2, int32_t trans,
+                                          int32_t sample_rows, b2m_gemm_report* report);
+/* device twin: dest, mt1, mt2 device memory; the report is host memory (the call synchronizes) */
+B2M_API int32_t b2m_dev_MatrixMultErrorReport(b2m_ctx* ctx, const double* dest, int64_t destLineWidth,
+                                              const double* mt1, const double* mt2, int64_t width1, int64_t height1,
+                                              int64_t width2, int64_t height2, int64_t LineWidth1,
+                                              int64_t LineWidth2, int32_t trans, int32_t sample_rows,
+                                              b2m_gemm_report* report);
+
 /* ------------------------------------------------------------------ LU (src/LinAlgLU.pas) */
 /* MatrixLUDecompInPlace LinAlgLU.pas:283-295 */
 B2M_API int32_t b2m_MatrixLUDecompInPlace(b2m_ctx* ctx, double* A, int64_t LineWidthA, int64_t width, int32_t* indx);
@@ -140,6 +188,32 @@ B2M_API int32_t b2m_dev_MatrixLinEQSolve(b2m_ctx* ctx, const double* A, int64_t 
                                  int64_t Width2, int64_t NumRefinements, int32_t* status);
 B2M_API int32_t b2m_dev_MatrixInverseInPlace(b2m_ctx* ctx, double* A, int64_t LineWidthA, int64_t width, int32_t* status);
 B2M_API int32_t b2m_dev_MatrixDeterminant(b2m_ctx* ctx, const double* A, int64_t LineWidthA, int64_t width, double* det);
+
+/* ------------------------------------------------------------------ Cholesky (src/LinAlgCholesky.pas)
+ * Results: 0 = crOk, 1 = crNoPositiveDefinite (TCholeskyResult, MatrixConst.pas:30): a diagonal
+ * element <= 0 or NaN before its square root; A is then left unchanged. */
+/* MatrixCholeskyInPlace4 LinAlgCholesky.pas:106-123 (the routine of TDoubleMatrix.Cholesky,
+ * DblMatrix.pas:967-990): A = L L^T with L in the lower triangle of A (diagonal included); the strict
+ * upper triangle is not written.  pnlSize (0 = 32) is accepted for the reference's signature; the
+ * device blocking is the library's own. */
+B2M_API int32_t b2m_MatrixCholeskyInPlace4(b2m_ctx* ctx, double* A, int64_t LineWidthA, int64_t width,
+                                           int64_t pnlSize);
+B2M_API int32_t b2m_dev_MatrixCholeskyInPlace4(b2m_ctx* ctx, double* A, int64_t LineWidthA, int64_t width,
+                                               int32_t* status);
+/* MatrixCholeskyInPlace LinAlgCholesky.pas:270-332 (Numerical-Recipes form): L strictly below the
+ * diagonal of A, its diagonal in P (element i at byte offset i * LineWidthP); A's diagonal and upper
+ * triangle are not written. */
+B2M_API int32_t b2m_MatrixCholeskyInPlace(b2m_ctx* ctx, double* A, int64_t LineWidthA, int64_t width, double* P,
+                                          int64_t LineWidthP);
+/* MatrixCholeskySolveLinEq LinAlgCholesky.pas:352-421, generalised to nrhs columns: A X = B from the
+ * factor of b2m_MatrixCholeskyInPlace (P not NULL: L below A's diagonal, diagonal in P) or of
+ * b2m_MatrixCholeskyInPlace4 (P NULL: diagonal on A's diagonal).  Only the lower triangle is read. */
+B2M_API int32_t b2m_MatrixCholeskySolveLinEq(b2m_ctx* ctx, const double* A, int64_t LineWidthA, int64_t width,
+                                             const double* P, int64_t LineWidthP, const double* B, int64_t LineWidthB,
+                                             double* X, int64_t LineWidthX, int64_t nrhs);
+B2M_API int32_t b2m_dev_MatrixCholeskySolveLinEq(b2m_ctx* ctx, const double* A, int64_t LineWidthA, int64_t width,
+                                                 const double* P, int64_t LineWidthP, const double* B,
+                                                 int64_t LineWidthB, double* X, int64_t LineWidthX, int64_t nrhs);
 
 /* ------------------------------------------------------------------ mixed-precision solve
  * No counterpart in the reference.  A X = B with an FP32 LU whose trailing and triangular-solve

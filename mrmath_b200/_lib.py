@@ -25,6 +25,12 @@ class SolveReport(C.Structure):
     _fields_ = [("iterations", C.c_int32), ("fell_back", C.c_int32), ("backward_error", C.c_double),
                 ("refinement_backward_error", C.c_double), ("forward_error", C.c_double)]
 
+class GemmReport(C.Structure):
+    """b2m_gemm_report"""
+    _fields_ = [("rows_checked", C.c_int32), ("reserved", C.c_int32), ("forward_error", C.c_double),
+                ("relative_error", C.c_double), ("bound", C.c_double)]
+
+
 # name -> (restype, argtypes); pointers are passed as integers (c_void_p) so that numpy
 # arrays (host) and torch tensors (device) use the same signatures.
 SIGNATURES: dict[str, tuple] = {
@@ -35,6 +41,11 @@ SIGNATURES: dict[str, tuple] = {
     "b2m_use_graphs": (i32, [vp, i32]),
     "b2m_synchronize": (i32, [vp]),
     "b2m_set_wait_limit": (i32, [vp, i64]),
+    "b2m_set_progress": (i32, [vp, vp, vp]),
+    "b2m_alloc": (i32, [vp, i64, i64, C.POINTER(vp), C.POINTER(i64)]),
+    "b2m_free": (i32, [vp, vp]),
+    "b2m_upload": (i32, [vp, vp, i64, vp, i64, i64, i64]),
+    "b2m_download": (i32, [vp, vp, i64, vp, i64, i64, i64]),
     "b2m_last_error": (C.c_char_p, [vp]),
     "b2m_status_string": (C.c_char_p, [i32]),
     "b2m_kernel_launches": (i64, [vp]),
@@ -42,6 +53,13 @@ SIGNATURES: dict[str, tuple] = {
     "b2m_profile_read": (i32, [vp, i32, C.POINTER(i64), C.POINTER(dbl), C.POINTER(dbl)]),
     "b2m_MatrixMultEx": (i32, [vp, vp, i64, vp, vp, i64, i64, i64, i64, i64, i64, i32, i32]),
     "b2m_dev_MatrixMultEx": (i32, [vp, vp, i64, vp, vp, i64, i64, i64, i64, i64, i64, i32, i32]),
+    "b2m_MatrixCholeskyInPlace4": (i32, [vp, vp, i64, i64, i64]),
+    "b2m_dev_MatrixCholeskyInPlace4": (i32, [vp, vp, i64, i64, vp]),
+    "b2m_MatrixCholeskyInPlace": (i32, [vp, vp, i64, i64, vp, i64]),
+    "b2m_MatrixCholeskySolveLinEq": (i32, [vp, vp, i64, i64, vp, i64, vp, i64, vp, i64, i64]),
+    "b2m_dev_MatrixCholeskySolveLinEq": (i32, [vp, vp, i64, i64, vp, i64, vp, i64, vp, i64, i64]),
+    "b2m_MatrixMultErrorReport": (i32, [vp, vp, i64, vp, vp, i64, i64, i64, i64, i64, i64, i32, i32, vp]),
+    "b2m_dev_MatrixMultErrorReport": (i32, [vp, vp, i64, vp, vp, i64, i64, i64, i64, i64, i64, i32, i32, vp]),
     "b2m_MatrixLUDecompInPlace": (i32, [vp, vp, i64, i64, vp]),
     "b2m_MatrixLUDecomp": (i32, [vp, vp, i64, vp, i64, i64, vp]),
     "b2m_MatrixLUBackSubst": (i32, [vp, vp, i64, i64, vp, vp, i64, i64]),
@@ -131,6 +149,14 @@ class Context:
     def synchronize(self) -> None:
         self.check(lib.b2m_synchronize(self.h))
 
+    PROGRESS_FN = C.CFUNCTYPE(None, C.c_int32, C.c_void_p)
+
+    def set_progress(self, fn) -> None:
+        """fn(percent) after every factored panel of the FP64 LU (TLinEquProgress); None removes it.
+        It runs on a CUDA host thread and must not call this library."""
+        self._progress = self.PROGRESS_FN(lambda pct, _user: fn(pct)) if fn is not None else None
+        self.check(lib.b2m_set_progress(self.h, C.cast(self._progress, vp) if fn is not None else None, None))
+
     def set_wait_limit(self, polls: int) -> None:
         """Poll limit of the refinement sweeps' bounded waits (< 0: the built-in limit)."""
         self.check(lib.b2m_set_wait_limit(self.h, polls))
@@ -150,6 +176,10 @@ class Context:
             self.check(lib.b2m_profile_read(self.h, i, C.byref(n), C.byref(ms), C.byref(w)))
             out[name] = {"launches": n.value, "ms": ms.value, "work": w.value}
         return out
+
+    def lib_call(self, name: str, *args) -> int:
+        """Raw status of a context entry point (no check)."""
+        return getattr(lib, name)(self.h, *args)
 
     def call(self, name: str, *args, allow=(OK,)) -> int:
         return self.check(getattr(lib, name)(self.h, *args), allow=allow)

@@ -766,3 +766,207 @@ extern "C" int32_t b2m_MatrixMultOzaki(b2m_ctx* h, double* dest, int64_t destLin
     B2M_TRY(download(ctx, dest, destLineWidth, (double*)pc, ldb, M, N));
     return finish(ctx);
 }
+
+// ======================================================================================= GEMM error report
+namespace {
+
+int32_t fill_gemm_report(Ctx* ctx, int32_t trans, const MultShape& s, const double* C, int64_t ldc, const double* A,
+                         int64_t lda, const double* B, int64_t ldb, int32_t rows, b2m_gemm_report* rep) {
+    double acc[4];
+    const int nrows = (int)std::min<int64_t>(rows <= 0 ? 16 : rows, s.M);
+    B2M_TRY(gemm_error_report(ctx, ctx->stream, C, ldc, A, lda, trans != 1, B, ldb, trans != 2, s.M, s.N, s.K, nrows,
+                              acc));
+    rep->rows_checked = nrows;
+    rep->reserved = 0;
+    rep->forward_error = acc[1] > 0 ? acc[0] / acc[1] : acc[0];
+    rep->relative_error = acc[3] > 0 ? std::sqrt(acc[2] / acc[3]) : std::sqrt(acc[2]);
+    rep->bound = (double)s.K * std::ldexp(1.0, -53);
+    return B2M_OK;
+}
+
+}  // namespace
+
+extern "C" int32_t b2m_dev_MatrixMultErrorReport(b2m_ctx* h, const double* dest, int64_t destLineWidth,
+                                                 const double* mt1, const double* mt2, int64_t width1,
+                                                 int64_t height1, int64_t width2, int64_t height2, int64_t LineWidth1,
+                                                 int64_t LineWidth2, int32_t trans, int32_t sample_rows,
+                                                 b2m_gemm_report* report) {
+    Ctx* ctx = as_ctx(h);
+    if (!ctx) return B2M_ERR_ARG;
+    std::lock_guard<std::mutex> lk(ctx->mtx);
+    if (!dest || !mt1 || !mt2 || !report) return fail(ctx, B2M_ERR_ARG, "null pointer");
+    MultShape s;
+    B2M_TRY(mult_shape(ctx, trans, width1, height1, width2, height2, &s));
+    if (!lw_ok(LineWidth1, width1) || !lw_ok(LineWidth2, width2) || !lw_ok(destLineWidth, s.N))
+        return fail(ctx, B2M_ERR_DIM, "Line widths do not match");
+    *report = b2m_gemm_report{};
+    if (s.M == 0 || s.N == 0) return B2M_OK;
+    cudaSetDevice(ctx->device);
+    return fill_gemm_report(ctx, trans, s, dest, destLineWidth / 8, mt1, LineWidth1 / 8, mt2, LineWidth2 / 8,
+                            sample_rows, report);
+}
+
+extern "C" int32_t b2m_MatrixMultErrorReport(b2m_ctx* h, const double* dest, int64_t destLineWidth, const double* mt1,
+                                             const double* mt2, int64_t width1, int64_t height1, int64_t width2,
+                                             int64_t height2, int64_t LineWidth1, int64_t LineWidth2, int32_t trans,
+                                             int32_t sample_rows, b2m_gemm_report* report) {
+    Ctx* ctx = as_ctx(h);
+    if (!ctx) return B2M_ERR_ARG;
+    std::lock_guard<std::mutex> lk(ctx->mtx);
+    if (!dest || !mt1 || !mt2 || !report) return fail(ctx, B2M_ERR_ARG, "null pointer");
+    MultShape s;
+    B2M_TRY(mult_shape(ctx, trans, width1, height1, width2, height2, &s));
+    if (!lw_ok(LineWidth1, width1) || !lw_ok(LineWidth2, width2) || !lw_ok(destLineWidth, s.N))
+        return fail(ctx, B2M_ERR_DIM, "Line widths do not match");
+    *report = b2m_gemm_report{};
+    if (s.M == 0 || s.N == 0) return B2M_OK;
+    cudaSetDevice(ctx->device);
+    const int64_t lda = padded_ld(width1), ldb = padded_ld(width2), ldc = padded_ld(s.N);
+    void *pa, *pb, *pc;
+    B2M_TRY(ws_get(ctx, kWsMatA, (size_t)(std::max<int64_t>(height1, 1) * lda * 8), &pa));
+    B2M_TRY(ws_get(ctx, kWsMatB, (size_t)(std::max<int64_t>(height2, 1) * ldb * 8), &pb));
+    B2M_TRY(ws_get(ctx, kWsMatC, (size_t)(s.M * ldc * 8), &pc));
+    B2M_TRY(upload(ctx, (double*)pa, lda, mt1, LineWidth1, height1, width1));
+    B2M_TRY(upload(ctx, (double*)pb, ldb, mt2, LineWidth2, height2, width2));
+    B2M_TRY(upload(ctx, (double*)pc, ldc, dest, destLineWidth, s.M, s.N));
+    return fill_gemm_report(ctx, trans, s, (double*)pc, ldc, (double*)pa, lda, (double*)pb, ldb, sample_rows, report);
+}
+
+// ======================================================================================= Cholesky
+extern "C" int32_t b2m_MatrixCholeskyInPlace4(b2m_ctx* h, double* A, int64_t LineWidthA, int64_t width,
+                                              int64_t pnlSize) {
+    Ctx* ctx = as_ctx(h);
+    if (!ctx) return B2M_ERR_ARG;
+    std::lock_guard<std::mutex> lk(ctx->mtx);
+    if (!A) return fail(ctx, B2M_ERR_ARG, "null pointer");
+    if (width <= 0 || !lw_ok(LineWidthA, width) || pnlSize < 0) return fail(ctx, B2M_ERR_DIM, "Dimension error");
+    cudaSetDevice(ctx->device);
+    const int64_t ld = padded_ld(width);
+    void *po, *pf;
+    B2M_TRY(ws_get(ctx, kWsMatA, (size_t)(width * ld * 8), &po));
+    B2M_TRY(ws_get(ctx, kWsMatC, (size_t)(width * ld * 8), &pf));
+    double *orig = (double*)po, *F = (double*)pf;
+    B2M_TRY(upload(ctx, orig, ld, A, LineWidthA, width, width));
+    B2M_TRY(reset_status(ctx));
+    B2M_TRY(copy_matrix(ctx, ctx->stream, F, ld * 8, orig, ld * 8, width, width));
+    B2M_TRY(chol_factor_f64(ctx, ctx->stream, F, ld, width));
+    // the caller's strict upper triangle comes back unchanged, as MatrixCholeskyInPlace4 leaves it
+    B2M_TRY(copy_lower(ctx, ctx->stream, orig, ld, F, ld, width, true));
+    B2M_TRY(download(ctx, A, LineWidthA, orig, ld, width, width));
+    return finish(ctx);
+}
+
+extern "C" int32_t b2m_dev_MatrixCholeskyInPlace4(b2m_ctx* h, double* A, int64_t LineWidthA, int64_t width,
+                                                  int32_t* status) {
+    Ctx* ctx = as_ctx(h);
+    if (!ctx) return B2M_ERR_ARG;
+    std::lock_guard<std::mutex> lk(ctx->mtx);
+    if (!A) return fail(ctx, B2M_ERR_ARG, "null pointer");
+    if (width <= 0 || !lw_ok(LineWidthA, width)) return fail(ctx, B2M_ERR_DIM, "Dimension error");
+    const int64_t ld = padded_ld(width);
+    void* pf;
+    B2M_TRY(ws_get(ctx, kWsMatC, (size_t)(width * ld * 8), &pf));
+    double* F = (double*)pf;
+    B2M_TRY(reset_status(ctx));
+    B2M_TRY(copy_matrix(ctx, ctx->stream, F, ld * 8, A, LineWidthA, width, width));
+    B2M_TRY(chol_factor_f64(ctx, ctx->stream, F, ld, width));
+    B2M_TRY(copy_lower(ctx, ctx->stream, A, LineWidthA / 8, F, ld, width, true));
+    if (status) B2M_TRY(publish_status(ctx, ctx->stream, ctx->d_status, status));
+    return B2M_OK;
+}
+
+extern "C" int32_t b2m_MatrixCholeskyInPlace(b2m_ctx* h, double* A, int64_t LineWidthA, int64_t width, double* P,
+                                             int64_t LineWidthP) {
+    Ctx* ctx = as_ctx(h);
+    if (!ctx) return B2M_ERR_ARG;
+    std::lock_guard<std::mutex> lk(ctx->mtx);
+    if (!A || !P) return fail(ctx, B2M_ERR_ARG, "null pointer");
+    if (width <= 0 || !lw_ok(LineWidthA, width) || LineWidthP < 8 || (LineWidthP % 8))
+        return fail(ctx, B2M_ERR_DIM, "Dimension error");
+    cudaSetDevice(ctx->device);
+    const int64_t ld = padded_ld(width), ldp = LineWidthP / 8;
+    void *po, *pf, *pp;
+    B2M_TRY(ws_get(ctx, kWsMatA, (size_t)(width * ld * 8), &po));
+    B2M_TRY(ws_get(ctx, kWsMatC, (size_t)(width * ld * 8), &pf));
+    B2M_TRY(ws_get(ctx, kWsF, (size_t)(width * ldp * 8), &pp));
+    double *orig = (double*)po, *F = (double*)pf, *dP = (double*)pp;
+    B2M_TRY(upload(ctx, orig, ld, A, LineWidthA, width, width));
+    B2M_TRY(upload(ctx, dP, ldp, P, LineWidthP, width, 1));
+    B2M_TRY(reset_status(ctx));
+    B2M_TRY(copy_matrix(ctx, ctx->stream, F, ld * 8, orig, ld * 8, width, width));
+    B2M_TRY(chol_factor_f64(ctx, ctx->stream, F, ld, width));
+    // MatrixCholeskyInPlace (LinAlgCholesky.pas:270-332): L below the diagonal, the diagonal in P;
+    // A's diagonal and upper triangle stay as they were
+    B2M_TRY(split_nr(ctx, ctx->stream, orig, ld, dP, LineWidthP, F, ld, width));
+    B2M_TRY(download(ctx, A, LineWidthA, orig, ld, width, width));
+    B2M_TRY(download(ctx, P, LineWidthP, dP, ldp, width, 1));
+    return finish(ctx);
+}
+
+namespace {
+// A X = B with the factor in F (lower with diagonal), or in Lnr + P (NR form) when P is not null
+int32_t chol_solve_dev(Ctx* ctx, const double* A, int64_t ldA, int64_t width, const double* P, int64_t LineWidthP,
+                       double* X, int64_t ldx, int64_t nrhs) {
+    const int64_t ld = padded_ld(width);
+    void* pw;
+    B2M_TRY(ws_get(ctx, kWsMatC, (size_t)(width * ld * 8), &pw));
+    double* W = (double*)pw;
+    if (P) {
+        void* pf;
+        B2M_TRY(ws_get(ctx, kWsMatD, (size_t)(width * ld * 8), &pf));
+        B2M_TRY(join_nr(ctx, ctx->stream, (double*)pf, ld, A, ldA, P, LineWidthP, width));
+        return chol_solve_f64(ctx, ctx->stream, (double*)pf, ld, width, W, ld, X, ldx, nrhs);
+    }
+    return chol_solve_f64(ctx, ctx->stream, A, ldA, width, W, ld, X, ldx, nrhs);
+}
+}  // namespace
+
+extern "C" int32_t b2m_MatrixCholeskySolveLinEq(b2m_ctx* h, const double* A, int64_t LineWidthA, int64_t width,
+                                                const double* P, int64_t LineWidthP, const double* B,
+                                                int64_t LineWidthB, double* X, int64_t LineWidthX, int64_t nrhs) {
+    Ctx* ctx = as_ctx(h);
+    if (!ctx) return B2M_ERR_ARG;
+    std::lock_guard<std::mutex> lk(ctx->mtx);
+    if (!A || !B || !X) return fail(ctx, B2M_ERR_ARG, "null pointer");
+    if (width <= 0 || nrhs <= 0 || !lw_ok(LineWidthA, width) || !lw_ok(LineWidthB, nrhs) || !lw_ok(LineWidthX, nrhs) ||
+        (P && (LineWidthP < 8 || (LineWidthP % 8))))
+        return fail(ctx, B2M_ERR_DIM, "Dimension error");
+    cudaSetDevice(ctx->device);
+    const int64_t ld = padded_ld(width), ldx = padded_ld(nrhs), ldp = P ? LineWidthP / 8 : 1;
+    void *pa, *px, *pp = nullptr;
+    B2M_TRY(ws_get(ctx, kWsMatA, (size_t)(width * ld * 8), &pa));
+    B2M_TRY(ws_get(ctx, kWsMatB, (size_t)(width * ldx * 8), &px));
+    if (P) B2M_TRY(ws_get(ctx, kWsF, (size_t)(width * ldp * 8), &pp));
+    B2M_TRY(upload(ctx, (double*)pa, ld, A, LineWidthA, width, width));
+    B2M_TRY(upload(ctx, (double*)px, ldx, B, LineWidthB, width, nrhs));
+    if (P) B2M_TRY(upload(ctx, (double*)pp, ldp, P, LineWidthP, width, 1));
+    B2M_TRY(reset_status(ctx));
+    B2M_TRY(chol_solve_dev(ctx, (double*)pa, ld, width, (double*)pp, LineWidthP, (double*)px, ldx, nrhs));
+    B2M_TRY(download(ctx, X, LineWidthX, (double*)px, ldx, width, nrhs));
+    return finish(ctx);
+}
+
+extern "C" int32_t b2m_dev_MatrixCholeskySolveLinEq(b2m_ctx* h, const double* A, int64_t LineWidthA, int64_t width,
+                                                    const double* P, int64_t LineWidthP, const double* B,
+                                                    int64_t LineWidthB, double* X, int64_t LineWidthX, int64_t nrhs) {
+    Ctx* ctx = as_ctx(h);
+    if (!ctx) return B2M_ERR_ARG;
+    std::lock_guard<std::mutex> lk(ctx->mtx);
+    if (!A || !B || !X) return fail(ctx, B2M_ERR_ARG, "null pointer");
+    if (width <= 0 || nrhs <= 0 || !lw_ok(LineWidthA, width) || !lw_ok(LineWidthB, nrhs) || !lw_ok(LineWidthX, nrhs) ||
+        (P && (LineWidthP < 8 || (LineWidthP % 8))))
+        return fail(ctx, B2M_ERR_DIM, "Dimension error");
+    // the sweeps need an even, 16-byte aligned X; a caller X that is not gets a padded copy
+    double* Xd = X;
+    int64_t ldx = LineWidthX / 8;
+    if (!aligned16(X) || (ldx & 1)) {
+        void* p;
+        ldx = padded_ld(nrhs);
+        B2M_TRY(ws_get(ctx, kWsG, (size_t)(width * ldx * 8), &p));
+        Xd = (double*)p;
+    }
+    B2M_TRY(copy_matrix(ctx, ctx->stream, Xd, ldx * 8, B, LineWidthB, width, nrhs));
+    B2M_TRY(chol_solve_dev(ctx, A, LineWidthA / 8, width, P, LineWidthP, Xd, ldx, nrhs));
+    if (Xd != X) B2M_TRY(copy_matrix(ctx, ctx->stream, X, LineWidthX, Xd, ldx * 8, width, nrhs));
+    return B2M_OK;
+}

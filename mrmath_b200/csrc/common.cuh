@@ -12,6 +12,7 @@
 #include <map>
 #include <mutex>
 #include <tuple>
+#include <type_traits>
 #include <string>
 #include <vector>
 
@@ -76,6 +77,13 @@ struct BatchTune {
     float ms;         // measured time of the whole batch with this shape
 };
 
+// one progress report, enqueued as a host function behind the panel it reports on
+struct ProgressNote {
+    b2m_progress_fn fn;
+    void* user;
+    int32_t percent;
+};
+
 struct Ctx {
     int device = 0;
     int num_sms = 148;
@@ -101,6 +109,9 @@ struct Ctx {
     int chain_priority = 0;                               // stream priority of the panel kernels
     std::string last_error;
     std::mutex mtx;
+    b2m_progress_fn progress = nullptr;          // LU progress callback (b2m_set_progress)
+    void* progress_user = nullptr;
+    std::vector<ProgressNote> progress_notes;    // host-function payloads of the current call
     std::map<uint64_t, BatchTune> batch_tunes;  // per batch plan
     uint64_t batch_plan_sig = 0;                 // plan whose metadata is on the device now
     void* batch_plan_dev = nullptr;

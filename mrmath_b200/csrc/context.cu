@@ -90,7 +90,7 @@ void prof_end(Ctx* ctx, cudaStream_t st, int cls, double work) {
 }
 
 int32_t run_graph(Ctx* ctx, cudaStream_t st, const GraphKey& key, const std::function<int32_t(cudaStream_t)>& issue) {
-    if (!ctx->use_graphs || ctx->prof.on) return issue(st);
+    if (!ctx->use_graphs || ctx->prof.on || ctx->progress) return issue(st);
     cudaStreamCaptureStatus cs_status = cudaStreamCaptureStatusNone;
     if (st != nullptr && st != cudaStreamLegacy) {
         B2M_CU(ctx, cudaStreamIsCapturing(st, &cs_status));
@@ -312,6 +312,76 @@ extern "C" int32_t b2m_set_wait_limit(b2m_ctx* h, int64_t polls) {
     for (auto& g : ctx->graphs) cudaGraphExecDestroy(g.second.exec);
     ctx->graphs.clear();
     ctx->wait_limit = polls < 0 ? -1 : polls;
+    return B2M_OK;
+}
+
+// ------------------------------------------------------------------ resident matrices
+extern "C" int32_t b2m_alloc(b2m_ctx* h, int64_t rows, int64_t cols, double** out, int64_t* LineWidth) {
+    Ctx* ctx = reinterpret_cast<Ctx*>(h);
+    if (!ctx || !out || !LineWidth) return B2M_ERR_ARG;
+    *out = nullptr;
+    *LineWidth = 0;
+    if (rows < 0 || cols < 0) return b2m::fail(ctx, B2M_ERR_DIM, "negative dimension");
+    // rows padded to 16 doubles (128 bytes): TMA-legal strides and coalesced rows, like the
+    // library's own workspaces; at least one element so that an empty matrix has an address
+    const int64_t ld = b2m::round_up(std::max<int64_t>(cols, 1), 16);
+    cudaSetDevice(ctx->device);
+    void* p = nullptr;
+    if (cudaMalloc(&p, (size_t)(std::max<int64_t>(rows, 1) * ld * 8)) != cudaSuccess) {
+        cudaGetLastError();
+        return b2m::fail(ctx, B2M_ERR_ALLOC, "b2m_alloc: %lld x %lld doubles", (long long)rows, (long long)cols);
+    }
+    *out = static_cast<double*>(p);
+    *LineWidth = ld * 8;
+    return B2M_OK;
+}
+
+extern "C" int32_t b2m_free(b2m_ctx* h, double* p) {
+    Ctx* ctx = reinterpret_cast<Ctx*>(h);
+    if (!ctx) return B2M_ERR_ARG;
+    if (!p) return B2M_OK;
+    cudaSetDevice(ctx->device);
+    B2M_CU(ctx, cudaStreamSynchronize(ctx->stream));  // queued work may still read it
+    B2M_CU(ctx, cudaFree(p));
+    return B2M_OK;
+}
+
+extern "C" int32_t b2m_upload(b2m_ctx* h, double* dst, int64_t dstLineWidth, const double* src, int64_t srcLineWidth,
+                              int64_t rows, int64_t cols) {
+    Ctx* ctx = reinterpret_cast<Ctx*>(h);
+    if (!ctx || !dst || !src) return B2M_ERR_ARG;
+    if (rows < 0 || cols < 0 || dstLineWidth < cols * 8 || srcLineWidth < cols * 8)
+        return b2m::fail(ctx, B2M_ERR_DIM, "Line widths do not match");
+    if (rows == 0 || cols == 0) return B2M_OK;
+    std::lock_guard<std::mutex> lk(ctx->mtx);
+    cudaSetDevice(ctx->device);
+    B2M_CU(ctx, cudaMemcpy2DAsync(dst, dstLineWidth, src, srcLineWidth, cols * 8, rows, cudaMemcpyHostToDevice,
+                                  ctx->stream));
+    B2M_CU(ctx, cudaStreamSynchronize(ctx->stream));
+    return B2M_OK;
+}
+
+extern "C" int32_t b2m_download(b2m_ctx* h, double* dst, int64_t dstLineWidth, const double* src,
+                                int64_t srcLineWidth, int64_t rows, int64_t cols) {
+    Ctx* ctx = reinterpret_cast<Ctx*>(h);
+    if (!ctx || !dst || !src) return B2M_ERR_ARG;
+    if (rows < 0 || cols < 0 || dstLineWidth < cols * 8 || srcLineWidth < cols * 8)
+        return b2m::fail(ctx, B2M_ERR_DIM, "Line widths do not match");
+    if (rows == 0 || cols == 0) return B2M_OK;
+    std::lock_guard<std::mutex> lk(ctx->mtx);
+    cudaSetDevice(ctx->device);
+    B2M_CU(ctx, cudaMemcpy2DAsync(dst, dstLineWidth, src, srcLineWidth, cols * 8, rows, cudaMemcpyDeviceToHost,
+                                  ctx->stream));
+    B2M_CU(ctx, cudaStreamSynchronize(ctx->stream));
+    return B2M_OK;
+}
+
+extern "C" int32_t b2m_set_progress(b2m_ctx* h, b2m_progress_fn fn, void* user) {
+    Ctx* ctx = reinterpret_cast<Ctx*>(h);
+    if (!ctx) return B2M_ERR_ARG;
+    std::lock_guard<std::mutex> lk(ctx->mtx);
+    ctx->progress = fn;
+    ctx->progress_user = user;
     return B2M_OK;
 }
 

@@ -200,6 +200,27 @@ int32_t launch_variant(Ctx* ctx, cudaStream_t st, const CUtensorMap& ta, const C
     return B2M_OK;
 }
 
+// C op= A(:, k0:k0+kt) B(k0:k0+kt, :) for a short k range (kt < 16): the tail of a K that ends inside
+// the operands' tensor maps, where the 16-wide TMA k-tile would read other data.  One thread per
+// output, K FMAs each; these tails are narrow (the 8-column leaves of very tall factorisations).
+__global__ void dgemm_ktail_kernel(const double* A, int64_t lda, int64_t ar0, int64_t ac0, int akmajor,
+                                   const double* B, int64_t ldb, int64_t br0, int64_t bc0, int bkmajor, double* C,
+                                   int64_t ldc, int M, int N, int k0, int kt, int op, const int32_t* status,
+                                   int check_info) {
+    if (check_info && status[kInfo] != 0) return;
+    const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= (int64_t)M * N) return;
+    const int m = (int)(e / N), n = (int)(e - (int64_t)m * N);
+    double s = 0.0;
+    for (int k = k0; k < k0 + kt; ++k) {
+        const double a = akmajor ? A[(ar0 + m) * lda + ac0 + k] : A[(ar0 + k) * lda + ac0 + m];
+        const double b = bkmajor ? B[(br0 + n) * ldb + bc0 + k] : B[(br0 + k) * ldb + bc0 + n];
+        s = fma(a, b, s);
+    }
+    double* c = C + (int64_t)m * ldc + n;
+    *c = op == B2M_DO_NONE ? s : (op == B2M_DO_ADD ? *c + s : *c - s);
+}
+
 }  // namespace
 
 int32_t dgemm_tiled(Ctx* ctx, cudaStream_t st, const DOperand& A, const DOperand& B, double* C, int64_t ldc, int64_t M,
@@ -207,6 +228,28 @@ int32_t dgemm_tiled(Ctx* ctx, cudaStream_t st, const DOperand& A, const DOperand
     if (M <= 0 || N <= 0) return B2M_OK;
     if (K <= 0) {
         if (op == B2M_DO_NONE) B2M_CU(ctx, cudaMemset2DAsync(C, ldc * 8, 0, N * 8, M, st));
+        return B2M_OK;
+    }
+    // A K that is not a multiple of the 16-wide k-tile is safe only where the k range ends at the
+    // tensor maps' extent (TMA fills beyond it with zeros); elsewhere the last partial k-tile runs
+    // as a separate short-K pass after the tiled product of the first K - K % 16.
+    const int64_t a_kend = A.kmajor ? A.c0 + K : A.r0 + K, a_ext = A.kmajor ? A.cols : A.rows;
+    const int64_t b_kend = B.kmajor ? B.c0 + K : B.r0 + K, b_ext = B.kmajor ? B.cols : B.rows;
+    if ((K & 15) && (a_kend != a_ext || b_kend != b_ext)) {
+        const int64_t K16 = K & ~int64_t(15);
+        int tail_op = op;
+        if (K16 > 0) {
+            B2M_TRY(dgemm_tiled(ctx, st, A, B, C, ldc, M, N, K16, op, check_info));
+            if (op == B2M_DO_NONE) tail_op = B2M_DO_ADD;
+        }
+        const int64_t outs = M * N;
+        prof_begin(ctx, st, kClsGemm);
+        dgemm_ktail_kernel<<<(unsigned)ceil_div(outs, 256), 256, 0, st>>>(
+            static_cast<const double*>(A.base), A.ld, A.r0, A.c0, A.kmajor ? 1 : 0, static_cast<const double*>(B.base),
+            B.ld, B.r0, B.c0, B.kmajor ? 1 : 0, C, ldc, (int)M, (int)N, (int)K16, (int)(K - K16), tail_op,
+            ctx->d_status, check_info ? 1 : 0);
+        prof_end(ctx, st, kClsGemm, 2.0 * M * N * (K - K16));
+        B2M_LAUNCHED(ctx);
         return B2M_OK;
     }
     if ((A.c0 & 1) || (B.c0 & 1) || (A.ld & 1) || (B.ld & 1))

@@ -17,7 +17,8 @@ struct DOperand {
 };
 
 // C(M x N) op= A(M x K) * B(K x N) in FP64 on the DMMA path.  Tensor-map origins c0 must be
-// even and K must end on a multiple of 16 unless the map's extent ends exactly at the operand.
+// even; any K works (a k range that ends inside the maps off the 16-wide k-tile runs its last
+// K % 16 columns as a separate short-K pass).
 int32_t dgemm_tiled(Ctx* ctx, cudaStream_t st, const DOperand& A, const DOperand& B, double* C, int64_t ldc,
                     int64_t M, int64_t N, int64_t K, int op, bool check_info);
 
@@ -48,6 +49,30 @@ int32_t solve_adjoint_f64(Ctx* ctx, cudaStream_t st, const double* LU, int64_t l
 // C (M x N) op= A (M x K) B (K x N) in FP64 emulated with int8 slices on tcgen05 (ozaki.cu)
 int32_t ozaki_gemm(Ctx* ctx, cudaStream_t st, const double* A, int64_t lda, const double* B, int64_t ldb, double* C,
                    int64_t ldc, int64_t M, int64_t N, int64_t K, int op, int s);
+
+// Compares `rows` sampled rows of C (M x N) with the compensated (Dot2) product A B and returns, in
+// host_out4, max |C - C*|, max |A||B|, sum (C - C*)^2, sum C*^2 over them (report.cu).  Element
+// (m, k) of A is A[m lda + k] when a_kmajor, else A[k lda + m]; (k, n) of B is B[k ldb + n] when
+// b_nmajor, else B[n ldb + k].  Synchronizes the stream.
+int32_t gemm_error_report(Ctx* ctx, cudaStream_t st, const double* C, int64_t ldc, const double* A, int64_t lda,
+                          bool a_kmajor, const double* B, int64_t ldb, bool b_nmajor, int64_t M, int64_t N, int64_t K,
+                          int rows, double* host_out4);
+
+// Cholesky (chol.cu).  chol_factor_f64: A = L L^T in place (lower triangle; the strict upper triangle
+// is scratch), status[kInfo] = 1 when A is not positive definite.  chol_solve_f64: B <- A^-1 B from
+// the factor F (lower, with diagonal), using W (n x ldw) as scratch.  copy_lower: dst's lower
+// triangle (with diagonal) <- src's (only when status[kInfo] == 0 if only_if_ok).  split_nr / join_nr:
+// between one factor and the Numerical-Recipes form (strict lower triangle + diagonal vector P at
+// byte stride lwp).
+int32_t chol_factor_f64(Ctx* ctx, cudaStream_t st, double* A, int64_t ld, int64_t n);
+int32_t chol_solve_f64(Ctx* ctx, cudaStream_t st, const double* F, int64_t ldf, int64_t n, double* W, int64_t ldw,
+                       double* B, int64_t ldb, int64_t nrhs);
+int32_t copy_lower(Ctx* ctx, cudaStream_t st, double* dst, int64_t ldd, const double* src, int64_t lds, int64_t n,
+                   bool only_if_ok);
+int32_t split_nr(Ctx* ctx, cudaStream_t st, double* Lnr, int64_t ldl, double* P, int64_t lwp, const double* F,
+                 int64_t ldf, int64_t n);
+int32_t join_nr(Ctx* ctx, cudaStream_t st, double* F, int64_t ldf, const double* Lnr, int64_t ldl, const double* P,
+                int64_t lwp, int64_t n);
 
 // Builds perm from ipiv on the device (used when factors come from outside: b2m_MatrixLUBackSubst).
 int32_t perm_from_ipiv(Ctx* ctx, cudaStream_t st, const int32_t* ipiv, int64_t n, int32_t* perm);

@@ -201,9 +201,11 @@ __global__ void gather_rows_kernel(double* X, int64_t ldx, const double* B, int6
     X[i * ldx + c] = B[(int64_t)perm[i] * ldb + c];
 }
 
-// perm from a LAPACK-style ipiv: sequential interchanges on a shared-memory copy (n <= 48k)
-__global__ void perm_from_ipiv_kernel(const int32_t* ipiv, int n, int32_t* perm) {
-    extern __shared__ int32_t pv[];
+// perm from a LAPACK-style ipiv: sequential interchanges, on a shared-memory copy when `in_smem`
+// (n ints fit), else directly in perm (global memory; one dependent swap per step)
+__global__ void perm_from_ipiv_kernel(const int32_t* ipiv, int n, int32_t* perm, int in_smem) {
+    extern __shared__ int32_t pv_dyn[];
+    int32_t* pv = in_smem ? pv_dyn : perm;
     for (int i = threadIdx.x; i < n; i += blockDim.x) pv[i] = i;
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -217,29 +219,36 @@ __global__ void perm_from_ipiv_kernel(const int32_t* ipiv, int n, int32_t* perm)
         }
     }
     __syncthreads();
-    for (int i = threadIdx.x; i < n; i += blockDim.x) perm[i] = pv[i];
+    if (in_smem)
+        for (int i = threadIdx.x; i < n; i += blockDim.x) perm[i] = pv[i];
 }
 
-// det = (-1)^{#i: ipiv[i] != i} * U[0][0] * U[1][1] * ... in this order (MatrixDeterminant :467-476)
-__global__ void determinant_kernel(const double* LU, int64_t ld, int n, const int32_t* ipiv, const int32_t* status,
-                                   double* det) {
-    extern __shared__ double dg[];
+// det = (-1)^{#i: ipiv[i] != i} * U[0][0] * U[1][1] * ... in this order (MatrixDeterminant :467-476);
+// the diagonal is staged through shared memory 1024 entries at a time (launch with 1024 threads)
+constexpr int kDetChunk = 1024;
+__global__ void __launch_bounds__(kDetChunk)
+    determinant_kernel(const double* LU, int64_t ld, int n, const int32_t* ipiv, const int32_t* status, double* det) {
+    __shared__ double dg[kDetChunk];
     __shared__ int flips;
     if (threadIdx.x == 0) flips = 0;
     __syncthreads();
     int local = 0;
-    for (int i = threadIdx.x; i < n; i += blockDim.x) {
-        dg[i] = LU[(int64_t)i * ld + i];
+    for (int i = threadIdx.x; i < n; i += blockDim.x)
         if (ipiv[i] != i) local++;
-    }
     atomicAdd(&flips, local);
     __syncthreads();
-    if (threadIdx.x == 0) {
-        if (status[kInfo] != 0) { *det = 0.0; return; }
-        double r = (flips & 1) ? -1.0 : 1.0;
-        for (int i = 0; i < n; ++i) r = r * dg[i];
-        *det = r;
+    double r = (flips & 1) ? -1.0 : 1.0;  // thread 0's running product
+    for (int c0 = 0; c0 < n; c0 += kDetChunk) {
+        const int i = c0 + (int)threadIdx.x;
+        if (i < n) dg[threadIdx.x] = LU[(int64_t)i * ld + i];
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            const int cnt = min(kDetChunk, n - c0);
+            for (int k = 0; k < cnt; ++k) r = r * dg[k];
+        }
+        __syncthreads();
     }
+    if (threadIdx.x == 0) *det = status[kInfo] != 0 ? 0.0 : r;
 }
 
 // ------------------------------------------------------------------------------------------
@@ -248,6 +257,11 @@ __global__ void determinant_kernel(const double* LU, int64_t ld, int n, const in
 namespace {
 
 int64_t split_cols(int64_t w) { return round_up((w + 1) / 2, kPanelW); }
+
+void CUDART_CB progress_trampoline(void* p) {
+    const ProgressNote* note = static_cast<const ProgressNote*>(p);
+    if (note->fn) note->fn(note->percent, note->user);
+}
 
 template <typename T>
 int32_t launch_swaps_impl(Ctx* ctx, cudaStream_t st, T* A, int64_t ld, int ncols, int c0, int w, const int32_t* ipiv,
@@ -313,9 +327,19 @@ int32_t lu_rec(Ctx* ctx, cudaStream_t st, double* A, int64_t ld, int64_t n, int6
     if (width <= leaf) {
         B2M_TRY(launch_panel<double>(ctx, st, A + c0 * ld + c0, ld, (int)(n - c0), (int)width, (int)c0, (int)c0,
                                      ipiv));
-        return launch_swaps_impl<double>(ctx, st, A, ld, (int)n, (int)c0, (int)width, ipiv, perm);
+        B2M_TRY(launch_swaps_impl<double>(ctx, st, A, ld, (int)n, (int)c0, (int)width, ipiv, perm));
+        if (ctx->progress && ctx->progress_notes.size() < ctx->progress_notes.capacity()) {
+            // TLinEquProgress: columns factored * 100 div n, queued behind this panel
+            ctx->progress_notes.push_back(
+                ProgressNote{ctx->progress, ctx->progress_user, (int32_t)((c0 + width) * 100 / n)});
+            B2M_CU(ctx, cudaLaunchHostFunc(st, progress_trampoline, &ctx->progress_notes.back()));
+        }
+        return B2M_OK;
     }
-    const int64_t nleft = round_up((width + 1) / 2, leaf), nright = width - nleft;
+    // splits on multiples of 16 above the leaf level keep the Schur GEMMs' K on whole TMA k-tiles
+    // (8-column leaves then meet only in their own narrow K = 8 updates)
+    const int64_t step = width > 16 ? std::max<int64_t>(leaf, 16) : leaf;
+    const int64_t nleft = round_up((width + 1) / 2, step), nright = width - nleft;
     B2M_TRY(lu_rec(ctx, st, A, ld, n, c0, nleft, ipiv, perm, leaf));
     // A12 <- L11^{-1} A12
     TriSolve t{A, ld, n, A, ld, n, n, c0 + nleft, nright};
@@ -350,8 +374,17 @@ int32_t lu_factor_f64(Ctx* ctx, cudaStream_t st, double* A, int64_t ld, int64_t 
     if (n <= 0) return B2M_OK;
     if ((ld & 1) || !aligned16(A)) return fail(ctx, B2M_ERR_DIM, "lu_factor_f64: ld must be even, A 16-byte aligned");
     if (n > (1 << 30)) return fail(ctx, B2M_ERR_UNSUPPORTED, "n too large");
-    const int64_t leaf = n <= panel_max_rows(true, 32) ? 32 : 16;
-    if (n > panel_max_rows(true, 16)) return fail(ctx, B2M_ERR_UNSUPPORTED, "FP64 LU supports n <= %d", panel_max_rows(true, 16));
+    // the leaf width shrinks as the first panel grows (the cluster holds a whole panel on chip)
+    const int64_t leaf = n <= panel_max_rows(true, 32) ? 32 : (n <= panel_max_rows(true, 16) ? 16 : 8);
+    if (n > panel_max_rows(true, 8))
+        return fail(ctx, B2M_ERR_UNSUPPORTED, "FP64 LU supports n <= %d", panel_max_rows(true, 8));
+    if (ctx->progress) {
+        // the notes are the host functions' payloads: wait until the previous call's have run, then
+        // reserve one per leaf so that none moves while queued
+        B2M_CU(ctx, cudaStreamSynchronize(st));
+        ctx->progress_notes.clear();
+        ctx->progress_notes.reserve((size_t)(n / 8 + 2));
+    }
     const GraphKey key{1, A, ipiv, perm, ctx->d_status, ld, n, 0, 0};
     return run_graph(ctx, st, key, [&](cudaStream_t s) -> int32_t {
         if (perm) {
@@ -389,23 +422,26 @@ int32_t lu_solve_f64(Ctx* ctx, cudaStream_t st, const double* LU, int64_t ld, in
 }
 
 int32_t perm_from_ipiv(Ctx* ctx, cudaStream_t st, const int32_t* ipiv, int64_t n, int32_t* perm) {
-    if (n > 48 * 1024) return fail(ctx, B2M_ERR_UNSUPPORTED, "perm_from_ipiv: n > 49152");
+    if (n > (1 << 30)) return fail(ctx, B2M_ERR_UNSUPPORTED, "perm_from_ipiv: n too large");
     const size_t smem = (size_t)n * sizeof(int32_t);
-    if (smem > 48 * 1024)
-        B2M_CU(ctx, cudaFuncSetAttribute(perm_from_ipiv_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)smem));
-    perm_from_ipiv_kernel<<<1, 1024, smem, st>>>(ipiv, (int)n, perm);
+    const bool in_smem = smem <= ctx->smem_optin;
+    if (in_smem && smem > 48 * 1024) {
+        std::atomic<int>& set = device_flag((const void*)perm_from_ipiv_kernel, 0, ctx->device);
+        if (!set.load()) {
+            B2M_CU(ctx, cudaFuncSetAttribute(perm_from_ipiv_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)ctx->smem_optin));
+            set.store(1);
+        }
+    }
+    perm_from_ipiv_kernel<<<1, 1024, in_smem ? smem : 0, st>>>(ipiv, (int)n, perm, in_smem ? 1 : 0);
     B2M_LAUNCHED(ctx);
     return B2M_OK;
 }
 
 int32_t lu_determinant(Ctx* ctx, cudaStream_t st, const double* LU, int64_t ld, int64_t n, const int32_t* ipiv,
                        double* d_det) {
-    if (n > 24 * 1024) return fail(ctx, B2M_ERR_UNSUPPORTED, "determinant: n > 24576");
-    const size_t smem = (size_t)n * sizeof(double);
-    if (smem > 48 * 1024)
-        B2M_CU(ctx, cudaFuncSetAttribute(determinant_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    determinant_kernel<<<1, 1024, smem, st>>>(LU, ld, (int)n, ipiv, ctx->d_status, d_det);
+    if (n > (1 << 30)) return fail(ctx, B2M_ERR_UNSUPPORTED, "determinant: n too large");
+    determinant_kernel<<<1, kDetChunk, 0, st>>>(LU, ld, (int)n, ipiv, ctx->d_status, d_det);
     B2M_LAUNCHED(ctx);
     return B2M_OK;
 }

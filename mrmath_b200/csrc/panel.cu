@@ -418,8 +418,10 @@ int32_t launch_push(Ctx* ctx, cudaStream_t st, int C, int R, T* P, int64_t ld, i
 
 }  // namespace
 
+// Tallest panel of width w: 16 CTAs x 256 threads x rows per thread (2 for w <= 32, 4 for w <= 16,
+// 8 for w <= 8), the register budget of a row's block columns setting the rows per thread.
 int panel_max_rows(bool fp64, int w) {
-    if (fp64) return w <= 16 ? kPMaxC * kPT * 4 : kPMaxC * kPT * 2;
+    if (fp64) return w <= 8 ? kPMaxC * kPT * 8 : (w <= 16 ? kPMaxC * kPT * 4 : kPMaxC * kPT * 2);
     return kPMaxC * kPT * 4;
 }
 
@@ -432,6 +434,12 @@ int32_t launch_panel(Ctx* ctx, cudaStream_t st, T* P, int64_t ld, int m, int w, 
             const int C = (int)ceil_div(m, kPT * 2);
             if (C > kPMaxC) return fail(ctx, B2M_ERR_UNSUPPORTED, "FP64 panel of %d rows needs width <= 16", m);
             return launch_push<T, 32, 2>(ctx, st, C, (int)ceil_div(m, C), P, ld, m, w, row_base, col_base, ipiv);
+        }
+        if (m > panel_max_rows(true, 16)) {  // very tall: 8 columns, 8 rows per thread
+            const int C = (int)ceil_div(m, kPT * 8);
+            if (w > 8 || C > kPMaxC)
+                return fail(ctx, B2M_ERR_UNSUPPORTED, "FP64 panel of %d x %d is too tall", m, w);
+            return launch_push<T, 8, 8>(ctx, st, C, (int)ceil_div(m, C), P, ld, m, w, row_base, col_base, ipiv);
         }
         const int C = (int)ceil_div(m, kPT * 4);
         if (C > kPMaxC) return fail(ctx, B2M_ERR_UNSUPPORTED, "FP64 panel of %d rows is too tall", m);

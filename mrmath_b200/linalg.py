@@ -15,7 +15,7 @@ import ctypes as C
 
 import numpy as np
 
-from ._lib import DO_ADD, DO_NONE, DO_SUB, MIXED_3XTF32, MIXED_TF32, OK, SINGULAR, Context, SolveReport
+from ._lib import DO_ADD, DO_NONE, DO_SUB, MIXED_3XTF32, MIXED_TF32, OK, SINGULAR, Context, GemmReport, SolveReport
 
 __all__ = [
     "default_context", "MatrixMult", "MatrixMultEx", "MatrixMultT1Ex", "MatrixMultT2Ex", "MatrixLUDecompInPlace",
@@ -74,6 +74,22 @@ def MatrixMult(mt1: np.ndarray, mt2: np.ndarray, ctx: Context | None = None) -> 
     dest = np.empty((mt1.shape[0], mt2.shape[1]))
     MatrixMultEx(dest, mt1, mt2, DO_NONE, 0, ctx)
     return dest
+
+
+def _grep(rep) -> dict:
+    return {"rows_checked": rep.rows_checked, "forward_error": rep.forward_error,
+            "relative_error": rep.relative_error, "bound": rep.bound}
+
+
+def MatrixMultErrorReport(dest: np.ndarray, mt1: np.ndarray, mt2: np.ndarray, trans: int = 0, sample_rows: int = 16,
+                          ctx: Context | None = None) -> dict:
+    """Error of a product dest = op(mt1) op(mt2) on sampled rows against the Dot2 product."""
+    h1, w1 = mt1.shape
+    h2, w2 = mt2.shape
+    rep = GemmReport()
+    _ctx_of(ctx).call("b2m_MatrixMultErrorReport", _ptr(dest), _lw(dest), _ptr(mt1), _ptr(mt2), w1, h1, w2, h2,
+                      _lw(mt1), _lw(mt2), trans, sample_rows, C.addressof(rep))
+    return _grep(rep)
 
 
 def MatrixMultT1Ex(dest, mt1, mt2, op=DO_NONE, ctx=None):
@@ -296,3 +312,117 @@ def dev_MatrixMultOzaki(dest, mt1, mt2, slices=8, op=DO_NONE, ctx=None):
     h2, w2 = mt2.shape
     c.call("b2m_dev_MatrixMultOzaki", _tptr(dest), _tlw(dest), _tptr(mt1), _tptr(mt2), w1, h1, w2, h2, _tlw(mt1),
            _tlw(mt2), op, slices)
+
+
+def dev_MatrixMultErrorReport(dest, mt1, mt2, trans=0, sample_rows=16, ctx=None) -> dict:
+    """Device twin of MatrixMultErrorReport (torch CUDA tensors); synchronizes the bound stream."""
+    c = _ctx_of(ctx)
+    _bind_stream(c, dest)
+    h1, w1 = mt1.shape
+    h2, w2 = mt2.shape
+    rep = GemmReport()
+    c.call("b2m_dev_MatrixMultErrorReport", _tptr(dest), _tlw(dest), _tptr(mt1), _tptr(mt2), w1, h1, w2, h2,
+           _tlw(mt1), _tlw(mt2), trans, sample_rows, C.addressof(rep))
+    return _grep(rep)
+
+
+# ----------------------------------------------------------------------------- Cholesky
+def MatrixCholeskyInPlace4(A: np.ndarray, pnl_size: int = 0, ctx: Context | None = None) -> int:
+    """A = L L^T, L in A's lower triangle (LinAlgCholesky.pas:106-123); 0 = crOk, 1 = not positive definite."""
+    return _ctx_of(ctx).call("b2m_MatrixCholeskyInPlace4", _ptr(A), _lw(A), A.shape[1], pnl_size, allow=(OK, 1))
+
+
+def MatrixCholeskyInPlace(A: np.ndarray, P: np.ndarray, ctx: Context | None = None) -> int:
+    """Numerical-Recipes form (LinAlgCholesky.pas:270-332): L below A's diagonal, the diagonal in P's
+    first column (P an (n, k) array: element i at byte offset i * LineWidthP)."""
+    return _ctx_of(ctx).call("b2m_MatrixCholeskyInPlace", _ptr(A), _lw(A), A.shape[1], _ptr(P), _lw(P),
+                             allow=(OK, 1))
+
+
+def MatrixCholeskySolveLinEq(A: np.ndarray, B: np.ndarray, P: np.ndarray | None = None,
+                             ctx: Context | None = None) -> np.ndarray:
+    """X with A X = B from a Cholesky factor (NR form with P, or the InPlace4 form without)."""
+    n, k = A.shape[1], B.shape[1]
+    X = np.zeros((n, k))
+    _ctx_of(ctx).call("b2m_MatrixCholeskySolveLinEq", _ptr(A), _lw(A), n, _ptr(P) if P is not None else None,
+                      _lw(P) if P is not None else 0, _ptr(B), _lw(B), _ptr(X), _lw(X), k)
+    return X
+
+
+def dev_MatrixCholeskyInPlace4(A, status=None, ctx=None):
+    c = _ctx_of(ctx)
+    _bind_stream(c, A)
+    c.call("b2m_dev_MatrixCholeskyInPlace4", _tptr(A), _tlw(A), A.shape[1],
+           _tptr(status) if status is not None else None)
+
+
+def dev_MatrixCholeskySolveLinEq(A, B, X, P=None, ctx=None):
+    c = _ctx_of(ctx)
+    _bind_stream(c, A)
+    c.call("b2m_dev_MatrixCholeskySolveLinEq", _tptr(A), _tlw(A), A.shape[1], _tptr(P) if P is not None else None,
+           P.stride(0) * 8 if P is not None else 0, _tptr(B), _tlw(B), _tptr(X), _tlw(X), B.shape[1])
+
+
+# ----------------------------------------------------------------------------- resident matrices
+class ResidentMatrix:
+    """A matrix kept in device memory across chained calls: the resident form a TDoubleMatrix
+    subclass keeps (b2m_alloc / b2m_upload / b2m_download and the b2m_dev_* entry points on the
+    context's own stream), without torch.  `sub` is a view into the parent (SetSubMatrix,
+    Matrix.pas:70): same storage, the parent's LineWidth."""
+
+    def __init__(self, ctx: Context, rows: int, cols: int, _view_of=None, _ptr=None, _lw=None):
+        self.ctx, self.rows, self.cols = ctx, rows, cols
+        self._parent = _view_of
+        if _view_of is None:
+            p, lw = C.c_void_p(), C.c_int64()
+            ctx.check(ctx.lib_call("b2m_alloc", rows, cols, C.byref(p), C.byref(lw)))
+            self.ptr, self.lw = p.value, lw.value
+        else:
+            self.ptr, self.lw = _ptr, _lw
+
+    @classmethod
+    def from_host(cls, a: np.ndarray, ctx: Context | None = None) -> "ResidentMatrix":
+        c = _ctx_of(ctx)
+        m = cls(c, a.shape[0], a.shape[1])
+        c.check(c.lib_call("b2m_upload", m.ptr, m.lw, _ptr(a), _lw(a), a.shape[0], a.shape[1]))
+        return m
+
+    def to_host(self) -> np.ndarray:
+        out = np.empty((self.rows, self.cols))
+        self.ctx.check(self.ctx.lib_call("b2m_download", _ptr(out), _lw(out), self.ptr, self.lw, self.rows,
+                                         self.cols))
+        return out
+
+    def sub(self, r0: int, c0: int, rows: int, cols: int) -> "ResidentMatrix":
+        if r0 < 0 or c0 < 0 or r0 + rows > self.rows or c0 + cols > self.cols:
+            raise ValueError("sub-matrix outside the matrix")
+        return ResidentMatrix(self.ctx, rows, cols, _view_of=self, _ptr=self.ptr + r0 * self.lw + c0 * 8,
+                              _lw=self.lw)
+
+    def mult(self, other: "ResidentMatrix", trans: int = 0) -> "ResidentMatrix":
+        """op(self) * op(other) into a new resident matrix (MultEx with doNone)."""
+        m = self.cols if trans == 1 else self.rows
+        n = other.rows if trans == 2 else other.cols
+        out = ResidentMatrix(self.ctx, m, n)
+        self.ctx.use_own_stream()
+        self.ctx.call("b2m_dev_MatrixMultEx", out.ptr, out.lw, self.ptr, other.ptr, self.cols, self.rows, other.cols,
+                      other.rows, self.lw, other.lw, DO_NONE, trans)
+        return out
+
+    def solve(self, rhs: "ResidentMatrix") -> tuple[int, "ResidentMatrix"]:
+        """SolveLinEQ: X with self X = rhs; returns (status, X)."""
+        x = ResidentMatrix(self.ctx, rhs.rows, rhs.cols)
+        st = ResidentMatrix(self.ctx, 1, 1)  # one int32 result word in the first bytes
+        try:
+            self.ctx.use_own_stream()
+            self.ctx.call("b2m_dev_MatrixLinEQSolve", self.ptr, self.lw, self.cols, rhs.ptr, rhs.lw, x.ptr, x.lw,
+                          rhs.cols, 0, st.ptr)
+            word = st.to_host().view(np.int32)[0, 0]
+        finally:
+            st.free()
+        return int(word), x
+
+    def free(self) -> None:
+        if self._parent is None and self.ptr:
+            self.ctx.check(self.ctx.lib_call("b2m_free", self.ptr))
+        self.ptr = 0

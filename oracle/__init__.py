@@ -72,6 +72,10 @@ def _load():
         "orc_residual_dot2": (None, [_pd, _i64, _i64, _pd, _i64, _pd, _i64, _i64, _pd, _i64]),
         "orc_backward_error": (_dbl, [_pd, _i64, _i64, _pd, _i64, _pd, _i64, _i64]),
         "orc_gemm_rows_dot2": (None, [_pd, _i64, _pd, _i64, _i64, _i64, _i64, _i64, _i64, _pd, _i64, _pd, _i64]),
+        "orc_cholesky_inplace4": (_i32, [_pd, _i64, _i64, _i64]),
+        "orc_cholesky_inplace2": (_i32, [_pd, _i64, _i64]),
+        "orc_cholesky_nr": (_i32, [_pd, _i64, _i64, _pd, _i64]),
+        "orc_cholesky_solve_nr": (None, [_pd, _i64, _i64, _pd, _i64, _pd, _i64, _pd, _i64]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)
@@ -259,3 +263,27 @@ def gemm_rows_dot2(a: np.ndarray, b: np.ndarray, r0: int, nr: int):
     absab = np.zeros((nr, n))
     lib.orc_gemm_rows_dot2(_p(a), _lw(a), _p(b), _lw(b), m, n, k, r0, nr, _p(c), _lw(c), _p(absab), _lw(absab))
     return c, absab
+
+
+# ------------------------------------------------------------------ Cholesky (LinAlgCholesky.pas)
+def cholesky_inplace4(a: np.ndarray, pnl: int = 0) -> int:
+    """MatrixCholeskyInPlace4 (TDoubleMatrix.Cholesky's routine): L in the lower triangle of a,
+    the strict upper triangle left as it was.  0 = crOk, 1 = crNoPositiveDefinite."""
+    return lib.orc_cholesky_inplace4(_p(a), _lw(a), a.shape[1], pnl)
+
+
+def cholesky_inplace2(a: np.ndarray) -> int:
+    return lib.orc_cholesky_inplace2(_p(a), _lw(a), a.shape[1])
+
+
+def cholesky_nr(a: np.ndarray, p: np.ndarray) -> int:
+    """MatrixCholeskyInPlace: L below the diagonal of a, its diagonal in p (an (n, k) view whose
+    first column is used, like the reference's LineWidthP)."""
+    return lib.orc_cholesky_nr(_p(a), _lw(a), a.shape[1], _p(p), _lw(p))
+
+
+def cholesky_solve_nr(a: np.ndarray, p: np.ndarray, b: np.ndarray) -> np.ndarray:
+    """MatrixCholeskySolveLinEq for one right-hand side column b (n, 1)."""
+    x = np.zeros_like(b)
+    lib.orc_cholesky_solve_nr(_p(a), _lw(a), a.shape[1], _p(p), _lw(p), _p(b), _lw(b), _p(x), _lw(x))
+    return x

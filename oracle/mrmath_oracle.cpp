@@ -1018,6 +1018,127 @@ extern "C" double orc_backward_error(const double* A, int64_t lwA, int64_t n, co
     return eta;
 }
 
+// ---------------- Cholesky (LinAlgCholesky.pas) ------------------------------------------------------------
+namespace {
+
+// GenericSymRankKUpd SimpleMatrixOperations.pas:3391-3423: lower triangle of dest (height x height)
+// = Beta*dest + Alpha*A A^T, A height x k, the inner sums in ascending l
+void sym_rank_k_upd(double* dest, int64_t lwd, const double* A, int64_t lwA, int64_t k, int64_t height, double alpha,
+                    double beta) {
+    if (k <= 0 || height <= 0) return;
+    for (int64_t j = 0; j < height; ++j) {
+        double* c = rowp(dest, j, lwd);
+        const double* aj = rowp(A, j, lwA);
+        for (int64_t i = 0; i <= j; ++i) {
+            const double* ai = rowp(A, i, lwA);
+            double temp = 0.0;
+            for (int64_t l = 0; l < k; ++l) temp = temp + ai[l] * aj[l];
+            c[i] = beta * c[i] + alpha * temp;
+        }
+    }
+}
+
+// GenericSolveLoTriMtxTranspNoUnit SimpleMatrixOperations.pas:3463-3510: B (height x width) <- B L^-T,
+// column k scaled by the reciprocal 1/L[k][k], then eliminated from the later columns
+void solve_lo_tri_transp(const double* A, int64_t lwA, double* B, int64_t lwB, int64_t width, int64_t height) {
+    if (width == 0 || height == 0) return;
+    for (int64_t k = 0; k < width; ++k) {
+        const double temp = 1.0 / rowp(A, k, lwA)[k];
+        for (int64_t i = 0; i < height; ++i) rowp(B, i, lwB)[k] = temp * rowp(B, i, lwB)[k];
+        for (int64_t j = k + 1; j < width; ++j) {
+            const double ajk = rowp(A, j, lwA)[k];
+            if (ajk != 0.0)
+                for (int64_t i = 0; i < height; ++i)
+                    rowp(B, i, lwB)[j] = rowp(B, i, lwB)[j] - ajk * rowp(B, i, lwB)[k];
+        }
+    }
+}
+
+// MatrixCholeskyInPlace2 LinAlgCholesky.pas:205-250: row-oriented unblocked lower Cholesky
+int32_t chol_inplace2(double* A, int64_t lwA, int64_t width) {
+    for (int64_t i = 0; i < width; ++i) {
+        double* ai = rowp(A, i, lwA);
+        for (int64_t j = 0; j <= i; ++j) {
+            double sum = ai[j];
+            const double* aj = rowp(A, j, lwA);
+            for (int64_t k = 0; k < j; ++k) sum = sum - ai[k] * aj[k];
+            if (i > j)
+                ai[j] = sum / aj[j];
+            else if (sum > 0)
+                ai[i] = std::sqrt(sum);
+            else
+                return 1;  // crNoPositiveDefinite
+        }
+    }
+    return 0;
+}
+
+// InternalBlkCholeskyInPlace LinAlgCholesky.pas:54-103 (left-looking, panels of pnl columns)
+int32_t chol_blocked(double* A, int64_t lwA, int64_t width, int64_t pnl) {
+    for (int64_t j = 0; j < width; j += pnl) {
+        const int64_t jb = std::min(pnl, width - j);
+        double* ajj = rowp(A, j, lwA) + j;
+        const double* a1 = rowp(A, j, lwA);
+        sym_rank_k_upd(ajj, lwA, a1, lwA, j, jb, -1.0, 1.0);
+        if (chol_inplace2(ajj, lwA, jb) != 0) return 1;
+        if (j + jb < width) {
+            double* ajb = rowp(A, j + jb, lwA);
+            const double* aj = rowp(A, j, lwA);
+            // MatrixMultT2Ex(pAjjb, ..., pAjb, pAj, j, width - j - jb, j, jb, ..., jb, doSub, multMem)
+            orc_block_mult_t2(ajb + j, lwA, ajb, aj, j, width - j - jb, j, jb, lwA, lwA, jb, 2);
+            solve_lo_tri_transp(ajj, lwA, ajb + j, lwA, jb, width - j - jb);
+        }
+    }
+    return 0;
+}
+
+}  // namespace
+
+extern "C" int32_t orc_cholesky_inplace4(double* A, int64_t lwA, int64_t width, int64_t pnl) {
+    // MatrixCholeskyInPlace4 LinAlgCholesky.pas:106-123 (pnlSize 0 = CholBlockSize = 32)
+    if (pnl == 0) pnl = 32;
+    if (width <= pnl) return chol_inplace2(A, lwA, width);
+    return chol_blocked(A, lwA, width, pnl);
+}
+
+extern "C" int32_t orc_cholesky_inplace2(double* A, int64_t lwA, int64_t width) { return chol_inplace2(A, lwA, width); }
+
+extern "C" int32_t orc_cholesky_nr(double* A, int64_t lwA, int64_t width, double* P, int64_t lwP) {
+    // MatrixCholeskyInPlace LinAlgCholesky.pas:270-332: L below the diagonal of A, its diagonal in P
+    // (P[i] at byte offset i*lwP); sums run k = i-1 down to 0
+    for (int64_t i = 0; i < width; ++i) {
+        const double* ai = rowp(A, i, lwA);
+        for (int64_t j = i; j < width; ++j) {
+            double* aj = rowp(A, j, lwA);
+            double sum = ai[j];
+            for (int64_t k = i - 1; k >= 0; --k) sum = sum - ai[k] * aj[k];
+            if (i == j) {
+                if (sum <= 0) return 1;
+                rowp(P, i, lwP)[0] = std::sqrt(sum);
+            } else {
+                aj[i] = sum / rowp(P, i, lwP)[0];
+            }
+        }
+    }
+    return 0;
+}
+
+extern "C" void orc_cholesky_solve_nr(const double* A, int64_t lwA, int64_t width, const double* P, int64_t lwP,
+                                      const double* B, int64_t lwB, double* X, int64_t lwX) {
+    // MatrixCholeskySolveLinEq LinAlgCholesky.pas:352-421: L y = b (k descending), L^T x = y (k ascending)
+    for (int64_t i = 0; i < width; ++i) {
+        double sum = rowp(B, i, lwB)[0];
+        const double* ai = rowp(A, i, lwA);
+        for (int64_t k = i - 1; k >= 0; --k) sum = sum - ai[k] * rowp(X, k, lwX)[0];
+        rowp(X, i, lwX)[0] = sum / rowp(P, i, lwP)[0];
+    }
+    for (int64_t i = width - 1; i >= 0; --i) {
+        double sum = rowp(X, i, lwX)[0];
+        for (int64_t k = i + 1; k < width; ++k) sum = sum - rowp(A, k, lwA)[i] * rowp(X, k, lwX)[0];
+        rowp(X, i, lwX)[0] = sum / rowp(P, i, lwP)[0];
+    }
+}
+
 extern "C" void orc_gemm_rows_dot2(const double* A, int64_t lwA, const double* B, int64_t lwB, int64_t /*m*/,
                                    int64_t n, int64_t k, int64_t r0, int64_t nr, double* C, int64_t lwC,
                                    double* absAB, int64_t lwAbs) {

@@ -114,6 +114,13 @@ void    orc_gemm_rows_dot2(const double* A, int64_t lwA, const double* B, int64_
                            int64_t m, int64_t n, int64_t k, int64_t r0, int64_t nr,
                            double* C, int64_t lwC, double* absAB, int64_t lwAbs);
 
+/* ---- Cholesky (LinAlgCholesky.pas); results 0 = crOk, 1 = crNoPositiveDefinite (MatrixConst.pas:30) */
+int32_t orc_cholesky_inplace4(double* A, int64_t lwA, int64_t width, int64_t pnl);   /* :106-123, :54-103 */
+int32_t orc_cholesky_inplace2(double* A, int64_t lwA, int64_t width);                /* :205-250 */
+int32_t orc_cholesky_nr(double* A, int64_t lwA, int64_t width, double* P, int64_t lwP); /* :270-332 */
+void    orc_cholesky_solve_nr(const double* A, int64_t lwA, int64_t width, const double* P, int64_t lwP,
+                              const double* B, int64_t lwB, double* X, int64_t lwX);   /* :352-421 */
+
 #ifdef __cplusplus
 }
 #endif

@@ -36,6 +36,27 @@ def test_python_signatures_cover_header():
     assert declared_symbols() <= set(_lib.SIGNATURES), set(declared_symbols()) - set(_lib.SIGNATURES)
 
 
+def test_reference_arm_loads_no_libb2m():
+    """bench.py --impl reference times the oracle's restatement of the reference alone: the run
+    (here on a small system) must not import the ctypes layer nor map libb2m.so."""
+    import json
+    import subprocess
+    import sys
+    code = (
+        "import sys, json, argparse; sys.path.insert(0, %r); sys.argv = ['bench.py'];"
+        "import bench;"
+        "a = argparse.Namespace(n=96, nrhs=2, kappa=1e4, steps=2, warmup=1, gpus=1);"
+        "bench.run_reference(a, 1, 0);"
+        "maps = open('/proc/self/maps').read();"
+        "print(json.dumps({'lib': 'mrmath_b200._lib' in sys.modules, 'mapped': 'libb2m.so' in maps}))" % ROOT)
+    out = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, check=True, timeout=600)
+    lines = [json.loads(x) for x in out.stdout.strip().splitlines()]
+    line, probe = lines[0], lines[-1]
+    assert line["impl"] == "reference" and line["config"]["n"] == 96 and line["steps"] == 2
+    assert line["backward_error"] <= 96 * 2.0 ** -53
+    assert probe == {"lib": False, "mapped": False}
+
+
 def test_status_strings_without_gpu():
     from mrmath_b200 import _lib
     assert _lib.lib.b2m_status_string(1) == b"matrix is singular"

@@ -47,8 +47,10 @@ def test_headline_system_mixed_and_plain(ctx, kappa):
     assert diff <= kappa * 4 * bound, (kappa, diff)
 
 
-@pytest.mark.parametrize("n", [8192, 9000])
+@pytest.mark.parametrize("n", [8192, 9000, 16500])
 def test_plain_lu_pivots_at_bench_sizes(ctx, n):
+    """32-column leaves (n <= 8192), 16-column leaves (n <= 16384) and 8-column leaves on
+    16-CTA clusters holding up to 32768 panel rows (n = 16500)."""
     r = oracle.Mersenne(seed=2 * n + 1)
     a = r.uniform(n, n) - 0.5
     ref = a.copy()
@@ -60,3 +62,23 @@ def test_plain_lu_pivots_at_bench_sizes(ctx, n):
     assert bad.size == 0, f"pivots differ at {bad[:5]} (n={n})"
     err = np.linalg.norm(lu - ref) / np.linalg.norm(ref)
     assert err <= 1e-12, (n, err)
+
+
+def test_plain_solve_20000(ctx):
+    """MatrixLinEQSolve's drop-in beyond n = 16384 (8-column leaves, short-K Schur updates),
+    checked by the oracle's compensated backward error (the oracle's own LU at this order would
+    take minutes on the host)."""
+    import torch
+    n = 20000
+    r = inputs.rng(20000)
+    a = r.random_sample((n, n)) - 0.5
+    b = r.standard_normal((n, 2))
+    A, B = torch.from_numpy(a).cuda(), torch.from_numpy(b).cuda()
+    X = torch.empty_like(B)
+    status = torch.zeros(1, dtype=torch.int32, device="cuda")
+    L.dev_MatrixLinEQSolve(A, B, X, status=status, ctx=ctx)
+    torch.cuda.synchronize()
+    assert int(status.item()) == 0
+    x = X.cpu().numpy()
+    assert np.all(np.isfinite(x))
+    assert oracle.backward_error(a, x, b) <= n * 2.0 ** -53

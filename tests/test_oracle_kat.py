@@ -193,3 +193,45 @@ def test_singular_zero_column_and_nan():
     rc, _ = oracle.lu_decomp_inplace(a.copy())
     assert rc == 1
     assert oracle.determinant(a) == 0.0
+
+
+CHOL_A = np.array([[1.0, 2, 2], [-1, 4, -2], [2, 2, -1]])
+CHOL_A2 = np.array([[1.0, 2, 2, 0.5], [-1, 4, -2, -0.1], [2, 2, -1, 1.2], [3, 2, -1, -1.1]])
+
+
+def test_cholesky_kats():
+    """TestCholesky (TestLineEquations.pas:494-524): X = A A^T factors (NR form), A itself does not,
+    and the solve of X x = (2, -1, -1) gives (0.338888889, 0.00555555556, -0.2666666667)."""
+    x = oracle.matrix_mult(CHOL_A, np.ascontiguousarray(CHOL_A.T))
+    p = np.zeros((3, 4))  # LineWidthP = 4 doubles
+    assert oracle.cholesky_nr(x, p) == 0
+    assert oracle.cholesky_nr(CHOL_A.copy(), np.zeros((3, 4))) == 1
+    res = oracle.cholesky_solve_nr(x, p, np.array([[2.0], [-1.0], [-1.0]]))
+    np.testing.assert_allclose(res.ravel(), [0.338888889, 0.00555555556, -0.2666666667], atol=1e-9)
+
+
+def test_cholesky2_kats_and_forms_agree():
+    """TestCholesky2 (:526-571): InPlace4 with 2-column panels and InPlace2 succeed on A A^T (3 x 3
+    and 4 x 4) and agree; InPlace2 reports crNoPositiveDefinite on A itself."""
+    for a in (CHOL_A, CHOL_A2):
+        x = oracle.matrix_mult(a, np.ascontiguousarray(a.T))
+        x4, x2 = x.copy(), x.copy()
+        assert oracle.cholesky_inplace4(x4, 2) == 0 and oracle.cholesky_inplace2(x2) == 0
+        np.testing.assert_allclose(np.tril(x4), np.tril(x2), rtol=1e-13, atol=1e-13)
+        lo = np.tril(x2)
+        np.testing.assert_allclose(lo @ lo.T, x, rtol=1e-13, atol=1e-12)
+    assert oracle.cholesky_inplace2(CHOL_A.copy()) == 1
+
+
+def test_cholesky3_differential():
+    """TestCholesky3 (:573-631) at n = 400 instead of 2048: unblocked, panel-24 and panel-32 (the
+    class default) forms of the same SPD matrix x x^T agree."""
+    r = oracle.Mersenne(seed=15)
+    x = r.uniform(400, 400)
+    a = oracle.matrix_mult(x, np.ascontiguousarray(x.T))
+    a2, a24, a32 = a.copy(), a.copy(), a.copy()
+    assert oracle.cholesky_inplace2(a2) == 0
+    assert oracle.cholesky_inplace4(a24, 24) == 0 and oracle.cholesky_inplace4(a32) == 0
+    for b in (a24, a32):
+        assert np.linalg.norm(np.tril(b) - np.tril(a2)) <= 1e-9 * np.linalg.norm(np.tril(a2))
+    assert np.array_equal(np.triu(a32, 1), np.triu(a, 1))
