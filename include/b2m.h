@@ -36,6 +36,7 @@ extern "C" {
 #define B2M_ERR_ARG         -5   /* null pointer / invalid enum */
 #define B2M_ERR_NOCONV      -6   /* mixed-precision refinement did not converge and fallback was disabled */
 #define B2M_ERR_UNSUPPORTED -7   /* size outside what this build supports */
+#define B2M_ERR_FORMAT      -8   /* a file is not a saved TDoubleMatrix stream */
 
 /* destination operation of the blocked multiplication, TMatrixMultDestOperation (MatrixConst.pas:147) */
 #define B2M_DO_NONE 0
@@ -90,6 +91,26 @@ B2M_API int32_t     b2m_upload(b2m_ctx* ctx, double* dst, int64_t dstLineWidth, 
                                int64_t srcLineWidth, int64_t rows, int64_t cols);
 B2M_API int32_t     b2m_download(b2m_ctx* ctx, double* dst, int64_t dstLineWidth, const double* src,
                                  int64_t srcLineWidth, int64_t rows, int64_t cols);
+/* ------------------------------------------------------------------ saved matrices
+ * The reference's binary persistence format ("RMCLS" streams of TBinaryReaderWriter,
+ * BinaryReaderWriter.pas) for TDoubleMatrix objects, the counterpart of ReadObjFromFile
+ * (BaseMathPersistence.pas:153) and TDoubleMatrix.SaveToFile(..., TBinaryReaderWriter): matrices a
+ * Pascal program saved, and the reference's fixtures (Test/MatrixData1.txt ...), load straight into
+ * host or device buffers.  `info` receives the full size and the saved sub-matrix view; with dst NULL
+ * the call only queries it.  B2M_ERR_FORMAT: not a saved TDoubleMatrix; B2M_ERR_ARG: no such file. */
+typedef struct b2m_matrix_info {
+    int64_t width, height;            /* the full matrix that "data" holds, row by row */
+    int64_t sub_width, sub_height;    /* the saved sub-matrix view (SetSubMatrix) */
+    int64_t offset_x, offset_y;
+} b2m_matrix_info;
+B2M_API int32_t     b2m_ReadMatrixFile(const char* path, b2m_matrix_info* info, double* dst, int64_t LineWidth);
+/* the same into device memory (dst a device pointer, e.g. from b2m_alloc); synchronous */
+B2M_API int32_t     b2m_dev_ReadMatrixFile(b2m_ctx* ctx, const char* path, b2m_matrix_info* info, double* dst,
+                                           int64_t LineWidth);
+/* writes width x height doubles (byte stride LineWidth) as a saved TDoubleMatrix (empty Name, the full
+ * matrix as its view), section for section as the reference's saved fixtures */
+B2M_API int32_t     b2m_WriteMatrixFile(const char* path, const double* src, int64_t LineWidth, int64_t width,
+                                        int64_t height);
 /* Number of polls after which a bounded wait of the mixed solve's refinement sweeps gives up
  * (polls < 0 restores the built-in limit, about a second of spinning).  No counterpart in the
  * reference: a lower limit exists to exercise the timeout path -- with 0 polls every dependent

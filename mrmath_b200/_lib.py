@@ -16,6 +16,7 @@ i32, i64, dbl, vp = C.c_int32, C.c_int64, C.c_double, C.c_void_p
 # status codes (b2m.h)
 OK, SINGULAR = 0, 1
 ERR_DIM, ERR_CUDA, ERR_ALLOC, ERR_TIMEOUT, ERR_ARG, ERR_NOCONV, ERR_UNSUPPORTED = -1, -2, -3, -4, -5, -6, -7
+ERR_FORMAT = -8
 DO_NONE, DO_ADD, DO_SUB = 0, 1, 2
 MIXED_TF32, MIXED_3XTF32 = 1, 3
 
@@ -24,6 +25,12 @@ class SolveReport(C.Structure):
     """b2m_solve_report"""
     _fields_ = [("iterations", C.c_int32), ("fell_back", C.c_int32), ("backward_error", C.c_double),
                 ("refinement_backward_error", C.c_double), ("forward_error", C.c_double)]
+
+class MatrixInfo(C.Structure):
+    """b2m_matrix_info"""
+    _fields_ = [("width", C.c_int64), ("height", C.c_int64), ("sub_width", C.c_int64), ("sub_height", C.c_int64),
+                ("offset_x", C.c_int64), ("offset_y", C.c_int64)]
+
 
 class GemmReport(C.Structure):
     """b2m_gemm_report"""
@@ -42,6 +49,9 @@ SIGNATURES: dict[str, tuple] = {
     "b2m_synchronize": (i32, [vp]),
     "b2m_set_wait_limit": (i32, [vp, i64]),
     "b2m_set_progress": (i32, [vp, vp, vp]),
+    "b2m_ReadMatrixFile": (i32, [C.c_char_p, vp, vp, i64]),
+    "b2m_dev_ReadMatrixFile": (i32, [vp, C.c_char_p, vp, vp, i64]),
+    "b2m_WriteMatrixFile": (i32, [C.c_char_p, vp, i64, i64, i64]),
     "b2m_alloc": (i32, [vp, i64, i64, C.POINTER(vp), C.POINTER(i64)]),
     "b2m_free": (i32, [vp, vp]),
     "b2m_upload": (i32, [vp, vp, i64, vp, i64, i64, i64]),

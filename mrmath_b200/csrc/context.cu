@@ -413,6 +413,7 @@ extern "C" const char* b2m_status_string(int32_t s) {
         case B2M_ERR_ARG: return "invalid argument";
         case B2M_ERR_NOCONV: return "refinement did not converge";
         case B2M_ERR_UNSUPPORTED: return "unsupported size or device";
+        case B2M_ERR_FORMAT: return "not a saved matrix stream";
         default: return "unknown status";
     }
 }

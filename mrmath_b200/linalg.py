@@ -15,7 +15,8 @@ import ctypes as C
 
 import numpy as np
 
-from ._lib import DO_ADD, DO_NONE, DO_SUB, MIXED_3XTF32, MIXED_TF32, OK, SINGULAR, Context, GemmReport, SolveReport
+from ._lib import (DO_ADD, DO_NONE, DO_SUB, MIXED_3XTF32, MIXED_TF32, OK, SINGULAR, B2MError, Context, GemmReport,
+                   SolveReport)
 
 __all__ = [
     "default_context", "MatrixMult", "MatrixMultEx", "MatrixMultT1Ex", "MatrixMultT2Ex", "MatrixLUDecompInPlace",
@@ -326,6 +327,31 @@ def dev_MatrixMultErrorReport(dest, mt1, mt2, trans=0, sample_rows=16, ctx=None)
     return _grep(rep)
 
 
+# ----------------------------------------------------------------------------- saved matrices
+def ReadMatrixFile(path: str) -> tuple[np.ndarray, dict]:
+    """ReadObjFromFile of a saved TDoubleMatrix ("RMCLS" binary stream): (full matrix, view info)."""
+    from ._lib import MatrixInfo, lib
+    info = MatrixInfo()
+    st = lib.b2m_ReadMatrixFile(path.encode(), C.addressof(info), None, 0)
+    if st != OK:
+        raise B2MError(st, f"{lib.b2m_status_string(st).decode()}: {path}")
+    out = np.empty((info.height, info.width))
+    st = lib.b2m_ReadMatrixFile(path.encode(), C.addressof(info), _ptr(out), max(out.strides[0], 8))
+    if st != OK:
+        raise B2MError(st, lib.b2m_status_string(st).decode())
+    view = {"sub_width": info.sub_width, "sub_height": info.sub_height, "offset_x": info.offset_x,
+            "offset_y": info.offset_y}
+    return out, view
+
+
+def WriteMatrixFile(path: str, a: np.ndarray) -> None:
+    """SaveToFile(path, TBinaryReaderWriter) of a matrix (empty Name, the full matrix as its view)."""
+    from ._lib import lib
+    st = lib.b2m_WriteMatrixFile(path.encode(), _ptr(a), _lw(a), a.shape[1], a.shape[0])
+    if st != OK:
+        raise B2MError(st, f"{lib.b2m_status_string(st).decode()}: {path}")
+
+
 # ----------------------------------------------------------------------------- Cholesky
 def MatrixCholeskyInPlace4(A: np.ndarray, pnl_size: int = 0, ctx: Context | None = None) -> int:
     """A = L L^T, L in A's lower triangle (LinAlgCholesky.pas:106-123); 0 = crOk, 1 = not positive definite."""
@@ -386,6 +412,19 @@ class ResidentMatrix:
         m = cls(c, a.shape[0], a.shape[1])
         c.check(c.lib_call("b2m_upload", m.ptr, m.lw, _ptr(a), _lw(a), a.shape[0], a.shape[1]))
         return m
+
+    @classmethod
+    def from_file(cls, path: str, ctx: Context | None = None) -> tuple["ResidentMatrix", dict]:
+        """A saved TDoubleMatrix read straight into device memory (b2m_dev_ReadMatrixFile): the
+        full matrix and its saved sub-matrix view (apply it with `sub`)."""
+        from ._lib import MatrixInfo
+        c = _ctx_of(ctx)
+        info = MatrixInfo()
+        c.check(c.lib_call("b2m_dev_ReadMatrixFile", path.encode(), C.addressof(info), None, 0))
+        m = cls(c, info.height, info.width)
+        c.check(c.lib_call("b2m_dev_ReadMatrixFile", path.encode(), C.addressof(info), m.ptr, m.lw))
+        return m, {"sub_width": info.sub_width, "sub_height": info.sub_height, "offset_x": info.offset_x,
+                   "offset_y": info.offset_y}
 
     def to_host(self) -> np.ndarray:
         out = np.empty((self.rows, self.cols))

@@ -68,6 +68,26 @@ def test_resident_chain_and_sub_matrix_view(ctx):
             m.free()
 
 
+def test_saved_matrix_straight_to_device(ctx, tmp_path):
+    """A matrix saved in the reference's binary format is read into device memory and solved."""
+    n = 257
+    a = oracle.Mersenne(seed=257).uniform(n, n) - 0.5
+    path = str(tmp_path / "a.bin")
+    L.WriteMatrixFile(path, a)
+    A, view = L.ResidentMatrix.from_file(path, ctx=ctx)
+    assert view == {"sub_width": n, "sub_height": n, "offset_x": 0, "offset_y": 0}
+    try:
+        assert A.to_host().tobytes() == a.tobytes()
+        b = L.ResidentMatrix.from_host(np.ones((n, 1)), ctx=ctx)
+        st, X = A.solve(b)
+        _, x_ref = oracle.lineq_solve(a, np.ones((n, 1)), row_quirk=False)
+        assert st == 0 and np.linalg.norm(X.to_host() - x_ref) <= 1e-12 * np.linalg.norm(x_ref)
+        b.free()
+        X.free()
+    finally:
+        A.free()
+
+
 def test_contexts_on_every_visible_device():
     """Launch attributes are set per device: a context on each visible device solves correctly."""
     import torch
