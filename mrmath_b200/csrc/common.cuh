@@ -43,6 +43,7 @@ enum WsSlot : int {
     kWsF,
     kWsG,          // the mixed solve's X when the caller's buffer cannot be used directly
     kWsH,
+    kWsPmap,       // row maps of the blocked FP64 LU's outer panels
     kNumWs
 };
 

@@ -48,15 +48,16 @@ __device__ __forceinline__ void warp_argmax(T& a, int& i) {
 constexpr int kPanelW = 32;  // largest leaf width
 
 // ------------------------------------------------------------------------------------------
-// Row interchanges of one leaf, applied to every column outside the leaf's own columns and to
-// the permutation vector.  Warp 0 turns the <= 32 sequential swaps into a list of row moves.
+// Row interchanges of one leaf, applied to the columns [col_lo, col_hi) outside the leaf's own
+// columns, to the permutation vector and (when given) to the outer panel's row map.  Warp 0 turns
+// the <= 32 sequential swaps into a list of row moves.
 // ------------------------------------------------------------------------------------------
 constexpr int kSwapThreads = 256;
 
 template <typename T>
 __global__ void __launch_bounds__(kSwapThreads)
-    leaf_swap_kernel(T* A, int64_t ld, int ncols, int c0, int w, const int32_t* ipiv, int32_t* perm,
-                     const int32_t* status) {
+    leaf_swap_kernel(T* A, int64_t ld, int col_lo, int col_hi, int c0, int w, const int32_t* ipiv, int32_t* perm,
+                     int32_t* pmap, const int32_t* status) {
     __shared__ int src_main[kPanelW];
     __shared__ int mv_dst[2 * kPanelW], mv_src[2 * kPanelW];
     __shared__ int n_moves;
@@ -113,10 +114,9 @@ __global__ void __launch_bounds__(kSwapThreads)
     __syncthreads();
     const int nm = n_moves;
     if (nm == 0) return;
-    const int gc = blockIdx.x * kSwapThreads + tid;
-    const int skip = w;
-    const int col = gc < c0 ? gc : gc + skip;
-    if (col < ncols) {
+    const int gc = col_lo + blockIdx.x * kSwapThreads + tid;
+    const int col = gc < c0 ? gc : gc + w;  // the leaf's own columns are skipped
+    if (col < col_hi) {
         T v[2 * kPanelW];
 #pragma unroll
         for (int k = 0; k < 2 * kPanelW; ++k)
@@ -125,11 +125,74 @@ __global__ void __launch_bounds__(kSwapThreads)
         for (int k = 0; k < 2 * kPanelW; ++k)
             if (k < nm) A[(int64_t)mv_dst[k] * ld + col] = v[k];
     }
-    if (perm && blockIdx.x == 0) {
-        int pv = 0;
-        if (tid < nm) pv = perm[mv_src[tid]];
+    if ((perm || pmap) && blockIdx.x == 0) {
+        int pv = 0, qv = 0;
+        if (tid < nm) {
+            if (perm) pv = perm[mv_src[tid]];
+            if (pmap) qv = pmap[mv_src[tid]];
+        }
         __syncthreads();
-        if (tid < nm) perm[mv_dst[tid]] = pv;
+        if (tid < nm) {
+            if (perm) perm[mv_dst[tid]] = pv;
+            if (pmap) pmap[mv_dst[tid]] = qv;
+        }
+    }
+}
+
+// The outer panel's net row permutation applied to the columns [col_begin, col_end) outside it:
+// row i of the rows [oc0, n) receives what row pmap[i] held when the panel started.  CTA per 32
+// columns; each CTA lists the moved rows (at most 2 x 256 for a 256-column panel; warp-aggregated
+// appends) and loads all of their sources into registers before any write.
+constexpr int kPpMax = 512;
+__global__ void __launch_bounds__(256) panel_permute_f64_kernel(double* A, int64_t ld, int n, int oc0, int col_begin,
+                                                                int col_end, const int32_t* pmap, int32_t* status) {
+    __shared__ int s_dst[kPpMax], s_src[kPpMax], s_cnt;
+    if (status[kInfo] != 0) return;
+    const int t = threadIdx.x, lane = t & 31;
+    if (t == 0) s_cnt = 0;
+    __syncthreads();
+    constexpr int kScan = 16;  // row-map entries per thread per pass, all loaded before use
+    for (int p0 = oc0; p0 < n; p0 += 256 * kScan) {
+        int src[kScan];
+#pragma unroll
+        for (int u = 0; u < kScan; ++u) {
+            const int i = p0 + 256 * u + t;
+            src[u] = i < n ? pmap[i] : i;
+        }
+#pragma unroll
+        for (int u = 0; u < kScan; ++u) {
+            const int i = p0 + 256 * u + t;
+            const bool mv = src[u] != i;
+            const unsigned bal = __ballot_sync(0xffffffffu, mv);
+            if (!bal) continue;  // warp-uniform
+            int base = 0;
+            if (lane == 0) base = atomicAdd(&s_cnt, __popc(bal));
+            base = __shfl_sync(0xffffffffu, base, 0);
+            if (mv) {
+                const int k = base + __popc(bal & ((1u << lane) - 1u));
+                if (k < kPpMax) { s_dst[k] = i; s_src[k] = src[u]; }
+            }
+        }
+    }
+    __syncthreads();
+    const int cnt = s_cnt;
+    if (cnt > kPpMax) {  // a 256-column panel moves at most 512 rows; anything else is an internal error
+        if (t == 0) atomicExch(&status[kTimeout], 202);
+        return;
+    }
+    const int col = col_begin + blockIdx.x * 32 + lane, rg = t >> 5;
+    const bool ok = col < col_end;
+    double x[kPpMax / 8];
+#pragma unroll
+    for (int q = 0; q < kPpMax / 8; ++q) {
+        const int k = rg + 8 * q;
+        x[q] = (ok && k < cnt) ? A[(int64_t)s_src[k] * ld + col] : 0.0;
+    }
+    __syncthreads();  // every source of this CTA's columns is read before any row is written
+#pragma unroll
+    for (int q = 0; q < kPpMax / 8; ++q) {
+        const int k = rg + 8 * q;
+        if (ok && k < cnt) A[(int64_t)s_dst[k] * ld + col] = x[q];
     }
 }
 
@@ -263,16 +326,24 @@ void CUDART_CB progress_trampoline(void* p) {
     if (note->fn) note->fn(note->percent, note->user);
 }
 
+// the leaf's interchanges on columns [col_lo, col_hi) (which contain the leaf's own columns)
 template <typename T>
-int32_t launch_swaps_impl(Ctx* ctx, cudaStream_t st, T* A, int64_t ld, int ncols, int c0, int w, const int32_t* ipiv,
-                     int32_t* perm) {
-    const int other = ncols - w;
+int32_t launch_swaps_range(Ctx* ctx, cudaStream_t st, T* A, int64_t ld, int col_lo, int col_hi, int c0, int w,
+                           const int32_t* ipiv, int32_t* perm, int32_t* pmap) {
+    const int other = col_hi - col_lo - w;
     const int blocks = std::max(1, (int)ceil_div(other, kSwapThreads));
     prof_begin(ctx, st, kClsSwap);
-    leaf_swap_kernel<T><<<blocks, kSwapThreads, 0, st>>>(A, ld, ncols, c0, w, ipiv, perm, ctx->d_status);
+    leaf_swap_kernel<T><<<blocks, kSwapThreads, 0, st>>>(A, ld, col_lo, col_hi, c0, w, ipiv, perm, pmap,
+                                                         ctx->d_status);
     prof_end(ctx, st, kClsSwap, 4.0 * w * other * sizeof(T));  // <= 2w rows read + written
     B2M_LAUNCHED(ctx);
     return B2M_OK;
+}
+
+template <typename T>
+int32_t launch_swaps_impl(Ctx* ctx, cudaStream_t st, T* A, int64_t ld, int ncols, int c0, int w, const int32_t* ipiv,
+                     int32_t* perm) {
+    return launch_swaps_range<T>(ctx, st, A, ld, 0, ncols, c0, w, ipiv, perm, nullptr);
 }
 
 template <typename T>
@@ -321,13 +392,21 @@ int32_t trsm_upper_rec(Ctx* ctx, cudaStream_t st, const TriSolve& t, int64_t r0,
     return trsm_upper_rec(ctx, st, t, r0, br0, k1);
 }
 
+// where a leaf's interchanges go: the columns [col_lo, col_hi) (the whole matrix, or one outer
+// panel whose other columns are permuted once per panel through the row map pmap)
+struct SwapScope {
+    int64_t col_lo, col_hi;
+    int32_t* pmap;
+};
+
 // factor columns [c0, c0+width), rows [c0, n); leaves of at most `leaf` columns
 int32_t lu_rec(Ctx* ctx, cudaStream_t st, double* A, int64_t ld, int64_t n, int64_t c0, int64_t width,
-               int32_t* ipiv, int32_t* perm, int64_t leaf) {
+               int32_t* ipiv, int32_t* perm, int64_t leaf, const SwapScope& sc) {
     if (width <= leaf) {
         B2M_TRY(launch_panel<double>(ctx, st, A + c0 * ld + c0, ld, (int)(n - c0), (int)width, (int)c0, (int)c0,
                                      ipiv));
-        B2M_TRY(launch_swaps_impl<double>(ctx, st, A, ld, (int)n, (int)c0, (int)width, ipiv, perm));
+        B2M_TRY(launch_swaps_range<double>(ctx, st, A, ld, (int)sc.col_lo, (int)sc.col_hi, (int)c0, (int)width, ipiv,
+                                           perm, sc.pmap));
         if (ctx->progress && ctx->progress_notes.size() < ctx->progress_notes.capacity()) {
             // TLinEquProgress: columns factored * 100 div n, queued behind this panel
             ctx->progress_notes.push_back(
@@ -340,7 +419,7 @@ int32_t lu_rec(Ctx* ctx, cudaStream_t st, double* A, int64_t ld, int64_t n, int6
     // (8-column leaves then meet only in their own narrow K = 8 updates)
     const int64_t step = width > 16 ? std::max<int64_t>(leaf, 16) : leaf;
     const int64_t nleft = round_up((width + 1) / 2, step), nright = width - nleft;
-    B2M_TRY(lu_rec(ctx, st, A, ld, n, c0, nleft, ipiv, perm, leaf));
+    B2M_TRY(lu_rec(ctx, st, A, ld, n, c0, nleft, ipiv, perm, leaf, sc));
     // A12 <- L11^{-1} A12
     TriSolve t{A, ld, n, A, ld, n, n, c0 + nleft, nright};
     B2M_TRY(trsm_lower_rec(ctx, st, t, c0, c0, nleft));
@@ -349,7 +428,88 @@ int32_t lu_rec(Ctx* ctx, cudaStream_t st, double* A, int64_t ld, int64_t n, int6
     DOperand a{A, ld, n, n, r1, c0, true};
     DOperand b{A, ld, n, n, c0, r1, false};
     B2M_TRY(dgemm_tiled(ctx, st, a, b, A + r1 * ld + r1, ld, n - r1, nright, nleft, B2M_DO_SUB, true));
-    return lu_rec(ctx, st, A, ld, n, r1, nright, ipiv, perm, leaf);
+    return lu_rec(ctx, st, A, ld, n, r1, nright, ipiv, perm, leaf, sc);
+}
+
+constexpr int64_t kOuterNB = 256;  // outer panel width of the blocked FP64 LU
+
+// Blocked right-looking LU with look-ahead (orders n > 2 kOuterNB).  Per outer panel of 256
+// columns: (1) the panel is factored by the recursion above with its leaves' interchanges kept
+// inside the panel (each recorded in the row map pmap); (2) the panel's net permutation is applied
+// once to the columns right of it (this stream: the next step reads them) and left of it (side
+// stream); (3) U12 = L11^-1 A12 and A22 -= A21 U12 for the next panel's 256 columns on this stream;
+// (4) the same for every further column on the side stream, where it overlaps the next panel's
+// factorisation (which reads and writes only the next panel's columns) and is joined before the
+// next step's permutation moves rows under it.  The row map alternates between two buffers by panel
+// parity, because the side stream may still read one panel's map while the next panel fills its own.
+// Every interchange reaches every column exactly once and in order, so the factors and the pivot
+// vector are those of the unblocked recursion.
+int32_t lu_blocked(Ctx* ctx, cudaStream_t q, double* A, int64_t ld, int64_t n, int32_t* ipiv, int32_t* perm,
+                   int32_t* pmap2, int64_t leaf) {
+    cudaStream_t q2 = ctx->side_stream;
+    bool side_busy = false;
+    auto join = [&]() -> int32_t {
+        if (!side_busy) return B2M_OK;
+        B2M_CU(ctx, cudaEventRecord(ctx->ev_side_join, q2));
+        B2M_CU(ctx, cudaStreamWaitEvent(q, ctx->ev_side_join, 0));
+        side_busy = false;
+        return B2M_OK;
+    };
+    auto fork = [&]() -> int32_t {
+        B2M_CU(ctx, cudaEventRecord(ctx->ev_side_fork, q));
+        B2M_CU(ctx, cudaStreamWaitEvent(q2, ctx->ev_side_fork, 0));
+        side_busy = true;
+        return B2M_OK;
+    };
+    const int64_t pm_ld = round_up(n, 64);
+    for (int64_t k0 = 0; k0 < n; k0 += kOuterNB) {
+        const int64_t w = std::min(kOuterNB, n - k0), k1 = k0 + w;
+        int32_t* pmap = pmap2 + ((k0 / kOuterNB) & 1) * pm_ld;
+        iota_kernel<<<(unsigned)ceil_div(n, 256), 256, 0, q>>>(pmap, n);
+        B2M_LAUNCHED(ctx);
+        B2M_TRY(lu_rec(ctx, q, A, ld, n, k0, w, ipiv, perm, leaf, SwapScope{k0, k1, pmap}));
+        B2M_TRY(join());  // the previous panel's wide update is done before rows move under it
+        auto permute = [&](cudaStream_t qs, int64_t c_begin, int64_t c_end) -> int32_t {
+            if (c_end <= c_begin) return B2M_OK;
+            prof_begin(ctx, qs, kClsSwap);
+            panel_permute_f64_kernel<<<(unsigned)ceil_div(c_end - c_begin, 32), 256, 0, qs>>>(
+                A, ld, (int)n, (int)k0, (int)c_begin, (int)c_end, pmap, ctx->d_status);
+            prof_end(ctx, qs, kClsSwap, 2.0 * 8.0 * 2 * w * (double)(c_end - c_begin));  // <= 2w rows moved
+            B2M_LAUNCHED(ctx);
+            return B2M_OK;
+        };
+        B2M_TRY(permute(q, k1, n));
+        if (k0 > 0) {
+            B2M_TRY(fork());
+            B2M_TRY(permute(q2, 0, k0));
+        }
+        if (k1 >= n) break;
+        const int64_t rest = n - k1, nw = std::min(kOuterNB, rest);
+        auto update = [&](cudaStream_t qs, int64_t cs, int64_t nc) -> int32_t {
+            TriSolve t{A, ld, n, A, ld, n, n, cs, nc};
+            B2M_TRY(trsm_lower_rec(ctx, qs, t, k0, k0, w));
+            DOperand a{A, ld, n, n, k1, k0, true};
+            DOperand b{A, ld, n, n, k0, cs, false};
+            return dgemm_tiled(ctx, qs, a, b, A + k1 * ld + cs, ld, n - k1, nc, w, B2M_DO_SUB, true);
+        };
+        B2M_TRY(update(q, k1, nw));
+        if (rest > nw) {
+            B2M_TRY(fork());
+            B2M_TRY(update(q2, k1 + nw, rest - nw));
+        }
+    }
+    return join();
+}
+
+int32_t ensure_side_stream(Ctx* ctx) {
+    if (ctx->side_stream) return B2M_OK;
+    int least = 0, greatest = 0;
+    B2M_CU(ctx, cudaDeviceGetStreamPriorityRange(&least, &greatest));
+    B2M_CU(ctx, cudaStreamCreateWithPriority(&ctx->side_stream, cudaStreamNonBlocking, least));
+    B2M_CU(ctx, cudaEventCreateWithFlags(&ctx->ev_side_fork, cudaEventDisableTiming));
+    B2M_CU(ctx, cudaEventCreateWithFlags(&ctx->ev_side_join, cudaEventDisableTiming));
+    ctx->chain_priority = greatest;
+    return B2M_OK;
 }
 
 }  // namespace
@@ -385,13 +545,24 @@ int32_t lu_factor_f64(Ctx* ctx, cudaStream_t st, double* A, int64_t ld, int64_t 
         ctx->progress_notes.clear();
         ctx->progress_notes.reserve((size_t)(n / 8 + 2));
     }
+    // orders above 2 outer panels take the blocked look-ahead driver (row maps in a workspace); smaller
+    // ones (and every call of the allocation-free entry point, n <= 512) the plain recursion
+    const bool blocked = n > 2 * kOuterNB;
+    int32_t* pmap2 = nullptr;
+    if (blocked) {
+        void* p = nullptr;
+        B2M_TRY(ws_get(ctx, kWsPmap, (size_t)(2 * round_up(n, 64)) * sizeof(int32_t), &p));
+        pmap2 = static_cast<int32_t*>(p);
+        B2M_TRY(ensure_side_stream(ctx));
+    }
     const GraphKey key{1, A, ipiv, perm, ctx->d_status, ld, n, 0, 0};
     return run_graph(ctx, st, key, [&](cudaStream_t s) -> int32_t {
         if (perm) {
             iota_kernel<<<(unsigned)ceil_div(n, 256), 256, 0, s>>>(perm, n);
             B2M_LAUNCHED(ctx);
         }
-        return lu_rec(ctx, s, A, ld, n, 0, n, ipiv, perm, leaf);
+        if (blocked) return lu_blocked(ctx, s, A, ld, n, ipiv, perm, pmap2, leaf);
+        return lu_rec(ctx, s, A, ld, n, 0, n, ipiv, perm, leaf, SwapScope{0, n, nullptr});
     });
 }
 

@@ -754,7 +754,7 @@ size_t f32_scratch_bytes(int64_t n) {
     b += 3 * 32 * kNB * sizeof(float);                          // top, mvals, wmat
     b += 256 * sizeof(int);                                     // moves
     b += 32 * (size_t)kTsRows * sizeof(float);                  // root multipliers
-    b += (size_t)round_up(n, 64) * sizeof(int32_t);              // panel row map
+    b += 2 * (size_t)round_up(n, 64) * sizeof(int32_t);          // panel row maps (by panel parity)
     b += (size_t)kNB * 32 * sizeof(float);                      // leaf L11^-1 blocks
     b += 4 * (size_t)round_up(n, 32) * kNB * sizeof(float);     // bth, btl, ah, al
     b += 4 * (size_t)nblk * kTrsvNB * kTrsvNB * sizeof(float);  // diagonal inverses, coupling blocks
@@ -779,7 +779,7 @@ F32Scratch f32_scratch_carve(void* base, int64_t n) {
     s.wmat = reinterpret_cast<float*>(take(32 * kNB * sizeof(float)));
     s.moves = reinterpret_cast<int*>(take(256 * sizeof(int)));
     s.lmul = reinterpret_cast<float*>(take(32 * (size_t)kTsRows * sizeof(float)));
-    s.pmap = reinterpret_cast<int32_t*>(take((size_t)round_up(n, 64) * sizeof(int32_t)));
+    s.pmap = reinterpret_cast<int32_t*>(take(2 * (size_t)round_up(n, 64) * sizeof(int32_t)));
     s.lpinv = reinterpret_cast<float*>(take((size_t)kNB * 32 * sizeof(float)));
     const size_t panel = (size_t)round_up(n, 32) * kNB * sizeof(float);
     s.bth = reinterpret_cast<float*>(take(panel));
@@ -851,10 +851,14 @@ int32_t lu_factor_f32(Ctx* ctx, cudaStream_t st, float* A, int64_t ld, int64_t n
         B2M_LAUNCHED(ctx);
         for (int64_t oc0 = 0; oc0 < n; oc0 += kNB) {
             const int pw = (int)std::min<int64_t>(kNB, n - oc0);
+            // the row map alternates between two buffers by panel parity: the side stream may still
+            // be permuting the previous panel's left columns with its map while this panel's first
+            // leaf initialises the other one (the join below orders the reuse two panels later)
+            int32_t* pmap = s.pmap + ((oc0 / kNB) & 1) * round_up(n, 64);
             for (int64_t lc0 = oc0; lc0 < oc0 + pw; lc0 += 32) {
                 const int w = (int)std::min<int64_t>(32, n - lc0);
                 TsArgs ta{A, ld, (int)n, (int)lc0, w, (int)oc0, pw, s.cand, s.counters, s.top, s.mvals, s.wmat,
-                          s.moves, s.lmul, lc0 == oc0 ? s.pmap : nullptr, s.lpinv, ctx->d_status};
+                          s.moves, s.lmul, lc0 == oc0 ? pmap : nullptr, s.lpinv, ctx->d_status};
                 prof_begin(ctx, q, kClsPanel);
                 {
                     const cudaLaunchConfig_t c = cfg_of((unsigned)ceil_div(n - lc0, kTsRows), kTsThreads, 0);
@@ -862,7 +866,7 @@ int32_t lu_factor_f32(Ctx* ctx, cudaStream_t st, float* A, int64_t ld, int64_t n
                 }
                 prof_end(ctx, q, kClsPanel, 4.0 * (n - lc0) * 32);  // bytes: the leaf's columns, read once
                 B2M_LAUNCHED(ctx);
-                ApArgs aa{A, ld, (int)n, (int)lc0, w, (int)oc0, pw, s.top, s.mvals, s.wmat, s.moves, perm, s.pmap,
+                ApArgs aa{A, ld, (int)n, (int)lc0, w, (int)oc0, pw, s.top, s.mvals, s.wmat, s.moves, perm, pmap,
                           ctx->d_status, 0};
                 aa.nR = (int)ceil_div(n - lc0, kApRows);
                 prof_begin(ctx, q, kClsSwap);
@@ -886,7 +890,7 @@ int32_t lu_factor_f32(Ctx* ctx, cudaStream_t st, float* A, int64_t ld, int64_t n
                 c.stream = qs;
                 prof_begin(ctx, qs, kClsSwap);
                 B2M_CU(ctx, cudaLaunchKernelEx(&c, panel_permute_kernel, A, ld, (int)n, (int)oc0, (int)c_begin,
-                                               (int)c_end, (const int32_t*)s.pmap, ctx->d_status));
+                                               (int)c_end, (const int32_t*)pmap, ctx->d_status));
                 // bytes: at most 64 moved rows per leaf, read and written
                 prof_end(ctx, qs, kClsSwap, 8.0 * 64 * (pw / 32) * (double)(c_end - c_begin));
                 B2M_LAUNCHED(ctx);

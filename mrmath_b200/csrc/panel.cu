@@ -390,18 +390,22 @@ int32_t launch_push(Ctx* ctx, cudaStream_t st, int C, int R, T* P, int64_t ld, i
     }
     // whether a cluster of C CTAs fits on this device: 1 yes, -1 no, 0 not asked yet
     std::atomic<int>& sched = device_flag((const void*)kern, 1 + C, ctx->device);
-    cudaLaunchAttribute at[1];
+    cudaLaunchAttribute at[2];
     at[0].id = cudaLaunchAttributeClusterDimension;
     at[0].val.clusterDim.x = C;
     at[0].val.clusterDim.y = 1;
     at[0].val.clusterDim.z = 1;
+    // the panel is the factorisation's critical path: when a look-ahead trailing update runs beside
+    // it, its CTAs take free SMs ahead of the update's tiles
+    at[1].id = cudaLaunchAttributePriority;
+    at[1].val.priority = ctx->chain_priority;
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(C, 1, 1);
     cfg.blockDim = dim3(kPT, 1, 1);
     cfg.dynamicSmemBytes = smem;
     cfg.stream = st;
     cfg.attrs = at;
-    cfg.numAttrs = 1;
+    cfg.numAttrs = 2;
     if (C > 8 && sched.load() == 0) {
         int clusters = 0;
         B2M_CU(ctx, cudaOccupancyMaxActiveClusters(&clusters, kern, &cfg));

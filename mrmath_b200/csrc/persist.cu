@@ -50,10 +50,14 @@ int32_t parse_matrix(const std::vector<unsigned char>& raw, Parsed* out) {
         const unsigned char* payload = &raw[pos + kSectHeader + nlen];
         const size_t plen = (size_t)len - kSectHeader - nlen;
         switch (typ) {
-            case kBsObjectDescription:
-                is_mtx = plen == 3 && std::memcmp(payload, "MTX", 3) == 0;
+            case kBsObjectDescription: {
+                // TDoubleMatrix ("MTX"), TThreadedMatrix ("TMTX", ThreadedMatrix.pas:115-118) and the
+                // TB2MMatrix class of the Pascal binding ("B2MMTX") save the same properties
+                const std::string cls(reinterpret_cast<const char*>(payload), plen);
+                is_mtx = cls == "MTX" || cls == "TMTX" || cls == "B2MMTX";
                 if (!is_mtx) return B2M_ERR_FORMAT;  // another persisted class
                 break;
+            }
             case kBsInteger: {
                 if (plen != 4) return B2M_ERR_FORMAT;
                 int32_t v;

@@ -53,6 +53,19 @@ def test_reader_takes_any_section_order_names_case_and_views(tmp_path):
     assert view == {"sub_width": 2, "sub_height": 1, "offset_x": 1, "offset_y": 2}
 
 
+@pytest.mark.parametrize("cls", [b"TMTX", b"B2MMTX"])
+def test_reader_takes_derived_matrix_classes(tmp_path, cls):
+    """TThreadedMatrix ('TMTX') and the Pascal binding's TB2MMatrix ('B2MMTX') save the same props."""
+    from mrmath_b200 import linalg as L
+    data = np.arange(6.0).reshape(2, 3)
+    body = (b"RMCLS" + struct.pack("<I", 1) + _section(10, "obj", cls) + _section(5, "Width", struct.pack("<i", 3))
+            + _section(5, "Height", struct.pack("<i", 2)) + _section(3, "data", data.tobytes()) + _section(13, ""))
+    path = str(tmp_path / "d.bin")
+    open(path, "wb").write(body)
+    back, _ = L.ReadMatrixFile(path)
+    assert np.array_equal(back, data)
+
+
 def test_reader_rejects_other_streams(tmp_path):
     from mrmath_b200 import _lib, linalg as L
     bad = {
