@@ -298,6 +298,14 @@ B2M_API int32_t b2m_BatchLinEQSolve(b2m_ctx* ctx, int64_t count, const int32_t* 
 B2M_API int32_t b2m_dev_BatchLinEQSolve(b2m_ctx* ctx, int64_t count, const int32_t* n, const int32_t* nrhs,
                                         const int64_t* a_off, const int64_t* b_off, const double* A,
                                         const double* B, double* X, int32_t mode, int32_t* info, int32_t* iters);
+/* The autotuner's table, persisted: b2m_batch_tune_save writes every tuned plan (plan signature and
+ * its tile shape) to a text file; b2m_batch_tune_load merges such a file into the context, so that a
+ * later process skips the timing of the candidate shapes for those plans (*loaded = plans taken;
+ * lines with shapes the kernel does not have are skipped; B2M_ERR_FORMAT if the file is not a
+ * table).  The reference tunes its block sizes at start-up and keeps nothing
+ * (BlockSizeSetup.pas:169-297); this is the persisted form of that step. */
+B2M_API int32_t b2m_batch_tune_save(b2m_ctx* ctx, const char* path);
+B2M_API int32_t b2m_batch_tune_load(b2m_ctx* ctx, const char* path, int32_t* loaded);
 /* The tile shape the autotuner chose for the last batch plan. */
 B2M_API int32_t b2m_batch_tune_read(b2m_ctx* ctx, int32_t* small_n, int32_t* group_warps, int32_t* pw_large,
                                     int32_t* pw_small, float* ms);

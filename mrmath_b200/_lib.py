@@ -89,6 +89,8 @@ SIGNATURES: dict[str, tuple] = {
     "b2m_BatchLinEQSolve": (i32, [vp, i64, vp, vp, vp, vp, vp, vp, vp, i32, vp, vp]),
     "b2m_dev_BatchLinEQSolve": (i32, [vp, i64, vp, vp, vp, vp, vp, vp, vp, i32, vp, vp]),
     "b2m_batch_tune_read": (i32, [vp, vp, vp, vp, vp, vp]),
+    "b2m_batch_tune_save": (i32, [vp, C.c_char_p]),
+    "b2m_batch_tune_load": (i32, [vp, C.c_char_p, vp]),
     "b2m_MatrixLinEQSolveAdjoint": (i32, [vp, vp, i64, i64, vp, vp, i64, vp, i64, i64, vp, i64, vp, i64, i32]),
     "b2m_dev_MatrixLinEQSolveAdjoint": (i32, [vp, vp, i64, i64, vp, vp, i64, vp, i64, i64, vp, i64, vp, i64, i32]),
 }

@@ -642,3 +642,52 @@ int32_t batch_solve(Ctx* ctx, cudaStream_t st, int64_t count, const int32_t* hn,
 }
 
 }  // namespace b2m
+
+// ------------------------------------------------------------------ persisted autotuner table
+// One text line per batch plan: "<plan signature, hex> <small_n> <group_warps> <pw_large> <pw_small>
+// <ms>", after the header line "b2m-batch-tune 1".  A later process that loads the table skips the
+// timing of the candidate shapes for every plan it lists (the signature covers the mode, every
+// system's order, right-hand sides and offsets).
+extern "C" int32_t b2m_batch_tune_save(b2m_ctx* h, const char* path) {
+    b2m::Ctx* ctx = reinterpret_cast<b2m::Ctx*>(h);
+    if (!ctx || !path) return B2M_ERR_ARG;
+    std::lock_guard<std::mutex> lk(ctx->mtx);
+    FILE* f = std::fopen(path, "w");
+    if (!f) return b2m::fail(ctx, B2M_ERR_ARG, "cannot write %s", path);
+    std::fprintf(f, "b2m-batch-tune 1\n");
+    for (const auto& e : ctx->batch_tunes)
+        std::fprintf(f, "%016llx %d %d %d %d %.6f\n", (unsigned long long)e.first, e.second.small_n,
+                     e.second.group_warps, e.second.pw_large, e.second.pw_small, (double)e.second.ms);
+    return std::fclose(f) == 0 ? B2M_OK : b2m::fail(ctx, B2M_ERR_ARG, "cannot write %s", path);
+}
+
+extern "C" int32_t b2m_batch_tune_load(b2m_ctx* h, const char* path, int32_t* loaded) {
+    b2m::Ctx* ctx = reinterpret_cast<b2m::Ctx*>(h);
+    if (!ctx || !path) return B2M_ERR_ARG;
+    std::lock_guard<std::mutex> lk(ctx->mtx);
+    if (loaded) *loaded = 0;
+    FILE* f = std::fopen(path, "r");
+    if (!f) return b2m::fail(ctx, B2M_ERR_ARG, "cannot read %s", path);
+    char head[32] = {0};
+    int version = 0;
+    if (std::fscanf(f, "%31s %d", head, &version) != 2 || std::strcmp(head, "b2m-batch-tune") != 0 || version != 1) {
+        std::fclose(f);
+        return b2m::fail(ctx, B2M_ERR_FORMAT, "%s is not a batch tuning table", path);
+    }
+    unsigned long long sig;
+    int sn, g, pwl, pws;
+    double ms;
+    int n = 0;
+    while (std::fscanf(f, "%llx %d %d %d %d %lf", &sig, &sn, &g, &pwl, &pws, &ms) == 6) {
+        // only shapes the kernel has: a damaged or foreign line is skipped, never launched
+        const bool ok = sn == 64 && (g == 1 || g == 2 || g == 4) && (pwl == 8 || pwl == 16 || pwl == 32) &&
+                        (pws == 8 || pws == 16) &&
+                        b2m::batch_smem_bytes(sn, g, pwl, pws) <= ctx->smem_optin;
+        if (!ok) continue;
+        ctx->batch_tunes[(uint64_t)sig] = b2m::BatchTune{sn, g, pwl, pws, (float)ms};
+        ++n;
+    }
+    std::fclose(f);
+    if (loaded) *loaded = n;
+    return B2M_OK;
+}

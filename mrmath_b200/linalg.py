@@ -306,6 +306,18 @@ def batch_tune(ctx=None) -> dict:
             "pw_small": vals[3].value, "ms": ms.value}
 
 
+def batch_tune_save(path: str, ctx=None) -> None:
+    """Writes the autotuner's table (every tuned batch plan and its tile shape) to `path`."""
+    _ctx_of(ctx).call("b2m_batch_tune_save", path.encode())
+
+
+def batch_tune_load(path: str, ctx=None) -> int:
+    """Merges a saved autotuner table into the context; returns the number of plans taken."""
+    n = C.c_int32(0)
+    _ctx_of(ctx).call("b2m_batch_tune_load", path.encode(), C.addressof(n))
+    return n.value
+
+
 def dev_MatrixMultOzaki(dest, mt1, mt2, slices=8, op=DO_NONE, ctx=None):
     c = _ctx_of(ctx)
     _bind_stream(c, dest)

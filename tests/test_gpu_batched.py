@@ -81,3 +81,32 @@ def test_batch_device_twin_replay(ctx):
         assert oracle.backward_error(a, x, b) <= 4 * a.shape[0] * 2.0 ** -53
     t = L.batch_tune(ctx)
     assert t["group_warps"] in (1, 2, 4) and t["pw_large"] in (8, 16, 32)
+
+
+def test_autotune_table_persists_across_contexts(ctx, tmp_path):
+    """The tuned tile shape of a plan, saved by one context and loaded by a fresh one, is reused
+    (the second context launches the saved shape without timing the candidates) and gives the same
+    answers."""
+    import mrmath_b200
+    mats, rhss = _systems(14, 40)
+    xs, info, _ = L.BatchLinEQSolve(mats, rhss, mode=0, ctx=ctx)
+    path = str(tmp_path / "tune.txt")
+    L.batch_tune_save(path, ctx=ctx)
+    shape = {k: v for k, v in L.batch_tune(ctx).items() if k != "ms"}
+    c2 = mrmath_b200.Context(0)
+    try:
+        assert L.batch_tune_load(path, ctx=c2) >= 1
+        launches0 = c2.kernel_launches()
+        xs2, info2, _ = L.BatchLinEQSolve(mats, rhss, mode=0, ctx=c2)
+        # no autotuning: one graph of one batch launch, not two launches per candidate shape
+        assert c2.kernel_launches() - launches0 <= 2
+        assert {k: v for k, v in L.batch_tune(c2).items() if k != "ms"} == shape
+        assert np.array_equal(info, info2)
+        for x, y in zip(xs, xs2):
+            assert np.array_equal(x, y)
+    finally:
+        c2.close()
+    bad = tmp_path / "bad.txt"
+    bad.write_text("not a table\n")
+    with pytest.raises(Exception):
+        L.batch_tune_load(str(bad), ctx=ctx)
