@@ -210,6 +210,29 @@ B2M_API int32_t b2m_dev_MatrixLinEQSolve(b2m_ctx* ctx, const double* A, int64_t 
 B2M_API int32_t b2m_dev_MatrixInverseInPlace(b2m_ctx* ctx, double* A, int64_t LineWidthA, int64_t width, int32_t* status);
 B2M_API int32_t b2m_dev_MatrixDeterminant(b2m_ctx* ctx, const double* A, int64_t LineWidthA, int64_t width, double* det);
 
+/* ------------------------------------------------------------------ complex LU (LinAlgLU.pas:1147-1603)
+ * TComplex matrices: interleaved (real, imag) doubles, 16 bytes per element, strides in bytes.
+ * Pivoting as the reference's complex leaf: largest |re| + |im| (CAbs1), first maximum wins,
+ * singular when it is <= 10/MaxDouble; the column is scaled by CInv(pivot); back substitution
+ * divides by U's diagonal with CDiv (Smith's formula). */
+/* CplxMatrixLUDecompInPlace LinAlgLU.pas:1308-1320 */
+B2M_API int32_t b2m_CplxMatrixLUDecompInPlace(b2m_ctx* ctx, double* A, int64_t LineWidthA, int64_t width,
+                                              int32_t* indx);
+/* CplxMatrixLUBackSubst LinAlgLU.pas:1322-1391, generalised to nrhs columns of B */
+B2M_API int32_t b2m_CplxMatrixLUBackSubst(b2m_ctx* ctx, const double* LUDecomp, int64_t LineWidthLU, int64_t width,
+                                          const int32_t* indx, double* B, int64_t LineWidthB, int64_t nrhs);
+/* CplxMatrixLinEQSolve LinAlgLU.pas:1393-1508 (no refinement: the reference's refinement branch
+ * calls the real back substitution on complex data and is not reproduced) */
+B2M_API int32_t b2m_CplxMatrixLinEQSolve(b2m_ctx* ctx, const double* A, int64_t LineWidthA, int64_t width,
+                                         const double* B, int64_t LineWidthB, double* X, int64_t LineWidthX,
+                                         int64_t Width2);
+/* CplxMatrixInverseInPlace LinAlgLU.pas:1510-1552 (A untouched when singular) */
+B2M_API int32_t b2m_CplxMatrixInverseInPlace(b2m_ctx* ctx, double* A, int64_t LineWidthA, int64_t width);
+/* CplxMatrixDeterminant LinAlgLU.pas:1554-1603: det[0] = real, det[1] = imag; (0, 0) for a singular
+ * matrix with status B2M_OK */
+B2M_API int32_t b2m_CplxMatrixDeterminant(b2m_ctx* ctx, const double* A, int64_t LineWidthA, int64_t width,
+                                          double* det);
+
 /* ------------------------------------------------------------------ Cholesky (src/LinAlgCholesky.pas)
  * Results: 0 = crOk, 1 = crNoPositiveDefinite (TCholeskyResult, MatrixConst.pas:30): a diagonal
  * element <= 0 or NaN before its square root; A is then left unchanged. */

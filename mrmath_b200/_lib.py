@@ -63,6 +63,11 @@ SIGNATURES: dict[str, tuple] = {
     "b2m_profile_read": (i32, [vp, i32, C.POINTER(i64), C.POINTER(dbl), C.POINTER(dbl)]),
     "b2m_MatrixMultEx": (i32, [vp, vp, i64, vp, vp, i64, i64, i64, i64, i64, i64, i32, i32]),
     "b2m_dev_MatrixMultEx": (i32, [vp, vp, i64, vp, vp, i64, i64, i64, i64, i64, i64, i32, i32]),
+    "b2m_CplxMatrixLUDecompInPlace": (i32, [vp, vp, i64, i64, vp]),
+    "b2m_CplxMatrixLUBackSubst": (i32, [vp, vp, i64, i64, vp, vp, i64, i64]),
+    "b2m_CplxMatrixLinEQSolve": (i32, [vp, vp, i64, i64, vp, i64, vp, i64, i64]),
+    "b2m_CplxMatrixInverseInPlace": (i32, [vp, vp, i64, i64]),
+    "b2m_CplxMatrixDeterminant": (i32, [vp, vp, i64, i64, vp]),
     "b2m_MatrixCholeskyInPlace4": (i32, [vp, vp, i64, i64, i64]),
     "b2m_dev_MatrixCholeskyInPlace4": (i32, [vp, vp, i64, i64, vp]),
     "b2m_MatrixCholeskyInPlace": (i32, [vp, vp, i64, i64, vp, i64]),

@@ -970,3 +970,158 @@ extern "C" int32_t b2m_dev_MatrixCholeskySolveLinEq(b2m_ctx* h, const double* A,
     if (Xd != X) B2M_TRY(copy_matrix(ctx, ctx->stream, X, LineWidthX, Xd, ldx * 8, width, nrhs));
     return B2M_OK;
 }
+
+// ======================================================================================= complex LU
+namespace {
+
+// a TComplex matrix (16 bytes per element, byte stride) on the device as two planes
+struct ZPlanes {
+    double *re, *im;
+    int64_t ld;
+};
+
+bool zlw_ok(int64_t lw, int64_t cols) { return lw >= cols * 16 && (lw % 16) == 0; }
+
+// host TComplex rows x cols -> planes in `slot` (the interleaved staging copy goes to kWsF)
+int32_t z_upload(Ctx* ctx, int slot, const double* host, int64_t lw, int64_t rows, int64_t cols, ZPlanes* out) {
+    const int64_t ld = padded_ld(cols);
+    void *pp, *ps;
+    B2M_TRY(ws_get(ctx, slot, (size_t)(2 * std::max<int64_t>(rows, 1) * ld * 8), &pp));
+    const int64_t lds = round_up(cols * 16, 128);
+    B2M_TRY(ws_get(ctx, kWsF, (size_t)(std::max<int64_t>(rows, 1) * lds), &ps));
+    *out = ZPlanes{(double*)pp, (double*)pp + rows * ld, ld};
+    B2M_CU(ctx, cudaMemcpy2DAsync(ps, lds, host, lw, cols * 16, rows, cudaMemcpyHostToDevice, ctx->stream));
+    return z_deinterleave(ctx, ctx->stream, (const double*)ps, lds, out->re, out->im, ld, rows, cols);
+}
+
+int32_t z_download(Ctx* ctx, const ZPlanes& p, double* host, int64_t lw, int64_t rows, int64_t cols, bool only_if_ok) {
+    const int64_t lds = round_up(cols * 16, 128);
+    void* ps;
+    B2M_TRY(ws_get(ctx, kWsF, (size_t)(std::max<int64_t>(rows, 1) * lds), &ps));
+    if (only_if_ok)  // keep the caller's data when the factorisation stopped: stage it first
+        B2M_CU(ctx, cudaMemcpy2DAsync(ps, lds, host, lw, cols * 16, rows, cudaMemcpyHostToDevice, ctx->stream));
+    B2M_TRY(z_interleave(ctx, ctx->stream, (double*)ps, lds, p.re, p.im, p.ld, rows, cols, only_if_ok));
+    B2M_CU(ctx, cudaMemcpy2DAsync(host, lw, ps, lds, cols * 16, rows, cudaMemcpyDeviceToHost, ctx->stream));
+    return B2M_OK;
+}
+
+int32_t z_factor_host(Ctx* ctx, const double* A, int64_t lwA, int64_t n, ZPlanes* P, int32_t** dpiv, int32_t** dperm) {
+    B2M_TRY(z_upload(ctx, kWsMatA, A, lwA, n, n, P));
+    void* pp;
+    B2M_TRY(ws_get(ctx, kWsPiv, (size_t)(2 * n * 4), &pp));
+    *dpiv = (int32_t*)pp;
+    *dperm = *dpiv + n;
+    B2M_CU(ctx, cudaMemsetAsync(*dpiv, 0, (size_t)n * 4, ctx->stream));
+    B2M_TRY(reset_status(ctx));
+    return zlu_factor(ctx, ctx->stream, P->re, P->im, P->ld, n, *dpiv, *dperm);
+}
+
+}  // namespace
+
+extern "C" int32_t b2m_CplxMatrixLUDecompInPlace(b2m_ctx* h, double* A, int64_t LineWidthA, int64_t width,
+                                                 int32_t* indx) {
+    Ctx* ctx = as_ctx(h);
+    if (!ctx) return B2M_ERR_ARG;
+    std::lock_guard<std::mutex> lk(ctx->mtx);
+    if (!A || !indx) return fail(ctx, B2M_ERR_ARG, "null pointer");
+    if (width <= 0 || !zlw_ok(LineWidthA, width)) return fail(ctx, B2M_ERR_DIM, "Dimension Error");
+    cudaSetDevice(ctx->device);
+    std::memset(indx, 0, (size_t)width * sizeof(int32_t));
+    ZPlanes P;
+    int32_t *dpiv, *dperm;
+    B2M_TRY(z_factor_host(ctx, A, LineWidthA, width, &P, &dpiv, &dperm));
+    B2M_TRY(z_download(ctx, P, A, LineWidthA, width, width, false));
+    B2M_CU(ctx, cudaMemcpyAsync(indx, dpiv, (size_t)width * 4, cudaMemcpyDeviceToHost, ctx->stream));
+    return finish(ctx);
+}
+
+extern "C" int32_t b2m_CplxMatrixLUBackSubst(b2m_ctx* h, const double* LUDecomp, int64_t LineWidthLU, int64_t width,
+                                             const int32_t* indx, double* B, int64_t LineWidthB, int64_t nrhs) {
+    Ctx* ctx = as_ctx(h);
+    if (!ctx) return B2M_ERR_ARG;
+    std::lock_guard<std::mutex> lk(ctx->mtx);
+    if (!LUDecomp || !indx || !B) return fail(ctx, B2M_ERR_ARG, "null pointer");
+    if (width <= 0 || nrhs <= 0 || !zlw_ok(LineWidthLU, width) || !zlw_ok(LineWidthB, nrhs))
+        return fail(ctx, B2M_ERR_DIM, "Dimension Error");
+    cudaSetDevice(ctx->device);
+    ZPlanes L, X;
+    B2M_TRY(z_upload(ctx, kWsMatA, LUDecomp, LineWidthLU, width, width, &L));
+    B2M_TRY(z_upload(ctx, kWsMatB, B, LineWidthB, width, nrhs, &X));
+    void *pp, *pt;
+    B2M_TRY(ws_get(ctx, kWsPiv, (size_t)(2 * width * 4), &pp));
+    B2M_TRY(ws_get(ctx, kWsE, (size_t)(2 * width * X.ld * 8), &pt));
+    int32_t* dpiv = (int32_t*)pp;
+    B2M_CU(ctx, cudaMemcpyAsync(dpiv, indx, (size_t)width * 4, cudaMemcpyHostToDevice, ctx->stream));
+    B2M_TRY(reset_status(ctx));
+    B2M_TRY(perm_from_ipiv(ctx, ctx->stream, dpiv, width, dpiv + width));
+    B2M_TRY(zlu_solve(ctx, ctx->stream, L.re, L.im, L.ld, width, dpiv + width, X.re, X.im, X.ld, nrhs, (double*)pt,
+                      (double*)pt + width * X.ld));
+    B2M_TRY(z_download(ctx, X, B, LineWidthB, width, nrhs, false));
+    return finish(ctx);
+}
+
+extern "C" int32_t b2m_CplxMatrixLinEQSolve(b2m_ctx* h, const double* A, int64_t LineWidthA, int64_t width,
+                                            const double* B, int64_t LineWidthB, double* X, int64_t LineWidthX,
+                                            int64_t Width2) {
+    Ctx* ctx = as_ctx(h);
+    if (!ctx) return B2M_ERR_ARG;
+    std::lock_guard<std::mutex> lk(ctx->mtx);
+    if (!A || !B || !X) return fail(ctx, B2M_ERR_ARG, "null pointer");
+    if (width <= 0 || Width2 <= 0 || !zlw_ok(LineWidthA, width) || !zlw_ok(LineWidthB, Width2) ||
+        !zlw_ok(LineWidthX, Width2))
+        return fail(ctx, B2M_ERR_DIM, "Dimension Error");
+    cudaSetDevice(ctx->device);
+    ZPlanes P, Xp;
+    int32_t *dpiv, *dperm;
+    B2M_TRY(z_factor_host(ctx, A, LineWidthA, width, &P, &dpiv, &dperm));
+    B2M_TRY(z_upload(ctx, kWsMatB, B, LineWidthB, width, Width2, &Xp));
+    void* pt;
+    B2M_TRY(ws_get(ctx, kWsE, (size_t)(2 * width * Xp.ld * 8), &pt));
+    B2M_TRY(zlu_solve(ctx, ctx->stream, P.re, P.im, P.ld, width, dperm, Xp.re, Xp.im, Xp.ld, Width2, (double*)pt,
+                      (double*)pt + width * Xp.ld));
+    B2M_TRY(z_download(ctx, Xp, X, LineWidthX, width, Width2, false));
+    return finish(ctx);
+}
+
+extern "C" int32_t b2m_CplxMatrixInverseInPlace(b2m_ctx* h, double* A, int64_t LineWidthA, int64_t width) {
+    Ctx* ctx = as_ctx(h);
+    if (!ctx) return B2M_ERR_ARG;
+    std::lock_guard<std::mutex> lk(ctx->mtx);
+    if (!A) return fail(ctx, B2M_ERR_ARG, "null pointer");
+    if (width <= 0 || !zlw_ok(LineWidthA, width)) return fail(ctx, B2M_ERR_DIM, "Dimension Error");
+    cudaSetDevice(ctx->device);
+    ZPlanes P;
+    int32_t *dpiv, *dperm;
+    B2M_TRY(z_factor_host(ctx, A, LineWidthA, width, &P, &dpiv, &dperm));
+    // the columns of the inverse: solves with the identity (CplxMatrixInverseInPlace :1531-1548)
+    const int64_t ld = padded_ld(width);
+    void *pi, *pt;
+    B2M_TRY(ws_get(ctx, kWsMatB, (size_t)(2 * width * ld * 8), &pi));
+    B2M_TRY(ws_get(ctx, kWsE, (size_t)(2 * width * ld * 8), &pt));
+    ZPlanes I{(double*)pi, (double*)pi + width * ld, ld};
+    B2M_CU(ctx, cudaMemsetAsync(pi, 0, (size_t)(2 * width * ld * 8), ctx->stream));
+    B2M_TRY(set_diagonal(ctx, ctx->stream, I.re, ld, width, 1.0));
+    B2M_TRY(zlu_solve(ctx, ctx->stream, P.re, P.im, P.ld, width, dperm, I.re, I.im, ld, width, (double*)pt,
+                      (double*)pt + width * ld));
+    B2M_TRY(z_download(ctx, I, A, LineWidthA, width, width, true));  // A is left as it was when singular
+    return finish(ctx);
+}
+
+extern "C" int32_t b2m_CplxMatrixDeterminant(b2m_ctx* h, const double* A, int64_t LineWidthA, int64_t width,
+                                             double* det) {
+    Ctx* ctx = as_ctx(h);
+    if (!ctx) return B2M_ERR_ARG;
+    std::lock_guard<std::mutex> lk(ctx->mtx);
+    if (!A || !det) return fail(ctx, B2M_ERR_ARG, "null pointer");
+    if (width <= 0 || !zlw_ok(LineWidthA, width)) return fail(ctx, B2M_ERR_DIM, "Dimension error");
+    cudaSetDevice(ctx->device);
+    ZPlanes P;
+    int32_t *dpiv, *dperm;
+    B2M_TRY(z_factor_host(ctx, A, LineWidthA, width, &P, &dpiv, &dperm));
+    void* pd;
+    B2M_TRY(ws_get(ctx, kWsSmall, 2 * sizeof(double), &pd));
+    B2M_TRY(z_determinant(ctx, ctx->stream, P.re, P.im, P.ld, width, dpiv, (double*)pd));
+    B2M_CU(ctx, cudaMemcpyAsync(det, pd, 2 * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    const int32_t r = finish(ctx);
+    return r == B2M_SINGULAR ? B2M_OK : r;  // a singular matrix has determinant 0, status leOk (:1578-1584)
+}

@@ -74,6 +74,22 @@ int32_t split_nr(Ctx* ctx, cudaStream_t st, double* Lnr, int64_t ldl, double* P,
 int32_t join_nr(Ctx* ctx, cudaStream_t st, double* F, int64_t ldf, const double* Lnr, int64_t ldl, const double* P,
                 int64_t lwp, int64_t n);
 
+// Complex LU (zlu.cu) on split real / imaginary planes (row stride ld, even, 16-byte aligned):
+// zlu_factor in place with the reference's CAbs1 pivot rule (ipiv as the reference's, perm the row
+// permutation, may be null); zlu_solve overwrites B (planes, ldb) with X using the factors, perm and
+// the scratch planes tre/tim (n x ldb); z_(de)interleave convert between TComplex arrays (byte
+// stride) and planes; z_determinant writes (re, im) to d_det2.
+int32_t zlu_factor(Ctx* ctx, cudaStream_t st, double* re, double* im, int64_t ld, int64_t n, int32_t* ipiv,
+                   int32_t* perm);
+int32_t zlu_solve(Ctx* ctx, cudaStream_t st, const double* lre, const double* lim, int64_t ld, int64_t n,
+                  const int32_t* perm, double* bre, double* bim, int64_t ldb, int64_t nrhs, double* tre, double* tim);
+int32_t z_deinterleave(Ctx* ctx, cudaStream_t st, const double* src, int64_t lws, double* re, double* im, int64_t ld,
+                       int64_t rows, int64_t cols);
+int32_t z_interleave(Ctx* ctx, cudaStream_t st, double* dst, int64_t lwd, const double* re, const double* im,
+                     int64_t ld, int64_t rows, int64_t cols, bool only_if_ok);
+int32_t z_determinant(Ctx* ctx, cudaStream_t st, const double* re, const double* im, int64_t ld, int64_t n,
+                      const int32_t* ipiv, double* d_det2);
+
 // Builds perm from ipiv on the device (used when factors come from outside: b2m_MatrixLUBackSubst).
 int32_t perm_from_ipiv(Ctx* ctx, cudaStream_t st, const int32_t* ipiv, int64_t n, int32_t* perm);
 

@@ -364,6 +364,43 @@ def WriteMatrixFile(path: str, a: np.ndarray) -> None:
         raise B2MError(st, f"{lib.b2m_status_string(st).decode()}: {path}")
 
 
+# ----------------------------------------------------------------------------- complex LU
+def _zlw(a: np.ndarray) -> int:
+    if a.ndim != 2 or a.dtype != np.complex128 or a.strides[1] != 16:
+        raise ValueError("expected a 2-D complex128 row-major array (rows may be padded)")
+    return a.strides[0]
+
+
+def CplxMatrixLUDecompInPlace(A: np.ndarray, ctx: Context | None = None):
+    """CplxMatrixLUDecompInPlace (LinAlgLU.pas:1308-1320) on a complex128 array; (status, indx)."""
+    indx = np.zeros(A.shape[1], dtype=np.int32)
+    st = _ctx_of(ctx).call("b2m_CplxMatrixLUDecompInPlace", _ptr(A), _zlw(A), A.shape[1], indx.ctypes.data,
+                           allow=(OK, SINGULAR))
+    return st, indx
+
+
+def CplxMatrixLUBackSubst(LU: np.ndarray, indx: np.ndarray, B: np.ndarray, ctx: Context | None = None) -> None:
+    _ctx_of(ctx).call("b2m_CplxMatrixLUBackSubst", _ptr(LU), _zlw(LU), LU.shape[1], indx.ctypes.data, _ptr(B),
+                      _zlw(B), B.shape[1])
+
+
+def CplxMatrixLinEQSolve(A: np.ndarray, B: np.ndarray, ctx: Context | None = None):
+    X = np.zeros(B.shape, dtype=np.complex128)
+    st = _ctx_of(ctx).call("b2m_CplxMatrixLinEQSolve", _ptr(A), _zlw(A), A.shape[1], _ptr(B), _zlw(B), _ptr(X),
+                           _zlw(X), B.shape[1], allow=(OK, SINGULAR))
+    return st, X
+
+
+def CplxMatrixInverseInPlace(A: np.ndarray, ctx: Context | None = None) -> int:
+    return _ctx_of(ctx).call("b2m_CplxMatrixInverseInPlace", _ptr(A), _zlw(A), A.shape[1], allow=(OK, SINGULAR))
+
+
+def CplxMatrixDeterminant(A: np.ndarray, ctx: Context | None = None) -> complex:
+    det = np.zeros(2)
+    _ctx_of(ctx).call("b2m_CplxMatrixDeterminant", _ptr(A), _zlw(A), A.shape[1], _ptr(det))
+    return complex(det[0], det[1])
+
+
 # ----------------------------------------------------------------------------- Cholesky
 def MatrixCholeskyInPlace4(A: np.ndarray, pnl_size: int = 0, ctx: Context | None = None) -> int:
     """A = L L^T, L in A's lower triangle (LinAlgCholesky.pas:106-123); 0 = crOk, 1 = not positive definite."""

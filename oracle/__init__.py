@@ -72,6 +72,11 @@ def _load():
         "orc_residual_dot2": (None, [_pd, _i64, _i64, _pd, _i64, _pd, _i64, _i64, _pd, _i64]),
         "orc_backward_error": (_dbl, [_pd, _i64, _i64, _pd, _i64, _pd, _i64, _i64]),
         "orc_gemm_rows_dot2": (None, [_pd, _i64, _pd, _i64, _i64, _i64, _i64, _i64, _i64, _pd, _i64, _pd, _i64]),
+        "orc_cplx_lu_decomp_inplace": (_i32, [_pd, _i64, _i64, _pi]),
+        "orc_cplx_lu_backsubst": (None, [_pd, _i64, _i64, _pi, _pd, _i64]),
+        "orc_cplx_lineq_solve": (_i32, [_pd, _i64, _i64, _pd, _i64, _pd, _i64, _i64]),
+        "orc_cplx_inverse_inplace": (_i32, [_pd, _i64, _i64]),
+        "orc_cplx_determinant": (None, [_pd, _i64, _i64, _pd]),
         "orc_cholesky_inplace4": (_i32, [_pd, _i64, _i64, _i64]),
         "orc_cholesky_inplace2": (_i32, [_pd, _i64, _i64]),
         "orc_cholesky_nr": (_i32, [_pd, _i64, _i64, _pd, _i64]),
@@ -287,3 +292,38 @@ def cholesky_solve_nr(a: np.ndarray, p: np.ndarray, b: np.ndarray) -> np.ndarray
     x = np.zeros_like(b)
     lib.orc_cholesky_solve_nr(_p(a), _lw(a), a.shape[1], _p(p), _lw(p), _p(b), _lw(b), _p(x), _lw(x))
     return x
+
+
+# ------------------------------------------------------------------ complex LU (LinAlgLU.pas:1147-1603)
+def _pc(a: np.ndarray):
+    assert a.dtype == np.complex128 and a.ndim == 2 and a.strides[1] == 16
+    return a.ctypes.data_as(_pd)
+
+
+def cplx_lu_decomp_inplace(a: np.ndarray) -> tuple[int, np.ndarray]:
+    """CplxMatrixLUDecompInPlace on a complex128 array (TComplex = (real, imag) doubles)."""
+    indx = np.zeros(a.shape[1], dtype=np.int32)
+    rc = lib.orc_cplx_lu_decomp_inplace(_pc(a), a.strides[0], a.shape[1], _pi32(indx))
+    return rc, indx
+
+
+def cplx_lu_backsubst(lu: np.ndarray, indx: np.ndarray, b: np.ndarray) -> None:
+    """CplxMatrixLUBackSubst in place on column 0 of b."""
+    lib.orc_cplx_lu_backsubst(_pc(lu), lu.strides[0], lu.shape[1], _pi32(indx), _pc(b), b.strides[0])
+
+
+def cplx_lineq_solve(a: np.ndarray, b: np.ndarray) -> tuple[int, np.ndarray]:
+    x = np.zeros(b.shape, dtype=np.complex128)
+    rc = lib.orc_cplx_lineq_solve(_pc(a), a.strides[0], a.shape[1], _pc(b), b.strides[0], _pc(x), x.strides[0],
+                                  b.shape[1])
+    return rc, x
+
+
+def cplx_inverse_inplace(a: np.ndarray) -> int:
+    return lib.orc_cplx_inverse_inplace(_pc(a), a.strides[0], a.shape[1])
+
+
+def cplx_determinant(a: np.ndarray) -> complex:
+    out = np.zeros(2)
+    lib.orc_cplx_determinant(_pc(a), a.strides[0], a.shape[1], _p(out))
+    return complex(out[0], out[1])

@@ -1018,6 +1018,256 @@ extern "C" double orc_backward_error(const double* A, int64_t lwA, int64_t n, co
     return eta;
 }
 
+// ---------------- complex LU (LinAlgLU.pas:1147-1603) ---------------------------------------------------------
+// TComplex = record real, imag : double (16 bytes); the arithmetic helpers of CplxSimpleMatrixOperations.pas
+// are restated with their evaluation order (the oracle is compiled without FP contraction).
+namespace {
+
+struct Cx {
+    double re, im;
+};
+inline Cx* crow(void* A, int64_t r, int64_t lw) { return reinterpret_cast<Cx*>(static_cast<char*>(A) + r * lw); }
+inline const Cx* crow(const void* A, int64_t r, int64_t lw) {
+    return reinterpret_cast<const Cx*>(static_cast<const char*>(A) + r * lw);
+}
+inline double cabs1(Cx v) { return std::fabs(v.re) + std::fabs(v.im); }                       // :208-211
+inline void cinc_mul(Cx& x1, Cx x2, Cx x3) {                                                   // CIncMul
+    x1.re = x1.re + x2.re * x3.re - x2.im * x3.im;
+    x1.im = x1.im + x2.re * x3.im + x2.im * x3.re;
+}
+inline Cx cadd_mul(Cx x1, Cx x2, Cx x3) {                                                      // CAddMul
+    return Cx{x1.re + x2.re * x3.re - x2.im * x3.im, x1.im + x2.re * x3.im + x2.im * x3.re};
+}
+inline Cx csub_mul(Cx x1, Cx x2, Cx x3) {                                                      // CSubMul
+    return Cx{x1.re - x2.re * x3.re + x2.im * x3.im, x1.im - x2.re * x3.im - x2.im * x3.re};
+}
+inline Cx cmul(Cx a, Cx b) { return Cx{a.re * b.re - a.im * b.im, a.re * b.im + a.im * b.re}; }  // CMul
+inline Cx cdiv(Cx x1, Cx x2) {                                                                 // CDiv (Smith)
+    if (std::fabs(x2.re) >= std::fabs(x2.im)) {
+        const double r = x2.im / x2.re, den = x2.re + x2.im * r;
+        return Cx{(x1.re + r * x1.im) / den, (x1.im - r * x1.re) / den};
+    }
+    const double r = x2.re / x2.im, den = x2.im + x2.re * r;
+    return Cx{(x1.re * r + x1.im) / den, (x1.im * r - x1.re) / den};
+}
+inline Cx cinv(Cx x1) {                                                                        // CInv
+    if (std::fabs(x1.re) >= std::fabs(x1.im)) {
+        const double r = x1.im / x1.re, den = x1.re + x1.im * r;
+        return Cx{1.0 / den, -r / den};
+    }
+    const double r = x1.re / x1.im, den = x1.im + r * x1.re;
+    return Cx{r / den, -1.0 / den};
+}
+
+// CplxGenericMtxMult CplxSimpleMatrixOperations.pas:983-1013: dest = mt1 mt2, sums from (0, 0) in order
+void cplx_mult(void* dest, int64_t lwd, const void* mt1, const void* mt2, int64_t w1, int64_t h1, int64_t w2,
+               int64_t lw1, int64_t lw2) {
+    for (int64_t y = 0; y < h1; ++y)
+        for (int64_t x = 0; x < w2; ++x) {
+            Cx s{0.0, 0.0};
+            for (int64_t k = 0; k < w1; ++k) cinc_mul(s, crow(mt1, y, lw1)[k], crow(mt2, k, lw2)[x]);
+            crow(dest, y, lwd)[x] = s;
+        }
+}
+
+// CplxGenericBlockMatrixMultiplication BlockedMult.pas:837-920 with op doSub: dest -= mt1 mt2 through
+// blockSize blocks, each block's products summed over the k-blocks into actBlk, then subtracted
+void cplx_block_mult_sub(void* dest, int64_t lwd, const void* mt1, const void* mt2, int64_t w1, int64_t h1,
+                         int64_t w2, int64_t lw1, int64_t lw2, int64_t bs) {
+    if (w1 == 0 || w2 == 0 || h1 == 0) return;
+    const bool h1Fit = (h1 % bs) == 0, w2Fit = (w2 % bs) == 0, w1Fit = (w1 % bs) == 0;
+    const int64_t h = h1 / bs + (h1Fit ? 0 : 1) - 1, w = w2 / bs + (w2Fit ? 0 : 1) - 1;
+    const int64_t gamma = w1 / bs + (w1Fit ? 0 : 1) - 1;
+    std::vector<Cx> act((size_t)(bs * bs)), mult((size_t)(bs * bs));
+    const int64_t bl = bs * 16;
+    for (int64_t by = 0; by <= h; ++by) {
+        const int64_t bh = (by == h && !h1Fit) ? h1 % bs : bs;
+        for (int64_t bx = 0; bx <= w; ++bx) {
+            const int64_t bw = (bx == w && !w2Fit) ? w2 % bs : bs;
+            std::fill(act.begin(), act.end(), Cx{0.0, 0.0});
+            for (int64_t idx = 0; idx <= gamma; ++idx) {
+                const int64_t gw = (idx == gamma && !w1Fit) ? w1 % bs : bs;
+                const Cx* pa = crow(mt1, by * bs, lw1) + idx * bs;
+                const Cx* pb = crow(mt2, idx * bs, lw2) + bx * bs;
+                cplx_mult(mult.data(), bl, pa, pb, gw, bh, bw, lw1, lw2);
+                for (int64_t y = 0; y < bh; ++y)
+                    for (int64_t x = 0; x < bw; ++x) {
+                        Cx& a = act[(size_t)(y * bs + x)];
+                        const Cx m = mult[(size_t)(y * bs + x)];
+                        a = Cx{a.re + m.re, a.im + m.im};
+                    }
+            }
+            for (int64_t y = 0; y < bh; ++y)
+                for (int64_t x = 0; x < bw; ++x) {
+                    Cx& d = crow(dest, by * bs + y, lwd)[bx * bs + x];
+                    const Cx a = act[(size_t)(y * bs + x)];
+                    d = Cx{d.re - a.re, d.im - a.im};
+                }
+        }
+    }
+}
+
+void cplx_lu_swap(void* A, int64_t lw, int64_t width, int64_t k1, int64_t k2, const int32_t* indx) {  // :1183-1200
+    for (int64_t i = k1; i <= k2; ++i)
+        if (indx[i] != i)
+            for (int64_t x = 0; x < width; ++x) std::swap(crow(A, i, lw)[x], crow(A, indx[i], lw)[x]);
+}
+
+void cplx_lu_backsup(const void* A, int64_t width, int64_t height, void* B, int64_t lw) {  // :1147-1181
+    for (int64_t k = 0; k < height; ++k)
+        for (int64_t i = k + 1; i < height; ++i) {
+            const Cx aik = crow(A, i, lw)[k];
+            for (int64_t j = 0; j < width; ++j)
+                crow(B, i, lw)[j] = csub_mul(crow(B, i, lw)[j], crow(B, k, lw)[j], aik);
+        }
+}
+
+// InternalRecursiveCplxMatrixLUDecompInPlace :1202-1306 (cBlkMultSize = 48)
+int32_t cplx_rec_lu(void* A, int64_t width, int64_t height, int32_t* indx, int64_t lw) {
+    const int64_t mn = std::min(width, height);
+    if (mn > 1) {
+        const int64_t nleft = mn / 2, nright = width - nleft;
+        int32_t r = cplx_rec_lu(A, nleft, height, indx, lw);
+        if (r != 0) return r;
+        Cx* pA = crow(A, 0, lw) + nleft;
+        cplx_lu_swap(pA, lw, nright, 0, nleft - 1, indx);
+        if (nright > 1) cplx_lu_backsup(A, nright, nleft, pA, lw);
+        Cx* pB = crow(A, nleft, lw) + nleft;
+        const Cx* a21 = crow(A, nleft, lw);
+        if (nright > 48 || height - nleft > 48) {
+            cplx_block_mult_sub(pB, lw, a21, pA, nleft, height - nleft, nright, lw, lw, 48);
+        } else {
+            const int64_t lwb = (nright + (nright & 1)) * 16;
+            std::vector<Cx> mem((size_t)((nright + 1) * (height - nleft + 1)));
+            cplx_mult(mem.data(), lwb, a21, pA, nleft, height - nleft, nright, lw, lw);
+            for (int64_t y = 0; y < height - nleft; ++y)
+                for (int64_t x = 0; x < nright; ++x) {
+                    Cx& d = crow(pB, y, lw)[x];
+                    const Cx m = crow(mem.data(), y, lwb)[x];
+                    d = Cx{d.re - m.re, d.im - m.im};
+                }
+        }
+        r = cplx_rec_lu(pB, nright, height - nleft, indx + nleft, lw);
+        if (r != 0) return r;
+        for (int64_t i = nleft; i < width; ++i) indx[i] += (int32_t)nleft;
+        cplx_lu_swap(A, lw, nleft, nleft, mn - 1, indx);
+        return 0;
+    }
+    Cx maxVal{0.0, 0.0};
+    double absMax = 0.0;
+    int64_t idx = -1;
+    for (int64_t i = 0; i < height; ++i) {
+        const double av = cabs1(crow(A, i, lw)[0]);
+        if (av > absMax) {
+            idx = i;
+            maxVal = crow(A, i, lw)[0];
+            absMax = av;
+        }
+    }
+    indx[0] = (int32_t)idx;
+    if (absMax > 10.0 / DBL_MAX) {
+        const Cx s = cinv(maxVal);  // CplxGenericMtxScaleAndAdd(A, LW, 1, Height, 0, CInv(maxVal)): x := 0 + x*s
+        for (int64_t i = 0; i < height; ++i) crow(A, i, lw)[0] = cadd_mul(Cx{0.0, 0.0}, crow(A, i, lw)[0], s);
+        crow(A, idx, lw)[0] = crow(A, 0, lw)[0];
+        crow(A, 0, lw)[0] = maxVal;
+        return 0;
+    }
+    return 1;
+}
+
+// CplxMatrixLUBackSubst :1322-1391 on one column of B
+void cplx_backsubst(const void* LU, int64_t lwLU, int64_t width, const int32_t* indx, void* B, int64_t lwB) {
+    int64_t ii = -1;
+    for (int64_t i = 0; i < width; ++i) {
+        const int64_t ip = indx[i];
+        Cx sum = crow(B, ip, lwB)[0];
+        crow(B, ip, lwB)[0] = crow(B, i, lwB)[0];
+        if (ii >= 0) {
+            for (int64_t j = ii; j < i; ++j) sum = csub_mul(sum, crow(LU, i, lwLU)[j], crow(B, j, lwB)[0]);
+        } else if (!(std::fabs(sum.re) <= 1e-12 && std::fabs(sum.im) <= 1e-12)) {
+            // CCmp(sum, cCplxZero) <> 0: CompareValue with eps 0 takes the RTL's zero resolution, 1e-12
+            ii = i;
+        }
+        crow(B, i, lwB)[0] = sum;
+    }
+    for (int64_t i = width - 1; i >= 0; --i) {
+        Cx sum = crow(B, i, lwB)[0];
+        for (int64_t j = 0; j < width - i - 1; ++j)
+            sum = csub_mul(sum, crow(LU, i, lwLU)[i + 1 + j], crow(B, i + 1 + j, lwB)[0]);
+        crow(B, i, lwB)[0] = cdiv(sum, crow(LU, i, lwLU)[i]);
+    }
+}
+
+}  // namespace
+
+extern "C" int32_t orc_cplx_lu_decomp_inplace(double* A, int64_t lwA, int64_t width, int32_t* indx) {
+    std::fill(indx, indx + width, 0);  // CplxMatrixLUDecompInPlace :1308-1320
+    return cplx_rec_lu(A, width, width, indx, lwA);
+}
+
+extern "C" void orc_cplx_lu_backsubst(const double* LU, int64_t lwLU, int64_t width, const int32_t* indx, double* B,
+                                      int64_t lwB) {
+    cplx_backsubst(LU, lwLU, width, indx, B, lwB);
+}
+
+extern "C" int32_t orc_cplx_lineq_solve(const double* A, int64_t lwA, int64_t width, const double* B, int64_t lwB,
+                                        double* X, int64_t lwX, int64_t nrhs) {
+    // CplxMatrixLinEQSolve :1393-1508 without refinement: a contiguous copy of A factored, then one
+    // back substitution per column of B
+    std::vector<Cx> lu((size_t)(width * width));
+    for (int64_t y = 0; y < width; ++y)
+        for (int64_t x = 0; x < width; ++x) lu[(size_t)(y * width + x)] = crow(A, y, lwA)[x];
+    std::vector<int32_t> indx((size_t)width);
+    const int32_t r = orc_cplx_lu_decomp_inplace(reinterpret_cast<double*>(lu.data()), width * 16, width, indx.data());
+    if (r != 0) return r;
+    std::vector<Cx> col((size_t)width);
+    for (int64_t c = 0; c < nrhs; ++c) {
+        for (int64_t y = 0; y < width; ++y) col[(size_t)y] = crow(B, y, lwB)[c];
+        cplx_backsubst(lu.data(), width * 16, width, indx.data(), col.data(), 16);
+        for (int64_t y = 0; y < width; ++y) crow(X, y, lwX)[c] = col[(size_t)y];
+    }
+    return 0;
+}
+
+extern "C" int32_t orc_cplx_inverse_inplace(double* A, int64_t lwA, int64_t width) {
+    // CplxMatrixInverseInPlace :1510-1552 (width rounded up to even for the factor's stride)
+    const int64_t w = width + (width & 1);
+    std::vector<Cx> Y((size_t)(w * w));
+    for (int64_t y = 0; y < width; ++y)
+        for (int64_t x = 0; x < width; ++x) Y[(size_t)(y * w + x)] = crow(A, y, lwA)[x];
+    std::vector<int32_t> indx((size_t)width);
+    const int32_t r = orc_cplx_lu_decomp_inplace(reinterpret_cast<double*>(Y.data()), w * 16, width, indx.data());
+    if (r != 0) return r;
+    std::vector<Cx> col((size_t)width);
+    for (int64_t j = 0; j < width; ++j) {
+        std::fill(col.begin(), col.end(), Cx{0.0, 0.0});
+        col[(size_t)j] = Cx{1.0, 0.0};
+        cplx_backsubst(Y.data(), w * 16, width, indx.data(), col.data(), 16);
+        for (int64_t i = 0; i < width; ++i) crow(A, i, lwA)[j] = col[(size_t)i];
+    }
+    return 0;
+}
+
+extern "C" void orc_cplx_determinant(const double* A, int64_t lwA, int64_t width, double* det) {
+    // CplxMatrixDeterminant :1554-1603: (+-1, 0) times the diagonal of U, in order
+    const int64_t w = width + (width & 1);
+    std::vector<Cx> lu((size_t)(w * w));
+    for (int64_t y = 0; y < width; ++y)
+        for (int64_t x = 0; x < width; ++x) lu[(size_t)(y * w + x)] = crow(A, y, lwA)[x];
+    std::vector<int32_t> indx((size_t)width);
+    if (cplx_rec_lu(lu.data(), width, width, indx.data(), w * 16) != 0) {
+        det[0] = det[1] = 0.0;
+        return;
+    }
+    int parity = 1;
+    for (int64_t i = 0; i < width; ++i)
+        if (indx[(size_t)i] != i) parity = -parity;
+    Cx r{(double)parity, 0.0};
+    for (int64_t i = 0; i < width; ++i) r = cmul(r, lu[(size_t)(i * w + i)]);
+    det[0] = r.re;
+    det[1] = r.im;
+}
+
 // ---------------- Cholesky (LinAlgCholesky.pas) ------------------------------------------------------------
 namespace {
 

@@ -114,6 +114,15 @@ void    orc_gemm_rows_dot2(const double* A, int64_t lwA, const double* B, int64_
                            int64_t m, int64_t n, int64_t k, int64_t r0, int64_t nr,
                            double* C, int64_t lwC, double* absAB, int64_t lwAbs);
 
+/* ---- complex LU (LinAlgLU.pas:1147-1603): interleaved (real, imag) doubles, strides in bytes */
+int32_t orc_cplx_lu_decomp_inplace(double* A, int64_t lwA, int64_t width, int32_t* indx);  /* :1308-1320 */
+void    orc_cplx_lu_backsubst(const double* LU, int64_t lwLU, int64_t width, const int32_t* indx, double* B,
+                              int64_t lwB);                                                /* :1322-1391 */
+int32_t orc_cplx_lineq_solve(const double* A, int64_t lwA, int64_t width, const double* B, int64_t lwB,
+                             double* X, int64_t lwX, int64_t nrhs);                        /* :1393-1508 */
+int32_t orc_cplx_inverse_inplace(double* A, int64_t lwA, int64_t width);                  /* :1510-1552 */
+void    orc_cplx_determinant(const double* A, int64_t lwA, int64_t width, double* det);   /* :1554-1603 */
+
 /* ---- Cholesky (LinAlgCholesky.pas); results 0 = crOk, 1 = crNoPositiveDefinite (MatrixConst.pas:30) */
 int32_t orc_cholesky_inplace4(double* A, int64_t lwA, int64_t width, int64_t pnl);   /* :106-123, :54-103 */
 int32_t orc_cholesky_inplace2(double* A, int64_t lwA, int64_t width);                /* :205-250 */

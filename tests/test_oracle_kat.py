@@ -195,6 +195,35 @@ def test_singular_zero_column_and_nan():
     assert oracle.determinant(a) == 0.0
 
 
+def _cx(pairs):
+    return np.array([[complex(re, im) for re, im in row] for row in pairs])
+
+
+def test_complex_lu_kats():
+    """TestCmplx.pas: TestLU (:616-631, bitwise), TestLU2 (:633-662, MT seed 12705677, last element
+    (486.05324, 9.5027968) within 1e-4), TestMtxInverse (:664-705, singular all-ones matrix, first
+    row of the reference inverse within 1e-5) and TestDeterminant (:516-552, 33120 + 4608i)."""
+    a = _cx([[(1.0, -1.0), (0.0, -1.0)], [(0.0, 2.0), (2.0, -1.0)]])
+    rc, idx = oracle.cplx_lu_decomp_inplace(a)
+    assert rc == 0 and a.tobytes() == _cx([[(1.0, -1.0), (0.0, -1.0)], [(-1.0, 1.0), (1.0, -2.0)]]).tobytes()
+    r = oracle.Mersenne(seed=12705677)
+    vals = [complex((r.u32() & 0x7FFFFFFF) % 200, (r.u32() & 0x7FFFFFFF) % 100) for _ in range(127 * 127)]
+    x = np.array(vals).reshape(127, 127)
+    rc, _ = oracle.cplx_lu_decomp_inplace(x)
+    assert rc == 0 and abs(x[-1, -1] - (486.05324 + 9.5027968j)) <= 1e-4
+    assert oracle.cplx_inverse_inplace(np.full((4, 4), 1 + 1j)) == 1
+    v = np.array([complex(i, i + 1) for i in range(16)])
+    v[::3] = -v[::3]
+    a4 = v.reshape(4, 4)
+    inv = a4.copy()
+    assert oracle.cplx_inverse_inplace(inv) == 0
+    np.testing.assert_allclose(inv[0], [0.242950984513183 - 0.232956465478163j, 0.027322404371585 - 0.032786885245902j,
+                                        0.007541478129713 - 0.008295625942685j, -0.041420435345218 + 0.025207287622910j],
+                               atol=1e-5)
+    det = oracle.cplx_determinant(a4)
+    assert abs(det - (33120 + 4608j)) <= 1e-12 * abs(det)
+
+
 CHOL_A = np.array([[1.0, 2, 2], [-1, 4, -2], [2, 2, -1]])
 CHOL_A2 = np.array([[1.0, 2, 2, 0.5], [-1, 4, -2, -0.1], [2, 2, -1, 1.2], [3, 2, -1, -1.1]])
 
