@@ -10,7 +10,8 @@ needed between steps.
   python bench.py [--gpus N] [--steps K] [--warmup W] [--form mixed|plain] [--impl b200|reference]
 
 --impl reference times the reference's own algorithm restated in C++ (the oracle's threaded
-ThrMatrixLinEQSolve, all host cores) on a bounded sample of the same workload.
+ThrMatrixLinEQSolve, all host cores) on the same n = 8192 system: the median of 5 solves after 1
+warm-up, whatever --steps / --warmup ask (the line reports the steps it ran).
 With N > 1 (torchrun) every rank solves its own system: replicas, no collective on the data path.
 """
 from __future__ import annotations
