@@ -342,6 +342,29 @@ def run_b200(args, world, rank, local):
         plain = {"value": pv, "unit": "GFLOP/s", "ms_per_step": pms / args.steps,
                  "backward_error": backward_error_torch(A, X, B), "mixed_over_plain": value / pv}
 
+    # ---- context only, never the product path: a library FP64 solve (torch.linalg.solve on the
+    # cuSOLVER backend: getrf + getrs) of the same system, timed the same way
+    library = None
+    if form == "mixed" and not args.no_plain:
+        try:
+            torch.backends.cuda.preferred_linalg_library("cusolver")
+            for _ in range(2):
+                Xl = torch.linalg.solve(A, B)
+            torch.cuda.synchronize()
+            q0, q1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            q0.record()
+            for _ in range(args.steps):
+                Xl = torch.linalg.solve(A, B)
+            q1.record()
+            torch.cuda.synchronize()
+            qms = max_over_ranks(world, q0.elapsed_time(q1))
+            library = {"what": "torch.linalg.solve, cuSOLVER getrf + getrs (context only)",
+                       "value": args.steps * world * flops / (qms / 1e3) / 1e9, "unit": "GFLOP/s",
+                       "ms_per_step": qms / args.steps, "backward_error": backward_error_torch(A, Xl, B)}
+            del Xl
+        except Exception as exc:
+            library = {"what": "torch.linalg.solve (cuSOLVER)", "unavailable": str(exc)[:200]}
+
     # ---- roofline of the dominant kernel class (by device time in the profiled pass).  The profiler
     # records FLOPs for the tensor-core GEMM classes and HBM bytes for every other class.
     dom_name, d = max(prof.items(), key=lambda kv: kv[1]["ms"])
@@ -389,6 +412,7 @@ def run_b200(args, world, rank, local):
                        "l2": "A (512 MiB) exceeds L2; no flush needed"},
             "backward_error": eta, "backward_error_bound": n * 2.0 ** -53,
             "e2e": e2e, "gpu_launches": launches, "roofline": roof, "cpu_baseline": cpu, "plain_fp64": plain,
+            "library_fp64_context": library,
             "kernel_classes": {kname: {"launches": v["launches"], "ms": round(v["ms"], 4)}
                                for kname, v in prof.items() if v["launches"]},
             "clocks": clk.summary(),

@@ -273,9 +273,11 @@ typedef struct b2m_solve_report {
     int32_t fell_back;       /* 1 if the plain FP64 solve produced X */
     double  backward_error;  /* normwise backward error of the returned X (FP64 residual) */
     double  refinement_backward_error;  /* the last refinement step's, before any fallback */
-    double  forward_error;   /* normwise forward-error estimate max_j ||d_j||inf / ||x_j||inf, d the last
-                                correction applied (refinement) or one extra correction computed with
-                                the FP64 factors (fallback); an upper-side estimate of ||x - x*|| / ||x*|| */
+    double  forward_error;   /* normwise forward-error estimate of ||x - x*|| / ||x*|| (max over columns j,
+                                inf-norms).  Refinement: ||d_j|| rho_j / ||x_j|| with d the last
+                                correction applied and rho_j = ||d_j|| / ||d_j of the step before|| (the
+                                observed contraction; 1 after a single step).  Fallback: ||d_j|| / ||x_j||
+                                with d one extra correction computed with the FP64 factors. */
 } b2m_solve_report;
 B2M_API int32_t b2m_MatrixLinEQSolveMixed(b2m_ctx* ctx, const double* A, int64_t LineWidthA, int64_t width,
                                           const double* B, int64_t LineWidthB, double* X, int64_t LineWidthX,

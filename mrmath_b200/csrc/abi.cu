@@ -90,7 +90,7 @@ extern "C" int32_t b2m_MatrixMultEx(b2m_ctx* h, double* dest, int64_t destLineWi
                                     int32_t trans) {
     Ctx* ctx = as_ctx(h);
     if (!ctx) return B2M_ERR_ARG;
-    std::lock_guard<std::mutex> lk(ctx->mtx);
+    CallLock lk(ctx);
     if (!dest || !mt1 || !mt2) return fail(ctx, B2M_ERR_ARG, "null pointer");
     if (op < 0 || op > 2) return fail(ctx, B2M_ERR_ARG, "op must be 0 (doNone), 1 (doAdd) or 2 (doSub)");
     MultShape s;
@@ -120,7 +120,7 @@ extern "C" int32_t b2m_dev_MatrixMultEx(b2m_ctx* h, double* dest, int64_t destLi
                                         int32_t trans) {
     Ctx* ctx = as_ctx(h);
     if (!ctx) return B2M_ERR_ARG;
-    std::lock_guard<std::mutex> lk(ctx->mtx);
+    CallLock lk(ctx);
     if (!dest || !mt1 || !mt2) return fail(ctx, B2M_ERR_ARG, "null pointer");
     if (op < 0 || op > 2) return fail(ctx, B2M_ERR_ARG, "invalid op");
     MultShape s;
@@ -177,7 +177,7 @@ extern "C" int32_t b2m_MatrixLUDecomp(b2m_ctx* h, const double* A, int64_t LineW
                                       int64_t LineWidthLU, int64_t width, int32_t* indx) {
     Ctx* ctx = as_ctx(h);
     if (!ctx) return B2M_ERR_ARG;
-    std::lock_guard<std::mutex> lk(ctx->mtx);
+    CallLock lk(ctx);
     if (!A || !LUDecomp || !indx) return fail(ctx, B2M_ERR_ARG, "null pointer");
     if (width <= 0 || !lw_ok(LineWidthA, width) || !lw_ok(LineWidthLU, width))
         return fail(ctx, B2M_ERR_DIM, "Dimension Error");
@@ -201,7 +201,7 @@ extern "C" int32_t b2m_MatrixLUBackSubst(b2m_ctx* h, const double* LUDecomp, int
                                          const int32_t* indx, double* B, int64_t LineWidthB, int64_t nrhs) {
     Ctx* ctx = as_ctx(h);
     if (!ctx) return B2M_ERR_ARG;
-    std::lock_guard<std::mutex> lk(ctx->mtx);
+    CallLock lk(ctx);
     if (!LUDecomp || !indx || !B) return fail(ctx, B2M_ERR_ARG, "null pointer");
     if (width <= 0 || nrhs <= 0 || !lw_ok(LineWidthLU, width) || !lw_ok(LineWidthB, nrhs))
         return fail(ctx, B2M_ERR_DIM, "Dimension Error");
@@ -226,7 +226,7 @@ extern "C" int32_t b2m_MatrixLUBackSubst(b2m_ctx* h, const double* LUDecomp, int
 extern "C" int32_t b2m_MatrixInverseInPlace(b2m_ctx* h, double* A, int64_t LineWidthA, int64_t width) {
     Ctx* ctx = as_ctx(h);
     if (!ctx) return B2M_ERR_ARG;
-    std::lock_guard<std::mutex> lk(ctx->mtx);
+    CallLock lk(ctx);
     if (!A) return fail(ctx, B2M_ERR_ARG, "null pointer");
     if (width <= 0 || !lw_ok(LineWidthA, width)) return fail(ctx, B2M_ERR_DIM, "Dimension Error");
     cudaSetDevice(ctx->device);
@@ -250,7 +250,7 @@ extern "C" int32_t b2m_MatrixDeterminant(b2m_ctx* h, const double* A, int64_t Li
                                          double* det) {
     Ctx* ctx = as_ctx(h);
     if (!ctx) return B2M_ERR_ARG;
-    std::lock_guard<std::mutex> lk(ctx->mtx);
+    CallLock lk(ctx);
     if (!A || !det) return fail(ctx, B2M_ERR_ARG, "null pointer");
     if (width <= 0 || !lw_ok(LineWidthA, width)) return fail(ctx, B2M_ERR_DIM, "Dimension error");
     cudaSetDevice(ctx->device);
@@ -305,7 +305,7 @@ extern "C" int32_t b2m_MatrixLinEQSolve(b2m_ctx* h, const double* A, int64_t Lin
                                         int64_t Width2, int64_t NumRefinements) {
     Ctx* ctx = as_ctx(h);
     if (!ctx) return B2M_ERR_ARG;
-    std::lock_guard<std::mutex> lk(ctx->mtx);
+    CallLock lk(ctx);
     if (!A || !B || !X) return fail(ctx, B2M_ERR_ARG, "null pointer");
     if (width <= 0 || Width2 <= 0 || !lw_ok(LineWidthA, width) || !lw_ok(LineWidthB, Width2) ||
         !lw_ok(LineWidthX, Width2) || NumRefinements < 0)
@@ -338,7 +338,7 @@ extern "C" int32_t b2m_dev_MatrixLUDecompInPlace(b2m_ctx* h, double* A, int64_t 
                                                  int32_t* indx, int32_t* status) {
     Ctx* ctx = as_ctx(h);
     if (!ctx) return B2M_ERR_ARG;
-    std::lock_guard<std::mutex> lk(ctx->mtx);
+    CallLock lk(ctx);
     if (!A || !indx) return fail(ctx, B2M_ERR_ARG, "null pointer");
     if (width <= 0 || !lw_ok(LineWidthA, width)) return fail(ctx, B2M_ERR_DIM, "Dimension Error");
     const int64_t n = width;
@@ -367,7 +367,7 @@ extern "C" int32_t b2m_dev_MatrixLUBackSubst(b2m_ctx* h, const double* LUDecomp,
                                              int64_t nrhs) {
     Ctx* ctx = as_ctx(h);
     if (!ctx) return B2M_ERR_ARG;
-    std::lock_guard<std::mutex> lk(ctx->mtx);
+    CallLock lk(ctx);
     if (!LUDecomp || !indx || !B) return fail(ctx, B2M_ERR_ARG, "null pointer");
     if (width <= 0 || nrhs <= 0 || !lw_ok(LineWidthLU, width) || !lw_ok(LineWidthB, nrhs))
         return fail(ctx, B2M_ERR_DIM, "Dimension Error");
@@ -406,7 +406,7 @@ extern "C" int32_t b2m_dev_MatrixLinEQSolve(b2m_ctx* h, const double* A, int64_t
                                             int64_t Width2, int64_t NumRefinements, int32_t* status) {
     Ctx* ctx = as_ctx(h);
     if (!ctx) return B2M_ERR_ARG;
-    std::lock_guard<std::mutex> lk(ctx->mtx);
+    CallLock lk(ctx);
     if (!A || !B || !X) return fail(ctx, B2M_ERR_ARG, "null pointer");
     if (width <= 0 || Width2 <= 0 || !lw_ok(LineWidthA, width) || !lw_ok(LineWidthB, Width2) ||
         !lw_ok(LineWidthX, Width2) || NumRefinements < 0)
@@ -441,7 +441,7 @@ extern "C" int32_t b2m_dev_MatrixInverseInPlace(b2m_ctx* h, double* A, int64_t L
                                                 int32_t* status) {
     Ctx* ctx = as_ctx(h);
     if (!ctx) return B2M_ERR_ARG;
-    std::lock_guard<std::mutex> lk(ctx->mtx);
+    CallLock lk(ctx);
     if (!A) return fail(ctx, B2M_ERR_ARG, "null pointer");
     if (width <= 0 || !lw_ok(LineWidthA, width)) return fail(ctx, B2M_ERR_DIM, "Dimension Error");
     const int64_t n = width, ld = padded_ld(n);
@@ -468,7 +468,7 @@ extern "C" int32_t b2m_dev_MatrixDeterminant(b2m_ctx* h, const double* A, int64_
                                              double* det) {
     Ctx* ctx = as_ctx(h);
     if (!ctx) return B2M_ERR_ARG;
-    std::lock_guard<std::mutex> lk(ctx->mtx);
+    CallLock lk(ctx);
     if (!A || !det) return fail(ctx, B2M_ERR_ARG, "null pointer");
     if (width <= 0 || !lw_ok(LineWidthA, width)) return fail(ctx, B2M_ERR_DIM, "Dimension error");
     const int64_t n = width, ld = padded_ld(n);
@@ -507,7 +507,7 @@ extern "C" int32_t b2m_dev_MatrixLinEQSolveMixed(b2m_ctx* h, const double* A, in
                                                  b2m_solve_report* report) {
     Ctx* ctx = as_ctx(h);
     if (!ctx) return B2M_ERR_ARG;
-    std::lock_guard<std::mutex> lk(ctx->mtx);
+    CallLock lk(ctx);
     if (!A || !B || !X) return fail(ctx, B2M_ERR_ARG, "null pointer");
     if (width <= 0 || Width2 <= 0 || !lw_ok(LineWidthA, width) || !lw_ok(LineWidthB, Width2) ||
         !lw_ok(LineWidthX, Width2))
@@ -551,7 +551,7 @@ extern "C" int32_t b2m_MatrixLinEQSolveMixed(b2m_ctx* h, const double* A, int64_
                                              b2m_solve_report* report) {
     Ctx* ctx = as_ctx(h);
     if (!ctx) return B2M_ERR_ARG;
-    std::lock_guard<std::mutex> lk(ctx->mtx);
+    CallLock lk(ctx);
     if (!A || !B || !X) return fail(ctx, B2M_ERR_ARG, "null pointer");
     if (width <= 0 || Width2 <= 0 || !lw_ok(LineWidthA, width) || !lw_ok(LineWidthB, Width2) ||
         !lw_ok(LineWidthX, Width2))
@@ -579,7 +579,7 @@ extern "C" int32_t b2m_dev_MatrixLinEQSolveAdjoint(b2m_ctx* h, const double* LUD
                                                    int64_t LineWidthdA, int32_t op) {
     Ctx* ctx = as_ctx(h);
     if (!ctx) return B2M_ERR_ARG;
-    std::lock_guard<std::mutex> lk(ctx->mtx);
+    CallLock lk(ctx);
     if (!LUDecomp || !indx || !X || !G || !Lambda) return fail(ctx, B2M_ERR_ARG, "null pointer");
     if (op != B2M_DO_NONE && op != B2M_DO_ADD) return fail(ctx, B2M_ERR_ARG, "op must be B2M_DO_NONE or B2M_DO_ADD");
     const int64_t n = width;
@@ -605,7 +605,7 @@ extern "C" int32_t b2m_MatrixLinEQSolveAdjoint(b2m_ctx* h, const double* LUDecom
                                                int64_t LineWidthLambda, double* dA, int64_t LineWidthdA, int32_t op) {
     Ctx* ctx = as_ctx(h);
     if (!ctx) return B2M_ERR_ARG;
-    std::lock_guard<std::mutex> lk(ctx->mtx);
+    CallLock lk(ctx);
     if (!LUDecomp || !indx || !X || !G || !Lambda) return fail(ctx, B2M_ERR_ARG, "null pointer");
     if (op != B2M_DO_NONE && op != B2M_DO_ADD) return fail(ctx, B2M_ERR_ARG, "op must be B2M_DO_NONE or B2M_DO_ADD");
     const int64_t n = width;
@@ -661,7 +661,7 @@ extern "C" int32_t b2m_dev_BatchLinEQSolve(b2m_ctx* h, int64_t count, const int3
                                            const double* B, double* X, int32_t mode, int32_t* info, int32_t* iters) {
     Ctx* ctx = as_ctx(h);
     if (!ctx) return B2M_ERR_ARG;
-    std::lock_guard<std::mutex> lk(ctx->mtx);
+    CallLock lk(ctx);
     int64_t ae, be;
     B2M_TRY(batch_check(ctx, count, n, nrhs, a_off, b_off, &ae, &be));
     if (count == 0) return B2M_OK;
@@ -674,7 +674,7 @@ extern "C" int32_t b2m_BatchLinEQSolve(b2m_ctx* h, int64_t count, const int32_t*
                                        double* X, int32_t mode, int32_t* info, int32_t* iters) {
     Ctx* ctx = as_ctx(h);
     if (!ctx) return B2M_ERR_ARG;
-    std::lock_guard<std::mutex> lk(ctx->mtx);
+    CallLock lk(ctx);
     int64_t ae, be;
     B2M_TRY(batch_check(ctx, count, n, nrhs, a_off, b_off, &ae, &be));
     if (count == 0) return B2M_OK;
@@ -703,7 +703,7 @@ extern "C" int32_t b2m_batch_tune_read(b2m_ctx* h, int32_t* small_n, int32_t* gr
                                        int32_t* pw_small, float* ms) {
     Ctx* ctx = as_ctx(h);
     if (!ctx) return B2M_ERR_ARG;
-    std::lock_guard<std::mutex> lk(ctx->mtx);
+    CallLock lk(ctx);
     if (ctx->batch_tunes.empty()) return fail(ctx, B2M_ERR_ARG, "no batch has been tuned yet");
     const BatchTune& t = ctx->batch_tunes.find(ctx->batch_plan_sig) != ctx->batch_tunes.end()
                              ? ctx->batch_tunes[ctx->batch_plan_sig]
@@ -723,7 +723,7 @@ extern "C" int32_t b2m_dev_MatrixMultOzaki(b2m_ctx* h, double* dest, int64_t des
                                            int32_t slices) {
     Ctx* ctx = as_ctx(h);
     if (!ctx) return B2M_ERR_ARG;
-    std::lock_guard<std::mutex> lk(ctx->mtx);
+    CallLock lk(ctx);
     if (!dest || !mt1 || !mt2) return fail(ctx, B2M_ERR_ARG, "null pointer");
     if (op < 0 || op > 2) return fail(ctx, B2M_ERR_ARG, "invalid op");
     if (width1 != height2 || width1 < 0 || height1 < 0 || width2 < 0)
@@ -740,7 +740,7 @@ extern "C" int32_t b2m_MatrixMultOzaki(b2m_ctx* h, double* dest, int64_t destLin
                                        int32_t slices) {
     Ctx* ctx = as_ctx(h);
     if (!ctx) return B2M_ERR_ARG;
-    std::lock_guard<std::mutex> lk(ctx->mtx);
+    CallLock lk(ctx);
     if (!dest || !mt1 || !mt2) return fail(ctx, B2M_ERR_ARG, "null pointer");
     if (op < 0 || op > 2) return fail(ctx, B2M_ERR_ARG, "invalid op");
     if (width1 != height2 || width1 < 0 || height1 < 0 || width2 < 0)
@@ -793,7 +793,7 @@ extern "C" int32_t b2m_dev_MatrixMultErrorReport(b2m_ctx* h, const double* dest,
                                                  b2m_gemm_report* report) {
     Ctx* ctx = as_ctx(h);
     if (!ctx) return B2M_ERR_ARG;
-    std::lock_guard<std::mutex> lk(ctx->mtx);
+    CallLock lk(ctx);
     if (!dest || !mt1 || !mt2 || !report) return fail(ctx, B2M_ERR_ARG, "null pointer");
     MultShape s;
     B2M_TRY(mult_shape(ctx, trans, width1, height1, width2, height2, &s));
@@ -812,7 +812,7 @@ extern "C" int32_t b2m_MatrixMultErrorReport(b2m_ctx* h, const double* dest, int
                                              int32_t sample_rows, b2m_gemm_report* report) {
     Ctx* ctx = as_ctx(h);
     if (!ctx) return B2M_ERR_ARG;
-    std::lock_guard<std::mutex> lk(ctx->mtx);
+    CallLock lk(ctx);
     if (!dest || !mt1 || !mt2 || !report) return fail(ctx, B2M_ERR_ARG, "null pointer");
     MultShape s;
     B2M_TRY(mult_shape(ctx, trans, width1, height1, width2, height2, &s));
@@ -837,7 +837,7 @@ extern "C" int32_t b2m_MatrixCholeskyInPlace4(b2m_ctx* h, double* A, int64_t Lin
                                               int64_t pnlSize) {
     Ctx* ctx = as_ctx(h);
     if (!ctx) return B2M_ERR_ARG;
-    std::lock_guard<std::mutex> lk(ctx->mtx);
+    CallLock lk(ctx);
     if (!A) return fail(ctx, B2M_ERR_ARG, "null pointer");
     if (width <= 0 || !lw_ok(LineWidthA, width) || pnlSize < 0) return fail(ctx, B2M_ERR_DIM, "Dimension error");
     cudaSetDevice(ctx->device);
@@ -860,7 +860,7 @@ extern "C" int32_t b2m_dev_MatrixCholeskyInPlace4(b2m_ctx* h, double* A, int64_t
                                                   int32_t* status) {
     Ctx* ctx = as_ctx(h);
     if (!ctx) return B2M_ERR_ARG;
-    std::lock_guard<std::mutex> lk(ctx->mtx);
+    CallLock lk(ctx);
     if (!A) return fail(ctx, B2M_ERR_ARG, "null pointer");
     if (width <= 0 || !lw_ok(LineWidthA, width)) return fail(ctx, B2M_ERR_DIM, "Dimension error");
     const int64_t ld = padded_ld(width);
@@ -879,7 +879,7 @@ extern "C" int32_t b2m_MatrixCholeskyInPlace(b2m_ctx* h, double* A, int64_t Line
                                              int64_t LineWidthP) {
     Ctx* ctx = as_ctx(h);
     if (!ctx) return B2M_ERR_ARG;
-    std::lock_guard<std::mutex> lk(ctx->mtx);
+    CallLock lk(ctx);
     if (!A || !P) return fail(ctx, B2M_ERR_ARG, "null pointer");
     if (width <= 0 || !lw_ok(LineWidthA, width) || LineWidthP < 8 || (LineWidthP % 8))
         return fail(ctx, B2M_ERR_DIM, "Dimension error");
@@ -926,7 +926,7 @@ extern "C" int32_t b2m_MatrixCholeskySolveLinEq(b2m_ctx* h, const double* A, int
                                                 int64_t LineWidthB, double* X, int64_t LineWidthX, int64_t nrhs) {
     Ctx* ctx = as_ctx(h);
     if (!ctx) return B2M_ERR_ARG;
-    std::lock_guard<std::mutex> lk(ctx->mtx);
+    CallLock lk(ctx);
     if (!A || !B || !X) return fail(ctx, B2M_ERR_ARG, "null pointer");
     if (width <= 0 || nrhs <= 0 || !lw_ok(LineWidthA, width) || !lw_ok(LineWidthB, nrhs) || !lw_ok(LineWidthX, nrhs) ||
         (P && (LineWidthP < 8 || (LineWidthP % 8))))
@@ -951,7 +951,7 @@ extern "C" int32_t b2m_dev_MatrixCholeskySolveLinEq(b2m_ctx* h, const double* A,
                                                     int64_t LineWidthB, double* X, int64_t LineWidthX, int64_t nrhs) {
     Ctx* ctx = as_ctx(h);
     if (!ctx) return B2M_ERR_ARG;
-    std::lock_guard<std::mutex> lk(ctx->mtx);
+    CallLock lk(ctx);
     if (!A || !B || !X) return fail(ctx, B2M_ERR_ARG, "null pointer");
     if (width <= 0 || nrhs <= 0 || !lw_ok(LineWidthA, width) || !lw_ok(LineWidthB, nrhs) || !lw_ok(LineWidthX, nrhs) ||
         (P && (LineWidthP < 8 || (LineWidthP % 8))))
@@ -1022,7 +1022,7 @@ extern "C" int32_t b2m_CplxMatrixLUDecompInPlace(b2m_ctx* h, double* A, int64_t 
                                                  int32_t* indx) {
     Ctx* ctx = as_ctx(h);
     if (!ctx) return B2M_ERR_ARG;
-    std::lock_guard<std::mutex> lk(ctx->mtx);
+    CallLock lk(ctx);
     if (!A || !indx) return fail(ctx, B2M_ERR_ARG, "null pointer");
     if (width <= 0 || !zlw_ok(LineWidthA, width)) return fail(ctx, B2M_ERR_DIM, "Dimension Error");
     cudaSetDevice(ctx->device);
@@ -1039,7 +1039,7 @@ extern "C" int32_t b2m_CplxMatrixLUBackSubst(b2m_ctx* h, const double* LUDecomp,
                                              const int32_t* indx, double* B, int64_t LineWidthB, int64_t nrhs) {
     Ctx* ctx = as_ctx(h);
     if (!ctx) return B2M_ERR_ARG;
-    std::lock_guard<std::mutex> lk(ctx->mtx);
+    CallLock lk(ctx);
     if (!LUDecomp || !indx || !B) return fail(ctx, B2M_ERR_ARG, "null pointer");
     if (width <= 0 || nrhs <= 0 || !zlw_ok(LineWidthLU, width) || !zlw_ok(LineWidthB, nrhs))
         return fail(ctx, B2M_ERR_DIM, "Dimension Error");
@@ -1065,7 +1065,7 @@ extern "C" int32_t b2m_CplxMatrixLinEQSolve(b2m_ctx* h, const double* A, int64_t
                                             int64_t Width2) {
     Ctx* ctx = as_ctx(h);
     if (!ctx) return B2M_ERR_ARG;
-    std::lock_guard<std::mutex> lk(ctx->mtx);
+    CallLock lk(ctx);
     if (!A || !B || !X) return fail(ctx, B2M_ERR_ARG, "null pointer");
     if (width <= 0 || Width2 <= 0 || !zlw_ok(LineWidthA, width) || !zlw_ok(LineWidthB, Width2) ||
         !zlw_ok(LineWidthX, Width2))
@@ -1086,7 +1086,7 @@ extern "C" int32_t b2m_CplxMatrixLinEQSolve(b2m_ctx* h, const double* A, int64_t
 extern "C" int32_t b2m_CplxMatrixInverseInPlace(b2m_ctx* h, double* A, int64_t LineWidthA, int64_t width) {
     Ctx* ctx = as_ctx(h);
     if (!ctx) return B2M_ERR_ARG;
-    std::lock_guard<std::mutex> lk(ctx->mtx);
+    CallLock lk(ctx);
     if (!A) return fail(ctx, B2M_ERR_ARG, "null pointer");
     if (width <= 0 || !zlw_ok(LineWidthA, width)) return fail(ctx, B2M_ERR_DIM, "Dimension Error");
     cudaSetDevice(ctx->device);
@@ -1111,7 +1111,7 @@ extern "C" int32_t b2m_CplxMatrixDeterminant(b2m_ctx* h, const double* A, int64_
                                              double* det) {
     Ctx* ctx = as_ctx(h);
     if (!ctx) return B2M_ERR_ARG;
-    std::lock_guard<std::mutex> lk(ctx->mtx);
+    CallLock lk(ctx);
     if (!A || !det) return fail(ctx, B2M_ERR_ARG, "null pointer");
     if (width <= 0 || !zlw_ok(LineWidthA, width)) return fail(ctx, B2M_ERR_DIM, "Dimension error");
     cudaSetDevice(ctx->device);

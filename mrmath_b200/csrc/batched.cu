@@ -651,7 +651,7 @@ int32_t batch_solve(Ctx* ctx, cudaStream_t st, int64_t count, const int32_t* hn,
 extern "C" int32_t b2m_batch_tune_save(b2m_ctx* h, const char* path) {
     b2m::Ctx* ctx = reinterpret_cast<b2m::Ctx*>(h);
     if (!ctx || !path) return B2M_ERR_ARG;
-    std::lock_guard<std::mutex> lk(ctx->mtx);
+    b2m::CallLock lk(ctx);
     FILE* f = std::fopen(path, "w");
     if (!f) return b2m::fail(ctx, B2M_ERR_ARG, "cannot write %s", path);
     std::fprintf(f, "b2m-batch-tune 1\n");
@@ -664,7 +664,7 @@ extern "C" int32_t b2m_batch_tune_save(b2m_ctx* h, const char* path) {
 extern "C" int32_t b2m_batch_tune_load(b2m_ctx* h, const char* path, int32_t* loaded) {
     b2m::Ctx* ctx = reinterpret_cast<b2m::Ctx*>(h);
     if (!ctx || !path) return B2M_ERR_ARG;
-    std::lock_guard<std::mutex> lk(ctx->mtx);
+    b2m::CallLock lk(ctx);
     if (loaded) *loaded = 0;
     FILE* f = std::fopen(path, "r");
     if (!f) return b2m::fail(ctx, B2M_ERR_ARG, "cannot read %s", path);

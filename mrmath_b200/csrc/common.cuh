@@ -97,6 +97,11 @@ struct Ctx {
     int32_t* h_status = nullptr;     // pinned mirror
     void* ws[kNumWs] = {};
     size_t ws_bytes[kNumWs] = {};
+    // run_graph's own capture is in progress: a workspace slot that must grow is recorded here
+    // (cudaMalloc is not allowed under capture) and the capture is redone after the allocation
+    bool capturing = false;
+    int ws_pending_slot = -1;
+    size_t ws_pending_bytes = 0;
     void* h_pinned = nullptr;        // pinned staging for host-buffer calls
     size_t h_pinned_bytes = 0;
     int64_t launches = 0;
@@ -120,6 +125,18 @@ struct Ctx {
 
 // records a message and returns the status (for `return fail(ctx, ...)`)
 int32_t fail(Ctx* ctx, int32_t status, const char* fmt, ...);
+
+// internal status (never returned by an entry point): a workspace slot must grow while run_graph
+// captures; run_graph allocates it and captures again
+constexpr int32_t kWsRetry = -1000;
+
+// an entry point's hold on its context: takes the context's mutex and clears a launch error that
+// earlier work in this thread left behind (a non-sticky error such as a failed launch of someone
+// else's kernel), so that the launch checks of this call report this call's errors only
+struct CallLock {
+    std::lock_guard<std::mutex> lk;
+    explicit CallLock(Ctx* ctx) : lk(ctx->mtx) { (void)cudaGetLastError(); }
+};
 
 #define B2M_CU(ctx, call)                                                                          \
     do {                                                                                           \

@@ -27,6 +27,11 @@ std::atomic<int>& device_flag(const void* key, int tag, int device) {
 
 int32_t ws_get(Ctx* ctx, int slot, size_t bytes, void** out) {
     bytes = (size_t)round_up((int64_t)std::max<size_t>(bytes, 256), 256);
+    if (ctx->ws_bytes[slot] < bytes && ctx->capturing) {
+        ctx->ws_pending_slot = slot;
+        ctx->ws_pending_bytes = bytes;
+        return kWsRetry;
+    }
     if (ctx->ws_bytes[slot] < bytes) {
         if (ctx->ws[slot]) {
             // the buffer may still be in use by queued work, and captured graphs hold its address:
@@ -110,14 +115,31 @@ int32_t run_graph(Ctx* ctx, cudaStream_t st, const GraphKey& key, const std::fun
         }
         cudaGraph_t g = nullptr;
         const int64_t l0 = ctx->launches;
-        B2M_CU(ctx, cudaStreamBeginCapture(gs, cudaStreamCaptureModeThreadLocal));
-        const int32_t r = issue(gs);
-        const cudaError_t ce = cudaStreamEndCapture(gs, &g);
-        if (r != B2M_OK) {
-            if (g) cudaGraphDestroy(g);
-            return r;
+        // a capture that needs a larger workspace slot is abandoned, the slot allocated outside
+        // capture, and the capture redone (at most once per slot)
+        for (int attempt = 0;; ++attempt) {
+            B2M_CU(ctx, cudaStreamBeginCapture(gs, cudaStreamCaptureModeThreadLocal));
+            ctx->capturing = true;
+            const int32_t r = issue(gs);
+            ctx->capturing = false;
+            const cudaError_t ce = cudaStreamEndCapture(gs, &g);
+            if (r != B2M_OK || ce != cudaSuccess) {
+                if (g) cudaGraphDestroy(g);
+                g = nullptr;
+                (void)cudaGetLastError();  // an abandoned capture leaves no error for later calls
+                ctx->launches = l0;
+            }
+            if (r == kWsRetry && attempt < 2 * kNumWs) {
+                void* p = nullptr;
+                B2M_TRY(ws_get(ctx, ctx->ws_pending_slot, ctx->ws_pending_bytes, &p));
+                continue;
+            }
+            if (r == kWsRetry) return fail(ctx, B2M_ERR_ALLOC, "workspace kept growing under capture");
+            if (r != B2M_OK) return r;
+            if (ce != cudaSuccess)
+                return fail(ctx, B2M_ERR_CUDA, "stream capture failed: %s", cudaGetErrorString(ce));
+            break;
         }
-        if (ce != cudaSuccess) return fail(ctx, B2M_ERR_CUDA, "stream capture failed: %s", cudaGetErrorString(ce));
         GraphEntry e;
         // per-node priorities: the LU's panel kernels are launched with the highest priority so that
         // they take SMs ahead of a concurrent trailing GEMM (a graph otherwise ignores them)
@@ -303,7 +325,7 @@ extern "C" int32_t b2m_use_graphs(b2m_ctx* h, int32_t enable) {
 extern "C" int32_t b2m_set_wait_limit(b2m_ctx* h, int64_t polls) {
     Ctx* ctx = reinterpret_cast<Ctx*>(h);
     if (!ctx) return B2M_ERR_ARG;
-    std::lock_guard<std::mutex> lk(ctx->mtx);
+    b2m::CallLock lk(ctx);
     if (polls > 0xFFFFFFFFll) return b2m::fail(ctx, B2M_ERR_ARG, "wait limit above 2^32 - 1 polls");
     cudaSetDevice(ctx->device);
     // the limit is a kernel argument, so captured graphs that hold the old one are dropped
@@ -353,7 +375,7 @@ extern "C" int32_t b2m_upload(b2m_ctx* h, double* dst, int64_t dstLineWidth, con
     if (rows < 0 || cols < 0 || dstLineWidth < cols * 8 || srcLineWidth < cols * 8)
         return b2m::fail(ctx, B2M_ERR_DIM, "Line widths do not match");
     if (rows == 0 || cols == 0) return B2M_OK;
-    std::lock_guard<std::mutex> lk(ctx->mtx);
+    b2m::CallLock lk(ctx);
     cudaSetDevice(ctx->device);
     B2M_CU(ctx, cudaMemcpy2DAsync(dst, dstLineWidth, src, srcLineWidth, cols * 8, rows, cudaMemcpyHostToDevice,
                                   ctx->stream));
@@ -368,7 +390,7 @@ extern "C" int32_t b2m_download(b2m_ctx* h, double* dst, int64_t dstLineWidth, c
     if (rows < 0 || cols < 0 || dstLineWidth < cols * 8 || srcLineWidth < cols * 8)
         return b2m::fail(ctx, B2M_ERR_DIM, "Line widths do not match");
     if (rows == 0 || cols == 0) return B2M_OK;
-    std::lock_guard<std::mutex> lk(ctx->mtx);
+    b2m::CallLock lk(ctx);
     cudaSetDevice(ctx->device);
     B2M_CU(ctx, cudaMemcpy2DAsync(dst, dstLineWidth, src, srcLineWidth, cols * 8, rows, cudaMemcpyDeviceToHost,
                                   ctx->stream));
@@ -379,7 +401,7 @@ extern "C" int32_t b2m_download(b2m_ctx* h, double* dst, int64_t dstLineWidth, c
 extern "C" int32_t b2m_set_progress(b2m_ctx* h, b2m_progress_fn fn, void* user) {
     Ctx* ctx = reinterpret_cast<Ctx*>(h);
     if (!ctx) return B2M_ERR_ARG;
-    std::lock_guard<std::mutex> lk(ctx->mtx);
+    b2m::CallLock lk(ctx);
     ctx->progress = fn;
     ctx->progress_user = user;
     return B2M_OK;

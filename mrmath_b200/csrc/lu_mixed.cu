@@ -718,14 +718,21 @@ double eta_from(const std::vector<unsigned long long>& h, int64_t nrhs, double n
     return eta;
 }
 
-// forward-error estimate max_c ||d_c||inf / ||x_c||inf from the column maxima [k,2k) |x| and
-// [3k,4k) |d|, d being the last correction (an upper estimate once refinement contracts)
-double fwd_from(const std::vector<unsigned long long>& h, int64_t nrhs) {
+// forward-error estimate max_c ||e_c||inf / ||x_c||inf from the column maxima [k,2k) |x| and
+// [3k,4k) |d| of the last correction d.  d_k is (to first order) the error of the iterate before
+// it, so ||d_k|| alone overstates the error of x_k by the contraction factor; with the previous
+// step's ||d_(k-1)|| (dprev, < 0 when there is none) the error of x_k is estimated as
+// ||d_k|| * rho with rho = ||d_k|| / ||d_(k-1)|| (linear convergence), and as ||d_k|| otherwise.
+// dprev is updated to this step's ||d_c||.
+double fwd_from(const std::vector<unsigned long long>& h, int64_t nrhs, std::vector<double>* dprev = nullptr) {
     double f = 0.0;
     for (int64_t c = 0; c < nrhs; ++c) {
         const double xn = __builtin_bit_cast(double, h[nrhs + c]);
         const double dn = __builtin_bit_cast(double, h[3 * nrhs + c]);
-        f = std::max(f, xn > 0 ? dn / xn : (dn > 0 ? INFINITY : 0.0));
+        double rho = 1.0;
+        if (dprev && (*dprev)[c] > 0.0) rho = std::min(1.0, dn / (*dprev)[c]);
+        if (dprev) (*dprev)[c] = dn;
+        f = std::max(f, xn > 0 ? dn * rho / xn : (dn > 0 ? INFINITY : 0.0));
     }
     return f;
 }
@@ -797,6 +804,7 @@ int32_t solve_mixed(Ctx* ctx, cudaStream_t st, const double* A, int64_t lda, int
             return B2M_OK;
         };
         double prev = INFINITY;
+        std::vector<double> dprev((size_t)nrhs, -1.0);
         for (int it = 0; it < max_iter; ++it) {
             B2M_TRY(run_graph(ctx, st, key, step));
             B2M_CU(ctx, cudaMemcpyAsync(h.data() + 1, nrm + 1, 4 * nrhs * sizeof(unsigned long long),
@@ -814,7 +822,7 @@ int32_t solve_mixed(Ctx* ctx, cudaStream_t st, const double* A, int64_t lda, int
             rep->iterations = it + 1;
             rep->backward_error = eta;
             rep->ir_backward_error = eta;
-            rep->forward_error = fwd_from(hv, nrhs);
+            rep->forward_error = fwd_from(hv, nrhs, &dprev);
             if (std::isfinite(eta) && eta <= tol) {
                 converged = true;
                 break;

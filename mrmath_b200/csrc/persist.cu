@@ -164,7 +164,7 @@ extern "C" int32_t b2m_dev_ReadMatrixFile(b2m_ctx* h, const char* path, b2m_matr
     if (!dst) return B2M_OK;
     if (LineWidth < p.width * 8 || (LineWidth % 8)) return fail(ctx, B2M_ERR_DIM, "Line widths do not match");
     if (p.width == 0 || p.height == 0) return B2M_OK;
-    std::lock_guard<std::mutex> lk(ctx->mtx);
+    CallLock lk(ctx);
     cudaSetDevice(ctx->device);
     B2M_CU(ctx, cudaMemcpy2DAsync(dst, LineWidth, p.data.data(), p.width * 8, p.width * 8, p.height,
                                   cudaMemcpyHostToDevice, ctx->stream));

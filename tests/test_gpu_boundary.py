@@ -39,8 +39,14 @@ def test_resident_chain_and_sub_matrix_view(ctx):
     and a solve on a sub-matrix view of a larger resident matrix, against the oracle."""
     r = oracle.Mersenne(seed=77)
     n = 384
-    a = r.uniform(n, n) - 0.5
+    # well-conditioned factors (kappa < 2 each) so that solutions can be held to 1e-12 against the
+    # oracle: A = R1 - 0.5 + 2 sqrt(n) I and B = R2 - 0.5 + 2 sqrt(n) S, S the cyclic shift by 23
+    # columns, so that the product's dominant entries C[i, i + 23] lie on the diagonal of the
+    # 200 x 200 view at (17, 40) as well
+    s = 2.0 * np.sqrt(n)
+    a = r.uniform(n, n) - 0.5 + s * np.eye(n)
     b = r.uniform(n, n) - 0.5
+    b[np.arange(n), (np.arange(n) + 23) % n] += s
     d = r.uniform(n, 3) - 0.5
     A, B, D = (L.ResidentMatrix.from_host(m, ctx=ctx) for m in (a, b, d))
     try:

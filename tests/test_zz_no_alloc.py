@@ -31,7 +31,9 @@ def test_noalloc_solve_matches_allocating_solve_twice(ctx):
     stream = torch.cuda.current_stream().cuda_stream
     for n, k, seed in ((300, 5, 1), (512, 64, 2)):
         r = inputs.rng(seed)
-        a_np, b_np = r.random_sample((n, n)) - 0.5, r.standard_normal((n, k))
+        # R - 0.5 + 2 sqrt(n) I has ||R - 0.5||_2 ~ 0.58 sqrt(n), so kappa < 2: two correct solves
+        # then agree to a few ulps, which is what the 1e-12 bar against the oracle can hold
+        a_np, b_np = r.random_sample((n, n)) - 0.5 + 2.0 * np.sqrt(n) * np.eye(n), r.standard_normal((n, k))
         a, b = torch.from_numpy(a_np).cuda(), torch.from_numpy(b_np).cuda()
         x_ref = torch.empty_like(b)
         st_ref = torch.zeros(1, dtype=torch.int32, device="cuda")
