@@ -89,6 +89,7 @@ struct Ctx {
     int device = 0;
     int num_sms = 148;
     int sweep_ctas = -1;  // co-resident CTAs of the persistent refinement sweep (-1: not queried yet)
+    int chain_clusters = -1;  // co-resident 8-CTA clusters of the chained sweep (0: unusable, -1: not probed)
     int64_t wait_limit = -1;  // polls of the refinement sweeps' bounded waits (-1: the built-in limit)
     size_t smem_optin = 0;
     cudaStream_t own_stream = nullptr;
@@ -230,6 +231,33 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int32_
         if (mbar_try_wait(bar, parity)) return true;
     if (timeout_word) atomicExch(timeout_word, site);
     return false;
+}
+
+// Distributed shared memory of a thread-block cluster: the address of `local` in CTA `rank`, a
+// 16-byte store into another CTA's shared memory completing on its mbarrier, and a wait on this
+// CTA's mbarrier that acquires at cluster scope.
+__device__ __forceinline__ uint32_t map_rank(const void* local, uint32_t rank) {
+    uint32_t r;
+    asm volatile("mapa.shared::cluster.u32 %0, %1, %2;\n" : "=r"(r) : "r"(smem_u32(local)), "r"(rank));
+    return r;
+}
+
+__device__ __forceinline__ void st_async16(uint32_t raddr, uint4 v, uint32_t rbar) {
+    asm volatile("st.async.shared::cluster.mbarrier::complete_tx::bytes.v4.b32 [%0], {%1, %2, %3, %4}, [%5];\n" ::"r"(
+                     raddr),
+                 "r"(v.x), "r"(v.y), "r"(v.z), "r"(v.w), "r"(rbar)
+                 : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait_cluster(uint64_t* bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.acquire.cluster.shared::cta.b64 p, [%1], %2;\n"
+        " selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
 }
 
 // 2-D tiled TMA load (no multicast) into shared memory, completing on `bar`.

@@ -19,8 +19,12 @@
 #include <cmath>
 #include <vector>
 
+#include <cooperative_groups.h>
+
 #include "common.cuh"
 #include "kernels.cuh"
+
+namespace cg = cooperative_groups;
 
 namespace b2m {
 namespace {
@@ -517,6 +521,219 @@ __global__ void __launch_bounds__(256, 1) trsv_sweep_kernel(SwArgs a) {
     }
 }
 
+// Chained variant of trsv_sweep_kernel on thread-block clusters of kChCl consecutive blocks (in
+// sweep order, one right-hand-side group per cluster row): besides publishing its solution to
+// global memory, a block pushes it into the shared memory of every later block of its cluster
+// (st.async completing on the receiver's mbarrier for that sender, 4 KiB each), and a block folds
+// the earlier blocks of its own cluster in from there.  Only the hop into the first block of a
+// cluster pays a round trip through L2; the other seven ride on distributed shared memory.  Every
+// wait is bounded; a wait that gives up flags status[kTimeout], which every other wait also polls,
+// so the whole sweep winds down quickly.  All CTAs of a cluster meet at a cluster barrier after
+// the mbarriers are initialised and before they exit.
+constexpr int kChCl = 8;
+constexpr int kChSlot = kTrsvNB * kSwRhs * (int)sizeof(float);        // one pushed solution block
+constexpr int kChSmem = kSwSmem + (kChCl - 1) * kChSlot;             // + receive slots
+
+__device__ __forceinline__ int ld_volatile_i32(const int32_t* p) { return *reinterpret_cast<const volatile int32_t*>(p); }
+
+__global__ void __cluster_dims__(kChCl, 1, 1) __launch_bounds__(256, 1) trsv_chain_kernel(SwArgs a, int nbp) {
+    extern __shared__ __align__(16) float4 sw_dyn[];
+    __shared__ __align__(16) float s_p[kTrsvNB][kSwRhs];  // x of a block from another cluster
+    __shared__ __align__(16) float s_y[kTrsvNB][kSwRhs];
+    __shared__ __align__(16) float s_h[kTrsvNB][kSwRhs];
+    __shared__ __align__(8) uint64_t s_bar[kChCl];       // one per earlier block of the cluster
+    __shared__ int s_abort;
+    float4* s_inv = sw_dyn;                        // [32][128]: s_inv[kq][r] = inv[r][4kq .. 4kq+3]
+    float4* s_w = sw_dyn + kTrsvNB * kTrsvNB / 4;  // same layout for W_b
+    float (*s_rx)[kTrsvNB][kSwRhs] = reinterpret_cast<float (*)[kTrsvNB][kSwRhs]>(sw_dyn + kTrsvNB * kTrsvNB / 2);
+    if (a.status[kInfo] != 0) return;  // uniform: written before the launch
+    cg::cluster_group cluster = cg::this_cluster();
+    const int t = threadIdx.x;
+    const int NB = kTrsvNB;
+    const int nblk = (int)ceil_div(a.n, NB);
+    const int g = blockIdx.x / nbp, bi = blockIdx.x - g * nbp;
+    const int rank = (int)cluster.block_rank();  // bi % kChCl: nbp is a multiple of kChCl
+    const int cl0 = bi - rank;
+    if (t == 0) {
+        for (int q = 0; q < rank; ++q) mbar_init(&s_bar[q], 1);
+        fence_barrier_init();
+        for (int q = 0; q < rank; ++q) mbar_arrive_expect_tx(&s_bar[q], kChSlot);
+        s_abort = 0;
+    }
+    cluster.sync();  // every receiver's mbarriers are armed before the first push
+    if (bi >= nblk) {  // padding CTA of the last cluster
+        cluster.sync();
+        return;
+    }
+    const int b = a.upper ? nblk - 1 - bi : bi;
+    const int b0 = b * NB, bs = min(NB, a.n - b0);
+    const int r = t & (NB - 1), h = t >> 7;
+    const int cgc = a.c0 + g * kSwRhs;
+    const int ncg = min(kSwRhs, a.nc - g * kSwRhs);
+    {
+        const float* inv = a.inv + (int64_t)b * NB * NB;
+        const float* w = a.w + (int64_t)b * NB * NB;
+#pragma unroll 4
+        for (int i = 0; i < 16; ++i) {
+            const int e = t + 256 * i, rr = e & (NB - 1), kq = e >> 7;
+            cp_async16(s_inv + kq * NB + rr, inv + rr * NB + 4 * kq, 16);
+            if (bi > 0) cp_async16(s_w + kq * NB + rr, w + rr * NB + 4 * kq, 16);
+        }
+        cp_async_commit();
+    }
+    float xb[kSwRhs];
+#pragma unroll
+    for (int q = 0; q < kSwRhs; ++q)
+        xb[q] = (h == 0 && r < bs && q < ncg) ? a.Xr[(int64_t)(b0 + r) * a.ldr + cgc + q] : 0.f;
+    float acc[kSwRhs];
+#pragma unroll
+    for (int q = 0; q < kSwRhs; ++q) acc[q] = 0.f;
+    const int ng = (int)ceil_div(a.nc, kSwRhs);
+    unsigned long long* ll_own = a.ll + (size_t)(b * ng + g) * (kTrsvNB * kSwRhs);
+    int32_t* tmo = &a.status[kTimeout];
+    auto abandon = [&]() {
+#pragma unroll
+        for (int e = 0; e < 4; ++e) st_relaxed64(ll_own + 4 * t + e, (unsigned long long)kSwAbort << 32);
+    };
+    // block j (sweep position jj) from another cluster: global words into s_p
+    auto wait_global = [&](int j) -> bool {
+        const int k = t >> 1, q0 = (t & 1) * 4;
+        const unsigned long long* src = a.ll + (size_t)(j * ng + g) * (kTrsvNB * kSwRhs) + k * kSwRhs + q0;
+        unsigned long long w[4] = {0ull, 0ull, 0ull, 0ull};
+        bool ready = false, bad = false;
+        for (uint32_t it = 0; it < a.spin && !ready && !bad; ++it) {
+#pragma unroll
+            for (int e = 0; e < 4; ++e) w[e] = ld_relaxed64(src + e);
+            ready = true;
+#pragma unroll
+            for (int e = 0; e < 4; ++e) {
+                const uint32_t f = (uint32_t)(w[e] >> 32);
+                ready = ready && f == 1u;
+                bad = bad || f == kSwAbort;
+            }
+            if ((it & 255u) == 255u && ld_volatile_i32(tmo) != 0) bad = true;
+        }
+        if (!ready && !bad) atomicCAS(tmo, 0, 503);
+        if (!ready) s_abort = 1;
+        const float4 v = make_float4(__uint_as_float((uint32_t)w[0]), __uint_as_float((uint32_t)w[1]),
+                                     __uint_as_float((uint32_t)w[2]), __uint_as_float((uint32_t)w[3]));
+        *reinterpret_cast<float4*>(&s_p[k][q0]) = v;
+        __syncthreads();
+        return !s_abort;
+    };
+    // the push of cluster rank q into s_rx[q]
+    auto wait_push = [&](int q) -> bool {
+        bool ready = false, bad = false;
+        for (uint32_t it = 0; it < a.spin && !ready && !bad; ++it) {
+            ready = mbar_try_wait_cluster(&s_bar[q], 0);
+            if (!ready && (it & 255u) == 255u && ld_volatile_i32(tmo) != 0) bad = true;
+        }
+        if (!ready && !bad) atomicCAS(tmo, 0, 504);
+        if (!ready) s_abort = 1;
+        __syncthreads();
+        return !s_abort;
+    };
+
+    bool ok = true;
+    for (int jj = 0; ok && jj + 1 < bi; ++jj) {
+        const int j = a.upper ? nblk - 1 - jj : jj;
+        const int p0 = j * NB, ps = min(NB, a.n - p0);
+        float4 tv[16];
+        {
+            const float* trow = a.T + (int64_t)(b0 + min(r, bs - 1)) * a.ld + p0;
+#pragma unroll
+            for (int i = 0; i < 16; ++i)
+                tv[i] = r < bs ? ld_row4(trow, 64 * h + 4 * i, ps) : make_float4(0.f, 0.f, 0.f, 0.f);
+        }
+        const bool local = jj >= cl0;
+        ok = local ? wait_push(jj - cl0) : wait_global(j);
+        if (!ok) break;
+        const float (*P)[kSwRhs] = local ? s_rx[jj - cl0] : s_p;
+#pragma unroll
+        for (int i = 0; i < 16; ++i) {
+            const float tk[4] = {tv[i].x, tv[i].y, tv[i].z, tv[i].w};
+#pragma unroll
+            for (int e = 0; e < 4; ++e) {
+                const int k = 64 * h + 4 * i + e;
+                const float4 x0 = *reinterpret_cast<const float4*>(&P[k][0]);
+                const float4 x1 = *reinterpret_cast<const float4*>(&P[k][4]);
+                acc[0] = fmaf(tk[e], x0.x, acc[0]);
+                acc[1] = fmaf(tk[e], x0.y, acc[1]);
+                acc[2] = fmaf(tk[e], x0.z, acc[2]);
+                acc[3] = fmaf(tk[e], x0.w, acc[3]);
+                acc[4] = fmaf(tk[e], x1.x, acc[4]);
+                acc[5] = fmaf(tk[e], x1.y, acc[5]);
+                acc[6] = fmaf(tk[e], x1.z, acc[6]);
+                acc[7] = fmaf(tk[e], x1.w, acc[7]);
+            }
+        }
+        __syncthreads();  // s_p is rewritten by the next global wait
+    }
+    if (ok) {
+        if (h == 1) {
+#pragma unroll
+            for (int q = 0; q < kSwRhs; ++q) s_h[r][q] = acc[q];
+        }
+        cp_async_wait<0>();
+        __syncthreads();
+        if (h == 0) {
+#pragma unroll
+            for (int q = 0; q < kSwRhs; ++q) s_y[r][q] = xb[q] - acc[q] - s_h[r][q];
+        }
+        __syncthreads();
+#pragma unroll
+        for (int q = 0; q < kSwRhs; ++q) acc[q] = 0.f;
+        sw_smem_product(s_inv, r, h, s_y, acc);
+        if (bi > 0) {  // x_b = z - W_b x_p
+            const bool local = bi - 1 >= cl0;
+            ok = local ? wait_push(bi - 1 - cl0) : wait_global(a.upper ? b + 1 : b - 1);
+            if (ok) {
+#pragma unroll
+                for (int q = 0; q < kSwRhs; ++q) acc[q] = -acc[q];
+                sw_smem_product(s_w, r, h, local ? s_rx[bi - 1 - cl0] : s_p, acc);
+#pragma unroll
+                for (int q = 0; q < kSwRhs; ++q) acc[q] = -acc[q];
+            }
+        }
+    }
+    if (ok) {
+        if (h == 1) {
+#pragma unroll
+            for (int q = 0; q < kSwRhs; ++q) s_h[r][q] = acc[q];
+        }
+        __syncthreads();
+        if (h == 0) {
+            float xv[kSwRhs];
+#pragma unroll
+            for (int q = 0; q < kSwRhs; ++q) xv[q] = (r < bs && q < ncg) ? acc[q] + s_h[r][q] : 0.f;
+            // the later blocks of this cluster first (they are on the chain), then global memory
+            for (int d = rank + 1; d < kChCl && cl0 + d < nblk; ++d) {
+                const uint32_t rb = map_rank(&s_bar[rank], (uint32_t)d);
+                const uint32_t dst = map_rank(&s_rx[rank][r][0], (uint32_t)d);
+                st_async16(dst, make_uint4(__float_as_uint(xv[0]), __float_as_uint(xv[1]), __float_as_uint(xv[2]),
+                                           __float_as_uint(xv[3])), rb);
+                st_async16(dst + 16, make_uint4(__float_as_uint(xv[4]), __float_as_uint(xv[5]),
+                                                __float_as_uint(xv[6]), __float_as_uint(xv[7])), rb);
+            }
+#pragma unroll
+            for (int q = 0; q < kSwRhs; ++q) st_relaxed64(ll_own + r * kSwRhs + q, (1ull << 32) | __float_as_uint(xv[q]));
+            if (r < bs) {
+#pragma unroll
+                for (int q = 0; q < kSwRhs; ++q)
+                    if (q < ncg) a.Xr[(int64_t)(b0 + r) * a.ldr + cgc + q] = xv[q];
+                if (a.upper) {  // the FP64 accumulation is off the chain
+#pragma unroll
+                    for (int q = 0; q < kSwRhs; ++q)
+                        if (q < ncg) a.X64[(int64_t)(b0 + r) * a.ldx + cgc + q] += (double)xv[q];
+                }
+            }
+        }
+    } else {
+        abandon();
+    }
+    cluster.sync();  // no CTA leaves while a push into its shared memory may be in flight
+}
+
 struct ReArgs {
     const double* A;
     int64_t lda;
@@ -643,6 +860,44 @@ __global__ void __launch_bounds__(256, 1) resid_kernel(ReArgs a) {
     }
 }
 
+// Whether the chained sweep can run here, and how many of its clusters fit at once: one launch
+// of it with no blocks to solve (every CTA is padding and only meets its cluster's barriers) as a
+// cooperative cluster launch, outside any capture.  A launch error leaves the chained sweep off.
+int32_t chain_probe(Ctx* ctx, cudaStream_t st) {
+    if (ctx->chain_clusters >= 0) return B2M_OK;
+    ctx->chain_clusters = 0;
+    if (cudaFuncSetAttribute(trsv_chain_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kChSmem) != cudaSuccess) {
+        (void)cudaGetLastError();
+        return B2M_OK;
+    }
+    cudaLaunchConfig_t cfg{};
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeCooperative;
+    at[0].val.cooperative = 1;
+    cfg.gridDim = dim3((unsigned)kChCl);
+    cfg.blockDim = dim3(256);
+    cfg.dynamicSmemBytes = kChSmem;
+    cfg.stream = st;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    int clusters = 0;
+    if (cudaOccupancyMaxActiveClusters(&clusters, trsv_chain_kernel, &cfg) != cudaSuccess || clusters < 1) {
+        (void)cudaGetLastError();
+        return B2M_OK;
+    }
+    SwArgs sa{};
+    sa.n = 0;  // no blocks: every CTA is padding
+    sa.status = ctx->d_status;
+    if (cudaLaunchKernelEx(&cfg, trsv_chain_kernel, sa, (int)kChCl) != cudaSuccess ||
+        cudaStreamSynchronize(st) != cudaSuccess) {
+        (void)cudaGetLastError();
+        return B2M_OK;
+    }
+    B2M_LAUNCHED(ctx);
+    ctx->chain_clusters = clusters;
+    return B2M_OK;
+}
+
 // FP32 solve of the refinement: Xr (already permuted) <- U^-1 L^-1 Xr, X64 += Xr.
 int32_t ir_solve(Ctx* ctx, cudaStream_t st, const float* LU, int64_t ld, int64_t n, const F32Scratch& s, float* Xr,
                  int64_t ldr, int64_t nrhs, double* X64, int64_t ldx) {
@@ -658,6 +913,32 @@ int32_t ir_solve(Ctx* ctx, cudaStream_t st, const float* LU, int64_t ld, int64_t
     for (int64_t c0 = 0; c0 < nrhs; c0 += kTrMaxRhs) {
         const int nc = (int)std::min<int64_t>(kTrMaxRhs, nrhs - c0);
         const int ng = (int)ceil_div(nc, kSwRhs);
+        const int nbp = (int)round_up(nblk, kChCl);
+        if (ng <= kSweepGroups && ng * nbp / kChCl <= ctx->chain_clusters) {
+            // chained sweeps on clusters: one cooperative launch each
+            for (int up = 0; up < 2; ++up) {
+                const size_t ll_words = (size_t)nblk * ng * kTrsvNB * kSwRhs;
+                unsigned long long* ll = s.ll + up * (size_t)nblk * kSweepGroups * kTrsvNB * kSwRhs;
+                B2M_CU(ctx, cudaMemsetAsync(ll, 0, ll_words * sizeof(unsigned long long), st));
+                SwArgs sa{LU,  ld, (int)n, up ? s.uinv : s.linv, up ? s.wu : s.wl, Xr, ldr, (int)c0, nc, X64, ldx, up,
+                          ll, ctx->d_status, ctx->wait_limit >= 0 ? (uint32_t)ctx->wait_limit : kSwSpin};
+                cudaLaunchConfig_t cfg{};
+                cudaLaunchAttribute at[1];
+                at[0].id = cudaLaunchAttributeCooperative;
+                at[0].val.cooperative = 1;
+                cfg.gridDim = dim3((unsigned)(nbp * ng));
+                cfg.blockDim = dim3(256);
+                cfg.dynamicSmemBytes = kChSmem;
+                cfg.stream = st;
+                cfg.attrs = at;
+                cfg.numAttrs = 1;
+                prof_begin(ctx, st, kClsSolve);
+                B2M_CU(ctx, cudaLaunchKernelEx(&cfg, trsv_chain_kernel, sa, nbp));
+                prof_end(ctx, st, kClsSolve, 4.0 * (double)n * n / 2 + 4.0 * nblk * kTrsvNB * kTrsvNB + 8.0 * n * nc);
+                B2M_LAUNCHED(ctx);
+            }
+            continue;
+        }
         if (nblk * ng <= coop_ctas && ng <= kSweepGroups) {
             // persistent sweeps: one cooperative launch each
             for (int up = 0; up < 2; ++up) {
@@ -775,6 +1056,7 @@ int32_t solve_mixed(Ctx* ctx, cudaStream_t st, const double* A, int64_t lda, int
     B2M_CU(ctx, cudaMemsetAsync(ctx->d_status, 0, kNumStatus * sizeof(int32_t), st));
     f64_to_f32_kernel<<<gsz(n * n), 256, 0, st>>>(A, lda, A32, ld32, n, n);
     B2M_LAUNCHED(ctx);
+    B2M_TRY(chain_probe(ctx, st));
     B2M_TRY(lu_factor_f32(ctx, st, A32, ld32, n, perm, mode, sc));
     B2M_CU(ctx, cudaMemsetAsync(nrm, 0, sizeof(unsigned long long), st));
     norm_inf_kernel<<<gsz(n, 8), 256, 0, st>>>(A, lda, n, nrm);

@@ -72,30 +72,6 @@ __device__ __forceinline__ void warp_best(float& a, int& i) {
     }
 }
 
-__device__ __forceinline__ uint32_t map_rank(const void* local, uint32_t rank) {
-    uint32_t r;
-    asm volatile("mapa.shared::cluster.u32 %0, %1, %2;\n" : "=r"(r) : "r"(smem_u32(local)), "r"(rank));
-    return r;
-}
-
-__device__ __forceinline__ void st_async16(uint32_t raddr, uint4 v, uint32_t rbar) {
-    asm volatile("st.async.shared::cluster.mbarrier::complete_tx::bytes.v4.b32 [%0], {%1, %2, %3, %4}, [%5];\n" ::"r"(
-                     raddr),
-                 "r"(v.x), "r"(v.y), "r"(v.z), "r"(v.w), "r"(rbar)
-                 : "memory");
-}
-
-__device__ __forceinline__ bool mbar_try_wait_cluster(uint64_t* bar, uint32_t parity) {
-    uint32_t ok;
-    asm volatile(
-        "{\n .reg .pred p;\n mbarrier.try_wait.parity.acquire.cluster.shared::cta.b64 p, [%1], %2;\n"
-        " selp.u32 %0, 1, 0, p;\n}\n"
-        : "=r"(ok)
-        : "r"(smem_u32(bar)), "r"(parity)
-        : "memory");
-    return ok != 0;
-}
-
 __device__ __forceinline__ uint4 pack_cand(double a, int i) {
     const unsigned long long b = __double_as_longlong(a);
     return make_uint4((uint32_t)b, (uint32_t)(b >> 32), (uint32_t)i, 0u);
