@@ -177,6 +177,7 @@ struct F32Scratch {
     float* mvals;
     float* wmat;
     int* moves;
+    float* lmul;
     int32_t* pmap;
     float* lpinv;
     float *bth, *btl, *ah, *al;

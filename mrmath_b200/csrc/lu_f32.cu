@@ -12,13 +12,10 @@
 //     K = 256): the next panel's columns first, the rest on a side stream under the next panel's
 //     leaves (look-ahead);
 //   * inside a panel, 32-column leaves.  tslu_select_kernel runs Gaussian elimination with
-//     partial pivoting warp by warp, with no block barrier inside an elimination: every warp of a
-//     CTA eliminates 128 rows of the CTA's 512-row chunk and nominates 32 candidate rows, and one
-//     warp eliminates the 4 x 32 candidates' original rows to the chunk's 32.  The last CTA of
-//     every group of 16 chunks (found with an atomic counter, no spinning) merges the group's
-//     candidate sets the same way (four warps over four sets each, then one warp over their
-//     four), up to a single root.  The root's pivots are the leaf's pivots and its eliminated rows
-//     are the leaf's L11\U11;
+//     partial pivoting on 512-row chunks in parallel; each chunk nominates 32 candidate rows, and
+//     the last CTA of every group of 16 chunks (found with an atomic counter, no spinning) runs
+//     the same elimination on the stacked candidates' original rows, up to a single root.  The
+//     root's pivots are the leaf's pivots and its eliminated rows are the leaf's L11\U11;
 //   * tslu_apply_kernel moves the chosen rows into place (a side buffer holds the rows whose
 //     slots get overwritten, so the move is race free), forms L21 = A21 U11^-1 and applies the
 //     leaf's rank-32 update to the rest of the panel; it records the moves in `perm` and in the
@@ -36,12 +33,10 @@
 namespace b2m {
 namespace {
 
-constexpr int kTsWarps = 4;
-constexpr int kTsThreads = 32 * kTsWarps;
-constexpr int kTsR = 4;                           // rows per lane in every elimination
-constexpr int kTsWarpRows = 32 * kTsR;            // rows per warp elimination (4 candidate sets)
-constexpr int kTsRows = kTsWarps * kTsWarpRows;   // rows per level-0 chunk (one CTA)
-constexpr int kTsFan = kTsWarps * kTsR;           // candidate sets merged per tree node (16)
+constexpr int kTsThreads = 256;
+constexpr int kTsRpt = 2;                         // rows per thread in the elimination
+constexpr int kTsRows = kTsThreads * kTsRpt;      // rows per chunk / per merge
+constexpr int kTsFan = kTsRows / 32;              // candidate sets merged per tree node (16)
 constexpr int kTsLevels = 4;
 constexpr int kTsMaxCand = 2048;                  // nodes per level (rows <= 1M)
 constexpr int kNB = 256;                          // outer panel width
@@ -57,6 +52,7 @@ struct TsArgs {
     float* mvals;         // [32][kNB]: original content of the top rows that move below the leaf
     float* wmat;          // [32][kNB]: U11^-1 in the leaf's columns, U11^-1 U12 right of them
     int* moves;           // [0] moves, [1] moves below the top block, [2..66) dst, [66..130) src
+    float* lmul;          // [32][kTsRows] the root elimination's multipliers
     int32_t* pmap;        // first leaf of a panel: pmap[i] = i for the panel's rows (identity)
     float* lpinv;         // [kNB / 32][32][32]: L11^-1 of each leaf of the outer panel
     int32_t* status;
@@ -70,74 +66,87 @@ __device__ __forceinline__ float rcp_nr(float x) {
     return r * fmaf(-x, r, 2.0f);
 }
 
-// Warp-synchronous Gaussian elimination with partial pivoting of up to 128 stacked rows (lane l
-// holds stack rows 32 r + l, r < 4, in registers) over w <= 32 columns: no block barrier, one
-// __syncwarp per column.  Per column the lane with the largest |v| (lowest lane, then lowest r,
-// among equals) publishes its row through a double-buffered shared slot and every lane reads it
-// back.  One column per iteration of a runtime loop: every row shifts left by one as its column
-// is eliminated (the update writes v[k - 1]), so the current column is always v[0].
-// win_rid[j] = row id of pivot j (-1 if the stack ran out).  The root (kRoot) also records the
-// pivot's stack slot (win_slot), the pivot rows as chosen (u[j] = row j of U from column j on)
-// and every row's multiplier of column j (lm[j][slot]), which give the rows of L.
-struct WarpElim {
-    float4 prow[2][8];
+// Gaussian elimination with partial pivoting of up to 512 stacked rows (thread t holds stack rows
+// t and t + 256 in registers) over w <= 32 columns.  Chooses w pivot rows (largest magnitude);
+// s_win[j] = row id of pivot j and s_loc[j] = its stack index (-1 if the stack ran out).
+//
+// One column per iteration of a runtime loop (a compact body: unrolled multi-column steps spill
+// out of the instruction cache).  Register indices stay compile-time because every row shifts
+// left by one as its column is eliminated (the update writes v[k - 1]), so the current column is
+// always v[0].  One barrier per column: every warp's best lane publishes its candidate row (and
+// key) before the barrier (double-buffered by column parity); afterwards all threads pick the
+// winning warp with a warp reduction over the keys and read its row directly.  For the root
+// (lm given) the winner of column j is copied to s_u[j] (row j of U, from column j on) and every
+// row's multiplier of column j goes to lm[j][stack index] (global scratch), which gives the rows
+// of L; keeping them out of shared memory lets the CTA share an SM with a tensor-core GEMM.
+struct GeppSmem {
+    float4 cand[2][kTsThreads / 32][8];  // candidate rows by column parity and warp (column j first)
+    unsigned key[2][kTsThreads / 32];
+    unsigned slot[2][kTsThreads / 32];
+    float4 u[32][8];                     // root: pivot rows as chosen
 };
 
-template <bool kRoot>
-__device__ __forceinline__ void warp_gepp(float (&v)[kTsR][32], const int (&rid)[kTsR], int w, WarpElim& we,
-                                          int* win_rid, int* win_slot, float* lm, float4 (*u)[8]) {
-    const int lane = threadIdx.x & 31;
-    bool live[kTsR];
+__device__ __forceinline__ void block_gepp(float (&v)[kTsRpt][32], const int (&rid)[kTsRpt], int w, int* s_win,
+                                           int* s_loc, GeppSmem& g, float* lm) {
+    const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+    bool live[kTsRpt];
 #pragma unroll
-    for (int r = 0; r < kTsR; ++r) live[r] = rid[r] >= 0;
-    win_rid[lane] = -1;
-    if (kRoot) win_slot[lane] = -1;
-    __syncwarp();
+    for (int r = 0; r < kTsRpt; ++r) live[r] = rid[r] >= 0;
+    if (t < 32) { s_win[t] = -1; s_loc[t] = -1; }
 #pragma unroll 1
     for (int j = 0; j < w; ++j) {
         const int b = j & 1;
         unsigned key = 0u;
         int rbest = 0;
 #pragma unroll
-        for (int r = 0; r < kTsR; ++r) {
+        for (int r = 0; r < kTsRpt; ++r) {
             const unsigned k = live[r] ? __float_as_uint(fabsf(v[r][0])) + 1u : 0u;
             if (k > key) { key = k; rbest = r; }
         }
         const unsigned wk = __reduce_max_sync(0xffffffffu, key);
-        if (wk == 0u) break;  // no live row left (uniform)
-        const int wl = __ffs(__ballot_sync(0xffffffffu, key == wk)) - 1;
-        if (lane == wl) {
+        const unsigned bal = __ballot_sync(0xffffffffu, key == wk && key != 0u);
+        if (lane == (bal ? __ffs(bal) - 1 : 0)) {
 #pragma unroll
-            for (int r = 0; r < kTsR; ++r) {
+            for (int r = 0; r < kTsRpt; ++r) {
                 if (r == rbest) {
 #pragma unroll
                     for (int q = 0; q < 8; ++q)
-                        we.prow[b][q] = make_float4(v[r][4 * q], v[r][4 * q + 1], v[r][4 * q + 2], v[r][4 * q + 3]);
-                    live[r] = false;
-                    win_rid[j] = rid[r];
-                    if (kRoot) win_slot[j] = r * 32 + lane;
+                        g.cand[b][warp][q] = make_float4(v[r][4 * q], v[r][4 * q + 1], v[r][4 * q + 2], v[r][4 * q + 3]);
                 }
             }
+            g.key[b][warp] = wk;
+            g.slot[b][warp] = (unsigned)(rbest * kTsThreads + t);
         }
-        __syncwarp();
+        __syncthreads();
+        // winning warp: largest key, lowest warp among equals
+        const unsigned kq = g.key[b][lane & (kTsThreads / 32 - 1)];
+        const unsigned pk = __reduce_max_sync(0xffffffffu, kq);
+        if (pk == 0u) break;  // no live row left anywhere (uniform)
+        const int pwarp = __ffs(__ballot_sync(0xffffffffu, kq == pk)) - 1;
+        const unsigned ps = g.slot[b][pwarp];
         float pr[32];
 #pragma unroll
         for (int q = 0; q < 8; ++q) {
-            const float4 f = we.prow[b][q];
+            const float4 f = g.cand[b][pwarp][q];
             pr[4 * q] = f.x; pr[4 * q + 1] = f.y; pr[4 * q + 2] = f.z; pr[4 * q + 3] = f.w;
         }
-        if (kRoot && lane < 8) u[j][lane] = we.prow[b][lane];
-        const float rcp = wk > 1u ? rcp_nr(pr[0]) : 0.0f;  // a zero column eliminates nothing
+        if (lm && t < 8) g.u[j][t] = g.cand[b][pwarp][t];
+        const float rcp = pk > 1u ? rcp_nr(pr[0]) : 0.0f;  // a zero column eliminates nothing
 #pragma unroll
-        for (int r = 0; r < kTsR; ++r) {
+        for (int r = 0; r < kTsRpt; ++r) {
+            if (ps == (unsigned)(r * kTsThreads + t)) {
+                live[r] = false;
+                s_win[j] = rid[r];
+                s_loc[j] = r * kTsThreads + t;
+            }
             const float l = live[r] ? v[r][0] * rcp : 0.f;
-            if (kRoot) lm[j * kTsWarpRows + r * 32 + lane] = l;
+            if (lm) lm[j * kTsRows + r * kTsThreads + t] = l;
 #pragma unroll
             for (int k = 1; k < 32; ++k) v[r][k - 1] = fmaf(-l, pr[k], v[r][k]);
             v[r][31] = 0.f;
         }
     }
-    __syncwarp();
+    __syncthreads();
 }
 
 // loads columns [c0, c0 + w) of row `row` (zeros past w); rows are 128-byte aligned
@@ -158,32 +167,9 @@ __device__ __forceinline__ void load_leaf_row(const float* A, int64_t ld, int ro
         if (k >= w) x[k] = 0.f;
 }
 
-// One merge by warp `warp`: sets [4 warp, 4 warp + 4) of `sets` (row ids, 32 per set, -1 = none;
-// only the first nsets exist) are stacked, their original rows loaded and eliminated; the warp's
-// 32 winners go to out[32].
-template <bool kRoot>
-__device__ __forceinline__ void warp_merge(const TsArgs& a, const int* sets, int nsets, WarpElim& we, int* out,
-                                           int* win_slot, float* lm, float4 (*u)[8]) {
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    int rid[kTsR];
-    float v[kTsR][32];
-#pragma unroll
-    for (int r = 0; r < kTsR; ++r) {
-        const int set = kTsR * warp + r;
-        rid[r] = set < nsets ? sets[set * 32 + lane] : -1;
-    }
-#pragma unroll
-    for (int r = 0; r < kTsR; ++r) load_leaf_row(a.A, a.ld, rid[r], a.lc0, a.w, v[r]);
-    warp_gepp<kRoot>(v, rid, a.w, we, out, win_slot, lm, u);
-}
-
 __global__ void __launch_bounds__(kTsThreads) tslu_select_kernel(TsArgs a) {
-    __shared__ __align__(16) WarpElim s_we[kTsWarps];
-    __shared__ int s_sets[kTsFan * 32];           // candidate sets being merged (row ids)
-    __shared__ int s_part[kTsWarps * 32];         // the merging warps' winners
+    __shared__ __align__(16) GeppSmem s_g;
     __shared__ int s_win[32], s_loc[32];
-    __shared__ __align__(16) float4 s_u[32][8];   // root: pivot rows as chosen
-    __shared__ float s_lm[32 * kTsWarpRows];      // root: multipliers by column and stack slot
     __shared__ float s_lu[32][33];
     __shared__ __align__(16) float s_lt[32][32];  // s_lt[j][k] = L(k, j) for k > j, else 0
     __shared__ __align__(16) float s_ut[32][32];  // s_ut[i][k] = U(k, i) for k < i, else 0
@@ -191,48 +177,22 @@ __global__ void __launch_bounds__(kTsThreads) tslu_select_kernel(TsArgs a) {
     __shared__ int s_last, s_bad;
     __shared__ int s_flag[32], s_outpos[32], s_mdst[64], s_msrc[64], s_nm, s_nout;
     if (a.status[kInfo] != 0) return;
-    const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+    const int t = threadIdx.x;
     const int m = a.n - a.lc0;
-    int count = (int)ceil_div(m, kTsRows), node = blockIdx.x, level = 0;
-
-    // ---- level 0: every warp eliminates its 128 rows of the chunk; a chunk of at most 128 rows is
-    // the whole leaf, and its single elimination is the root
-    {
-        const bool root = m <= kTsWarpRows;
-        int rid[kTsR];
-        float v[kTsR][32];
+    float v[kTsRpt][32];
+    int rid[kTsRpt];
 #pragma unroll
-        for (int r = 0; r < kTsR; ++r) {
-            const int row = a.lc0 + blockIdx.x * kTsRows + warp * kTsWarpRows + r * 32 + lane;
-            rid[r] = row < a.n ? row : -1;
-            if (a.pmap && row < a.n) a.pmap[row] = row;
-        }
-        if (root) {
-            if (warp == 0) {
-#pragma unroll
-                for (int r = 0; r < kTsR; ++r) load_leaf_row(a.A, a.ld, rid[r], a.lc0, a.w, v[r]);
-                warp_gepp<true>(v, rid, a.w, s_we[0], s_win, s_loc, s_lm, s_u);
-            }
-            count = 0;  // done: the root ran
-        } else {
-#pragma unroll
-            for (int r = 0; r < kTsR; ++r) load_leaf_row(a.A, a.ld, rid[r], a.lc0, a.w, v[r]);
-            warp_gepp<false>(v, rid, a.w, s_we[warp], s_sets + warp * 32, nullptr, nullptr, nullptr);
-        }
+    for (int r = 0; r < kTsRpt; ++r) {
+        const int row = a.lc0 + blockIdx.x * kTsRows + r * kTsThreads + t;
+        rid[r] = row < a.n ? row : -1;
+        load_leaf_row(a.A, a.ld, rid[r], a.lc0, a.w, v[r]);
+        if (a.pmap && row < a.n) a.pmap[row] = row;
     }
-    __syncthreads();
-    // ---- the chunk's merge: warp 0 reduces the 4 warps' sets to the chunk's 32 candidates (the
-    // root when the chunk is the whole leaf)
-    if (count == 1) {
-        if (warp == 0) warp_merge<true>(a, s_sets, kTsWarps, s_we[0], s_win, s_loc, s_lm, s_u);
-        count = 0;
-    } else if (count > 1) {
-        if (warp == 0) warp_merge<false>(a, s_sets, kTsWarps, s_we[0], s_win, nullptr, nullptr, nullptr);
-    }
-    __syncthreads();
-    // ---- tree levels: publish the node's candidates; the last member of each group of 16 merges
-    // them (four warps over four sets each, then warp 0 over the four results)
-    while (count > 1) {
+    int node = blockIdx.x, count = (int)ceil_div(m, kTsRows), level = 0;
+    for (;;) {
+        block_gepp(v, rid, a.w, s_win, s_loc, s_g, count == 1 ? a.lmul : nullptr);
+        if (count == 1) break;
+        // publish this node's candidates; the last member of the group merges them
         if (t < 32) a.cand[((int64_t)level * kTsMaxCand + node) * 32 + t] = s_win[t];
         __threadfence();
         __syncthreads();
@@ -247,30 +207,17 @@ __global__ void __launch_bounds__(kTsThreads) tslu_select_kernel(TsArgs a) {
         __syncthreads();
         if (!s_last) return;
         __threadfence();
-        for (int e = t; e < members * 32; e += kTsThreads)
-            s_sets[e] = __ldcg(a.cand + ((int64_t)level * kTsMaxCand + parent * kTsFan) * 32 + e);
-        __syncthreads();
-        const int next = (int)ceil_div(count, kTsFan);
-        const bool root = next == 1;
-        const int nw = (int)ceil_div(members, kTsR);  // merging warps of the first stage
-        if (members == 1 && !root) {
-            if (t < 32) s_win[t] = s_sets[t];  // a lone set passes through
-        } else if (nw == 1) {
-            if (warp == 0) {
-                if (root) warp_merge<true>(a, s_sets, members, s_we[0], s_win, s_loc, s_lm, s_u);
-                else warp_merge<false>(a, s_sets, members, s_we[0], s_win, nullptr, nullptr, nullptr);
-            }
-        } else {
-            if (warp < nw) warp_merge<false>(a, s_sets, members, s_we[warp], s_part + warp * 32, nullptr, nullptr, nullptr);
-            __syncthreads();
-            if (warp == 0) {
-                if (root) warp_merge<true>(a, s_part, nw, s_we[0], s_win, s_loc, s_lm, s_u);
-                else warp_merge<false>(a, s_part, nw, s_we[0], s_win, nullptr, nullptr, nullptr);
-            }
+#pragma unroll
+        for (int r = 0; r < kTsRpt; ++r) {
+            const int sidx = r * kTsThreads + t, mem = sidx >> 5;
+            rid[r] = mem < members
+                         ? __ldcg(a.cand + ((int64_t)level * kTsMaxCand + parent * kTsFan + mem) * 32 + (sidx & 31))
+                         : -1;
         }
-        __syncthreads();
+#pragma unroll
+        for (int r = 0; r < kTsRpt; ++r) load_leaf_row(a.A, a.ld, rid[r], a.lc0, a.w, v[r]);
         node = parent;
-        count = next;
+        count = (int)ceil_div(count, kTsFan);
         ++level;
     }
 
@@ -282,9 +229,9 @@ __global__ void __launch_bounds__(kTsThreads) tslu_select_kernel(TsArgs a) {
         float x = 0.f;
         if (j < w && l >= 0 && k < w) {
             if (k < j) {
-                x = s_lm[k * kTsWarpRows + l];
+                x = __ldcg(a.lmul + k * kTsRows + l);
             } else {
-                const float4 f = s_u[j][(k - j) >> 2];
+                const float4 f = s_g.u[j][(k - j) >> 2];
                 const int e4 = (k - j) & 3;
                 x = e4 == 0 ? f.x : e4 == 1 ? f.y : e4 == 2 ? f.z : f.w;
             }
@@ -311,6 +258,7 @@ __global__ void __launch_bounds__(kTsThreads) tslu_select_kernel(TsArgs a) {
     if (s_bad) return;
     // row moves: top slot lc0+j <- winner j; the displaced top rows fill the winners' old slots
     if (t < 32) {
+        const int lane = t;
         const int p = lane < w ? s_win[lane] : -1;
         if (lane < w && p < lc0 + w) s_flag[p - lc0] = 1;
         __syncwarp();
@@ -339,12 +287,12 @@ __global__ void __launch_bounds__(kTsThreads) tslu_select_kernel(TsArgs a) {
     const int nm = s_nm, nout = s_nout;
     if (t == 0) { a.moves[0] = nm; a.moves[1] = nout; }
     if (t < nm) { a.moves[2 + t] = s_mdst[t]; a.moves[66 + t] = s_msrc[t]; }
-    // thread t owns columns c = t, t + 128 of the outer panel.  It writes the top rows' final content
+    // thread t owns column c = t of the outer panel.  It writes the top rows' final content
     // (original rows left of the leaf, L11\U11 inside it, U12 = L11^-1 * original rows right of
     // it), the column of M = [U11^-1 | U11^-1 U12] that the apply kernel multiplies by, and the
     // original content of the rows that leave the top block.  All loads are issued before use.
-    const int lo = lc0 - a.oc0, pw = a.pw;
-    for (int c = t; c < pw; c += kTsThreads) {
+    const int lo = lc0 - a.oc0, pw = a.pw, c = t;
+    if (c < pw) {
         const bool in_leaf = c >= lo && c < lo + w;
         const float* col = a.A + a.oc0 + c;
         float x[32], y[32];
@@ -805,6 +753,7 @@ size_t f32_scratch_bytes(int64_t n) {
     b += (size_t)kTsLevels * kTsMaxCand * sizeof(unsigned);   // counters
     b += 3 * 32 * kNB * sizeof(float);                          // top, mvals, wmat
     b += 256 * sizeof(int);                                     // moves
+    b += 32 * (size_t)kTsRows * sizeof(float);                  // root multipliers
     b += 2 * (size_t)round_up(n, 64) * sizeof(int32_t);          // panel row maps (by panel parity)
     b += (size_t)kNB * 32 * sizeof(float);                      // leaf L11^-1 blocks
     b += 4 * (size_t)round_up(n, 32) * kNB * sizeof(float);     // bth, btl, ah, al
@@ -829,6 +778,7 @@ F32Scratch f32_scratch_carve(void* base, int64_t n) {
     s.mvals = reinterpret_cast<float*>(take(32 * kNB * sizeof(float)));
     s.wmat = reinterpret_cast<float*>(take(32 * kNB * sizeof(float)));
     s.moves = reinterpret_cast<int*>(take(256 * sizeof(int)));
+    s.lmul = reinterpret_cast<float*>(take(32 * (size_t)kTsRows * sizeof(float)));
     s.pmap = reinterpret_cast<int32_t*>(take(2 * (size_t)round_up(n, 64) * sizeof(int32_t)));
     s.lpinv = reinterpret_cast<float*>(take((size_t)kNB * 32 * sizeof(float)));
     const size_t panel = (size_t)round_up(n, 32) * kNB * sizeof(float);
@@ -908,7 +858,7 @@ int32_t lu_factor_f32(Ctx* ctx, cudaStream_t st, float* A, int64_t ld, int64_t n
             for (int64_t lc0 = oc0; lc0 < oc0 + pw; lc0 += 32) {
                 const int w = (int)std::min<int64_t>(32, n - lc0);
                 TsArgs ta{A, ld, (int)n, (int)lc0, w, (int)oc0, pw, s.cand, s.counters, s.top, s.mvals, s.wmat,
-                          s.moves, lc0 == oc0 ? pmap : nullptr, s.lpinv, ctx->d_status};
+                          s.moves, s.lmul, lc0 == oc0 ? pmap : nullptr, s.lpinv, ctx->d_status};
                 prof_begin(ctx, q, kClsPanel);
                 {
                     const cudaLaunchConfig_t c = cfg_of((unsigned)ceil_div(n - lc0, kTsRows), kTsThreads, 0);
