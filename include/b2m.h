@@ -120,6 +120,17 @@ B2M_API const char* b2m_last_error(b2m_ctx* ctx);
 B2M_API const char* b2m_status_string(int32_t status);
 /* Number of kernels this context has launched so far (device work accounting). */
 B2M_API int64_t     b2m_kernel_launches(b2m_ctx* ctx);
+/* Execution facts of this context (no counterpart in the reference): B2M_INFO_NUM_SMS, the
+ * device's SM count; B2M_INFO_SWEEP_CTAS, the co-resident CTAs of the refinement sweep (-1 before
+ * the first mixed solve); B2M_INFO_CHAIN_CLUSTERS, the co-resident 8-CTA clusters of the chained
+ * sweep (0: not usable here, -1: not probed yet); B2M_INFO_CHAIN_PROBE, why the chained sweep is not
+ * used (0 it is, 1 shared-memory attribute refused, 2 occupancy query failed, 3 launch failed, 4 no
+ * cluster fits) times 1000 plus the CUDA error code. */
+#define B2M_INFO_NUM_SMS        1
+#define B2M_INFO_SWEEP_CTAS     2
+#define B2M_INFO_CHAIN_CLUSTERS 3
+#define B2M_INFO_CHAIN_PROBE    4
+B2M_API int32_t     b2m_ctx_info(b2m_ctx* ctx, int32_t what, int64_t* value);
 /* Event profiler: when enabled, every launch is bracketed by CUDA events on its own stream and
  * its algorithmic work is recorded per kernel class (0 FP64 GEMM, 1 panel, 2 row swaps,
  * 3 triangular solve, 4 tensor-core GEMM, 5 solve/refinement kernels, 6 other, e.g. the FP64

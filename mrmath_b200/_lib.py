@@ -59,6 +59,7 @@ SIGNATURES: dict[str, tuple] = {
     "b2m_last_error": (C.c_char_p, [vp]),
     "b2m_status_string": (C.c_char_p, [i32]),
     "b2m_kernel_launches": (i64, [vp]),
+    "b2m_ctx_info": (i32, [vp, i32, C.POINTER(i64)]),
     "b2m_profile": (i32, [vp, i32]),
     "b2m_profile_read": (i32, [vp, i32, C.POINTER(i64), C.POINTER(dbl), C.POINTER(dbl)]),
     "b2m_MatrixMultEx": (i32, [vp, vp, i64, vp, vp, i64, i64, i64, i64, i64, i64, i32, i32]),
@@ -180,6 +181,14 @@ class Context:
 
     def kernel_launches(self) -> int:
         return lib.b2m_kernel_launches(self.h)
+
+    INFO_KEYS = {"num_sms": 1, "sweep_ctas": 2, "chain_clusters": 3, "chain_probe": 4}
+
+    def info(self, key: str) -> int:
+        """b2m_ctx_info: an execution fact of this context (see INFO_KEYS)."""
+        v = C.c_int64(0)
+        self.check(lib.b2m_ctx_info(self.h, self.INFO_KEYS[key], C.byref(v)))
+        return v.value
 
     KERNEL_CLASSES = ("gemm_f64", "panel", "row_swap", "trsm", "gemm_tc", "solve", "other")
 

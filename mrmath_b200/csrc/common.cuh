@@ -90,6 +90,7 @@ struct Ctx {
     int num_sms = 148;
     int sweep_ctas = -1;  // co-resident CTAs of the persistent refinement sweep (-1: not queried yet)
     int chain_clusters = -1;  // co-resident 8-CTA clusters of the chained sweep (0: unusable, -1: not probed)
+    int chain_probe_why = 0;  // why it is unusable: step * 1000 + CUDA error (b2m_ctx_info)
     int64_t wait_limit = -1;  // polls of the refinement sweeps' bounded waits (-1: the built-in limit)
     size_t smem_optin = 0;
     cudaStream_t own_stream = nullptr;

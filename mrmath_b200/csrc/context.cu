@@ -424,6 +424,19 @@ extern "C" int64_t b2m_kernel_launches(b2m_ctx* h) {
     return ctx ? ctx->launches : -1;
 }
 
+extern "C" int32_t b2m_ctx_info(b2m_ctx* h, int32_t what, int64_t* value) {
+    Ctx* ctx = reinterpret_cast<Ctx*>(h);
+    if (!ctx || !value) return B2M_ERR_ARG;
+    b2m::CallLock lk(ctx);
+    switch (what) {
+        case B2M_INFO_NUM_SMS: *value = ctx->num_sms; return B2M_OK;
+        case B2M_INFO_SWEEP_CTAS: *value = ctx->sweep_ctas; return B2M_OK;
+        case B2M_INFO_CHAIN_CLUSTERS: *value = ctx->chain_clusters; return B2M_OK;
+        case B2M_INFO_CHAIN_PROBE: *value = ctx->chain_probe_why; return B2M_OK;
+        default: return b2m::fail(ctx, B2M_ERR_ARG, "unknown info key %d", what);
+    }
+}
+
 extern "C" const char* b2m_status_string(int32_t s) {
     switch (s) {
         case B2M_OK: return "ok";

@@ -1,9 +1,11 @@
 // lu.cu -- partial-pivoting LU and the triangular solves built on it (FP64 plain form).
 //
 // Structure (a B200 re-design of InternalRecursiveMatrixLUDecompInPlace, LinAlgLU.pas:181-281):
-//   * the recursion splits the column range in two halves rounded to the 32-column leaf width
-//     (the reference halves exactly: mn div 2); the leaves are factored by one thread-block
-//     cluster per panel with the panel resident in distributed shared memory;
+//   * orders up to 512: the recursion splits the column range in two halves rounded to the
+//     32-column leaf width (the reference halves exactly: mn div 2); larger orders: 256-column
+//     outer panels with look-ahead, factored right-looking by leaves (lu_blocked below); the
+//     leaves are factored by one thread-block cluster per panel with the panel resident in
+//     distributed shared memory;
 //   * a leaf's <= 32 row interchanges are applied at once to every other column of the matrix
 //     (and to a row-permutation vector) by one swap launch, which replaces the reference's two
 //     LUSwap calls per recursion level (:205, :237) -- the final matrix and pivot vector are the
@@ -135,6 +137,171 @@ __global__ void __launch_bounds__(kSwapThreads)
         if (tid < nm) {
             if (perm) perm[mv_dst[tid]] = pv;
             if (pmap) pmap[mv_dst[tid]] = qv;
+        }
+    }
+}
+
+// Inside an outer panel of the blocked FP64 LU, right-looking by leaves: after a leaf is factored,
+// (1) leaf_swap_u12_kernel applies its interchanges to the panel's other columns and, for the
+// panel columns right of the leaf, turns the leaf's rows into U12 = L11^-1 A12 (thread per column:
+// the <= 32 values of the column in the leaf's rows after the interchanges, then the unit-lower
+// forward substitution with contributions in ascending order, as trsm_small_kernel computes it);
+// (2) rank_update_kernel subtracts L21 U12 from the rest of the panel (rows below the leaf).  Both
+// only touch the outer panel's columns; the other columns get the panel's net permutation and one
+// K = 256 update per panel.
+template <typename T>
+__global__ void __launch_bounds__(kSwapThreads)
+    leaf_swap_u12_kernel(T* A, int64_t ld, int col_lo, int col_hi, int c0, int w, const int32_t* ipiv, int32_t* perm,
+                         int32_t* pmap, const int32_t* status) {
+    __shared__ int src_main[kPanelW];
+    __shared__ int mv_dst[2 * kPanelW], mv_src[2 * kPanelW];
+    __shared__ int n_moves;
+    __shared__ T s_l[kPanelW][kPanelW + 1];  // L11 (strictly lower part), s_l[j][i] = L(c0 + j, c0 + i)
+    if (status[kInfo] != 0) return;
+    const int tid = threadIdx.x, lane = tid & 31;
+    for (int e = tid; e < kPanelW * kPanelW; e += kSwapThreads) {
+        const int j = e / kPanelW, i = e - j * kPanelW;
+        s_l[j][i] = (i < j && j < w) ? A[(int64_t)(c0 + j) * ld + c0 + i] : T(0);
+    }
+    if (tid < 32) {
+        if (lane < w) src_main[lane] = c0 + lane;
+        __syncwarp();
+        int my_pos = -1, my_src = -1, n_extra = 0;
+        const int qv = lane < w ? ipiv[c0 + lane] : 0;
+        for (int j = 0; j < w; ++j) {
+            const int q = __shfl_sync(0xffffffffu, qv, j);
+            if (q < c0 + w) {
+                if (lane == 0 && q != c0 + j) {
+                    const int t = src_main[j];
+                    src_main[j] = src_main[q - c0];
+                    src_main[q - c0] = t;
+                }
+            } else {
+                const unsigned hit = __ballot_sync(0xffffffffu, my_pos == q);
+                int owner;
+                if (hit) {
+                    owner = __ffs(hit) - 1;
+                } else {
+                    owner = n_extra++;
+                    if (lane == owner) { my_pos = q; my_src = q; }
+                }
+                if (lane == owner) {
+                    const int t = src_main[j];
+                    src_main[j] = my_src;
+                    my_src = t;
+                }
+            }
+            __syncwarp();
+        }
+        const bool mv_main = lane < w && src_main[lane] != c0 + lane;
+        const bool mv_extra = lane < n_extra && my_src != my_pos;
+        const unsigned bm = __ballot_sync(0xffffffffu, mv_main);
+        const unsigned be = __ballot_sync(0xffffffffu, mv_extra);
+        const int below = (1u << lane) - 1u;
+        if (mv_main) {
+            const int k = __popc(bm & below);
+            mv_dst[k] = c0 + lane;
+            mv_src[k] = src_main[lane];
+        }
+        if (mv_extra) {
+            const int k = __popc(bm) + __popc(be & below);
+            mv_dst[k] = my_pos;
+            mv_src[k] = my_src;
+        }
+        if (lane == 0) n_moves = __popc(bm) + __popc(be);
+    }
+    __syncthreads();
+    const int nm = n_moves;
+    const int gc = col_lo + blockIdx.x * kSwapThreads + tid;
+    const int col = gc < c0 ? gc : gc + w;  // the leaf's own columns are skipped
+    if (col < col_hi) {
+        // every read of this column happens before its first write
+        T v[2 * kPanelW];
+#pragma unroll
+        for (int k = 0; k < 2 * kPanelW; ++k)
+            if (k < nm) v[k] = A[(int64_t)mv_src[k] * ld + col];
+        if (col > c0) {  // right of the leaf: the leaf's rows after the interchanges, then U12
+            T x[kPanelW];
+#pragma unroll
+            for (int j = 0; j < kPanelW; ++j) x[j] = j < w ? A[(int64_t)src_main[j] * ld + col] : T(0);
+#pragma unroll
+            for (int k = 0; k < 2 * kPanelW; ++k)
+                if (k < nm && (mv_dst[k] < c0 || mv_dst[k] >= c0 + w)) A[(int64_t)mv_dst[k] * ld + col] = v[k];
+#pragma unroll
+            for (int i = 0; i < kPanelW - 1; ++i) {
+#pragma unroll
+                for (int j = i + 1; j < kPanelW; ++j) x[j] = fma(-s_l[j][i], x[i], x[j]);
+            }
+#pragma unroll
+            for (int j = 0; j < kPanelW; ++j)
+                if (j < w) A[(int64_t)(c0 + j) * ld + col] = x[j];
+        } else {
+#pragma unroll
+            for (int k = 0; k < 2 * kPanelW; ++k)
+                if (k < nm) A[(int64_t)mv_dst[k] * ld + col] = v[k];
+        }
+    }
+    if ((perm || pmap) && blockIdx.x == 0 && nm > 0) {
+        int pv = 0, qv = 0;
+        if (tid < nm) {
+            if (perm) pv = perm[mv_src[tid]];
+            if (pmap) qv = pmap[mv_src[tid]];
+        }
+        __syncthreads();
+        if (tid < nm) {
+            if (perm) perm[mv_dst[tid]] = pv;
+            if (pmap) pmap[mv_dst[tid]] = qv;
+        }
+    }
+}
+
+// A[r][c] -= sum_{k < w} A[r][c0 + k] * A[c0 + k][c] for rows [r_lo, n) and columns [cl, ch): the
+// leaf's rank-w update of the rest of its outer panel.  64 x 64 tiles, 4 x 4 per thread, the
+// L21 and U12 slices staged in shared memory; the w products of each element are accumulated in
+// ascending k and subtracted once (as the GEMM's doSub epilogue does).
+constexpr int kRuT = 64;
+__global__ void __launch_bounds__(256, 3) rank_update_kernel(double* A, int64_t ld, int n, int r_lo, int cl, int ch,
+                                                          int c0, int w, const int32_t* status) {
+    __shared__ double s_a[kRuT][kPanelW + 1];  // L21 rows of the tile
+    __shared__ __align__(16) double s_b[kPanelW][kRuT];  // U12 columns of the tile
+    if (status[kInfo] != 0) return;
+    const int t = threadIdx.x, tx = t & 15, ty = t >> 4;
+    const int r0 = r_lo + blockIdx.y * kRuT, cb = cl + blockIdx.x * kRuT;
+    for (int e = t; e < kRuT * kPanelW; e += 256) {
+        const int rr = e >> 5, k = e & 31;
+        const int row = r0 + rr;
+        s_a[rr][k] = (row < n && k < w) ? A[(int64_t)row * ld + c0 + k] : 0.0;
+    }
+    for (int e = t; e < kPanelW * kRuT; e += 256) {
+        const int k = e / kRuT, cc = e - k * kRuT;
+        const int col = cb + cc;
+        s_b[k][cc] = (k < w && col < ch) ? A[(int64_t)(c0 + k) * ld + col] : 0.0;
+    }
+    __syncthreads();
+    double acc[4][4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) acc[i][j] = 0.0;
+#pragma unroll 8
+    for (int k = 0; k < kPanelW; ++k) {
+        const double2 b01 = *reinterpret_cast<const double2*>(&s_b[k][4 * tx]);
+        const double2 b23 = *reinterpret_cast<const double2*>(&s_b[k][4 * tx + 2]);
+        const double bv[4] = {b01.x, b01.y, b23.x, b23.y};
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            const double av = s_a[4 * ty + i][k];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) acc[i][j] = fma(av, bv[j], acc[i][j]);
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        const int row = r0 + 4 * ty + i;
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const int col = cb + 4 * tx + j;
+            if (row < n && col < ch) A[(int64_t)row * ld + col] -= acc[i][j];
         }
     }
 }
@@ -434,10 +601,12 @@ int32_t lu_rec(Ctx* ctx, cudaStream_t st, double* A, int64_t ld, int64_t n, int6
 constexpr int64_t kOuterNB = 256;  // outer panel width of the blocked FP64 LU
 
 // Blocked right-looking LU with look-ahead (orders n > 2 kOuterNB).  Per outer panel of 256
-// columns: (1) the panel is factored by the recursion above with its leaves' interchanges kept
-// inside the panel (each recorded in the row map pmap); (2) the panel's net permutation is applied
-// once to the columns right of it (this stream: the next step reads them) and left of it (side
-// stream); (3) U12 = L11^-1 A12 and A22 -= A21 U12 for the next panel's 256 columns on this stream;
+// columns: (1) the panel is factored right-looking by leaves, each leaf's interchanges kept inside
+// the panel (and recorded in the row map pmap), its U12 formed by the same launch and its rank-w
+// update applied to the rest of the panel (leaf_swap_u12_kernel, rank_update_kernel); (2) the
+// panel's net permutation is applied to the next panel's columns on this stream, and to every
+// further column right of the panel and the factored columns left of it on the side stream;
+// (3) U12 = L11^-1 A12 and A22 -= A21 U12 for the next panel's 256 columns on this stream;
 // (4) the same for every further column on the side stream, where it overlaps the next panel's
 // factorisation (which reads and writes only the next panel's columns) and is joined before the
 // next step's permutation moves rows under it.  The row map alternates between two buffers by panel
@@ -467,7 +636,30 @@ int32_t lu_blocked(Ctx* ctx, cudaStream_t q, double* A, int64_t ld, int64_t n, i
         int32_t* pmap = pmap2 + ((k0 / kOuterNB) & 1) * pm_ld;
         iota_kernel<<<(unsigned)ceil_div(n, 256), 256, 0, q>>>(pmap, n);
         B2M_LAUNCHED(ctx);
-        B2M_TRY(lu_rec(ctx, q, A, ld, n, k0, w, ipiv, perm, leaf, SwapScope{k0, k1, pmap}));
+        // the panel, right-looking by leaves (all of it on this stream: it is the critical path)
+        for (int64_t c0 = k0; c0 < k1; c0 += leaf) {
+            const int64_t wl = std::min(leaf, k1 - c0);
+            B2M_TRY(launch_panel<double>(ctx, q, A + c0 * ld + c0, ld, (int)(n - c0), (int)wl, (int)c0, (int)c0, ipiv));
+            prof_begin(ctx, q, kClsSwap);
+            leaf_swap_u12_kernel<double><<<1, kSwapThreads, 0, q>>>(A, ld, (int)k0, (int)k1, (int)c0, (int)wl, ipiv,
+                                                                    perm, pmap, ctx->d_status);
+            prof_end(ctx, q, kClsSwap, 16.0 * wl * (double)(w - wl));
+            B2M_LAUNCHED(ctx);
+            const int64_t rl = c0 + wl;
+            if (rl < k1) {
+                dim3 grid((unsigned)ceil_div(k1 - rl, kRuT), (unsigned)ceil_div(n - rl, kRuT));
+                prof_begin(ctx, q, kClsGemm);
+                rank_update_kernel<<<grid, 256, 0, q>>>(A, ld, (int)n, (int)rl, (int)rl, (int)k1, (int)c0, (int)wl,
+                                                        ctx->d_status);
+                prof_end(ctx, q, kClsGemm, 2.0 * (double)(n - rl) * (double)(k1 - rl) * (double)wl);  // flops
+                B2M_LAUNCHED(ctx);
+            }
+            if (ctx->progress && ctx->progress_notes.size() < ctx->progress_notes.capacity()) {
+                ctx->progress_notes.push_back(
+                    ProgressNote{ctx->progress, ctx->progress_user, (int32_t)((c0 + wl) * 100 / n)});
+                B2M_CU(ctx, cudaLaunchHostFunc(q, progress_trampoline, &ctx->progress_notes.back()));
+            }
+        }
         B2M_TRY(join());  // the previous panel's wide update is done before rows move under it
         auto permute = [&](cudaStream_t qs, int64_t c_begin, int64_t c_end) -> int32_t {
             if (c_end <= c_begin) return B2M_OK;
@@ -478,13 +670,16 @@ int32_t lu_blocked(Ctx* ctx, cudaStream_t q, double* A, int64_t ld, int64_t n, i
             B2M_LAUNCHED(ctx);
             return B2M_OK;
         };
-        B2M_TRY(permute(q, k1, n));
-        if (k0 > 0) {
+        const int64_t rest = n - k1, nw = std::min(kOuterNB, std::max<int64_t>(rest, 0));
+        // only the next panel's columns are permuted on this stream; the other columns right of
+        // the panel and the factored columns left of it on the side stream, ahead of their update
+        B2M_TRY(permute(q, k1, k1 + nw));
+        if (k0 > 0 || rest > nw) {
             B2M_TRY(fork());
+            B2M_TRY(permute(q2, k1 + nw, n));
             B2M_TRY(permute(q2, 0, k0));
         }
         if (k1 >= n) break;
-        const int64_t rest = n - k1, nw = std::min(kOuterNB, rest);
         auto update = [&](cudaStream_t qs, int64_t cs, int64_t nc) -> int32_t {
             TriSolve t{A, ld, n, A, ld, n, n, cs, nc};
             B2M_TRY(trsm_lower_rec(ctx, qs, t, k0, k0, w));
@@ -492,11 +687,8 @@ int32_t lu_blocked(Ctx* ctx, cudaStream_t q, double* A, int64_t ld, int64_t n, i
             DOperand b{A, ld, n, n, k0, cs, false};
             return dgemm_tiled(ctx, qs, a, b, A + k1 * ld + cs, ld, n - k1, nc, w, B2M_DO_SUB, true);
         };
+        if (rest > nw) B2M_TRY(update(q2, k1 + nw, rest - nw));
         B2M_TRY(update(q, k1, nw));
-        if (rest > nw) {
-            B2M_TRY(fork());
-            B2M_TRY(update(q2, k1 + nw, rest - nw));
-        }
     }
     return join();
 }

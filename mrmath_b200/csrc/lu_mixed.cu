@@ -866,8 +866,10 @@ __global__ void __launch_bounds__(256, 1) resid_kernel(ReArgs a) {
 int32_t chain_probe(Ctx* ctx, cudaStream_t st) {
     if (ctx->chain_clusters >= 0) return B2M_OK;
     ctx->chain_clusters = 0;
-    if (cudaFuncSetAttribute(trsv_chain_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kChSmem) != cudaSuccess) {
+    cudaError_t e = cudaFuncSetAttribute(trsv_chain_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kChSmem);
+    if (e != cudaSuccess) {
         (void)cudaGetLastError();
+        ctx->chain_probe_why = 1000 + (int)e;
         return B2M_OK;
     }
     cudaLaunchConfig_t cfg{};
@@ -881,16 +883,20 @@ int32_t chain_probe(Ctx* ctx, cudaStream_t st) {
     cfg.attrs = at;
     cfg.numAttrs = 1;
     int clusters = 0;
-    if (cudaOccupancyMaxActiveClusters(&clusters, trsv_chain_kernel, &cfg) != cudaSuccess || clusters < 1) {
+    e = cudaOccupancyMaxActiveClusters(&clusters, trsv_chain_kernel, &cfg);
+    if (e != cudaSuccess || clusters < 1) {
         (void)cudaGetLastError();
+        ctx->chain_probe_why = e != cudaSuccess ? 2000 + (int)e : 4000;
         return B2M_OK;
     }
     SwArgs sa{};
     sa.n = 0;  // no blocks: every CTA is padding
     sa.status = ctx->d_status;
-    if (cudaLaunchKernelEx(&cfg, trsv_chain_kernel, sa, (int)kChCl) != cudaSuccess ||
-        cudaStreamSynchronize(st) != cudaSuccess) {
+    e = cudaLaunchKernelEx(&cfg, trsv_chain_kernel, sa, (int)kChCl);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) {
         (void)cudaGetLastError();
+        ctx->chain_probe_why = 3000 + (int)e;
         return B2M_OK;
     }
     B2M_LAUNCHED(ctx);
