@@ -130,6 +130,7 @@ B2M_API int64_t     b2m_kernel_launches(b2m_ctx* ctx);
 #define B2M_INFO_SWEEP_CTAS     2
 #define B2M_INFO_CHAIN_CLUSTERS 3
 #define B2M_INFO_CHAIN_PROBE    4
+#define B2M_INFO_CHAIN_CLUSTERS4 5  /* the same as B2M_INFO_CHAIN_CLUSTERS for 4-CTA clusters */
 B2M_API int32_t     b2m_ctx_info(b2m_ctx* ctx, int32_t what, int64_t* value);
 /* Event profiler: when enabled, every launch is bracketed by CUDA events on its own stream and
  * its algorithmic work is recorded per kernel class (0 FP64 GEMM, 1 panel, 2 row swaps,

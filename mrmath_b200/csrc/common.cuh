@@ -90,6 +90,7 @@ struct Ctx {
     int num_sms = 148;
     int sweep_ctas = -1;  // co-resident CTAs of the persistent refinement sweep (-1: not queried yet)
     int chain_clusters = -1;  // co-resident 8-CTA clusters of the chained sweep (0: unusable, -1: not probed)
+    int chain_clusters4 = -1; // the same for 4-CTA clusters
     int chain_probe_why = 0;  // why it is unusable: step * 1000 + CUDA error (b2m_ctx_info)
     int64_t wait_limit = -1;  // polls of the refinement sweeps' bounded waits (-1: the built-in limit)
     size_t smem_optin = 0;
@@ -233,6 +234,16 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int32_
     if (timeout_word) atomicExch(timeout_word, site);
     return false;
 }
+
+// 16-byte asynchronous global -> shared copy (src_bytes < 16 zero-fills the rest), its commit
+// group and the wait for all but N groups.
+__device__ __forceinline__ void cp_async16(void* dst, const void* src, int src_bytes) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(smem_u32(dst)), "l"(src), "r"(src_bytes)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
 
 // Distributed shared memory of a thread-block cluster: the address of `local` in CTA `rank`, a
 // 16-byte store into another CTA's shared memory completing on its mbarrier, and a wait on this

@@ -433,6 +433,7 @@ extern "C" int32_t b2m_ctx_info(b2m_ctx* h, int32_t what, int64_t* value) {
         case B2M_INFO_SWEEP_CTAS: *value = ctx->sweep_ctas; return B2M_OK;
         case B2M_INFO_CHAIN_CLUSTERS: *value = ctx->chain_clusters; return B2M_OK;
         case B2M_INFO_CHAIN_PROBE: *value = ctx->chain_probe_why; return B2M_OK;
+        case B2M_INFO_CHAIN_CLUSTERS4: *value = ctx->chain_clusters4; return B2M_OK;
         default: return b2m::fail(ctx, B2M_ERR_ARG, "unknown info key %d", what);
     }
 }

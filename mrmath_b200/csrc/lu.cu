@@ -149,8 +149,9 @@ __global__ void __launch_bounds__(kSwapThreads)
 // (2) rank_update_kernel subtracts L21 U12 from the rest of the panel (rows below the leaf).  Both
 // only touch the outer panel's columns; the other columns get the panel's net permutation and one
 // K = 256 update per panel.
+constexpr int kSuThreads = 64;  // columns per CTA of leaf_swap_u12_kernel
 template <typename T>
-__global__ void __launch_bounds__(kSwapThreads)
+__global__ void __launch_bounds__(kSuThreads)
     leaf_swap_u12_kernel(T* A, int64_t ld, int col_lo, int col_hi, int c0, int w, const int32_t* ipiv, int32_t* perm,
                          int32_t* pmap, const int32_t* status) {
     __shared__ int src_main[kPanelW];
@@ -159,7 +160,7 @@ __global__ void __launch_bounds__(kSwapThreads)
     __shared__ T s_l[kPanelW][kPanelW + 1];  // L11 (strictly lower part), s_l[j][i] = L(c0 + j, c0 + i)
     if (status[kInfo] != 0) return;
     const int tid = threadIdx.x, lane = tid & 31;
-    for (int e = tid; e < kPanelW * kPanelW; e += kSwapThreads) {
+    for (int e = tid; e < kPanelW * kPanelW; e += kSuThreads) {
         const int j = e / kPanelW, i = e - j * kPanelW;
         s_l[j][i] = (i < j && j < w) ? A[(int64_t)(c0 + j) * ld + c0 + i] : T(0);
     }
@@ -212,7 +213,7 @@ __global__ void __launch_bounds__(kSwapThreads)
     }
     __syncthreads();
     const int nm = n_moves;
-    const int gc = col_lo + blockIdx.x * kSwapThreads + tid;
+    const int gc = col_lo + blockIdx.x * kSuThreads + tid;
     const int col = gc < c0 ? gc : gc + w;  // the leaf's own columns are skipped
     if (col < col_hi) {
         // every read of this column happens before its first write
@@ -260,7 +261,7 @@ __global__ void __launch_bounds__(kSwapThreads)
 // L21 and U12 slices staged in shared memory; the w products of each element are accumulated in
 // ascending k and subtracted once (as the GEMM's doSub epilogue does).
 constexpr int kRuT = 64;
-__global__ void __launch_bounds__(256, 3) rank_update_kernel(double* A, int64_t ld, int n, int r_lo, int cl, int ch,
+__global__ void __launch_bounds__(256, 2) rank_update_kernel(double* A, int64_t ld, int n, int r_lo, int cl, int ch,
                                                           int c0, int w, const int32_t* status) {
     __shared__ double s_a[kRuT][kPanelW + 1];  // L21 rows of the tile
     __shared__ __align__(16) double s_b[kPanelW][kRuT];  // U12 columns of the tile
@@ -276,6 +277,17 @@ __global__ void __launch_bounds__(256, 3) rank_update_kernel(double* A, int64_t 
         const int k = e / kRuT, cc = e - k * kRuT;
         const int col = cb + cc;
         s_b[k][cc] = (k < w && col < ch) ? A[(int64_t)(c0 + k) * ld + col] : 0.0;
+    }
+    // the tile's own values, loaded while the slices arrive
+    double c[4][4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        const int row = r0 + 4 * ty + i;
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const int col = cb + 4 * tx + j;
+            c[i][j] = (row < n && col < ch) ? A[(int64_t)row * ld + col] : 0.0;
+        }
     }
     __syncthreads();
     double acc[4][4];
@@ -301,8 +313,93 @@ __global__ void __launch_bounds__(256, 3) rank_update_kernel(double* A, int64_t 
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
             const int col = cb + 4 * tx + j;
-            if (row < n && col < ch) A[(int64_t)row * ld + col] -= acc[i][j];
+            if (row < n && col < ch) A[(int64_t)row * ld + col] = c[i][j] - acc[i][j];
         }
+    }
+}
+
+// U12 = L11^-1 A12 for one outer panel in a single launch: L11 unit lower (k <= 256 rows, at L with
+// row stride ldl), the right-hand sides k x ncols at B.  A CTA owns 32 columns, held in shared
+// memory for the whole solve; per 32-row block of L11 (staged in shared memory by cp.async, the
+// next block column while the current one is used): warp 0 substitutes the block's diagonal
+// triangle (lane = column; contributions in ascending order, as trsm_small_kernel computes them),
+// then every warp subtracts the block's contribution from the rows below it (each element's 32
+// products accumulated in ascending order and subtracted once).
+constexpr int kTpK = 256;   // rows of the panel
+constexpr int kTpC = 32;    // columns per CTA
+constexpr int kTpSmem = (kTpK * kTpC + 2 * kTpK * kPanelW) * (int)sizeof(double);  // 192 KiB
+
+__global__ void __launch_bounds__(256, 1) trsm_panel_kernel(const double* L, int64_t ldl, double* B, int64_t ldb,
+                                                            int k, int ncols, const int32_t* status) {
+    extern __shared__ __align__(16) double tp_dyn[];
+    double* s_x = tp_dyn;                         // [kTpK][kTpC] this CTA's columns
+    double* s_l = tp_dyn + kTpK * kTpC;           // [2][kTpK][kPanelW] block columns of L11 (rows 32 i ..)
+    if (status[kInfo] != 0) return;
+    const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+    const int cb = blockIdx.x * kTpC;
+    const int nb = (int)ceil_div(k, kPanelW);
+    // block column i of L11: rows [32 i, k), columns [32 i, 32 i + 32) -> buffer i & 1 (16-byte pieces)
+    auto stage = [&](int i) {
+        double* dst = s_l + (i & 1) * kTpK * kPanelW;
+        const int r0 = kPanelW * i, rows = k - r0;
+        for (int e = t; e < rows * (kPanelW / 2); e += 256) {
+            const int rr = e / (kPanelW / 2), q2 = e - rr * (kPanelW / 2);
+            const int col = r0 + 2 * q2;
+            const double* src = L + (int64_t)(r0 + rr) * ldl + col;
+            cp_async16(dst + rr * kPanelW + 2 * q2, src, col + 1 < k ? 16 : (col < k ? 8 : 0));
+        }
+        cp_async_commit();
+    };
+    stage(0);
+    for (int e = t; e < kTpK * kTpC; e += 256) {
+        const int r = e / kTpC, c = e - r * kTpC;
+        s_x[e] = (r < k && cb + c < ncols) ? B[(int64_t)r * ldb + cb + c] : 0.0;
+    }
+    for (int i = 0; i < nb; ++i) {
+        if (i + 1 < nb) {
+            stage(i + 1);
+            cp_async_wait<1>();
+        } else {
+            cp_async_wait<0>();
+        }
+        __syncthreads();
+        const double* lb = s_l + (i & 1) * kTpK * kPanelW;  // lb[(r - 32 i) * 32 + q] = L[r][32 i + q]
+        const int r0 = kPanelW * i, bw = min(kPanelW, k - r0);
+        if (warp == 0) {
+            double x[kPanelW];
+#pragma unroll
+            for (int j = 0; j < kPanelW; ++j) x[j] = s_x[(r0 + min(j, bw - 1)) * kTpC + lane];
+#pragma unroll
+            for (int q = 0; q < kPanelW - 1; ++q) {
+#pragma unroll
+                for (int j = q + 1; j < kPanelW; ++j)
+                    if (j < bw) x[j] = fma(-lb[j * kPanelW + q], x[q], x[j]);
+            }
+#pragma unroll
+            for (int j = 0; j < kPanelW; ++j)
+                if (j < bw) s_x[(r0 + j) * kTpC + lane] = x[j];
+        }
+        __syncthreads();
+        // rows below the block: thread (warp, lane) updates rows r0 + bw + warp + 8 m of column lane
+        double xb[kPanelW];
+#pragma unroll
+        for (int q = 0; q < kPanelW; ++q) xb[q] = q < bw ? s_x[(r0 + q) * kTpC + lane] : 0.0;
+        for (int r = r0 + bw + warp; r < k; r += 8) {
+            const double* lr = lb + (r - r0) * kPanelW;
+            double acc = 0.0;
+#pragma unroll
+            for (int q = 0; q < kPanelW; q += 2) {
+                const double2 l2 = *reinterpret_cast<const double2*>(lr + q);
+                acc = fma(l2.x, xb[q], acc);
+                acc = fma(l2.y, xb[q + 1], acc);
+            }
+            s_x[r * kTpC + lane] -= acc;
+        }
+        __syncthreads();  // the buffer of block i is restaged for block i + 2
+    }
+    for (int e = t; e < kTpK * kTpC; e += 256) {
+        const int r = e / kTpC, c = e - r * kTpC;
+        if (r < k && cb + c < ncols) B[(int64_t)r * ldb + cb + c] = s_x[e];
     }
 }
 
@@ -599,6 +696,7 @@ int32_t lu_rec(Ctx* ctx, cudaStream_t st, double* A, int64_t ld, int64_t n, int6
 }
 
 constexpr int64_t kOuterNB = 256;  // outer panel width of the blocked FP64 LU
+static_assert(kOuterNB == kTpK, "the panel triangular solve holds one outer panel's rows");
 
 // Blocked right-looking LU with look-ahead (orders n > 2 kOuterNB).  Per outer panel of 256
 // columns: (1) the panel is factored right-looking by leaves, each leaf's interchanges kept inside
@@ -606,7 +704,8 @@ constexpr int64_t kOuterNB = 256;  // outer panel width of the blocked FP64 LU
 // update applied to the rest of the panel (leaf_swap_u12_kernel, rank_update_kernel); (2) the
 // panel's net permutation is applied to the next panel's columns on this stream, and to every
 // further column right of the panel and the factored columns left of it on the side stream;
-// (3) U12 = L11^-1 A12 and A22 -= A21 U12 for the next panel's 256 columns on this stream;
+// (3) U12 = L11^-1 A12 (trsm_panel_kernel, one launch) and A22 -= A21 U12 for the next panel's
+// 256 columns on this stream;
 // (4) the same for every further column on the side stream, where it overlaps the next panel's
 // factorisation (which reads and writes only the next panel's columns) and is joined before the
 // next step's permutation moves rows under it.  The row map alternates between two buffers by panel
@@ -631,6 +730,11 @@ int32_t lu_blocked(Ctx* ctx, cudaStream_t q, double* A, int64_t ld, int64_t n, i
         return B2M_OK;
     };
     const int64_t pm_ld = round_up(n, 64);
+    std::atomic<int>& attr = device_flag((const void*)trsm_panel_kernel, 0, ctx->device);
+    if (!attr.load()) {
+        B2M_CU(ctx, cudaFuncSetAttribute(trsm_panel_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kTpSmem));
+        attr.store(1);
+    }
     for (int64_t k0 = 0; k0 < n; k0 += kOuterNB) {
         const int64_t w = std::min(kOuterNB, n - k0), k1 = k0 + w;
         int32_t* pmap = pmap2 + ((k0 / kOuterNB) & 1) * pm_ld;
@@ -641,8 +745,8 @@ int32_t lu_blocked(Ctx* ctx, cudaStream_t q, double* A, int64_t ld, int64_t n, i
             const int64_t wl = std::min(leaf, k1 - c0);
             B2M_TRY(launch_panel<double>(ctx, q, A + c0 * ld + c0, ld, (int)(n - c0), (int)wl, (int)c0, (int)c0, ipiv));
             prof_begin(ctx, q, kClsSwap);
-            leaf_swap_u12_kernel<double><<<1, kSwapThreads, 0, q>>>(A, ld, (int)k0, (int)k1, (int)c0, (int)wl, ipiv,
-                                                                    perm, pmap, ctx->d_status);
+            leaf_swap_u12_kernel<double><<<(unsigned)std::max<int64_t>(1, ceil_div(w - wl, kSuThreads)), kSuThreads, 0, q>>>(
+                A, ld, (int)k0, (int)k1, (int)c0, (int)wl, ipiv, perm, pmap, ctx->d_status);
             prof_end(ctx, q, kClsSwap, 16.0 * wl * (double)(w - wl));
             B2M_LAUNCHED(ctx);
             const int64_t rl = c0 + wl;
@@ -681,8 +785,11 @@ int32_t lu_blocked(Ctx* ctx, cudaStream_t q, double* A, int64_t ld, int64_t n, i
         }
         if (k1 >= n) break;
         auto update = [&](cudaStream_t qs, int64_t cs, int64_t nc) -> int32_t {
-            TriSolve t{A, ld, n, A, ld, n, n, cs, nc};
-            B2M_TRY(trsm_lower_rec(ctx, qs, t, k0, k0, w));
+            prof_begin(ctx, qs, kClsTrsm);
+            trsm_panel_kernel<<<(unsigned)ceil_div(nc, kTpC), 256, kTpSmem, qs>>>(
+                A + k0 * ld + k0, ld, A + k0 * ld + cs, ld, (int)w, (int)nc, ctx->d_status);
+            prof_end(ctx, qs, kClsTrsm, 8.0 * (w * (double)w / 2 + 2.0 * w * (double)nc));  // bytes
+            B2M_LAUNCHED(ctx);
             DOperand a{A, ld, n, n, k1, k0, true};
             DOperand b{A, ld, n, n, k0, cs, false};
             return dgemm_tiled(ctx, qs, a, b, A + k1 * ld + cs, ld, n - k1, nc, w, B2M_DO_SUB, true);

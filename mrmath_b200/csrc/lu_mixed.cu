@@ -288,13 +288,6 @@ __global__ void __launch_bounds__(256) trsv_block_kernel(TrArgs a, int b) {
     }
 }
 
-__device__ __forceinline__ void cp_async16(void* dst, const void* src, int src_bytes) {
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(smem_u32(dst)), "l"(src), "r"(src_bytes)
-                 : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-template <int N>
-__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
 
 // ------------------------------------------------------------------ persistent sweep
 // One cooperative launch per sweep: CTA (block b, group g) owns rows [128 b, +128) and right-hand
@@ -521,21 +514,22 @@ __global__ void __launch_bounds__(256, 1) trsv_sweep_kernel(SwArgs a) {
     }
 }
 
-// Chained variant of trsv_sweep_kernel on thread-block clusters of kChCl consecutive blocks (in
+// Chained variant of trsv_sweep_kernel on thread-block clusters of kChCl (8 or 4) consecutive blocks (in
 // sweep order, one right-hand-side group per cluster row): besides publishing its solution to
 // global memory, a block pushes it into the shared memory of every later block of its cluster
 // (st.async completing on the receiver's mbarrier for that sender, 4 KiB each), and a block folds
 // the earlier blocks of its own cluster in from there.  Only the hop into the first block of a
-// cluster pays a round trip through L2; the other seven ride on distributed shared memory.  Every
+// cluster pays a round trip through L2; the others ride on distributed shared memory.  Every
 // wait is bounded; a wait that gives up flags status[kTimeout], which every other wait also polls,
 // so the whole sweep winds down quickly.  All CTAs of a cluster meet at a cluster barrier after
 // the mbarriers are initialised and before they exit.
-constexpr int kChCl = 8;
 constexpr int kChSlot = kTrsvNB * kSwRhs * (int)sizeof(float);        // one pushed solution block
-constexpr int kChSmem = kSwSmem + (kChCl - 1) * kChSlot;             // + receive slots
+template <int CL>
+constexpr int chain_smem() { return kSwSmem + (CL - 1) * kChSlot; }  // + receive slots
 
 __device__ __forceinline__ int ld_volatile_i32(const int32_t* p) { return *reinterpret_cast<const volatile int32_t*>(p); }
 
+template <int kChCl>
 __global__ void __cluster_dims__(kChCl, 1, 1) __launch_bounds__(256, 1) trsv_chain_kernel(SwArgs a, int nbp) {
     extern __shared__ __align__(16) float4 sw_dyn[];
     __shared__ __align__(16) float s_p[kTrsvNB][kSwRhs];  // x of a block from another cluster
@@ -863,44 +857,56 @@ __global__ void __launch_bounds__(256, 1) resid_kernel(ReArgs a) {
 // Whether the chained sweep can run here, and how many of its clusters fit at once: one launch
 // of it with no blocks to solve (every CTA is padding and only meets its cluster's barriers) as a
 // cooperative cluster launch, outside any capture.  A launch error leaves the chained sweep off.
-int32_t chain_probe(Ctx* ctx, cudaStream_t st) {
-    if (ctx->chain_clusters >= 0) return B2M_OK;
-    ctx->chain_clusters = 0;
-    cudaError_t e = cudaFuncSetAttribute(trsv_chain_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kChSmem);
+template <int CL>
+int chain_probe_one(Ctx* ctx, cudaStream_t st, int* why) {
+    cudaError_t e = cudaFuncSetAttribute(trsv_chain_kernel<CL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         chain_smem<CL>());
     if (e != cudaSuccess) {
         (void)cudaGetLastError();
-        ctx->chain_probe_why = 1000 + (int)e;
-        return B2M_OK;
+        *why = 1000 + (int)e;
+        return 0;
     }
     cudaLaunchConfig_t cfg{};
     cudaLaunchAttribute at[1];
     at[0].id = cudaLaunchAttributeCooperative;
     at[0].val.cooperative = 1;
-    cfg.gridDim = dim3((unsigned)kChCl);
+    cfg.gridDim = dim3((unsigned)CL);
     cfg.blockDim = dim3(256);
-    cfg.dynamicSmemBytes = kChSmem;
+    cfg.dynamicSmemBytes = chain_smem<CL>();
     cfg.stream = st;
     cfg.attrs = at;
     cfg.numAttrs = 1;
     int clusters = 0;
-    e = cudaOccupancyMaxActiveClusters(&clusters, trsv_chain_kernel, &cfg);
+    e = cudaOccupancyMaxActiveClusters(&clusters, trsv_chain_kernel<CL>, &cfg);
     if (e != cudaSuccess || clusters < 1) {
         (void)cudaGetLastError();
-        ctx->chain_probe_why = e != cudaSuccess ? 2000 + (int)e : 4000;
-        return B2M_OK;
+        *why = e != cudaSuccess ? 2000 + (int)e : 4000;
+        return 0;
     }
     SwArgs sa{};
     sa.n = 0;  // no blocks: every CTA is padding
     sa.status = ctx->d_status;
-    e = cudaLaunchKernelEx(&cfg, trsv_chain_kernel, sa, (int)kChCl);
+    e = cudaLaunchKernelEx(&cfg, trsv_chain_kernel<CL>, sa, CL);
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     if (e != cudaSuccess) {
         (void)cudaGetLastError();
-        ctx->chain_probe_why = 3000 + (int)e;
-        return B2M_OK;
+        *why = 3000 + (int)e;
+        return 0;
     }
-    B2M_LAUNCHED(ctx);
-    ctx->chain_clusters = clusters;
+    ctx->launches++;
+    return clusters;
+}
+
+// Whether the chained sweep can run here, and how many of its clusters (of 8 and of 4 CTAs) fit at
+// once: one launch of each with no blocks to solve (every CTA is padding and only meets its
+// cluster's barriers) as a cooperative cluster launch, outside any capture.  A launch error leaves
+// that cluster size off.
+int32_t chain_probe(Ctx* ctx, cudaStream_t st) {
+    if (ctx->chain_clusters >= 0) return B2M_OK;
+    int why8 = 0, why4 = 0;
+    ctx->chain_clusters = chain_probe_one<8>(ctx, st, &why8);
+    ctx->chain_clusters4 = chain_probe_one<4>(ctx, st, &why4);
+    ctx->chain_probe_why = why8 ? why8 : why4;
     return B2M_OK;
 }
 
@@ -919,8 +925,12 @@ int32_t ir_solve(Ctx* ctx, cudaStream_t st, const float* LU, int64_t ld, int64_t
     for (int64_t c0 = 0; c0 < nrhs; c0 += kTrMaxRhs) {
         const int nc = (int)std::min<int64_t>(kTrMaxRhs, nrhs - c0);
         const int ng = (int)ceil_div(nc, kSwRhs);
-        const int nbp = (int)round_up(nblk, kChCl);
-        if (ng <= kSweepGroups && ng * nbp / kChCl <= ctx->chain_clusters) {
+        const int nbp8 = (int)round_up(nblk, 8), nbp4 = (int)round_up(nblk, 4);
+        const int chain = ng > kSweepGroups ? 0
+                          : ng * nbp8 / 8 <= ctx->chain_clusters ? 8
+                          : ng * nbp4 / 4 <= ctx->chain_clusters4 ? 4 : 0;
+        if (chain) {
+            const int nbp = chain == 8 ? nbp8 : nbp4;
             // chained sweeps on clusters: one cooperative launch each
             for (int up = 0; up < 2; ++up) {
                 const size_t ll_words = (size_t)nblk * ng * kTrsvNB * kSwRhs;
@@ -934,12 +944,13 @@ int32_t ir_solve(Ctx* ctx, cudaStream_t st, const float* LU, int64_t ld, int64_t
                 at[0].val.cooperative = 1;
                 cfg.gridDim = dim3((unsigned)(nbp * ng));
                 cfg.blockDim = dim3(256);
-                cfg.dynamicSmemBytes = kChSmem;
+                cfg.dynamicSmemBytes = chain == 8 ? chain_smem<8>() : chain_smem<4>();
                 cfg.stream = st;
                 cfg.attrs = at;
                 cfg.numAttrs = 1;
                 prof_begin(ctx, st, kClsSolve);
-                B2M_CU(ctx, cudaLaunchKernelEx(&cfg, trsv_chain_kernel, sa, nbp));
+                if (chain == 8) B2M_CU(ctx, cudaLaunchKernelEx(&cfg, trsv_chain_kernel<8>, sa, nbp));
+                else B2M_CU(ctx, cudaLaunchKernelEx(&cfg, trsv_chain_kernel<4>, sa, nbp));
                 prof_end(ctx, st, kClsSolve, 4.0 * (double)n * n / 2 + 4.0 * nblk * kTrsvNB * kTrsvNB + 8.0 * n * nc);
                 B2M_LAUNCHED(ctx);
             }
