@@ -11,6 +11,7 @@
 #include <functional>
 #include <map>
 #include <mutex>
+#include <utility>
 #include <tuple>
 #include <type_traits>
 #include <string>
@@ -116,6 +117,7 @@ struct Ctx {
     cudaStream_t side_stream = nullptr;                  // look-ahead trailing updates of the FP32 LU
     cudaEvent_t ev_side_fork = nullptr, ev_side_join = nullptr;
     int chain_priority = 0;                               // stream priority of the panel kernels
+    bool launch_hi = false;  // launch_k adds the launch attribute `priority = chain_priority` (PriorityScope)
     std::string last_error;
     std::mutex mtx;
     b2m_progress_fn progress = nullptr;          // LU progress callback (b2m_set_progress)
@@ -164,6 +166,34 @@ struct CallLock {
             return ::b2m::fail((ctx), B2M_ERR_CUDA, "kernel launch failed: %s (%s:%d)",            \
                                cudaGetErrorString(e_), __FILE__, __LINE__);                        \
     } while (0)
+
+// Launches `kern` on `st`; while a PriorityScope marks the launches as the critical path, with the
+// launch attribute priority = ctx->chain_priority (graphs keep it per node: they are instantiated
+// with per-node priorities), so that they take SMs ahead of a concurrent look-ahead update.
+template <typename... KArgs, typename... Args>
+cudaError_t launch_k(Ctx* ctx, void (*kern)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t st,
+                     Args&&... args) {
+    cudaLaunchConfig_t c{};
+    c.gridDim = grid;
+    c.blockDim = block;
+    c.dynamicSmemBytes = smem;
+    c.stream = st;
+    cudaLaunchAttribute at[1];
+    if (ctx->launch_hi) {
+        at[0].id = cudaLaunchAttributePriority;
+        at[0].val.priority = ctx->chain_priority;
+        c.attrs = at;
+        c.numAttrs = 1;
+    }
+    return cudaLaunchKernelEx(&c, kern, std::forward<Args>(args)...);
+}
+// marks (hi = true) or unmarks the launches issued while it lives
+struct PriorityScope {
+    Ctx* ctx;
+    bool prev;
+    PriorityScope(Ctx* c, bool hi) : ctx(c), prev(c->launch_hi) { c->launch_hi = hi; }
+    ~PriorityScope() { ctx->launch_hi = prev; }
+};
 
 // Event profiler: brackets one launch on stream `st` (no-ops unless enabled).
 void prof_begin(Ctx* ctx, cudaStream_t st, int cls);

@@ -194,7 +194,7 @@ int32_t launch_variant(Ctx* ctx, cudaStream_t st, const CUtensorMap& ta, const C
     }
     const int tiles = (int)(ceil_div(a.M, BM) * ceil_div(a.N, BN));
     prof_begin(ctx, st, kClsGemm);
-    dgemm_tma_kernel<AK, BKM><<<tiles, kThreads, kSmemBytes, st>>>(ta, tb, a);
+    B2M_CU(ctx, launch_k(ctx, dgemm_tma_kernel<AK, BKM>, dim3(tiles), dim3(kThreads), kSmemBytes, st, ta, tb, a));
     prof_end(ctx, st, kClsGemm, 2.0 * a.M * a.N * a.K);
     B2M_LAUNCHED(ctx);
     return B2M_OK;
@@ -244,10 +244,10 @@ int32_t dgemm_tiled(Ctx* ctx, cudaStream_t st, const DOperand& A, const DOperand
         }
         const int64_t outs = M * N;
         prof_begin(ctx, st, kClsGemm);
-        dgemm_ktail_kernel<<<(unsigned)ceil_div(outs, 256), 256, 0, st>>>(
-            static_cast<const double*>(A.base), A.ld, A.r0, A.c0, A.kmajor ? 1 : 0, static_cast<const double*>(B.base),
-            B.ld, B.r0, B.c0, B.kmajor ? 1 : 0, C, ldc, (int)M, (int)N, (int)K16, (int)(K - K16), tail_op,
-            ctx->d_status, check_info ? 1 : 0);
+        B2M_CU(ctx, launch_k(ctx, dgemm_ktail_kernel, dim3((unsigned)ceil_div(outs, 256)), dim3(256), 0, st,
+                             static_cast<const double*>(A.base), A.ld, A.r0, A.c0, A.kmajor ? 1 : 0,
+                             static_cast<const double*>(B.base), B.ld, B.r0, B.c0, B.kmajor ? 1 : 0, C, ldc, (int)M,
+                             (int)N, (int)K16, (int)(K - K16), tail_op, ctx->d_status, check_info ? 1 : 0));
         prof_end(ctx, st, kClsGemm, 2.0 * M * N * (K - K16));
         B2M_LAUNCHED(ctx);
         return B2M_OK;

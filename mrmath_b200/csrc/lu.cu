@@ -146,7 +146,7 @@ __global__ void __launch_bounds__(kSwapThreads)
 // panel columns right of the leaf, turns the leaf's rows into U12 = L11^-1 A12 (thread per column:
 // the <= 32 values of the column in the leaf's rows after the interchanges, then the unit-lower
 // forward substitution with contributions in ascending order, as trsm_small_kernel computes it);
-// (2) rank_update_kernel subtracts L21 U12 from the rest of the panel (rows below the leaf).  Both
+// (2) panel_rank_update_kernel subtracts L21 U12 from the rest of the panel (rows below the leaf).  Both
 // only touch the outer panel's columns; the other columns get the panel's net permutation and one
 // K = 256 update per panel.
 constexpr int kSuThreads = 64;  // columns per CTA of leaf_swap_u12_kernel
@@ -261,7 +261,7 @@ __global__ void __launch_bounds__(kSuThreads)
 // L21 and U12 slices staged in shared memory; the w products of each element are accumulated in
 // ascending k and subtracted once (as the GEMM's doSub epilogue does).
 constexpr int kRuT = 64;
-__global__ void __launch_bounds__(256, 2) rank_update_kernel(double* A, int64_t ld, int n, int r_lo, int cl, int ch,
+__global__ void __launch_bounds__(256, 2) panel_rank_update_kernel(double* A, int64_t ld, int n, int r_lo, int cl, int ch,
                                                           int c0, int w, const int32_t* status) {
     __shared__ double s_a[kRuT][kPanelW + 1];  // L21 rows of the tile
     __shared__ __align__(16) double s_b[kPanelW][kRuT];  // U12 columns of the tile
@@ -701,7 +701,7 @@ static_assert(kOuterNB == kTpK, "the panel triangular solve holds one outer pane
 // Blocked right-looking LU with look-ahead (orders n > 2 kOuterNB).  Per outer panel of 256
 // columns: (1) the panel is factored right-looking by leaves, each leaf's interchanges kept inside
 // the panel (and recorded in the row map pmap), its U12 formed by the same launch and its rank-w
-// update applied to the rest of the panel (leaf_swap_u12_kernel, rank_update_kernel); (2) the
+// update applied to the rest of the panel (leaf_swap_u12_kernel, panel_rank_update_kernel); (2) the
 // panel's net permutation is applied to the next panel's columns on this stream, and to every
 // further column right of the panel and the factored columns left of it on the side stream;
 // (3) U12 = L11^-1 A12 (trsm_panel_kernel, one launch) and A22 -= A21 U12 for the next panel's
@@ -730,6 +730,7 @@ int32_t lu_blocked(Ctx* ctx, cudaStream_t q, double* A, int64_t ld, int64_t n, i
         return B2M_OK;
     };
     const int64_t pm_ld = round_up(n, 64);
+    PriorityScope hi(ctx, true);  // this stream's launches are the critical path (see launch_k)
     std::atomic<int>& attr = device_flag((const void*)trsm_panel_kernel, 0, ctx->device);
     if (!attr.load()) {
         B2M_CU(ctx, cudaFuncSetAttribute(trsm_panel_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kTpSmem));
@@ -738,23 +739,25 @@ int32_t lu_blocked(Ctx* ctx, cudaStream_t q, double* A, int64_t ld, int64_t n, i
     for (int64_t k0 = 0; k0 < n; k0 += kOuterNB) {
         const int64_t w = std::min(kOuterNB, n - k0), k1 = k0 + w;
         int32_t* pmap = pmap2 + ((k0 / kOuterNB) & 1) * pm_ld;
-        iota_kernel<<<(unsigned)ceil_div(n, 256), 256, 0, q>>>(pmap, n);
+        B2M_CU(ctx, launch_k(ctx, iota_kernel, dim3((unsigned)ceil_div(n, 256)), dim3(256), 0, q, pmap, n));
         B2M_LAUNCHED(ctx);
         // the panel, right-looking by leaves (all of it on this stream: it is the critical path)
         for (int64_t c0 = k0; c0 < k1; c0 += leaf) {
             const int64_t wl = std::min(leaf, k1 - c0);
             B2M_TRY(launch_panel<double>(ctx, q, A + c0 * ld + c0, ld, (int)(n - c0), (int)wl, (int)c0, (int)c0, ipiv));
             prof_begin(ctx, q, kClsSwap);
-            leaf_swap_u12_kernel<double><<<(unsigned)std::max<int64_t>(1, ceil_div(w - wl, kSuThreads)), kSuThreads, 0, q>>>(
-                A, ld, (int)k0, (int)k1, (int)c0, (int)wl, ipiv, perm, pmap, ctx->d_status);
+            B2M_CU(ctx, launch_k(ctx, leaf_swap_u12_kernel<double>,
+                                 dim3((unsigned)std::max<int64_t>(1, ceil_div(w - wl, kSuThreads))), dim3(kSuThreads), 0,
+                                 q, A, ld, (int)k0, (int)k1, (int)c0, (int)wl, ipiv, perm, pmap,
+                                 (const int32_t*)ctx->d_status));
             prof_end(ctx, q, kClsSwap, 16.0 * wl * (double)(w - wl));
             B2M_LAUNCHED(ctx);
             const int64_t rl = c0 + wl;
             if (rl < k1) {
                 dim3 grid((unsigned)ceil_div(k1 - rl, kRuT), (unsigned)ceil_div(n - rl, kRuT));
                 prof_begin(ctx, q, kClsGemm);
-                rank_update_kernel<<<grid, 256, 0, q>>>(A, ld, (int)n, (int)rl, (int)rl, (int)k1, (int)c0, (int)wl,
-                                                        ctx->d_status);
+                B2M_CU(ctx, launch_k(ctx, panel_rank_update_kernel, grid, dim3(256), 0, q, A, ld, (int)n, (int)rl,
+                                     (int)rl, (int)k1, (int)c0, (int)wl, (const int32_t*)ctx->d_status));
                 prof_end(ctx, q, kClsGemm, 2.0 * (double)(n - rl) * (double)(k1 - rl) * (double)wl);  // flops
                 B2M_LAUNCHED(ctx);
             }
@@ -768,8 +771,9 @@ int32_t lu_blocked(Ctx* ctx, cudaStream_t q, double* A, int64_t ld, int64_t n, i
         auto permute = [&](cudaStream_t qs, int64_t c_begin, int64_t c_end) -> int32_t {
             if (c_end <= c_begin) return B2M_OK;
             prof_begin(ctx, qs, kClsSwap);
-            panel_permute_f64_kernel<<<(unsigned)ceil_div(c_end - c_begin, 32), 256, 0, qs>>>(
-                A, ld, (int)n, (int)k0, (int)c_begin, (int)c_end, pmap, ctx->d_status);
+            B2M_CU(ctx, launch_k(ctx, panel_permute_f64_kernel, dim3((unsigned)ceil_div(c_end - c_begin, 32)), dim3(256), 0,
+                                 qs, A, ld, (int)n, (int)k0, (int)c_begin, (int)c_end, (const int32_t*)pmap,
+                                 ctx->d_status));
             prof_end(ctx, qs, kClsSwap, 2.0 * 8.0 * 2 * w * (double)(c_end - c_begin));  // <= 2w rows moved
             B2M_LAUNCHED(ctx);
             return B2M_OK;
@@ -780,21 +784,26 @@ int32_t lu_blocked(Ctx* ctx, cudaStream_t q, double* A, int64_t ld, int64_t n, i
         B2M_TRY(permute(q, k1, k1 + nw));
         if (k0 > 0 || rest > nw) {
             B2M_TRY(fork());
+            PriorityScope side(ctx, false);
             B2M_TRY(permute(q2, k1 + nw, n));
             B2M_TRY(permute(q2, 0, k0));
         }
         if (k1 >= n) break;
         auto update = [&](cudaStream_t qs, int64_t cs, int64_t nc) -> int32_t {
             prof_begin(ctx, qs, kClsTrsm);
-            trsm_panel_kernel<<<(unsigned)ceil_div(nc, kTpC), 256, kTpSmem, qs>>>(
-                A + k0 * ld + k0, ld, A + k0 * ld + cs, ld, (int)w, (int)nc, ctx->d_status);
+            B2M_CU(ctx, launch_k(ctx, trsm_panel_kernel, dim3((unsigned)ceil_div(nc, kTpC)), dim3(256), (size_t)kTpSmem,
+                                 qs, (const double*)(A + k0 * ld + k0), ld, A + k0 * ld + cs, ld, (int)w, (int)nc,
+                                 (const int32_t*)ctx->d_status));
             prof_end(ctx, qs, kClsTrsm, 8.0 * (w * (double)w / 2 + 2.0 * w * (double)nc));  // bytes
             B2M_LAUNCHED(ctx);
             DOperand a{A, ld, n, n, k1, k0, true};
             DOperand b{A, ld, n, n, k0, cs, false};
             return dgemm_tiled(ctx, qs, a, b, A + k1 * ld + cs, ld, n - k1, nc, w, B2M_DO_SUB, true);
         };
-        if (rest > nw) B2M_TRY(update(q2, k1 + nw, rest - nw));
+        if (rest > nw) {
+            PriorityScope side(ctx, false);
+            B2M_TRY(update(q2, k1 + nw, rest - nw));
+        }
         B2M_TRY(update(q, k1, nw));
     }
     return join();

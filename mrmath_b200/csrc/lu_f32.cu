@@ -833,6 +833,7 @@ int32_t lu_factor_f32(Ctx* ctx, cudaStream_t st, float* A, int64_t ld, int64_t n
         // priority so that they take SMs ahead of the wide GEMM's tiles.
         cudaStream_t q2 = ctx->side_stream;
         bool side_busy = false;
+        PriorityScope hi(ctx, true);  // launch_k launches on this stream are the critical path
         cudaLaunchAttribute pri[1];
         pri[0].id = cudaLaunchAttributePriority;
         pri[0].val.priority = ctx->chain_priority;
@@ -843,7 +844,7 @@ int32_t lu_factor_f32(Ctx* ctx, cudaStream_t st, float* A, int64_t ld, int64_t n
             c.dynamicSmemBytes = smem;
             c.stream = q;
             c.attrs = pri;
-            c.numAttrs = 1;
+            c.numAttrs = ctx->launch_hi ? 1 : 0;  // the side stream's launches (PriorityScope) go without
             return c;
         };
         B2M_CU(ctx, cudaMemsetAsync(s.counters, 0, s.counters_bytes, q));
@@ -907,6 +908,7 @@ int32_t lu_factor_f32(Ctx* ctx, cudaStream_t st, float* A, int64_t ld, int64_t n
                 if (oc0 > 0) {
                     B2M_CU(ctx, cudaEventRecord(ctx->ev_side_fork, q));
                     B2M_CU(ctx, cudaStreamWaitEvent(q2, ctx->ev_side_fork, 0));
+                    PriorityScope side(ctx, false);
                     B2M_TRY(permute(q2, 0, oc0));
                     side_busy = true;
                 }
@@ -917,7 +919,7 @@ int32_t lu_factor_f32(Ctx* ctx, cudaStream_t st, float* A, int64_t ld, int64_t n
                 OuArgs oa{A, ld, (int)n, (int)oc0, pw, mode, (int)ceil_div(ncols, 32), (int)cs0, (int)ncols,
                           s.bth, s.btl, s.ah, s.al, s.lpinv, ctx->d_status};
                 prof_begin(ctx, qs, kClsTrsm);
-                lu_outer_kernel<<<oa.nU + nl, 256, ou_smem, qs>>>(oa);
+                B2M_CU(ctx, launch_k(ctx, lu_outer_kernel, dim3((unsigned)(oa.nU + nl)), dim3(256), (size_t)ou_smem, qs, oa));
                 // bytes: U12 read and written, its GEMM copies written, L21 read and split (3xTF32)
                 prof_end(ctx, qs, kClsTrsm,
                          8.0 * pw * ncols + 4.0 * ncols * pw * (mode == 3 ? 2 : 1) + (nl ? 12.0 * M * pw : 0.0));
@@ -938,6 +940,7 @@ int32_t lu_factor_f32(Ctx* ctx, cudaStream_t st, float* A, int64_t ld, int64_t n
             if (M > nw || oc0 > 0) {
                 B2M_CU(ctx, cudaEventRecord(ctx->ev_side_fork, q));
                 B2M_CU(ctx, cudaStreamWaitEvent(q2, ctx->ev_side_fork, 0));
+                PriorityScope side(ctx, false);
                 if (M > nw) B2M_TRY(permute(q2, c1 + nw, n));
                 if (oc0 > 0) B2M_TRY(permute(q2, 0, oc0));
                 if (M > nw) {

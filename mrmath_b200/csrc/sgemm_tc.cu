@@ -281,7 +281,8 @@ int32_t launch_tc(Ctx* ctx, cudaStream_t st, const CUtensorMap* maps, const TcAr
     }
     const int tiles = (int)(ceil_div(a.M, TBM) * ceil_div(a.N, TBN));
     prof_begin(ctx, st, kClsTcGemm);
-    sgemm_tc_kernel<SPLIT><<<tiles, kTcThreads, smem, st>>>(maps[0], maps[1], maps[2], maps[3], maps[4], a);
+    B2M_CU(ctx, launch_k(ctx, sgemm_tc_kernel<SPLIT>, dim3(tiles), dim3(kTcThreads), smem, st, maps[0], maps[1],
+                         maps[2], maps[3], maps[4], a));
     prof_end(ctx, st, kClsTcGemm, 2.0 * a.M * a.N * a.K * SPLIT);
     B2M_LAUNCHED(ctx);
     return B2M_OK;
