@@ -712,8 +712,10 @@ static_assert(kOuterNB == kTpK, "the panel triangular solve holds one outer pane
 // parity, because the side stream may still read one panel's map while the next panel fills its own.
 // Every interchange reaches every column exactly once and in order, so the factors and the pivot
 // vector are those of the unblocked recursion.
+// part 0 issues the first outer panel's leaves only, part 1 everything after them (two graphs: the
+// device factors the first panel while the host submits the second).
 int32_t lu_blocked(Ctx* ctx, cudaStream_t q, double* A, int64_t ld, int64_t n, int32_t* ipiv, int32_t* perm,
-                   int32_t* pmap2, int64_t leaf) {
+                   int32_t* pmap2, int64_t leaf, int part) {
     cudaStream_t q2 = ctx->side_stream;
     bool side_busy = false;
     auto join = [&]() -> int32_t {
@@ -739,10 +741,13 @@ int32_t lu_blocked(Ctx* ctx, cudaStream_t q, double* A, int64_t ld, int64_t n, i
     for (int64_t k0 = 0; k0 < n; k0 += kOuterNB) {
         const int64_t w = std::min(kOuterNB, n - k0), k1 = k0 + w;
         int32_t* pmap = pmap2 + ((k0 / kOuterNB) & 1) * pm_ld;
-        B2M_CU(ctx, launch_k(ctx, iota_kernel, dim3((unsigned)ceil_div(n, 256)), dim3(256), 0, q, pmap, n));
-        B2M_LAUNCHED(ctx);
+        const bool leaves = (part == 0) == (k0 == 0);
+        if (leaves) {
+            B2M_CU(ctx, launch_k(ctx, iota_kernel, dim3((unsigned)ceil_div(n, 256)), dim3(256), 0, q, pmap, n));
+            B2M_LAUNCHED(ctx);
+        }
         // the panel, right-looking by leaves (all of it on this stream: it is the critical path)
-        for (int64_t c0 = k0; c0 < k1; c0 += leaf) {
+        for (int64_t c0 = k0; leaves && c0 < k1; c0 += leaf) {
             const int64_t wl = std::min(leaf, k1 - c0);
             B2M_TRY(launch_panel<double>(ctx, q, A + c0 * ld + c0, ld, (int)(n - c0), (int)wl, (int)c0, (int)c0, ipiv));
             prof_begin(ctx, q, kClsSwap);
@@ -767,6 +772,7 @@ int32_t lu_blocked(Ctx* ctx, cudaStream_t q, double* A, int64_t ld, int64_t n, i
                 B2M_CU(ctx, cudaLaunchHostFunc(q, progress_trampoline, &ctx->progress_notes.back()));
             }
         }
+        if (part == 0) return B2M_OK;
         B2M_TRY(join());  // the previous panel's wide update is done before rows move under it
         auto permute = [&](cudaStream_t qs, int64_t c_begin, int64_t c_end) -> int32_t {
             if (c_end <= c_begin) return B2M_OK;
@@ -864,13 +870,18 @@ int32_t lu_factor_f64(Ctx* ctx, cudaStream_t st, double* A, int64_t ld, int64_t 
         B2M_TRY(ensure_side_stream(ctx));
     }
     const GraphKey key{1, A, ipiv, perm, ctx->d_status, ld, n, 0, 0};
-    return run_graph(ctx, st, key, [&](cudaStream_t s) -> int32_t {
+    const GraphKey key1{1, A, ipiv, perm, ctx->d_status, ld, n, 0, 1};
+    B2M_TRY(run_graph(ctx, st, key, [&](cudaStream_t s) -> int32_t {
         if (perm) {
             iota_kernel<<<(unsigned)ceil_div(n, 256), 256, 0, s>>>(perm, n);
             B2M_LAUNCHED(ctx);
         }
-        if (blocked) return lu_blocked(ctx, s, A, ld, n, ipiv, perm, pmap2, leaf);
+        if (blocked) return lu_blocked(ctx, s, A, ld, n, ipiv, perm, pmap2, leaf, 0);
         return lu_rec(ctx, s, A, ld, n, 0, n, ipiv, perm, leaf, SwapScope{0, n, nullptr});
+    }));
+    if (!blocked) return B2M_OK;
+    return run_graph(ctx, st, key1, [&](cudaStream_t s) -> int32_t {
+        return lu_blocked(ctx, s, A, ld, n, ipiv, perm, pmap2, leaf, 1);
     });
 }
 

@@ -824,8 +824,12 @@ int32_t lu_factor_f32(Ctx* ctx, cudaStream_t st, float* A, int64_t ld, int64_t n
         B2M_CU(ctx, cudaEventCreateWithFlags(&ctx->ev_side_join, cudaEventDisableTiming));
         ctx->chain_priority = greatest;
     }
-    const GraphKey key{3 + mode * 10, A, perm, s.cand, s.bth, ld, n, 0, 0};
-    return run_graph(ctx, st, key, [&](cudaStream_t q) -> int32_t {
+    const GraphKey key0{3 + mode * 10, A, perm, s.cand, s.bth, ld, n, 0, 1};
+    const GraphKey key1{3 + mode * 10, A, perm, s.cand, s.bth, ld, n, 0, 2};
+    // part 0: the first outer panel's leaves; part 1: everything after them.  Two graphs, so that the
+    // device factors the first panel while the host still submits the large second graph (a graph's
+    // launch costs host time per node).
+    auto issue = [&](cudaStream_t q, int part) -> int32_t {
         // Look-ahead: after a panel, only the next panel's columns are updated on this stream; the
         // rest of the trailing update runs on the side stream, overlapping the next panel's leaves
         // (which touch neither those columns nor the previous panel's L21), and is joined before
@@ -847,16 +851,19 @@ int32_t lu_factor_f32(Ctx* ctx, cudaStream_t st, float* A, int64_t ld, int64_t n
             c.numAttrs = ctx->launch_hi ? 1 : 0;  // the side stream's launches (PriorityScope) go without
             return c;
         };
-        B2M_CU(ctx, cudaMemsetAsync(s.counters, 0, s.counters_bytes, q));
-        iota_f32_kernel<<<(unsigned)ceil_div(n, 256), 256, 0, q>>>(perm, n);
-        B2M_LAUNCHED(ctx);
+        if (part == 0) {
+            B2M_CU(ctx, cudaMemsetAsync(s.counters, 0, s.counters_bytes, q));
+            iota_f32_kernel<<<(unsigned)ceil_div(n, 256), 256, 0, q>>>(perm, n);
+            B2M_LAUNCHED(ctx);
+        }
         for (int64_t oc0 = 0; oc0 < n; oc0 += kNB) {
             const int pw = (int)std::min<int64_t>(kNB, n - oc0);
             // the row map alternates between two buffers by panel parity: the side stream may still
             // be permuting the previous panel's left columns with its map while this panel's first
             // leaf initialises the other one (the join below orders the reuse two panels later)
             int32_t* pmap = s.pmap + ((oc0 / kNB) & 1) * round_up(n, 64);
-            for (int64_t lc0 = oc0; lc0 < oc0 + pw; lc0 += 32) {
+            const bool leaves = (part == 0) == (oc0 == 0);
+            for (int64_t lc0 = oc0; leaves && lc0 < oc0 + pw; lc0 += 32) {
                 const int w = (int)std::min<int64_t>(32, n - lc0);
                 TsArgs ta{A, ld, (int)n, (int)lc0, w, (int)oc0, pw, s.cand, s.counters, s.top, s.mvals, s.wmat,
                           s.moves, s.lmul, lc0 == oc0 ? pmap : nullptr, s.lpinv, ctx->d_status};
@@ -879,6 +886,7 @@ int32_t lu_factor_f32(Ctx* ctx, cudaStream_t st, float* A, int64_t ld, int64_t n
                 prof_end(ctx, q, kClsSwap, 8.0 * (n - lc0) * (pw - (lc0 - oc0)));
                 B2M_LAUNCHED(ctx);
             }
+            if (part == 0) return B2M_OK;
             if (side_busy) {  // the previous panel's wide update must be done before rows move under it
                 B2M_CU(ctx, cudaEventRecord(ctx->ev_side_join, q2));
                 B2M_CU(ctx, cudaStreamWaitEvent(q, ctx->ev_side_join, 0));
@@ -961,7 +969,9 @@ int32_t lu_factor_f32(Ctx* ctx, cudaStream_t st, float* A, int64_t ld, int64_t n
         coupling_kernel<<<2 * nblk, 256, kCpSmem, q>>>(A, ld, (int)n, s.linv, s.uinv, s.wl, s.wu, ctx->d_status);
         B2M_LAUNCHED(ctx);
         return B2M_OK;
-    });
+    };
+    B2M_TRY(run_graph(ctx, st, key0, [&](cudaStream_t q) { return issue(q, 0); }));
+    return run_graph(ctx, st, key1, [&](cudaStream_t q) { return issue(q, 1); });
 }
 
 }  // namespace b2m
