@@ -514,96 +514,38 @@ __global__ void __launch_bounds__(256, 1) trsv_sweep_kernel(SwArgs a) {
     }
 }
 
-// Chained variant of trsv_sweep_kernel on thread-block clusters of kChCl (8 or 4) consecutive blocks
-// (in sweep order, one right-hand-side group per cluster row), with its products on the tensor
-// cores.  Besides publishing its solution to global memory, a block pushes it into the shared
-// memory of every later block of its cluster (st.async completing on the receiver's mbarrier for
-// that sender, 4 KiB each), and a block folds the earlier blocks of its own cluster in from there:
-// only the hop into the first block of a cluster pays a round trip through L2.
-//
-// Every 128 x 128 x 8 product (the folds T_bj x_j, z = T_bb^-1 y and W_b x_p) is a 3xTF32
-// mma.sync.m16n8k8 product (a = a_hi + a_lo split, a_hi b_hi + a_hi b_lo + a_lo b_hi, FP32
-// accumulation): warp w owns rows 16 w .. 16 w + 15 of the block and the whole K = 128, lane
-// (g, t) = (lane / 4, lane % 4) holds C at rows 16 w + g (+8) and right-hand sides 2 t, 2 t + 1.
-// Within each 16-column group the k slots are permuted consistently in A and B (slots t, t + 4 of
-// the first k-step are columns 4 t, 4 t + 1, of the second 4 t + 2, 4 t + 3), so a thread reads its
-// A elements as one float4 per row.  Right-hand-side blocks live in shared memory transposed,
-// [8][144] (right-hand side, row), and the staged T_bb^-1 and W_b row-major with row stride 144:
-// both read conflict-free as float4s.
-//
-// Every wait is bounded; a wait that gives up flags status[kTimeout], which every other wait also
-// polls, so the whole sweep winds down quickly.  All CTAs of a cluster meet at a cluster barrier
-// after the mbarriers are initialised and before they exit.
-constexpr int kChS = 144;                                              // row stride of the staged blocks
-constexpr int kChSlot = kSwRhs * kTrsvNB * (int)sizeof(float);          // one pushed solution block (4 KiB)
-constexpr int kChBlk = kSwRhs * kChS;                                   // floats of one transposed x block
+// Chained variant of trsv_sweep_kernel on thread-block clusters of kChCl (8 or 4) consecutive blocks (in
+// sweep order, one right-hand-side group per cluster row): besides publishing its solution to
+// global memory, a block pushes it into the shared memory of every later block of its cluster
+// (st.async completing on the receiver's mbarrier for that sender, 4 KiB each), and a block folds
+// the earlier blocks of its own cluster in from there.  Only the hop into the first block of a
+// cluster pays a round trip through L2; the others ride on distributed shared memory.  Every
+// wait is bounded; a wait that gives up flags status[kTimeout], which every other wait also polls,
+// so the whole sweep winds down quickly.  All CTAs of a cluster meet at a cluster barrier after
+// the mbarriers are initialised and before they exit.
+constexpr int kChSlot = kTrsvNB * kSwRhs * (int)sizeof(float);        // one pushed solution block
 template <int CL>
-constexpr int chain_smem() {
-    return (2 * kTrsvNB * kChS + (CL - 1) * kChBlk) * (int)sizeof(float);  // T_bb^-1, W_b, receive slots
-}
+constexpr int chain_smem() { return kSwSmem + (CL - 1) * kChSlot; }  // + receive slots
 
 __device__ __forceinline__ int ld_volatile_i32(const int32_t* p) { return *reinterpret_cast<const volatile int32_t*>(p); }
 
-__device__ __forceinline__ void mma_tf32(float (&d)[4], uint32_t a0, uint32_t a1, uint32_t a2, uint32_t a3, uint32_t b0,
-                                         uint32_t b1) {
-    asm volatile("mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};\n"
-                 : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
-                 : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
-}
-// x = hi + lo with hi the top 10 mantissa bits (the tensor cores read the TF32 bits of each operand)
-__device__ __forceinline__ uint32_t tf32_hi_bits(float x) { return __float_as_uint(x) & 0xFFFFE000u; }
-__device__ __forceinline__ uint32_t tf32_lo_bits(float x) { return __float_as_uint(x - __uint_as_float(__float_as_uint(x) & 0xFFFFE000u)); }
-
-// acc += A (rows 16 w + g, + 8; 16-column groups q: ra[q] = row g, rb[q] = row g + 8) times the
-// transposed right-hand-side block P ([8][kChS]) over K = 128, 3xTF32
-__device__ __forceinline__ void chain_mma(float (&acc)[4], const float4 (&ra)[8], const float4 (&rb)[8], const float* P) {
-    const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
-#pragma unroll
-    for (int q = 0; q < 8; ++q) {
-        const float4 pb = *reinterpret_cast<const float4*>(P + g * kChS + 16 * q + 4 * t);  // columns 4t .. 4t+3
-        const float av[2][4] = {{ra[q].x, rb[q].x, ra[q].y, rb[q].y}, {ra[q].z, rb[q].z, ra[q].w, rb[q].w}};
-        const float bv[2][2] = {{pb.x, pb.y}, {pb.z, pb.w}};
-#pragma unroll
-        for (int s = 0; s < 2; ++s) {
-            const uint32_t ah0 = tf32_hi_bits(av[s][0]), ah1 = tf32_hi_bits(av[s][1]), ah2 = tf32_hi_bits(av[s][2]),
-                           ah3 = tf32_hi_bits(av[s][3]);
-            const uint32_t al0 = tf32_lo_bits(av[s][0]), al1 = tf32_lo_bits(av[s][1]), al2 = tf32_lo_bits(av[s][2]),
-                           al3 = tf32_lo_bits(av[s][3]);
-            const uint32_t bh0 = tf32_hi_bits(bv[s][0]), bh1 = tf32_hi_bits(bv[s][1]);
-            const uint32_t bl0 = tf32_lo_bits(bv[s][0]), bl1 = tf32_lo_bits(bv[s][1]);
-            mma_tf32(acc, al0, al1, al2, al3, bh0, bh1);
-            mma_tf32(acc, ah0, ah1, ah2, ah3, bl0, bl1);
-            mma_tf32(acc, ah0, ah1, ah2, ah3, bh0, bh1);
-        }
-    }
-}
-// the A rows of a product from a staged [128][kChS] block
-__device__ __forceinline__ void chain_rows_smem(const float* M, float4 (&ra)[8], float4 (&rb)[8]) {
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, g = lane >> 2, t = lane & 3;
-    const float* r0 = M + (16 * warp + g) * kChS + 4 * t;
-#pragma unroll
-    for (int q = 0; q < 8; ++q) {
-        ra[q] = *reinterpret_cast<const float4*>(r0 + 16 * q);
-        rb[q] = *reinterpret_cast<const float4*>(r0 + 8 * kChS + 16 * q);
-    }
-}
-
 template <int kChCl>
 __global__ void __cluster_dims__(kChCl, 1, 1) __launch_bounds__(256, 1) trsv_chain_kernel(SwArgs a, int nbp) {
-    extern __shared__ __align__(16) float ch_dyn[];
-    __shared__ __align__(16) float s_p[kChBlk];   // x of a block from another cluster (transposed)
-    __shared__ __align__(16) float s_y[kChBlk];   // y, then this block's own x (transposed)
-    __shared__ __align__(8) uint64_t s_bar[kChCl];  // one per earlier block of the cluster
+    extern __shared__ __align__(16) float4 sw_dyn[];
+    __shared__ __align__(16) float s_p[kTrsvNB][kSwRhs];  // x of a block from another cluster
+    __shared__ __align__(16) float s_y[kTrsvNB][kSwRhs];
+    __shared__ __align__(16) float s_h[kTrsvNB][kSwRhs];
+    __shared__ __align__(8) uint64_t s_bar[kChCl];       // one per earlier block of the cluster
     __shared__ int s_abort;
-    float* s_inv = ch_dyn;                       // [128][kChS] T_bb^-1
-    float* s_w = ch_dyn + kTrsvNB * kChS;        // [128][kChS] W_b
-    float* s_rx = ch_dyn + 2 * kTrsvNB * kChS;   // [kChCl - 1][kChBlk] pushed blocks (transposed)
+    float4* s_inv = sw_dyn;                        // [32][128]: s_inv[kq][r] = inv[r][4kq .. 4kq+3]
+    float4* s_w = sw_dyn + kTrsvNB * kTrsvNB / 4;  // same layout for W_b
+    float (*s_rx)[kTrsvNB][kSwRhs] = reinterpret_cast<float (*)[kTrsvNB][kSwRhs]>(sw_dyn + kTrsvNB * kTrsvNB / 2);
     if (a.status[kInfo] != 0) return;  // uniform: written before the launch
     cg::cluster_group cluster = cg::this_cluster();
-    const int t = threadIdx.x, lane = t & 31, warp = t >> 5, g = lane >> 2, tq = lane & 3;
+    const int t = threadIdx.x;
     const int NB = kTrsvNB;
     const int nblk = (int)ceil_div(a.n, NB);
-    const int grp = blockIdx.x / nbp, bi = blockIdx.x - grp * nbp;
+    const int g = blockIdx.x / nbp, bi = blockIdx.x - g * nbp;
     const int rank = (int)cluster.block_rank();  // bi % kChCl: nbp is a multiple of kChCl
     const int cl0 = bi - rank;
     if (t == 0) {
@@ -619,39 +561,38 @@ __global__ void __cluster_dims__(kChCl, 1, 1) __launch_bounds__(256, 1) trsv_cha
     }
     const int b = a.upper ? nblk - 1 - bi : bi;
     const int b0 = b * NB, bs = min(NB, a.n - b0);
-    const int cg0 = a.c0 + grp * kSwRhs;
-    const int ncg = min(kSwRhs, a.nc - grp * kSwRhs);
-    const int r1 = 16 * warp + g, r2 = r1 + 8;  // this thread's rows of the block
+    const int r = t & (NB - 1), h = t >> 7;
+    const int cgc = a.c0 + g * kSwRhs;
+    const int ncg = min(kSwRhs, a.nc - g * kSwRhs);
     {
         const float* inv = a.inv + (int64_t)b * NB * NB;
         const float* w = a.w + (int64_t)b * NB * NB;
 #pragma unroll 4
         for (int i = 0; i < 16; ++i) {
-            const int e = t + 256 * i, rr = e >> 5, c4 = (e & 31) * 4;  // 128 rows x 32 float4
-            cp_async16(s_inv + rr * kChS + c4, inv + rr * NB + c4, 16);
-            if (bi > 0) cp_async16(s_w + rr * kChS + c4, w + rr * NB + c4, 16);
+            const int e = t + 256 * i, rr = e & (NB - 1), kq = e >> 7;
+            cp_async16(s_inv + kq * NB + rr, inv + rr * NB + 4 * kq, 16);
+            if (bi > 0) cp_async16(s_w + kq * NB + rr, w + rr * NB + 4 * kq, 16);
         }
         cp_async_commit();
     }
-    // this thread's right-hand-side values at (r1, 2tq), (r1, 2tq+1), (r2, 2tq), (r2, 2tq+1)
-    float xb[4];
+    float xb[kSwRhs];
 #pragma unroll
-    for (int e = 0; e < 4; ++e) {
-        const int row = e < 2 ? r1 : r2, q = 2 * tq + (e & 1);
-        xb[e] = (row < bs && q < ncg) ? a.Xr[(int64_t)(b0 + row) * a.ldr + cg0 + q] : 0.f;
-    }
-    float acc[4] = {0.f, 0.f, 0.f, 0.f};
+    for (int q = 0; q < kSwRhs; ++q)
+        xb[q] = (h == 0 && r < bs && q < ncg) ? a.Xr[(int64_t)(b0 + r) * a.ldr + cgc + q] : 0.f;
+    float acc[kSwRhs];
+#pragma unroll
+    for (int q = 0; q < kSwRhs; ++q) acc[q] = 0.f;
     const int ng = (int)ceil_div(a.nc, kSwRhs);
-    unsigned long long* ll_own = a.ll + (size_t)(b * ng + grp) * (kTrsvNB * kSwRhs);
+    unsigned long long* ll_own = a.ll + (size_t)(b * ng + g) * (kTrsvNB * kSwRhs);
     int32_t* tmo = &a.status[kTimeout];
     auto abandon = [&]() {
 #pragma unroll
         for (int e = 0; e < 4; ++e) st_relaxed64(ll_own + 4 * t + e, (unsigned long long)kSwAbort << 32);
     };
-    // block j from another cluster: its global words (row-major [128][8]) into s_p (transposed)
+    // block j (sweep position jj) from another cluster: global words into s_p
     auto wait_global = [&](int j) -> bool {
         const int k = t >> 1, q0 = (t & 1) * 4;
-        const unsigned long long* src = a.ll + (size_t)(j * ng + grp) * (kTrsvNB * kSwRhs) + k * kSwRhs + q0;
+        const unsigned long long* src = a.ll + (size_t)(j * ng + g) * (kTrsvNB * kSwRhs) + k * kSwRhs + q0;
         unsigned long long w[4] = {0ull, 0ull, 0ull, 0ull};
         bool ready = false, bad = false;
         for (uint32_t it = 0; it < a.spin && !ready && !bad; ++it) {
@@ -668,12 +609,13 @@ __global__ void __cluster_dims__(kChCl, 1, 1) __launch_bounds__(256, 1) trsv_cha
         }
         if (!ready && !bad) atomicCAS(tmo, 0, 503);
         if (!ready) s_abort = 1;
-#pragma unroll
-        for (int e = 0; e < 4; ++e) s_p[(q0 + e) * kChS + k] = __uint_as_float((uint32_t)w[e]);
+        const float4 v = make_float4(__uint_as_float((uint32_t)w[0]), __uint_as_float((uint32_t)w[1]),
+                                     __uint_as_float((uint32_t)w[2]), __uint_as_float((uint32_t)w[3]));
+        *reinterpret_cast<float4*>(&s_p[k][q0]) = v;
         __syncthreads();
         return !s_abort;
     };
-    // the push of cluster rank q into its receive slot
+    // the push of cluster rank q into s_rx[q]
     auto wait_push = [&](int q) -> bool {
         bool ready = false, bad = false;
         for (uint32_t it = 0; it < a.spin && !ready && !bad; ++it) {
@@ -685,107 +627,99 @@ __global__ void __cluster_dims__(kChCl, 1, 1) __launch_bounds__(256, 1) trsv_cha
         __syncthreads();
         return !s_abort;
     };
-    // this thread's rows of T_bj (16-column groups), zeros past the block and past the matrix
-    auto load_fold = [&](int j, float4 (&ra)[8], float4 (&rb)[8]) {
-        const int p0 = j * NB, ps = min(NB, a.n - p0);
-        const float* t1 = a.T + (int64_t)(b0 + min(r1, bs - 1)) * a.ld + p0 + 4 * tq;
-        const float* t2 = a.T + (int64_t)(b0 + min(r2, bs - 1)) * a.ld + p0 + 4 * tq;
-#pragma unroll
-        for (int q = 0; q < 8; ++q) {
-            ra[q] = r1 < bs ? ld_row4(t1, 16 * q, ps - 4 * tq) : make_float4(0.f, 0.f, 0.f, 0.f);
-            rb[q] = r2 < bs ? ld_row4(t2, 16 * q, ps - 4 * tq) : make_float4(0.f, 0.f, 0.f, 0.f);
-        }
-    };
-    // the fold after next is prefetched into L2 while the current one waits: lane tq of a row takes
-    // the row's 128-byte line tq
-    auto prefetch_fold = [&](int jj) {
-        if (jj + 1 >= bi) return;
-        const int j = a.upper ? nblk - 1 - jj : jj;
-        if ((int64_t)j * NB + 32 * tq + 32 > a.ld) return;
-        if (r1 < bs) asm volatile("prefetch.global.L2 [%0];\n" ::"l"(a.T + (int64_t)(b0 + r1) * a.ld + j * NB + 32 * tq));
-        if (r2 < bs) asm volatile("prefetch.global.L2 [%0];\n" ::"l"(a.T + (int64_t)(b0 + r2) * a.ld + j * NB + 32 * tq));
-    };
 
     bool ok = true;
-    prefetch_fold(0);
-    prefetch_fold(1);
     for (int jj = 0; ok && jj + 1 < bi; ++jj) {
         const int j = a.upper ? nblk - 1 - jj : jj;
-        float4 ra[8], rb[8];
-        load_fold(j, ra, rb);
-        prefetch_fold(jj + 2);
+        const int p0 = j * NB, ps = min(NB, a.n - p0);
+        float4 tv[16];
+        {
+            const float* trow = a.T + (int64_t)(b0 + min(r, bs - 1)) * a.ld + p0;
+#pragma unroll
+            for (int i = 0; i < 16; ++i)
+                tv[i] = r < bs ? ld_row4(trow, 64 * h + 4 * i, ps) : make_float4(0.f, 0.f, 0.f, 0.f);
+        }
         const bool local = jj >= cl0;
         ok = local ? wait_push(jj - cl0) : wait_global(j);
         if (!ok) break;
-        chain_mma(acc, ra, rb, local ? s_rx + (jj - cl0) * kChBlk : s_p);
+        const float (*P)[kSwRhs] = local ? s_rx[jj - cl0] : s_p;
+#pragma unroll
+        for (int i = 0; i < 16; ++i) {
+            const float tk[4] = {tv[i].x, tv[i].y, tv[i].z, tv[i].w};
+#pragma unroll
+            for (int e = 0; e < 4; ++e) {
+                const int k = 64 * h + 4 * i + e;
+                const float4 x0 = *reinterpret_cast<const float4*>(&P[k][0]);
+                const float4 x1 = *reinterpret_cast<const float4*>(&P[k][4]);
+                acc[0] = fmaf(tk[e], x0.x, acc[0]);
+                acc[1] = fmaf(tk[e], x0.y, acc[1]);
+                acc[2] = fmaf(tk[e], x0.z, acc[2]);
+                acc[3] = fmaf(tk[e], x0.w, acc[3]);
+                acc[4] = fmaf(tk[e], x1.x, acc[4]);
+                acc[5] = fmaf(tk[e], x1.y, acc[5]);
+                acc[6] = fmaf(tk[e], x1.z, acc[6]);
+                acc[7] = fmaf(tk[e], x1.w, acc[7]);
+            }
+        }
         __syncthreads();  // s_p is rewritten by the next global wait
     }
-    float xv[4] = {0.f, 0.f, 0.f, 0.f};
     if (ok) {
-        // y = X_b - sum_{j before p} T_bj x_j (transposed into s_y) ;  z = T_bb^-1 y
+        if (h == 1) {
 #pragma unroll
-        for (int e = 0; e < 4; ++e) {
-            const int row = e < 2 ? r1 : r2, q = 2 * tq + (e & 1);
-            s_y[q * kChS + row] = xb[e] - acc[e];
+            for (int q = 0; q < kSwRhs; ++q) s_h[r][q] = acc[q];
         }
         cp_async_wait<0>();
         __syncthreads();
-        float z[4] = {0.f, 0.f, 0.f, 0.f};
-        {
-            float4 ra[8], rb[8];
-            chain_rows_smem(s_inv, ra, rb);
-            chain_mma(z, ra, rb, s_y);
+        if (h == 0) {
+#pragma unroll
+            for (int q = 0; q < kSwRhs; ++q) s_y[r][q] = xb[q] - acc[q] - s_h[r][q];
         }
+        __syncthreads();
+#pragma unroll
+        for (int q = 0; q < kSwRhs; ++q) acc[q] = 0.f;
+        sw_smem_product(s_inv, r, h, s_y, acc);
         if (bi > 0) {  // x_b = z - W_b x_p
             const bool local = bi - 1 >= cl0;
             ok = local ? wait_push(bi - 1 - cl0) : wait_global(a.upper ? b + 1 : b - 1);
             if (ok) {
-                float wx[4] = {0.f, 0.f, 0.f, 0.f};
-                float4 ra[8], rb[8];
-                chain_rows_smem(s_w, ra, rb);
-                chain_mma(wx, ra, rb, local ? s_rx + (bi - 1 - cl0) * kChBlk : s_p);
 #pragma unroll
-                for (int e = 0; e < 4; ++e) z[e] -= wx[e];
+                for (int q = 0; q < kSwRhs; ++q) acc[q] = -acc[q];
+                sw_smem_product(s_w, r, h, local ? s_rx[bi - 1 - cl0] : s_p, acc);
+#pragma unroll
+                for (int q = 0; q < kSwRhs; ++q) acc[q] = -acc[q];
             }
-        }
-#pragma unroll
-        for (int e = 0; e < 4; ++e) {
-            const int row = e < 2 ? r1 : r2, q = 2 * tq + (e & 1);
-            xv[e] = (row < bs && q < ncg) ? z[e] : 0.f;  // zeros past the matrix and past the right-hand sides
         }
     }
     if (ok) {
-        __syncthreads();  // every read of s_y (the z product) is done: it now takes this block's x
+        if (h == 1) {
 #pragma unroll
-        for (int e = 0; e < 4; ++e) {
-            const int row = e < 2 ? r1 : r2, q = 2 * tq + (e & 1);
-            s_y[q * kChS + row] = xv[e];
+            for (int q = 0; q < kSwRhs; ++q) s_h[r][q] = acc[q];
         }
         __syncthreads();
-        // the later blocks of this cluster first (they are on the chain): 256 float4 of the
-        // transposed block (8 right-hand sides x 32 row quads), then global memory
-        {
-            const int q = t >> 5, r4 = (t & 31) * 4;
-            const float4 v4 = *reinterpret_cast<const float4*>(&s_y[q * kChS + r4]);
-            const uint4 u4 = make_uint4(__float_as_uint(v4.x), __float_as_uint(v4.y), __float_as_uint(v4.z),
-                                        __float_as_uint(v4.w));
+        if (h == 0) {
+            float xv[kSwRhs];
+#pragma unroll
+            for (int q = 0; q < kSwRhs; ++q) xv[q] = (r < bs && q < ncg) ? acc[q] + s_h[r][q] : 0.f;
+            // the later blocks of this cluster first (they are on the chain), then global memory
             for (int d = rank + 1; d < kChCl && cl0 + d < nblk; ++d) {
-                const uint32_t rbar = map_rank(&s_bar[rank], (uint32_t)d);
-                const uint32_t dst = map_rank(s_rx + rank * kChBlk + q * kChS + r4, (uint32_t)d);
-                st_async16(dst, u4, rbar);
+                const uint32_t rb = map_rank(&s_bar[rank], (uint32_t)d);
+                const uint32_t dst = map_rank(&s_rx[rank][r][0], (uint32_t)d);
+                st_async16(dst, make_uint4(__float_as_uint(xv[0]), __float_as_uint(xv[1]), __float_as_uint(xv[2]),
+                                           __float_as_uint(xv[3])), rb);
+                st_async16(dst + 16, make_uint4(__float_as_uint(xv[4]), __float_as_uint(xv[5]),
+                                                __float_as_uint(xv[6]), __float_as_uint(xv[7])), rb);
             }
-        }
 #pragma unroll
-        for (int e = 0; e < 4; ++e) {
-            const int row = e < 2 ? r1 : r2, q = 2 * tq + (e & 1);
-            st_relaxed64(ll_own + row * kSwRhs + q, (1ull << 32) | __float_as_uint(xv[e]));
-        }
+            for (int q = 0; q < kSwRhs; ++q) st_relaxed64(ll_own + r * kSwRhs + q, (1ull << 32) | __float_as_uint(xv[q]));
+            if (r < bs) {
 #pragma unroll
-        for (int e = 0; e < 4; ++e) {
-            const int row = e < 2 ? r1 : r2, q = 2 * tq + (e & 1);
-            if (row < bs && q < ncg) {
-                a.Xr[(int64_t)(b0 + row) * a.ldr + cg0 + q] = xv[e];
-                if (a.upper) a.X64[(int64_t)(b0 + row) * a.ldx + cg0 + q] += (double)xv[e];  // off the chain
+                for (int q = 0; q < kSwRhs; ++q)
+                    if (q < ncg) a.Xr[(int64_t)(b0 + r) * a.ldr + cgc + q] = xv[q];
+                if (a.upper) {  // the FP64 accumulation is off the chain
+#pragma unroll
+                    for (int q = 0; q < kSwRhs; ++q)
+                        if (q < ncg) a.X64[(int64_t)(b0 + r) * a.ldx + cgc + q] += (double)xv[q];
+                }
             }
         }
     } else {
