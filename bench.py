@@ -29,6 +29,10 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 N_DEFAULT, NRHS_DEFAULT, KAPPA_DEFAULT = 8192, 16, 1e5
+# DRAM bytes per algorithmic byte of a dominant kernel class, from a single-launch ncu capture
+# (dram__bytes_read.sum + dram__bytes_write.sum over the bytes the event profiler charges to that
+# launch): the tournament leaf of the mixed solve, profiles/tslu_select_n8192_dram.md
+NCU_TRAFFIC_RATIO = {"panel": 1.143}
 METRIC = "LU-solve GFLOP/s at n=8192 to FP64 backward error: mixed-precision IR vs plain FP64"
 
 
@@ -389,8 +393,10 @@ def run_b200(args, world, rank, local):
         roof = {"bound": "hbm", "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if "hbm_gbs" in peaks
                 else "fallback 6650 GB/s (of fallback)"}
         unit = "GB/s"
+    traffic = per_launch * NCU_TRAFFIC_RATIO[dom_name] if (dom_name in NCU_TRAFFIC_RATIO and roof["bound"] == "hbm") else None
     roof.update({"kernel_class": dom_name, "achieved": achieved, "peak": pk, "unit": unit, "frac": achieved / pk,
-                 "traffic": None, "launches": d["launches"], "avg_launch_us": avg_s * 1e6,
+                 "traffic": traffic, "traffic_unit": "bytes per launch (DRAM read + write, ncu-measured ratio)",
+                 "launches": d["launches"], "avg_launch_us": avg_s * 1e6,
                  "work_per_launch": per_launch, "share_of_device_time": share})
 
     cpu = None
