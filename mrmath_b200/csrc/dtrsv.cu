@@ -67,13 +67,23 @@ __global__ void __launch_bounds__(256) dtrsv_block_kernel(DtArgs a, int b) {
         const int r = t & (kDtNB - 1), h = t >> 7;
         double acc[kDtRhs] = {0.0, 0.0, 0.0, 0.0};
         if (r < bs) {
-#pragma unroll 8
-            for (int kk = 0; kk < 64; ++kk) {
-                const int k = 64 * h + kk;
-                if (k < ps) {
-                    const double tv = tri_at<MODE>(a.LU, a.ld, b0 + r, p0 + k);
+            // all 64 loads of this thread's half row are in flight before the first product (same
+            // ascending order of contributions as one load per step)
 #pragma unroll
-                    for (int q = 0; q < kDtRhs; ++q) acc[q] = fma(tv, s_p[k][q], acc[q]);
+            for (int k2 = 0; k2 < 64; k2 += 32) {
+                double tv[32];
+#pragma unroll
+                for (int kk = 0; kk < 32; ++kk) {
+                    const int k = 64 * h + k2 + kk;
+                    tv[kk] = k < ps ? tri_at<MODE>(a.LU, a.ld, b0 + r, p0 + k) : 0.0;
+                }
+#pragma unroll
+                for (int kk = 0; kk < 32; ++kk) {
+                    const int k = 64 * h + k2 + kk;
+                    if (k < ps) {
+#pragma unroll
+                        for (int q = 0; q < kDtRhs; ++q) acc[q] = fma(tv[kk], s_p[k][q], acc[q]);
+                    }
                 }
             }
         }
@@ -126,10 +136,13 @@ __global__ void __launch_bounds__(256) dtrsv_block_kernel(DtArgs a, int b) {
             const int rlo = lower ? s0 + sw : 0, rhi = lower ? bs : s0;
             for (int e = t; e < (rhi - rlo) * kDtRhs; e += 256) {
                 const int rr = rlo + (e >> 2), q = e & 3;
+                double tv[32];
+#pragma unroll
+                for (int j = 0; j < 32; ++j) tv[j] = j < sw ? tri_at<MODE>(a.LU, a.ld, b0 + rr, b0 + s0 + j) : 0.0;
                 double acc2 = 0.0;
-#pragma unroll 8
+#pragma unroll
                 for (int j = 0; j < 32; ++j)
-                    if (j < sw) acc2 = fma(tri_at<MODE>(a.LU, a.ld, b0 + rr, b0 + s0 + j), s_y[s0 + j][q], acc2);
+                    if (j < sw) acc2 = fma(tv[j], s_y[s0 + j][q], acc2);
                 s_y[rr][q] -= acc2;
             }
             __syncthreads();
@@ -157,14 +170,19 @@ __global__ void __launch_bounds__(256) dtrsv_block_kernel(DtArgs a, int b) {
 #pragma unroll
     for (int c = 0; c < kDtMaxRhs; ++c) acc[c] = 0.0;
     if (row < uend) {
-#pragma unroll 4
+        double tv[32];  // all loads in flight before the first product
+#pragma unroll
         for (int i = 0; i < 32; ++i) {
             const int k = 4 * i + kq;  // interleaved quarters: the four lanes of a row read adjacent k
+            tv[i] = k < ps ? tri_at<MODE>(a.LU, a.ld, row, p0 + k) : 0.0;
+        }
+#pragma unroll
+        for (int i = 0; i < 32; ++i) {
+            const int k = 4 * i + kq;
             if (k < ps) {
-                const double tv = tri_at<MODE>(a.LU, a.ld, row, p0 + k);
 #pragma unroll
                 for (int c = 0; c < kDtMaxRhs; ++c)
-                    if (c < a.nc) acc[c] = fma(tv, s_p[k][c], acc[c]);
+                    if (c < a.nc) acc[c] = fma(tv[i], s_p[k][c], acc[c]);
             }
         }
     }
