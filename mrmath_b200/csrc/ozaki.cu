@@ -11,7 +11,8 @@
 //     d <= s + 1 (the dropped pairs are below 2^-7(s+1) of the scaled products).  Every S_d is an
 //     exact int32 sum (|A_p B_q| <= 127^2 K per pair; K is cut into chunks that keep s 127^2 K below
 //     2^31), accumulated on tcgen05.mma kind::i8 in TMEM;
-//   * ozaki_gemm_kernel: warp 8 issues the TMA loads of 128 x 128 int8 tiles (128-byte swizzle),
+//   * ozaki_kmajor_kernel (s <= 8, the default s = 8): see its comment below; ozaki_gemm_kernel
+//     (s = 9, 10): warp 8 issues the TMA loads of 128 x 128 int8 tiles (128-byte swizzle),
 //     one thread of warp 9 issues 4 MMAs (K = 32) per tile pair into one of two 128-column TMEM
 //     accumulators, and warps 0-7 drain each finished S_d into FP64 registers (warp w: TMEM lanes
 //     32 (w % 4).., columns 64 (w / 4)..), scaling by 2^-7d, while the next S_d accumulates in the
@@ -239,6 +240,172 @@ __global__ void __launch_bounds__(kOzThreads, 1)
     }
 }
 
+// ---- k-major variant (s <= 8 slices): every slice tile is loaded once per k-step and reused by
+// every pair it belongs to.  A CTA computes a 128 x 64 tile of C with all s accumulators S_d
+// (d = 2 .. s + 1, 64 TMEM columns each, 512 in all) live for the whole K range: per 64-wide
+// k-step the producer (warp 8) loads the s slice tiles of A (128 x 64 bytes) and of B (64 x 64),
+// 64-byte swizzle, into one of two stages; the MMA issuer (one thread of warp 9) runs the
+// s (s + 1) / 2 pairs of the step (two K = 32 MMAs each) into the accumulator of d = p + q; the
+// epilogue warps drain the accumulators into FP64 once per K chunk (a chunk keeps every S_d an
+// exact int32 sum).  Per k-step the tensor pipe gets s (s + 1) MMAs for 12 s KiB of operands, about
+// three times the reuse of the pair-major kernel above, whose slice pairs each reload both tiles.
+constexpr int KBM = 128, KBN = 64, KBK = 64;
+constexpr int kKmTileA = KBM * KBK, kKmTileB = KBN * KBK;  // 8 KiB, 4 KiB
+constexpr int kKmMaxSlices = 8;
+constexpr int kKmStages = 2;
+
+// K-major operand tile, 64-byte swizzle: 64-byte rows, 8-row groups 512 bytes apart
+__device__ __forceinline__ uint64_t sw64_desc(uint32_t saddr) {
+    return (uint64_t)((saddr & 0x3FFFFu) >> 4) | ((uint64_t)1 << 16) | ((uint64_t)(512 >> 4) << 32) |
+           ((uint64_t)1 << 46) | ((uint64_t)4 << 61);
+}
+__host__ __device__ constexpr uint32_t i8_idesc_m128n64() {
+    return (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(KBN >> 3) << 17) | ((uint32_t)(KBM >> 4) << 24);
+}
+
+__global__ void __launch_bounds__(kOzThreads, 1)
+    ozaki_kmajor_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, OzArgs p) {
+    extern __shared__ uint8_t km_smem_raw[];
+    __shared__ __align__(8) uint64_t full_bar[kKmStages];
+    __shared__ __align__(8) uint64_t empty_bar[kKmStages];
+    __shared__ __align__(8) uint64_t accf_bar;   // the chunk's accumulators are complete
+    __shared__ __align__(8) uint64_t acce_bar;   // ... and drained by the epilogue
+    __shared__ uint32_t tmem_base_sh;
+
+    uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(km_smem_raw) + 1023) & ~uintptr_t(1023));
+    const int s = p.s;
+    const int stage_bytes = s * (kKmTileA + kKmTileB);
+    const int tiles_m = (p.M + KBM - 1) / KBM, tiles_n = (p.N + KBN - 1) / KBN;
+    constexpr int kGroup = 8;
+    const int bid = blockIdx.x;
+    const int group = bid / (kGroup * tiles_n);
+    const int first_m = group * kGroup;
+    const int gsize = min(tiles_m - first_m, kGroup);
+    const int in_group = bid % (kGroup * tiles_n);
+    const int tm = first_m + in_group % gsize, tn = in_group / gsize;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int KT = (p.K + KBK - 1) / KBK;
+    const int nchunks = (KT + p.kchunk - 1) / p.kchunk;
+
+    if (warp == 9) {
+        tmem_alloc(&tmem_base_sh, 512);
+        tmem_relinquish();
+    }
+    if (threadIdx.x == 0) {
+        for (int i = 0; i < kKmStages; ++i) {
+            mbar_init(&full_bar[i], 1);
+            mbar_init(&empty_bar[i], 1);
+        }
+        mbar_init(&accf_bar, 1);
+        mbar_init(&acce_bar, 8);
+        fence_barrier_init();
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = tmem_base_sh;
+    int32_t* tmo = &p.status[kTimeout];
+
+    if (warp == 8) {
+        if (lane == 0) {
+            tma_prefetch_desc(&tmA);
+            tma_prefetch_desc(&tmB);
+            bool ok = true;
+            for (int kt = 0; kt < KT && ok; ++kt) {
+                const int st = kt % kKmStages;
+                if (!mbar_wait(&empty_bar[st], ((kt / kKmStages) & 1) ^ 1, tmo, 411)) { ok = false; break; }
+                uint8_t* sp = smem + st * stage_bytes;
+                mbar_arrive_expect_tx(&full_bar[st], stage_bytes);
+                for (int q = 0; q < s; ++q) {
+                    tma_load_2d(sp + q * kKmTileA, &tmA, kt * KBK, q * p.M + tm * KBM, &full_bar[st]);
+                    tma_load_2d(sp + s * kKmTileA + q * kKmTileB, &tmB, kt * KBK, q * p.N + tn * KBN, &full_bar[st]);
+                }
+            }
+        }
+    } else if (warp == 9) {
+        if (lane == 0) {
+            constexpr uint32_t idesc = i8_idesc_m128n64();
+            bool ok = true;
+            for (int ch = 0; ch < nchunks && ok; ++ch) {
+                const int k0 = ch * p.kchunk, k1 = min(KT, k0 + p.kchunk);
+                // the epilogue must have drained the previous chunk before the accumulators restart
+                if (ch > 0 && !mbar_wait(&acce_bar, (ch - 1) & 1, tmo, 412)) { ok = false; break; }
+                tc_fence_after();
+                uint32_t started = 0u;  // accumulators written in this chunk (bit d - 2)
+                for (int kt = k0; kt < k1; ++kt) {
+                    const int st = kt % kKmStages;
+                    if (!mbar_wait(&full_bar[st], (kt / kKmStages) & 1, tmo, 413)) { ok = false; break; }
+                    tc_fence_after();
+                    const uint32_t sa = smem_u32(smem + st * stage_bytes);
+                    const uint32_t sb = sa + (uint32_t)(s * kKmTileA);
+                    for (int pa = 1; pa <= s; ++pa) {
+                        for (int pb = 1; pa + pb <= s + 1; ++pb) {
+                            const int d = pa + pb;
+                            const uint32_t tacc = tmem + (uint32_t)((d - 2) * KBN);
+#pragma unroll
+                            for (int kk = 0; kk < KBK / 32; ++kk) {
+                                const uint32_t acc = (started >> (d - 2)) & 1u;
+                                umma_i8(tacc, sw64_desc(sa + (uint32_t)((pa - 1) * kKmTileA + kk * 32)),
+                                        sw64_desc(sb + (uint32_t)((pb - 1) * kKmTileB + kk * 32)), idesc, acc);
+                                started |= 1u << (d - 2);
+                            }
+                        }
+                    }
+                    umma_commit(&empty_bar[st]);
+                }
+                umma_commit(&accf_bar);
+            }
+        }
+    } else {
+        // epilogue warps 0-7: rows 32 (warp % 4) + lane, columns 32 (warp / 4) .. + 31
+        const int q4 = warp & 3, h = warp >> 2;
+        double acc[32];
+#pragma unroll
+        for (int c = 0; c < 32; ++c) acc[c] = 0.0;
+        bool ok = true;
+        for (int ch = 0; ch < nchunks && ok; ++ch) {
+            if (!mbar_wait(&accf_bar, ch & 1, tmo, 414)) { ok = false; break; }
+            tc_fence_after();
+            for (int d = 2; d <= s + 1; ++d) {
+                const double sc = ldexp(1.0, -7 * d);
+                const uint32_t ta = tmem + ((uint32_t)(q4 * 32) << 16) + (uint32_t)((d - 2) * KBN + h * 32);
+#pragma unroll
+                for (int c0 = 0; c0 < 32; c0 += 16) {
+                    uint32_t r[16];
+                    tmem_ld16(ta + (uint32_t)c0, r);
+#pragma unroll
+                    for (int e = 0; e < 16; ++e) acc[c0 + e] = fma((double)(int32_t)r[e], sc, acc[c0 + e]);
+                }
+            }
+            tc_fence_before();
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&acce_bar);
+        }
+        const int row = tm * KBM + q4 * 32 + lane;
+        if (ok && row < p.M) {
+            const double sa = ldexp(1.0, p.ea[row]);
+            double* crow = p.C + (int64_t)row * p.ldc + tn * KBN + h * 32;
+            const int cbase = tn * KBN + h * 32;
+#pragma unroll
+            for (int c = 0; c < 32; ++c) {
+                const int col = cbase + c;
+                if (col < p.N) {
+                    const double v = acc[c] * sa * ldexp(1.0, p.eb[col]);
+                    if (p.op == B2M_DO_NONE) crow[c] = v;
+                    else if (p.op == B2M_DO_ADD) crow[c] += v;
+                    else crow[c] -= v;
+                }
+            }
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 9) {
+        tc_fence_after();
+        tmem_dealloc(tmem, 512);
+    }
+}
+
 // exponent e with max|x| * 2^-e < 1 (0 for an all-zero row/column)
 __device__ __forceinline__ int exp_of(double m) {
     if (!(m > 0.0)) return 0;
@@ -347,6 +514,30 @@ int32_t ozaki_gemm(Ctx* ctx, cudaStream_t st, const double* A, int64_t lda, cons
     prof_end(ctx, st, kClsOther, 8.0 * (M * K + K * N) + (double)s * Kp * (M + N));  // bytes
     B2M_LAUNCHED(ctx);
     CUtensorMap ma, mb;
+    if (s <= kKmMaxSlices) {
+        // k-major kernel: all s accumulators in TMEM, K chunks that keep each S_d an exact int32 sum
+        const int64_t kc_elems = ((int64_t)2147483647 / ((int64_t)s * 127 * 127)) / KBK * KBK;
+        const int kc = (int)std::max<int64_t>(1, kc_elems / KBK);
+        B2M_TRY(encode_tmap_2d(ctx, &ma, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, A8, (uint64_t)K, (uint64_t)s * M,
+                               (uint64_t)Kp, KBK, KBM, CU_TENSOR_MAP_SWIZZLE_64B));
+        B2M_TRY(encode_tmap_2d(ctx, &mb, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, B8, (uint64_t)K, (uint64_t)s * N,
+                               (uint64_t)Kp, KBK, KBN, CU_TENSOR_MAP_SWIZZLE_64B));
+        // the full-size request for every s: one CTA per SM, so that no second CTA waits for TMEM
+        const int ksmem = kKmStages * kKmMaxSlices * (kKmTileA + kKmTileB) + 1024;
+        std::atomic<int>& kattr = device_flag((const void*)ozaki_kmajor_kernel, 0, ctx->device);
+        if (!kattr.load()) {
+            B2M_CU(ctx, cudaFuncSetAttribute(ozaki_kmajor_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, ksmem));
+            kattr.store(1);
+        }
+        OzArgs ka{(int)M, (int)N, (int)K, s, kc, ea, eb, C, ldc, op, ctx->d_status};
+        const int ktiles = (int)(ceil_div(M, KBM) * ceil_div(N, KBN));
+        const double kpairs = (double)s * (s + 1) / 2.0;
+        prof_begin(ctx, st, kClsTcGemm);
+        ozaki_kmajor_kernel<<<ktiles, kOzThreads, ksmem, st>>>(ma, mb, ka);
+        prof_end(ctx, st, kClsTcGemm, 2.0 * M * N * Kp * kpairs);  // int8 MMA operations
+        B2M_LAUNCHED(ctx);
+        return B2M_OK;
+    }
     B2M_TRY(encode_tmap_2d(ctx, &ma, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, A8, (uint64_t)K, (uint64_t)s * M, (uint64_t)Kp,
                            OBK, OBM, CU_TENSOR_MAP_SWIZZLE_128B));
     B2M_TRY(encode_tmap_2d(ctx, &mb, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, B8, (uint64_t)K, (uint64_t)s * N, (uint64_t)Kp,
