@@ -36,6 +36,11 @@ NCU_TRAFFIC_RATIO = {"panel": 1.143}
 METRIC = "LU-solve GFLOP/s at n=8192 to FP64 backward error: mixed-precision IR vs plain FP64"
 
 
+def metric_for(n: int) -> str:
+    """The headline metric's name; other orders (the C1 case) say which n they ran."""
+    return METRIC if n == N_DEFAULT else METRIC.replace("n=8192", f"n={n}")
+
+
 def parse():
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
@@ -408,7 +413,7 @@ def run_b200(args, world, rank, local):
 
     if rank == 0:
         line = {
-            "metric": METRIC, "value": value, "unit": "GFLOP/s", "n_gpus": world, "steps": args.steps,
+            "metric": metric_for(n), "value": value, "unit": "GFLOP/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64" if form == "plain" else "f32/tf32 factor + f64 refinement",
             "data": "synthetic: A = U diag(s) V^T from MT19937-seeded Gaussians (seed 15 + rank), 16 Gaussian RHS",

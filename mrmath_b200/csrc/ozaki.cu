@@ -30,7 +30,6 @@ constexpr int kOzTile = OBM * OBK;               // 16 KiB per operand tile
 constexpr int kOzStages = 6;
 constexpr int kOzThreads = 320;                  // 8 epilogue warps, producer, MMA
 constexpr int kOzMaxSlices = 10;
-constexpr int kOzChunkSteps = 8;                 // k-steps per accumulation chunk, at most
 
 struct OzArgs {
     int M, N, K, s;
@@ -491,10 +490,7 @@ int32_t ozaki_gemm(Ctx* ctx, cudaStream_t st, const double* A, int64_t lda, cons
     const int64_t Kp = round_up(K, 128);
     // exact int32 accumulation: s pairs of |127 * 127| products over one chunk
     const int64_t kchunk_elems = ((int64_t)2147483647 / ((int64_t)s * 127 * 127)) / OBK * OBK;
-    // and at most kOzChunkSteps k-steps, so that the slices one chunk streams for the CTAs in flight
-    // (s slices x ~27 row tiles x 1 KiB rows ~= 28 MB at s = 8) stay in L2 while every slice pair
-    // re-reads them; a chunk over the whole of K streams ~1 GB per wave and re-reads it from DRAM
-    const int kchunk = (int)std::min<int64_t>(kOzChunkSteps, std::max<int64_t>(1, kchunk_elems / OBK));
+    const int kchunk = (int)std::max<int64_t>(1, kchunk_elems / OBK);
     void *pe, *pa, *pb;
     B2M_TRY(ws_get(ctx, kWsSmall, (size_t)(M + N) * 4 + 256, &pe));
     B2M_TRY(ws_get(ctx, kWsMatD, (size_t)s * M * Kp, &pa));
