@@ -241,22 +241,23 @@ __global__ void __launch_bounds__(kOzThreads, 1)
 
 // ---- k-major variant (s <= 8 slices): every slice tile is loaded once per k-step and reused by
 // every pair it belongs to.  A CTA computes a 128 x 64 tile of C with all s accumulators S_d
-// (d = 2 .. s + 1, 64 TMEM columns each, 512 in all) live for the whole K range: per 64-wide
-// k-step the producer (warp 8) loads the s slice tiles of A (128 x 64 bytes) and of B (64 x 64),
-// 64-byte swizzle, into one of two stages; the MMA issuer (one thread of warp 9) runs the
-// s (s + 1) / 2 pairs of the step (two K = 32 MMAs each) into the accumulator of d = p + q; the
+// (d = 2 .. s + 1, 64 TMEM columns each, 512 in all) live for the whole K range: per 32-wide
+// k-step the producer (warp 8) loads the s slice tiles of A (128 x 32 bytes) and of B (64 x 32),
+// 32-byte swizzle, into one of four stages; the MMA issuer (one thread of warp 9) runs the
+// s (s + 1) / 2 pairs of the step (one K = 32 MMA each) into the accumulator of d = p + q; the
 // epilogue warps drain the accumulators into FP64 once per K chunk (a chunk keeps every S_d an
-// exact int32 sum).  Per k-step the tensor pipe gets s (s + 1) MMAs for 12 s KiB of operands, about
-// three times the reuse of the pair-major kernel above, whose slice pairs each reload both tiles.
-constexpr int KBM = 128, KBN = 64, KBK = 64;
-constexpr int kKmTileA = KBM * KBK, kKmTileB = KBN * KBK;  // 8 KiB, 4 KiB
+// exact int32 sum).  Per k-step the tensor pipe gets s (s + 1) / 2 MMAs for 6 s KiB of operands,
+// about three times the reuse of the pair-major kernel above, whose slice pairs each reload both
+// tiles.
+constexpr int KBM = 128, KBN = 64, KBK = 32;
+constexpr int kKmTileA = KBM * KBK, kKmTileB = KBN * KBK;  // 4 KiB, 2 KiB
 constexpr int kKmMaxSlices = 8;
-constexpr int kKmStages = 2;
+constexpr int kKmStages = 4;  // 4 x 48 KiB: three stages in flight hide the TMA latency behind the MMAs
 
-// K-major operand tile, 64-byte swizzle: 64-byte rows, 8-row groups 512 bytes apart
-__device__ __forceinline__ uint64_t sw64_desc(uint32_t saddr) {
-    return (uint64_t)((saddr & 0x3FFFFu) >> 4) | ((uint64_t)1 << 16) | ((uint64_t)(512 >> 4) << 32) |
-           ((uint64_t)1 << 46) | ((uint64_t)4 << 61);
+// K-major operand tile, 32-byte swizzle: 32-byte rows (one K = 32 MMA), 8-row groups 256 bytes apart
+__device__ __forceinline__ uint64_t sw32_desc(uint32_t saddr) {
+    return (uint64_t)((saddr & 0x3FFFFu) >> 4) | ((uint64_t)1 << 16) | ((uint64_t)(256 >> 4) << 32) |
+           ((uint64_t)1 << 46) | ((uint64_t)6 << 61);
 }
 __host__ __device__ constexpr uint32_t i8_idesc_m128n64() {
     return (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(KBN >> 3) << 17) | ((uint32_t)(KBM >> 4) << 24);
@@ -341,13 +342,10 @@ __global__ void __launch_bounds__(kOzThreads, 1)
                         for (int pb = 1; pa + pb <= s + 1; ++pb) {
                             const int d = pa + pb;
                             const uint32_t tacc = tmem + (uint32_t)((d - 2) * KBN);
-#pragma unroll
-                            for (int kk = 0; kk < KBK / 32; ++kk) {
-                                const uint32_t acc = (started >> (d - 2)) & 1u;
-                                umma_i8(tacc, sw64_desc(sa + (uint32_t)((pa - 1) * kKmTileA + kk * 32)),
-                                        sw64_desc(sb + (uint32_t)((pb - 1) * kKmTileB + kk * 32)), idesc, acc);
-                                started |= 1u << (d - 2);
-                            }
+                            const uint32_t acc = (started >> (d - 2)) & 1u;
+                            umma_i8(tacc, sw32_desc(sa + (uint32_t)((pa - 1) * kKmTileA)),
+                                    sw32_desc(sb + (uint32_t)((pb - 1) * kKmTileB)), idesc, acc);
+                            started |= 1u << (d - 2);
                         }
                     }
                     umma_commit(&empty_bar[st]);
@@ -515,9 +513,9 @@ int32_t ozaki_gemm(Ctx* ctx, cudaStream_t st, const double* A, int64_t lda, cons
         const int64_t kc_elems = ((int64_t)2147483647 / ((int64_t)s * 127 * 127)) / KBK * KBK;
         const int kc = (int)std::max<int64_t>(1, kc_elems / KBK);
         B2M_TRY(encode_tmap_2d(ctx, &ma, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, A8, (uint64_t)K, (uint64_t)s * M,
-                               (uint64_t)Kp, KBK, KBM, CU_TENSOR_MAP_SWIZZLE_64B));
+                               (uint64_t)Kp, KBK, KBM, CU_TENSOR_MAP_SWIZZLE_32B));
         B2M_TRY(encode_tmap_2d(ctx, &mb, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, B8, (uint64_t)K, (uint64_t)s * N,
-                               (uint64_t)Kp, KBK, KBN, CU_TENSOR_MAP_SWIZZLE_64B));
+                               (uint64_t)Kp, KBK, KBN, CU_TENSOR_MAP_SWIZZLE_32B));
         // the full-size request for every s: one CTA per SM, so that no second CTA waits for TMEM
         const int ksmem = kKmStages * kKmMaxSlices * (kKmTileA + kKmTileB) + 1024;
         std::atomic<int>& kattr = device_flag((const void*)ozaki_kmajor_kernel, 0, ctx->device);
