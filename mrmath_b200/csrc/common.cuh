@@ -45,6 +45,7 @@ enum WsSlot : int {
     kWsG,          // the mixed solve's X when the caller's buffer cannot be used directly
     kWsH,
     kWsPmap,       // row maps of the blocked FP64 LU's outer panels
+    kWsTri,        // the FP64 blocked sweeps' diagonal inverses, coupling blocks and published blocks
     kNumWs
 };
 
@@ -93,6 +94,7 @@ struct Ctx {
     int chain_clusters = -1;  // co-resident 8-CTA clusters of the chained sweep (0: unusable, -1: not probed)
     int chain_clusters4 = -1; // the same for 4-CTA clusters
     int chain_probe_why = 0;  // why it is unusable: step * 1000 + CUDA error (b2m_ctx_info)
+    int dsweep_ctas = -1;     // co-resident CTAs of the FP64 blocked sweep (-1: not queried yet)
     int64_t wait_limit = -1;  // polls of the refinement sweeps' bounded waits (-1: the built-in limit)
     size_t smem_optin = 0;
     cudaStream_t own_stream = nullptr;

@@ -13,6 +13,8 @@
 // contribution from every row outside blocks <= b (forward) or >= b (backward), 64 rows each.
 // The transposed triangles read the factors column-wise, which is coalesced across the rows a
 // warp handles.
+#include <algorithm>
+
 #include "common.cuh"
 #include "kernels.cuh"
 
@@ -222,16 +224,333 @@ int32_t launch_sweeps(Ctx* ctx, cudaStream_t st, const double* LU, int64_t ld, i
     return B2M_OK;
 }
 
+// ---- One persistent launch per sweep (orders > 128).  The triangle is cut into 64-row blocks;
+// each diagonal block's inverse (substitution by columns of the identity, with the true division
+// for U and U^T) and each coupling block W_b = T_bb^-1 T_{b,p} (p the block before b in sweep
+// order) are formed first, then a CTA per (block, 8 right-hand sides) folds in the earlier blocks
+// as they are published and finishes x_b = T_bb^-1 y_b - W_b x_p, so one 64 x 64 x 8 product per
+// block is on the chain.  A block is published as 512 doubles and a flag (release/acquire); every
+// wait is bounded and a CTA that gives up marks its flag 2 so that its dependants stop at once.
+constexpr int kDsNB = 64;
+constexpr int kDsRhs = 8;
+constexpr int kDsThreads = 128;
+constexpr int kDsMaxRhs = 16;  // right-hand sides per sweep launch
+constexpr int kDsSmem = 2 * kDsNB * kDsNB * (int)sizeof(double);  // T_bb^-1 and W_b, transposed
+constexpr int kDsTriSmem = 2 * kDsNB * (kDsNB + 1) * (int)sizeof(double);
+constexpr uint32_t kDsSpin = 1u << 22;
+
+__device__ __forceinline__ int ld_acquire_i32(const int32_t* p) {
+    int v;
+    asm volatile("ld.acquire.gpu.global.b32 %0, [%1];\n" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_release_i32(int32_t* p, int v) {
+    asm volatile("st.release.gpu.global.b32 [%0], %1;\n" ::"l"(p), "r"(v) : "memory");
+}
+
+// inverse of the diagonal block b of the triangle (thread per column; zero past the matrix)
+template <int MODE>
+__global__ void __launch_bounds__(kDsNB) dinv_kernel(const double* LU, int64_t ld, int n, double* inv,
+                                                     const int32_t* status) {
+    extern __shared__ double dt_sm[];
+    if (status[kInfo] != 0) return;
+    constexpr bool lower = tri_lower<MODE>(), unit = tri_unit<MODE>();
+    const int b = blockIdx.x, b0 = b * kDsNB, bs = min(kDsNB, n - b0), c = threadIdx.x;
+    constexpr int SP = kDsNB + 1;
+    double* s_t = dt_sm;
+    double* s_x = dt_sm + kDsNB * SP;
+    for (int r = 0; r < kDsNB; ++r) s_t[r * SP + c] = (r < bs && c < bs) ? tri_at<MODE>(LU, ld, b0 + r, b0 + c) : 0.0;
+    __syncthreads();
+    if (lower) {
+        for (int i = 0; i < kDsNB; ++i) {
+            double acc = (i == c) ? 1.0 : 0.0;
+            if (i < bs && c < bs) {
+                for (int k = c; k < i; ++k) acc = fma(-s_t[i * SP + k], s_x[k * SP + c], acc);
+                if (!unit && i >= c) acc = acc / s_t[i * SP + i];
+            }
+            s_x[i * SP + c] = (i < bs && c < bs && i >= c) ? acc : 0.0;
+        }
+    } else {
+        for (int i = kDsNB - 1; i >= 0; --i) {
+            double acc = (i == c) ? 1.0 : 0.0;
+            if (i < bs && c < bs) {
+                for (int k = i + 1; k <= c; ++k) acc = fma(-s_t[i * SP + k], s_x[k * SP + c], acc);
+                if (!unit && i <= c) acc = acc / s_t[i * SP + i];
+            }
+            s_x[i * SP + c] = (i < bs && c < bs && i <= c) ? acc : 0.0;
+        }
+    }
+    __syncthreads();
+    double* out = inv + (int64_t)b * kDsNB * kDsNB;
+    for (int r = 0; r < kDsNB; ++r) out[r * kDsNB + c] = s_x[r * SP + c];
+}
+
+// W_b = T_bb^-1 T_{b,p} for every block b with a predecessor p in sweep order (zero past the matrix)
+template <int MODE>
+__global__ void __launch_bounds__(256) dcouple_kernel(const double* LU, int64_t ld, int n, const double* inv, double* w,
+                                                      const int32_t* status) {
+    extern __shared__ double dc_sm[];
+    if (status[kInfo] != 0) return;
+    constexpr bool lower = tri_lower<MODE>();
+    const int nblk = (int)ceil_div(n, kDsNB);
+    const int b = blockIdx.x;
+    if (lower ? b == 0 : b == nblk - 1) return;
+    const int b0 = b * kDsNB, bs = min(kDsNB, n - b0);
+    const int p0 = lower ? b0 - kDsNB : b0 + kDsNB, ps = min(kDsNB, n - p0);
+    constexpr int SP = kDsNB + 1;
+    double* s_i = dc_sm;
+    double* s_t = dc_sm + kDsNB * SP;
+    const int t = threadIdx.x;
+    for (int e = t; e < kDsNB * kDsNB; e += 256) {
+        const int r = e / kDsNB, c = e % kDsNB;
+        s_i[r * SP + c] = inv[(int64_t)b * kDsNB * kDsNB + e];
+        s_t[r * SP + c] = (r < bs && c < ps) ? tri_at<MODE>(LU, ld, b0 + r, p0 + c) : 0.0;
+    }
+    __syncthreads();
+    const int r0 = 4 * (t >> 4), c0 = t & 15;
+    double acc[4][4] = {};
+    for (int k = 0; k < kDsNB; ++k) {
+        double iv[4], tv[4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) iv[i] = s_i[(r0 + i) * SP + k];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) tv[j] = s_t[k * SP + c0 + 16 * j];
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+#pragma unroll
+            for (int j = 0; j < 4; ++j) acc[i][j] = fma(iv[i], tv[j], acc[i][j]);
+    }
+    double* out = w + (int64_t)b * kDsNB * kDsNB;
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) out[(r0 + i) * kDsNB + c0 + 16 * j] = acc[i][j];
+}
+
+struct DsArgs {
+    const double* LU;
+    int64_t ld;
+    int n;
+    const double* inv;  // [nblk][64][64]
+    const double* w;    // [nblk][64][64]
+    double* X;
+    int64_t ldx;
+    int c0, nc;
+    double* pub;        // [nblk][ng][64][8] published blocks
+    int32_t* flags;     // [nblk][ng]: 0 pending, 1 published, 2 abandoned (zeroed before the launch)
+    int32_t* status;
+    uint32_t spin;
+};
+
+template <int MODE>
+__global__ void __launch_bounds__(kDsThreads) dsweep_kernel(DsArgs a) {
+    extern __shared__ __align__(16) double ds_dyn[];
+    __shared__ double s_p[kDsNB][kDsRhs + 1];  // x of the block being folded in
+    __shared__ double s_y[kDsNB][kDsRhs + 1];
+    __shared__ double s_h[kDsNB][kDsRhs + 1];  // second-half partial sums
+    __shared__ int s_abort;
+    double* s_inv = ds_dyn;                    // [k][r]: T_bb^-1 transposed
+    double* s_w = ds_dyn + kDsNB * kDsNB;      // [k][r]: W_b transposed
+    if (a.status[kInfo] != 0) return;
+    constexpr bool lower = tri_lower<MODE>();
+    const int t = threadIdx.x, r = t & (kDsNB - 1), h = t >> 6;
+    const int nblk = (int)ceil_div(a.n, kDsNB), ng = (int)ceil_div(a.nc, kDsRhs);
+    const int bi = blockIdx.x / ng, g = blockIdx.x - bi * ng;
+    const int b = lower ? bi : nblk - 1 - bi;
+    const int b0 = b * kDsNB, bs = min(kDsNB, a.n - b0);
+    const int cg = a.c0 + g * kDsRhs, ncg = min(kDsRhs, a.nc - g * kDsRhs);
+    for (int e = t; e < kDsNB * kDsNB; e += kDsThreads) {  // row-major blocks, stored transposed
+        const int rr = e / kDsNB, k = e - rr * kDsNB;
+        s_inv[k * kDsNB + rr] = a.inv[(int64_t)b * kDsNB * kDsNB + e];
+        if (bi > 0) s_w[k * kDsNB + rr] = a.w[(int64_t)b * kDsNB * kDsNB + e];
+    }
+    double xb[kDsRhs], acc[kDsRhs];
+#pragma unroll
+    for (int q = 0; q < kDsRhs; ++q) {
+        xb[q] = (h == 0 && r < bs && q < ncg) ? a.X[(int64_t)(b0 + r) * a.ldx + cg + q] : 0.0;
+        acc[q] = 0.0;
+    }
+    if (t == 0) s_abort = 0;
+    __syncthreads();
+    // block j published: its 64 x 8 values into s_p
+    auto wait_block = [&](int j) -> bool {
+        if (t == 0) {
+            const int32_t* f = a.flags + j * ng + g;
+            int v = 0;
+            for (uint32_t it = 0; it < a.spin && v == 0; ++it) {
+                v = ld_acquire_i32(f);
+                if (v == 0 && (it & 255u) == 255u && *reinterpret_cast<volatile int32_t*>(&a.status[kTimeout]) != 0) v = 2;
+            }
+            if (v == 0) atomicCAS(&a.status[kTimeout], 0, 505);
+            if (v != 1) s_abort = 1;
+        }
+        __syncthreads();
+        if (s_abort) return false;
+        const double* src = a.pub + (size_t)(j * ng + g) * (kDsNB * kDsRhs);
+        for (int e = t; e < kDsNB * kDsRhs; e += kDsThreads) s_p[e >> 3][e & 7] = __ldcg(src + e);
+        __syncthreads();
+        return true;
+    };
+    bool ok = true;
+    for (int jj = 0; ok && jj + 1 < bi; ++jj) {
+        const int j = lower ? jj : nblk - 1 - jj;
+        const int p0 = j * kDsNB, ps = min(kDsNB, a.n - p0);
+        double tv[32];  // this thread's half row of T_bj, all loads in flight
+#pragma unroll
+        for (int k = 0; k < 32; ++k) {
+            const int kk = 32 * h + k;
+            tv[k] = (r < bs && kk < ps) ? tri_at<MODE>(a.LU, a.ld, b0 + r, p0 + kk) : 0.0;
+        }
+        ok = wait_block(j);
+        if (!ok) break;
+#pragma unroll
+        for (int k = 0; k < 32; ++k)
+#pragma unroll
+            for (int q = 0; q < kDsRhs; ++q) acc[q] = fma(tv[k], s_p[32 * h + k][q], acc[q]);
+        __syncthreads();  // s_p is rewritten by the next wait
+    }
+    if (ok) {
+        // y = X_b - sum T_bj x_j ;  z = T_bb^-1 y
+        if (h == 1) {
+#pragma unroll
+            for (int q = 0; q < kDsRhs; ++q) s_h[r][q] = acc[q];
+        }
+        __syncthreads();
+        if (h == 0) {
+#pragma unroll
+            for (int q = 0; q < kDsRhs; ++q) s_y[r][q] = xb[q] - acc[q] - s_h[r][q];
+        }
+        __syncthreads();
+#pragma unroll
+        for (int q = 0; q < kDsRhs; ++q) acc[q] = 0.0;
+#pragma unroll 8
+        for (int k = 0; k < 32; ++k) {
+            const int kk = 32 * h + k;
+            const double m = s_inv[kk * kDsNB + r];
+#pragma unroll
+            for (int q = 0; q < kDsRhs; ++q) acc[q] = fma(m, s_y[kk][q], acc[q]);
+        }
+        if (bi > 0) {  // x_b = z - W_b x_p
+            ok = wait_block(lower ? b - 1 : b + 1);
+            if (ok) {
+#pragma unroll 8
+                for (int k = 0; k < 32; ++k) {
+                    const int kk = 32 * h + k;
+                    const double m = s_w[kk * kDsNB + r];
+#pragma unroll
+                    for (int q = 0; q < kDsRhs; ++q) acc[q] = fma(-m, s_p[kk][q], acc[q]);
+                }
+            }
+        }
+    }
+    if (ok) {
+        if (h == 1) {
+#pragma unroll
+            for (int q = 0; q < kDsRhs; ++q) s_h[r][q] = acc[q];
+        }
+        __syncthreads();
+        if (h == 0) {
+            double* dst = a.pub + (size_t)(b * ng + g) * (kDsNB * kDsRhs) + r * kDsRhs;
+#pragma unroll
+            for (int q = 0; q < kDsRhs; ++q) {
+                const double xv = (r < bs && q < ncg) ? acc[q] + s_h[r][q] : 0.0;
+                dst[q] = xv;
+                if (r < bs && q < ncg) a.X[(int64_t)(b0 + r) * a.ldx + cg + q] = xv;
+            }
+        }
+        __syncthreads();
+        if (t == 0) {
+            __threadfence();
+            st_release_i32(a.flags + b * ng + g, 1);
+        }
+    } else if (t == 0) {
+        st_release_i32(a.flags + b * ng + g, 2);  // dependants stop at once
+    }
+}
+
+template <int MODE>
+int32_t launch_chain(Ctx* ctx, cudaStream_t st, const double* LU, int64_t ld, int64_t n, double* X, int64_t ldx,
+                     int64_t nrhs, bool* used) {
+    *used = false;
+    const int nblk = (int)ceil_div(n, kDsNB);
+    std::atomic<int>& attr = device_flag((const void*)dsweep_kernel<MODE>, 0, ctx->device);
+    if (!attr.load()) {
+        B2M_CU(ctx, cudaFuncSetAttribute(dsweep_kernel<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, kDsSmem));
+        B2M_CU(ctx, cudaFuncSetAttribute(dinv_kernel<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, kDsTriSmem));
+        B2M_CU(ctx, cudaFuncSetAttribute(dcouple_kernel<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, kDsTriSmem));
+        attr.store(1);
+    }
+    if (ctx->dsweep_ctas < 0) {
+        int per_sm = 0, coop = 0;
+        B2M_CU(ctx, cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, ctx->device));
+        B2M_CU(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, dsweep_kernel<MODE>, kDsThreads, kDsSmem));
+        ctx->dsweep_ctas = coop ? per_sm * ctx->num_sms : 0;
+    }
+    const int ngmax = (int)ceil_div(std::min<int64_t>(nrhs, kDsMaxRhs), kDsRhs);
+    if ((int64_t)nblk * ngmax > ctx->dsweep_ctas) return B2M_OK;  // not co-resident: per-block launches
+    const size_t blk_doubles = (size_t)nblk * kDsNB * kDsNB;
+    const size_t pub_doubles = (size_t)nblk * 2 * kDsNB * kDsRhs;
+    void* p = nullptr;
+    B2M_TRY(ws_get(ctx, kWsTri, (2 * blk_doubles + pub_doubles) * sizeof(double) + (size_t)nblk * 2 * sizeof(int32_t),
+                   &p));
+    double* inv = static_cast<double*>(p);
+    double* w = inv + blk_doubles;
+    double* pub = w + blk_doubles;
+    int32_t* flags = reinterpret_cast<int32_t*>(pub + pub_doubles);
+    prof_begin(ctx, st, kClsSolve);
+    dinv_kernel<MODE><<<nblk, kDsNB, kDsTriSmem, st>>>(LU, ld, (int)n, inv, ctx->d_status);
+    prof_end(ctx, st, kClsSolve, 8.0 * 2 * blk_doubles);
+    B2M_LAUNCHED(ctx);
+    prof_begin(ctx, st, kClsSolve);
+    dcouple_kernel<MODE><<<nblk, 256, kDsTriSmem, st>>>(LU, ld, (int)n, inv, w, ctx->d_status);
+    prof_end(ctx, st, kClsSolve, 8.0 * 3 * blk_doubles);
+    B2M_LAUNCHED(ctx);
+    for (int64_t c0 = 0; c0 < nrhs; c0 += kDsMaxRhs) {
+        const int nc = (int)std::min<int64_t>(kDsMaxRhs, nrhs - c0);
+        const int ng = (int)ceil_div(nc, kDsRhs);
+        B2M_CU(ctx, cudaMemsetAsync(flags, 0, (size_t)nblk * ng * sizeof(int32_t), st));
+        DsArgs da{LU, ld, (int)n, inv, w, X, ldx, (int)c0, nc, pub, flags, ctx->d_status,
+                  ctx->wait_limit >= 0 ? (uint32_t)ctx->wait_limit : kDsSpin};
+        cudaLaunchConfig_t cfg{};
+        cudaLaunchAttribute at[1];
+        at[0].id = cudaLaunchAttributeCooperative;
+        at[0].val.cooperative = 1;
+        cfg.gridDim = dim3((unsigned)(nblk * ng));
+        cfg.blockDim = dim3(kDsThreads);
+        cfg.dynamicSmemBytes = kDsSmem;
+        cfg.stream = st;
+        cfg.attrs = at;
+        cfg.numAttrs = 1;
+        prof_begin(ctx, st, kClsSolve);
+        B2M_CU(ctx, cudaLaunchKernelEx(&cfg, dsweep_kernel<MODE>, da));
+        prof_end(ctx, st, kClsSolve, 4.0 * (double)n * n + 16.0 * n * nc);
+        B2M_LAUNCHED(ctx);
+    }
+    *used = true;
+    return B2M_OK;
+}
+
+template <int MODE>
+int32_t solve_tri(Ctx* ctx, cudaStream_t st, const double* LU, int64_t ld, int64_t n, double* X, int64_t ldx,
+                  int64_t nrhs) {
+    if (n > 2 * kDsNB) {
+        bool used = false;
+        B2M_TRY(launch_chain<MODE>(ctx, st, LU, ld, n, X, ldx, nrhs, &used));
+        if (used) return B2M_OK;
+    }
+    return launch_sweeps<MODE>(ctx, st, LU, ld, n, X, ldx, nrhs);
+}
+
 }  // namespace
 
 int32_t tri_solve_f64(Ctx* ctx, cudaStream_t st, const double* LU, int64_t ld, int64_t n, int mode, double* X,
                       int64_t ldx, int64_t nrhs) {
     if (n <= 0 || nrhs <= 0) return B2M_OK;
     switch (mode) {
-        case kTriL: return launch_sweeps<kTriL>(ctx, st, LU, ld, n, X, ldx, nrhs);
-        case kTriU: return launch_sweeps<kTriU>(ctx, st, LU, ld, n, X, ldx, nrhs);
-        case kTriUt: return launch_sweeps<kTriUt>(ctx, st, LU, ld, n, X, ldx, nrhs);
-        case kTriLt: return launch_sweeps<kTriLt>(ctx, st, LU, ld, n, X, ldx, nrhs);
+        case kTriL: return solve_tri<kTriL>(ctx, st, LU, ld, n, X, ldx, nrhs);
+        case kTriU: return solve_tri<kTriU>(ctx, st, LU, ld, n, X, ldx, nrhs);
+        case kTriUt: return solve_tri<kTriUt>(ctx, st, LU, ld, n, X, ldx, nrhs);
+        case kTriLt: return solve_tri<kTriLt>(ctx, st, LU, ld, n, X, ldx, nrhs);
     }
     return fail(ctx, B2M_ERR_ARG, "tri_solve_f64: unknown triangle %d", mode);
 }
