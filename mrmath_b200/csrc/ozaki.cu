@@ -263,6 +263,22 @@ __host__ __device__ constexpr uint32_t i8_idesc_m128n64() {
     return (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(KBN >> 3) << 17) | ((uint32_t)(KBM >> 4) << 24);
 }
 
+// the s (s + 1) / 2 MMAs of one k-step for a compile-time s: descriptors are the stage's base
+// descriptors plus constants, and the first MMA of every accumulator (pa = 1 in this order) of a
+// chunk's first k-step starts it
+template <int S>
+__device__ __forceinline__ void km_issue_step(uint32_t tmem, uint64_t da0, uint64_t db0, uint32_t idesc, bool first) {
+#pragma unroll
+    for (int pa = 1; pa <= S; ++pa) {
+#pragma unroll
+        for (int pb = 1; pa + pb <= S + 1; ++pb) {
+            const int d = pa + pb;
+            umma_i8(tmem + (uint32_t)((d - 2) * KBN), da0 + (uint64_t)(((pa - 1) * kKmTileA) >> 4),
+                    db0 + (uint64_t)(((pb - 1) * kKmTileB) >> 4), idesc, (first && pa == 1) ? 0u : 1u);
+        }
+    }
+}
+
 __global__ void __launch_bounds__(kOzThreads, 1)
     ozaki_kmajor_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, OzArgs p) {
     extern __shared__ uint8_t km_smem_raw[];
@@ -338,14 +354,18 @@ __global__ void __launch_bounds__(kOzThreads, 1)
                     tc_fence_after();
                     const uint32_t sa = smem_u32(smem + st * stage_bytes);
                     const uint32_t sb = sa + (uint32_t)(s * kKmTileA);
-                    for (int pa = 1; pa <= s; ++pa) {
-                        for (int pb = 1; pa + pb <= s + 1; ++pb) {
-                            const int d = pa + pb;
-                            const uint32_t tacc = tmem + (uint32_t)((d - 2) * KBN);
-                            const uint32_t acc = (started >> (d - 2)) & 1u;
-                            umma_i8(tacc, sw32_desc(sa + (uint32_t)((pa - 1) * kKmTileA)),
-                                    sw32_desc(sb + (uint32_t)((pb - 1) * kKmTileB)), idesc, acc);
-                            started |= 1u << (d - 2);
+                    if (s == kKmMaxSlices) {
+                        km_issue_step<kKmMaxSlices>(tmem, sw32_desc(sa), sw32_desc(sb), idesc, kt == k0);
+                    } else {
+                        for (int pa = 1; pa <= s; ++pa) {
+                            for (int pb = 1; pa + pb <= s + 1; ++pb) {
+                                const int d = pa + pb;
+                                const uint32_t tacc = tmem + (uint32_t)((d - 2) * KBN);
+                                const uint32_t acc = (started >> (d - 2)) & 1u;
+                                umma_i8(tacc, sw32_desc(sa + (uint32_t)((pa - 1) * kKmTileA)),
+                                        sw32_desc(sb + (uint32_t)((pb - 1) * kKmTileB)), idesc, acc);
+                                started |= 1u << (d - 2);
+                            }
                         }
                     }
                     umma_commit(&empty_bar[st]);
