@@ -25,6 +25,7 @@
 #include <algorithm>
 #include <cfloat>
 #include <chrono>
+#include <climits>
 #include <cstring>
 #include <numeric>
 #include <type_traits>
@@ -40,6 +41,7 @@ constexpr int kBThreads = 256;
 constexpr int kBMaxN = 256;
 constexpr int kBMaxK = 8;
 constexpr int kBMaxPW = 32;
+constexpr int kStrip = 2;  // 16 x 8 tiles per warp step of the trailing update
 
 struct BatchArgs {
     int count;
@@ -127,6 +129,31 @@ __device__ __forceinline__ void grp_argmax(const Grp& g, const Slice& s, double 
     g.sync();
 }
 
+// pivot search over the group: the largest candidate magnitude v >= 0, the lowest row index among
+// equal magnitudes (the first maximum of the reference's scan).  A thread without a candidate
+// passes v = 0 and i = INT_MAX.  Non-negative doubles order like their bit patterns, so the
+// comparison runs on the 64-bit key as two 32-bit warp reductions, then a minimum over the
+// indices of the lanes that hold the maximum; the warps' winners are combined the same way.
+__device__ __forceinline__ void warp_pivot(double v, int i, double& bv, int& bi) {
+    const unsigned long long key = (unsigned long long)__double_as_longlong(v);
+    const unsigned hi = (unsigned)(key >> 32), lo = (unsigned)key;
+    const unsigned mhi = __reduce_max_sync(0xffffffffu, hi);
+    const unsigned mlo = __reduce_max_sync(0xffffffffu, hi == mhi ? lo : 0u);
+    const unsigned mi = __reduce_min_sync(0xffffffffu, (hi == mhi && lo == mlo) ? (unsigned)i : 0xffffffffu);
+    bv = __longlong_as_double((long long)(((unsigned long long)mhi << 32) | mlo));
+    bi = (int)mi;
+}
+
+__device__ __forceinline__ void grp_pivot(const Grp& g, const Slice& s, double v, int i, double& bv, int& bi) {
+    const int lane = g.tid & 31, w = g.tid >> 5, nw = g.nt >> 5;
+    warp_pivot(v, i, bv, bi);
+    if (nw == 1) return;
+    if (lane == 0) { s.red[w] = bv; s.redi[w] = bi; }
+    g.sync();
+    warp_pivot(lane < nw ? s.red[lane] : 0.0, lane < nw ? s.redi[lane] : INT_MAX, bv, bi);
+    g.sync();
+}
+
 // Blocked LU of the n x n matrix A0 (FP64, row-major, ld n) into W (element type T, same layout)
 // with row permutation perm.  The first panel reads A0 directly and its updates write every entry
 // of W, so A0 is never copied separately.  Global loads are issued in groups before they are used
@@ -159,14 +186,15 @@ __device__ int grp_lu(const Grp& g, const Slice& s, const double* A0, T* W, int 
         g.sync();
         for (int j = 0; j < pw; ++j) {
             double v = -1.0;
-            int vi = -1;
+            int vi = INT_MAX;
             for (int r = j + g.tid; r < m; r += g.nt) {
                 const double a = fabs(s.pan[r * pwp + j]);
-                if (vi < 0 || a > v) { v = a; vi = r; }
+                if (a > v) { v = a; vi = r; }  // a NaN never wins
             }
+            if (vi == INT_MAX) v = 0.0;
             double bv;
             int pr;
-            grp_argmax(g, s, v, vi, bv, pr);
+            grp_pivot(g, s, v, vi, bv, pr);
             if (!(bv > (double)sing_thresh<T>())) return 1;
             if (pr != j) {
                 for (int c = g.tid; c < pw; c += g.nt) {
@@ -221,36 +249,50 @@ __device__ int grp_lu(const Grp& g, const Slice& s, const double* A0, T* W, int 
                 // trailing update A22 -= L21 U12 on the FP64 tensor cores: warps walk 16 x 8 tiles;
                 // m16n8k4 fragments (g = lane / 4, t = lane % 4): a = (L21[g][k+t], L21[g+8][k+t]),
                 // b = U12[k+t][g], c = C[g][2t..2t+1], C[g+8][2t..2t+1]
+                // A warp takes a 16 x 8 kStrip strip (kStrip 16 x 8 tiles sharing the L21
+                // fragment), so that its 4 kStrip loads of C are in flight together.
                 const int lane = g.tid & 31, nw = g.nt >> 5, gq = lane >> 2, tq = lane & 3;
-                const int tm = (nr + 15) / 16, tn = (nr + 7) / 8;
+                const int tm = (nr + 15) / 16, tn = (nr + 8 * kStrip - 1) / (8 * kStrip);
                 for (int tile = g.tid >> 5; tile < tm * tn; tile += nw) {
-                    const int r0 = (tile / tn) * 16, q0 = (tile % tn) * 8;
-                    const int ra = r0 + gq, rb = r0 + gq + 8, cc = q0 + 2 * tq;
+                    const int r0 = (tile / tn) * 16, q0 = (tile % tn) * 8 * kStrip;
+                    const int ra = r0 + gq, rb = r0 + gq + 8;
                     const bool oka = ra < nr, okb = rb < nr;
-                    const int64_t rowa = oka ? (int64_t)s.perm[c1 + ra] * n : 0, rowb = okb ? (int64_t)s.perm[c1 + rb] * n : 0;
-                    double d[4];
-                    d[0] = (oka && cc < nr) ? (double)at(rowa / n, c1 + cc) : 0.0;
-                    d[1] = (oka && cc + 1 < nr) ? (double)at(rowa / n, c1 + cc + 1) : 0.0;
-                    d[2] = (okb && cc < nr) ? (double)at(rowb / n, c1 + cc) : 0.0;
-                    d[3] = (okb && cc + 1 < nr) ? (double)at(rowb / n, c1 + cc + 1) : 0.0;
+                    const int rowa = oka ? s.perm[c1 + ra] : 0, rowb = okb ? s.perm[c1 + rb] : 0;
+                    double d[kStrip][4];
+#pragma unroll
+                    for (int u = 0; u < kStrip; ++u) {
+                        const int cc = q0 + 8 * u + 2 * tq;
+                        d[u][0] = (oka && cc < nr) ? (double)at(rowa, c1 + cc) : 0.0;
+                        d[u][1] = (oka && cc + 1 < nr) ? (double)at(rowa, c1 + cc + 1) : 0.0;
+                        d[u][2] = (okb && cc < nr) ? (double)at(rowb, c1 + cc) : 0.0;
+                        d[u][3] = (okb && cc + 1 < nr) ? (double)at(rowb, c1 + cc + 1) : 0.0;
+                    }
                     const double* la = s.pan + (pw + min(ra, nr - 1)) * pwp;
                     const double* lb = s.pan + (pw + min(rb, nr - 1)) * pwp;
-                    const int cb = min(q0 + gq, nr - 1);
                     for (int k = 0; k < pw; k += 4) {
                         const int kk = k + tq;
                         const double a0 = kk < pw ? -la[kk] : 0.0;
                         const double a1 = kk < pw ? -lb[kk] : 0.0;
-                        const double b0 = kk < pw ? s.u[kk * s.us + cb] : 0.0;
-                        asm volatile(
-                            "mma.sync.aligned.m16n8k4.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5}, {%6}, "
-                            "{%0,%1,%2,%3};\n"
-                            : "+d"(d[0]), "+d"(d[1]), "+d"(d[2]), "+d"(d[3])
-                            : "d"(a0), "d"(a1), "d"(b0));
+#pragma unroll
+                        for (int u = 0; u < kStrip; ++u) {
+                            const int cb = min(q0 + 8 * u + gq, nr - 1);
+                            const double b0 = kk < pw ? s.u[kk * s.us + cb] : 0.0;
+                            asm volatile(
+                                "mma.sync.aligned.m16n8k4.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5}, {%6}, "
+                                "{%0,%1,%2,%3};\n"
+                                : "+d"(d[u][0]), "+d"(d[u][1]), "+d"(d[u][2]), "+d"(d[u][3])
+                                : "d"(a0), "d"(a1), "d"(b0));
+                        }
                     }
-                    if (oka && cc < nr) W[rowa + c1 + cc] = (T)d[0];
-                    if (oka && cc + 1 < nr) W[rowa + c1 + cc + 1] = (T)d[1];
-                    if (okb && cc < nr) W[rowb + c1 + cc] = (T)d[2];
-                    if (okb && cc + 1 < nr) W[rowb + c1 + cc + 1] = (T)d[3];
+                    const int64_t oa = (int64_t)rowa * n + c1, ob = (int64_t)rowb * n + c1;
+#pragma unroll
+                    for (int u = 0; u < kStrip; ++u) {
+                        const int cc = q0 + 8 * u + 2 * tq;
+                        if (oka && cc < nr) W[oa + cc] = (T)d[u][0];
+                        if (oka && cc + 1 < nr) W[oa + cc + 1] = (T)d[u][1];
+                        if (okb && cc < nr) W[ob + cc] = (T)d[u][2];
+                        if (okb && cc + 1 < nr) W[ob + cc + 1] = (T)d[u][3];
+                    }
                 }
             } else {
             // trailing update A22 -= L21 U12: thread per column, 8 rows per step, loads first
@@ -313,20 +355,32 @@ __device__ void grp_solve(const Grp& g, const Slice& s, const T* W, int n, int k
                 if (lane < bs) s.y[row * kBMaxK + q] = yv;
             }
             g.sync();
+            // fold the block into the other rows: a thread per row, every right-hand side (the
+            // row of the factor is read once, 8 loads in flight; same order of terms per entry)
             const int rlo = lower ? b0 + bs : 0, rhi = lower ? n : b0;
-            for (int e = g.tid; e < (rhi - rlo) * kk; e += g.nt) {
-                const int r = rlo + e / kk, q = e % kk;
+            for (int r = rlo + g.tid; r < rhi; r += g.nt) {
                 const T* lr = W + (int64_t)s.perm[r] * n + b0;
-                T acc = (T)s.y[r * kBMaxK + q];
-                for (int j0 = 0; j0 < bs; j0 += 8) {
+                T acc[kBMaxK];
+#pragma unroll
+                for (int q = 0; q < kBMaxK; ++q) acc[q] = q < kk ? (T)s.y[r * kBMaxK + q] : (T)0;
+#pragma unroll
+                for (int j0 = 0; j0 < 32; j0 += 8) {
                     T v[8];
 #pragma unroll
                     for (int e2 = 0; e2 < 8; ++e2) v[e2] = j0 + e2 < bs ? lr[j0 + e2] : (T)0;
 #pragma unroll
-                    for (int e2 = 0; e2 < 8; ++e2)
-                        if (j0 + e2 < bs) acc -= v[e2] * (T)s.y[(b0 + j0 + e2) * kBMaxK + q];
+                    for (int e2 = 0; e2 < 8; ++e2) {
+                        if (j0 + e2 < bs) {
+                            const double* yr = s.y + (b0 + j0 + e2) * kBMaxK;
+#pragma unroll
+                            for (int q = 0; q < kBMaxK; ++q)
+                                if (q < kk) acc[q] -= v[e2] * (T)yr[q];
+                        }
+                    }
                 }
-                s.y[r * kBMaxK + q] = (double)acc;
+#pragma unroll
+                for (int q = 0; q < kBMaxK; ++q)
+                    if (q < kk) s.y[r * kBMaxK + q] = (double)acc[q];
             }
             g.sync();
         }
@@ -445,7 +499,10 @@ __device__ int solve_mixed(const Grp& g, const Slice& s, const BatchArgs& a, int
     return -1;
 }
 
-__global__ void __launch_bounds__(kBThreads, 1) batch_solve_kernel(BatchArgs a) {
+// MODE 0 plain FP64, 1 FP32 factor + FP64 refinement.  At most 128 registers a thread, so that
+// two CTAs share an SM whenever the tile shape's shared memory allows it.
+template <int MODE>
+__global__ void __launch_bounds__(kBThreads, 2) batch_solve_kernel(BatchArgs a) {
     extern __shared__ __align__(16) double bsm[];
     __shared__ int s_sys[8];
     const int t = threadIdx.x;
@@ -462,7 +519,7 @@ __global__ void __launch_bounds__(kBThreads, 1) batch_solve_kernel(BatchArgs a) 
             const Grp g{t, kBThreads, 1};
             const Slice s = carve(bsm, kBMaxN, a.pw_large);
             int st, iters = 0;
-            if (a.mode == 1) {
+            if (MODE == 1) {
                 iters = solve_mixed(g, s, a, sys, W);
                 st = iters < 0 ? solve_plain(g, s, a, sys, W) : 0;
             } else {
@@ -492,7 +549,7 @@ __global__ void __launch_bounds__(kBThreads, 1) batch_solve_kernel(BatchArgs a) 
             const Slice s = carve(bsm + (size_t)gi * slice_doubles(a.small_n, a.pw_small), a.small_n, a.pw_small);
             double* Wg = W + (size_t)gi * a.small_n * a.small_n;
             int st, iters = 0;
-            if (a.mode == 1) {
+            if (MODE == 1) {
                 iters = solve_mixed(g, s, a, msys, Wg);
                 st = iters < 0 ? solve_plain(g, s, a, msys, Wg) : 0;
             } else {
@@ -581,9 +638,10 @@ int32_t batch_solve(Ctx* ctx, cudaStream_t st, int64_t count, const int32_t* hn,
 
     auto launch = [&](const BatchTune& tc, cudaStream_t q) -> int32_t {
         const size_t smem = batch_smem_bytes(tc.small_n, tc.group_warps, tc.pw_large, tc.pw_small);
-        B2M_CU(ctx, cudaFuncSetAttribute(batch_solve_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        void (*kern)(BatchArgs) = mode == 1 ? batch_solve_kernel<1> : batch_solve_kernel<0>;
+        B2M_CU(ctx, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         int per_sm = 0;
-        B2M_CU(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_solve_kernel, kBThreads, smem));
+        B2M_CU(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kBThreads, smem));
         if (per_sm < 1) return fail(ctx, B2M_ERR_UNSUPPORTED, "batch: tile shape does not fit one SM");
         const int grid = occ_sms * per_sm;
         void* pscr;
@@ -596,7 +654,7 @@ int32_t batch_solve(Ctx* ctx, cudaStream_t st, int64_t count, const int32_t* hn,
         b.pw_small = tc.pw_small;
         B2M_CU(ctx, cudaMemsetAsync(dctr, 0, sizeof(int32_t), q));
         prof_begin(ctx, q, kClsSolve);
-        batch_solve_kernel<<<grid, kBThreads, smem, q>>>(b);
+        kern<<<grid, kBThreads, smem, q>>>(b);
         prof_end(ctx, q, kClsSolve, 0.0);
         B2M_LAUNCHED(ctx);
         return B2M_OK;

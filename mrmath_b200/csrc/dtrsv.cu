@@ -229,8 +229,10 @@ int32_t launch_sweeps(Ctx* ctx, cudaStream_t st, const double* LU, int64_t ld, i
 // for U and U^T) and each coupling block W_b = T_bb^-1 T_{b,p} (p the block before b in sweep
 // order) are formed first, then a CTA per (block, 8 right-hand sides) folds in the earlier blocks
 // as they are published and finishes x_b = T_bb^-1 y_b - W_b x_p, so one 64 x 64 x 8 product per
-// block is on the chain.  A block is published as 512 doubles and a flag (release/acquire); every
-// wait is bounded and a CTA that gives up marks its flag 2 so that its dependants stop at once.
+// block is on the chain.  A block is published as 512 doubles over words preset to an empty
+// pattern (all bits set, which no arithmetic result has): each 64-bit store carries its own
+// readiness, so there is neither a fence nor a flag round trip; every wait is bounded and a CTA
+// that gives up writes the abort pattern so that its dependants stop at once.
 constexpr int kDsNB = 64;
 constexpr int kDsRhs = 8;
 constexpr int kDsThreads = 128;
@@ -238,14 +240,16 @@ constexpr int kDsMaxRhs = 16;  // right-hand sides per sweep launch
 constexpr int kDsSmem = 2 * kDsNB * kDsNB * (int)sizeof(double);  // T_bb^-1 and W_b, transposed
 constexpr int kDsTriSmem = 2 * kDsNB * (kDsNB + 1) * (int)sizeof(double);
 constexpr uint32_t kDsSpin = 1u << 22;
+constexpr unsigned long long kDsEmpty = ~0ull;        // a word not yet published
+constexpr unsigned long long kDsAbort = ~0ull - 1ull;  // a block whose CTA gave up
 
-__device__ __forceinline__ int ld_acquire_i32(const int32_t* p) {
-    int v;
-    asm volatile("ld.acquire.gpu.global.b32 %0, [%1];\n" : "=r"(v) : "l"(p) : "memory");
+__device__ __forceinline__ unsigned long long ds_ld64(const unsigned long long* p) {
+    unsigned long long v;
+    asm volatile("ld.relaxed.gpu.global.b64 %0, [%1];\n" : "=l"(v) : "l"(p) : "memory");
     return v;
 }
-__device__ __forceinline__ void st_release_i32(int32_t* p, int v) {
-    asm volatile("st.release.gpu.global.b32 [%0], %1;\n" ::"l"(p), "r"(v) : "memory");
+__device__ __forceinline__ void ds_st64(unsigned long long* p, unsigned long long v) {
+    asm volatile("st.relaxed.gpu.global.b64 [%0], %1;\n" ::"l"(p), "l"(v) : "memory");
 }
 
 // inverse of the diagonal block b of the triangle (thread per column; zero past the matrix)
@@ -336,8 +340,7 @@ struct DsArgs {
     double* X;
     int64_t ldx;
     int c0, nc;
-    double* pub;        // [nblk][ng][64][8] published blocks
-    int32_t* flags;     // [nblk][ng]: 0 pending, 1 published, 2 abandoned (zeroed before the launch)
+    unsigned long long* pub;  // [nblk][ng][64][8] published blocks (double bits; preset to kDsEmpty)
     int32_t* status;
     uint32_t spin;
 };
@@ -372,24 +375,31 @@ __global__ void __launch_bounds__(kDsThreads) dsweep_kernel(DsArgs a) {
     }
     if (t == 0) s_abort = 0;
     __syncthreads();
-    // block j published: its 64 x 8 values into s_p
+    // block j published: its 64 x 8 values into s_p (thread t polls words t, t + 128, ...)
     auto wait_block = [&](int j) -> bool {
-        if (t == 0) {
-            const int32_t* f = a.flags + j * ng + g;
-            int v = 0;
-            for (uint32_t it = 0; it < a.spin && v == 0; ++it) {
-                v = ld_acquire_i32(f);
-                if (v == 0 && (it & 255u) == 255u && *reinterpret_cast<volatile int32_t*>(&a.status[kTimeout]) != 0) v = 2;
+        const unsigned long long* src = a.pub + (size_t)(j * ng + g) * (kDsNB * kDsRhs);
+        unsigned long long w[4];
+        bool ready = false, bad = false;
+        for (uint32_t it = 0; it < a.spin && !ready && !bad; ++it) {
+            ready = true;
+#pragma unroll
+            for (int e = 0; e < 4; ++e) {
+                w[e] = ds_ld64(src + t + kDsThreads * e);
+                ready = ready && w[e] != kDsEmpty;
+                bad = bad || w[e] == kDsAbort;
             }
-            if (v == 0) atomicCAS(&a.status[kTimeout], 0, 505);
-            if (v != 1) s_abort = 1;
+            if (!ready && (it & 255u) == 255u && *reinterpret_cast<volatile int32_t*>(&a.status[kTimeout]) != 0)
+                bad = true;
+        }
+        if (!ready && !bad) atomicCAS(&a.status[kTimeout], 0, 505);
+        if (!ready || bad) s_abort = 1;
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+            const int idx = t + kDsThreads * e;
+            s_p[idx >> 3][idx & 7] = __longlong_as_double((long long)w[e]);
         }
         __syncthreads();
-        if (s_abort) return false;
-        const double* src = a.pub + (size_t)(j * ng + g) * (kDsNB * kDsRhs);
-        for (int e = t; e < kDsNB * kDsRhs; e += kDsThreads) s_p[e >> 3][e & 7] = __ldcg(src + e);
-        __syncthreads();
-        return true;
+        return !s_abort;
     };
     bool ok = true;
     for (int jj = 0; ok && jj + 1 < bi; ++jj) {
@@ -450,21 +460,20 @@ __global__ void __launch_bounds__(kDsThreads) dsweep_kernel(DsArgs a) {
         }
         __syncthreads();
         if (h == 0) {
-            double* dst = a.pub + (size_t)(b * ng + g) * (kDsNB * kDsRhs) + r * kDsRhs;
+            unsigned long long* dst = a.pub + (size_t)(b * ng + g) * (kDsNB * kDsRhs) + r * kDsRhs;
 #pragma unroll
             for (int q = 0; q < kDsRhs; ++q) {
                 const double xv = (r < bs && q < ncg) ? acc[q] + s_h[r][q] : 0.0;
-                dst[q] = xv;
+                unsigned long long bits = (unsigned long long)__double_as_longlong(xv);
+                if (bits >= kDsAbort) bits = 0x7FF8000000000000ull;  // a NaN carrying a reserved pattern
+                ds_st64(dst + q, bits);
                 if (r < bs && q < ncg) a.X[(int64_t)(b0 + r) * a.ldx + cg + q] = xv;
             }
         }
-        __syncthreads();
-        if (t == 0) {
-            __threadfence();
-            st_release_i32(a.flags + b * ng + g, 1);
-        }
-    } else if (t == 0) {
-        st_release_i32(a.flags + b * ng + g, 2);  // dependants stop at once
+    } else {  // dependants stop at once
+        unsigned long long* dst = a.pub + (size_t)(b * ng + g) * (kDsNB * kDsRhs);
+#pragma unroll
+        for (int e = 0; e < 4; ++e) ds_st64(dst + t + kDsThreads * e, kDsAbort);
     }
 }
 
@@ -491,12 +500,10 @@ int32_t launch_chain(Ctx* ctx, cudaStream_t st, const double* LU, int64_t ld, in
     const size_t blk_doubles = (size_t)nblk * kDsNB * kDsNB;
     const size_t pub_doubles = (size_t)nblk * 2 * kDsNB * kDsRhs;
     void* p = nullptr;
-    B2M_TRY(ws_get(ctx, kWsTri, (2 * blk_doubles + pub_doubles) * sizeof(double) + (size_t)nblk * 2 * sizeof(int32_t),
-                   &p));
+    B2M_TRY(ws_get(ctx, kWsTri, (2 * blk_doubles + pub_doubles) * sizeof(double), &p));
     double* inv = static_cast<double*>(p);
     double* w = inv + blk_doubles;
-    double* pub = w + blk_doubles;
-    int32_t* flags = reinterpret_cast<int32_t*>(pub + pub_doubles);
+    unsigned long long* pub = reinterpret_cast<unsigned long long*>(w + blk_doubles);
     prof_begin(ctx, st, kClsSolve);
     dinv_kernel<MODE><<<nblk, kDsNB, kDsTriSmem, st>>>(LU, ld, (int)n, inv, ctx->d_status);
     prof_end(ctx, st, kClsSolve, 8.0 * 2 * blk_doubles);
@@ -508,8 +515,8 @@ int32_t launch_chain(Ctx* ctx, cudaStream_t st, const double* LU, int64_t ld, in
     for (int64_t c0 = 0; c0 < nrhs; c0 += kDsMaxRhs) {
         const int nc = (int)std::min<int64_t>(kDsMaxRhs, nrhs - c0);
         const int ng = (int)ceil_div(nc, kDsRhs);
-        B2M_CU(ctx, cudaMemsetAsync(flags, 0, (size_t)nblk * ng * sizeof(int32_t), st));
-        DsArgs da{LU, ld, (int)n, inv, w, X, ldx, (int)c0, nc, pub, flags, ctx->d_status,
+        B2M_CU(ctx, cudaMemsetAsync(pub, 0xFF, (size_t)nblk * ng * kDsNB * kDsRhs * sizeof(double), st));  // kDsEmpty
+        DsArgs da{LU, ld, (int)n, inv, w, X, ldx, (int)c0, nc, pub, ctx->d_status,
                   ctx->wait_limit >= 0 ? (uint32_t)ctx->wait_limit : kDsSpin};
         cudaLaunchConfig_t cfg{};
         cudaLaunchAttribute at[1];
