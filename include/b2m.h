@@ -131,6 +131,9 @@ B2M_API int64_t     b2m_kernel_launches(b2m_ctx* ctx);
 #define B2M_INFO_CHAIN_CLUSTERS 3
 #define B2M_INFO_CHAIN_PROBE    4
 #define B2M_INFO_CHAIN_CLUSTERS4 5  /* the same as B2M_INFO_CHAIN_CLUSTERS for 4-CTA clusters */
+#define B2M_INFO_BATCH_BIG_WARPS 6  /* warps per system of order > small_n in the tile shape chosen for
+                                       the last batch plan (8: a whole CTA, 4: two systems per CTA;
+                                       0 before any batch) */
 B2M_API int32_t     b2m_ctx_info(b2m_ctx* ctx, int32_t what, int64_t* value);
 /* Event profiler: when enabled, every launch is bracketed by CUDA events on its own stream and
  * its algorithmic work is recorded per kernel class (0 FP64 GEMM, 1 panel, 2 row swaps,

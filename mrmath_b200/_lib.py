@@ -182,7 +182,8 @@ class Context:
     def kernel_launches(self) -> int:
         return lib.b2m_kernel_launches(self.h)
 
-    INFO_KEYS = {"num_sms": 1, "sweep_ctas": 2, "chain_clusters": 3, "chain_probe": 4, "chain_clusters4": 5}
+    INFO_KEYS = {"num_sms": 1, "sweep_ctas": 2, "chain_clusters": 3, "chain_probe": 4, "chain_clusters4": 5,
+                 "batch_big_warps": 6}
 
     def info(self, key: str) -> int:
         """b2m_ctx_info: an execution fact of this context (see INFO_KEYS)."""

@@ -60,6 +60,7 @@ struct BatchArgs {
     int mode;
     int small_n;
     int group_warps;
+    int big_warps;
     int pw_large, pw_small;
     int max_iter;
 };
@@ -80,6 +81,7 @@ struct Slice {
     int* perm;     // [nmax] storage row of factor row i
     int* flag;     // [4]
     int us;        // row stride of u
+    int pw;        // panel width
 };
 
 __host__ __device__ inline size_t slice_doubles(int nmax, int pw) {
@@ -96,7 +98,15 @@ __device__ Slice carve(double* base, int nmax, int pw) {
     s.perm = s.redi + 8;
     s.flag = s.perm + nmax;
     s.us = nmax + 1;
+    s.pw = pw;
     return s;
+}
+
+// factor scratch of one CTA: a matrix of the slice's order per group
+__host__ __device__ inline size_t batch_scratch_doubles(int small_n, int G, int GB) {
+    const size_t big = (size_t)((kBThreads / 32) / GB) * kBMaxN * kBMaxN;
+    const size_t small = (size_t)((kBThreads / 32) / G) * small_n * small_n;
+    return big > small ? big : small;
 }
 
 template <typename T> __device__ __forceinline__ T sing_thresh();
@@ -391,7 +401,7 @@ __device__ void grp_solve(const Grp& g, const Slice& s, const T* W, int n, int k
 __device__ int solve_plain(const Grp& g, const Slice& s, const BatchArgs& a, int sys, double* W) {
     const int n = a.n[sys], kk = a.k[sys];
     const double* A = a.A + a.a_off[sys];
-    if (grp_lu<double>(g, s, A, W, n, g.nt == kBThreads ? a.pw_large : a.pw_small)) return 1;
+    if (grp_lu<double>(g, s, A, W, n, s.pw)) return 1;
     const double* B = a.B + a.b_off[sys];
     for (int e = g.tid; e < n * kk; e += g.nt) {
         const int i = e / kk, q = e - i * kk;
@@ -415,7 +425,7 @@ __device__ int solve_mixed(const Grp& g, const Slice& s, const BatchArgs& a, int
     const double* A = a.A + a.a_off[sys];
     const double* B = a.B + a.b_off[sys];
     double* X = a.X + a.b_off[sys];
-    if (grp_lu<float>(g, s, A, W, n, g.nt == kBThreads ? a.pw_large : a.pw_small)) return -1;
+    if (grp_lu<float>(g, s, A, W, n, s.pw)) return -1;
     // ||A||inf: a warp per row
     const int lane = g.tid & 31, wp = g.tid >> 5, nw = g.nt >> 5;
     double an = 0.0;
@@ -506,48 +516,33 @@ __global__ void __launch_bounds__(kBThreads, 2) batch_solve_kernel(BatchArgs a) 
     extern __shared__ __align__(16) double bsm[];
     __shared__ int s_sys[8];
     const int t = threadIdx.x;
-    double* W = a.scratch + (size_t)blockIdx.x * kBMaxN * kBMaxN;
-    const int G = a.group_warps, ngroups = (kBThreads / 32) / G;
+    double* W = a.scratch + (size_t)blockIdx.x * batch_scratch_doubles(a.small_n, a.group_warps, a.big_warps);
     for (;;) {
         if (t == 0) s_sys[0] = atomicAdd(a.counter, 1);
         __syncthreads();
         const int idx = s_sys[0];
         __syncthreads();
         if (idx >= a.count) return;
-        const int sys = a.order[idx];
-        if (a.n[sys] > a.small_n) {
-            const Grp g{t, kBThreads, 1};
-            const Slice s = carve(bsm, kBMaxN, a.pw_large);
-            int st, iters = 0;
-            if (MODE == 1) {
-                iters = solve_mixed(g, s, a, sys, W);
-                st = iters < 0 ? solve_plain(g, s, a, sys, W) : 0;
-            } else {
-                st = solve_plain(g, s, a, sys, W);
-            }
-            if (t == 0) {
-                a.info[sys] = st;
-                if (a.iters) a.iters[sys] = iters;
-            }
-            __syncthreads();
-            continue;
-        }
-        // small systems: this one plus up to ngroups - 1 more from the queue, one per group
+        // this system and up to ng - 1 more from the queue, one per group; the first one decides
+        // the round's group size and slice shape (the queue is sorted largest first, so a round
+        // that starts with a large system may end with small ones, which fit its slices too)
+        const bool big = a.n[a.order[idx]] > a.small_n;
+        const int gw = big ? a.big_warps : a.group_warps, ng = (kBThreads / 32) / gw;
+        const int nmax = big ? kBMaxN : a.small_n, pw = big ? a.pw_large : a.pw_small;
         if (t == 0) {
-            s_sys[0] = idx;
-            for (int q = 1; q < ngroups; ++q) {
+            for (int q = 1; q < ng; ++q) {
                 const int j = atomicAdd(a.counter, 1);
                 s_sys[q] = j < a.count ? j : -1;
             }
         }
         __syncthreads();
-        const int gi = t / (32 * G);
+        const int gi = t / (32 * gw);
         const int myidx = s_sys[gi];
         if (myidx >= 0) {
             const int msys = a.order[myidx];
-            const Grp g{t - gi * 32 * G, 32 * G, 2 + gi};
-            const Slice s = carve(bsm + (size_t)gi * slice_doubles(a.small_n, a.pw_small), a.small_n, a.pw_small);
-            double* Wg = W + (size_t)gi * a.small_n * a.small_n;
+            const Grp g{t - gi * 32 * gw, 32 * gw, 2 + gi};
+            const Slice s = carve(bsm + (size_t)gi * slice_doubles(nmax, pw), nmax, pw);
+            double* Wg = W + (size_t)gi * nmax * nmax;
             int st, iters = 0;
             if (MODE == 1) {
                 iters = solve_mixed(g, s, a, msys, Wg);
@@ -564,8 +559,8 @@ __global__ void __launch_bounds__(kBThreads, 2) batch_solve_kernel(BatchArgs a) 
     }
 }
 
-size_t batch_smem_bytes(int small_n, int G, int pw_large, int pw_small) {
-    const size_t big = slice_doubles(kBMaxN, pw_large);
+size_t batch_smem_bytes(int small_n, int G, int pw_large, int pw_small, int GB) {
+    const size_t big = slice_doubles(kBMaxN, pw_large) * ((kBThreads / 32) / GB);
     const size_t small = slice_doubles(small_n, pw_small) * ((kBThreads / 32) / G);
     return std::max(big, small) * sizeof(double);
 }
@@ -637,7 +632,7 @@ int32_t batch_solve(Ctx* ctx, cudaStream_t st, int64_t count, const int32_t* hn,
     a.max_iter = 10;
 
     auto launch = [&](const BatchTune& tc, cudaStream_t q) -> int32_t {
-        const size_t smem = batch_smem_bytes(tc.small_n, tc.group_warps, tc.pw_large, tc.pw_small);
+        const size_t smem = batch_smem_bytes(tc.small_n, tc.group_warps, tc.pw_large, tc.pw_small, tc.big_warps);
         void (*kern)(BatchArgs) = mode == 1 ? batch_solve_kernel<1> : batch_solve_kernel<0>;
         B2M_CU(ctx, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         int per_sm = 0;
@@ -645,11 +640,14 @@ int32_t batch_solve(Ctx* ctx, cudaStream_t st, int64_t count, const int32_t* hn,
         if (per_sm < 1) return fail(ctx, B2M_ERR_UNSUPPORTED, "batch: tile shape does not fit one SM");
         const int grid = occ_sms * per_sm;
         void* pscr;
-        B2M_TRY(ws_get(ctx, kWsMatD, (size_t)grid * kBMaxN * kBMaxN * sizeof(double), &pscr));
+        B2M_TRY(ws_get(ctx, kWsMatD,
+                       (size_t)grid * batch_scratch_doubles(tc.small_n, tc.group_warps, tc.big_warps) * sizeof(double),
+                       &pscr));
         BatchArgs b = a;
         b.scratch = static_cast<double*>(pscr);
         b.small_n = tc.small_n;
         b.group_warps = tc.group_warps;
+        b.big_warps = tc.big_warps;
         b.pw_large = tc.pw_large;
         b.pw_small = tc.pw_small;
         B2M_CU(ctx, cudaMemsetAsync(dctr, 0, sizeof(int32_t), q));
@@ -667,15 +665,16 @@ int32_t batch_solve(Ctx* ctx, cudaStream_t st, int64_t count, const int32_t* hn,
         best = it->second;
     } else {
         std::vector<BatchTune> cands;
-        for (int pwl : {8, 16, 32})
-            for (int G : {1, 2, 4})
-                for (int pws : {8, 16}) cands.push_back(BatchTune{64, G, pwl, pws, 0.0f});
+        for (int GB : {8, 4})
+            for (int pwl : {8, 16, 32})
+                for (int G : {1, 2, 4})
+                    for (int pws : {8, 16}) cands.push_back(BatchTune{64, G, pwl, pws, GB, 0.0f});
         cudaEvent_t e0, e1;
         B2M_CU(ctx, cudaEventCreate(&e0));
         B2M_CU(ctx, cudaEventCreate(&e1));
         float best_ms = 1e30f;
         for (auto& c : cands) {
-            const size_t smem = batch_smem_bytes(c.small_n, c.group_warps, c.pw_large, c.pw_small);
+            const size_t smem = batch_smem_bytes(c.small_n, c.group_warps, c.pw_large, c.pw_small, c.big_warps);
             if (smem > ctx->smem_optin) continue;
             B2M_TRY(launch(c, st));  // warm
             B2M_CU(ctx, cudaEventRecord(e0, st));
@@ -694,7 +693,7 @@ int32_t batch_solve(Ctx* ctx, cudaStream_t st, int64_t count, const int32_t* hn,
     }
     if (tune_out) *tune_out = best;
     const GraphKey key{7 + mode * 10, A, B, X, info, count, (int64_t)sig,
-                       best.pw_large * 10000 + best.pw_small * 100 + best.group_warps,
+                       best.big_warps * 1000000 + best.pw_large * 10000 + best.pw_small * 100 + best.group_warps,
                        (int64_t)reinterpret_cast<intptr_t>(iters)};
     return run_graph(ctx, st, key, [&](cudaStream_t q) { return launch(best, q); });
 }
@@ -703,7 +702,8 @@ int32_t batch_solve(Ctx* ctx, cudaStream_t st, int64_t count, const int32_t* hn,
 
 // ------------------------------------------------------------------ persisted autotuner table
 // One text line per batch plan: "<plan signature, hex> <small_n> <group_warps> <pw_large> <pw_small>
-// <ms>", after the header line "b2m-batch-tune 1".  A later process that loads the table skips the
+// <big_warps> <ms>", after the header line "b2m-batch-tune 2" (a version-1 table, without the
+// big_warps column, is read as big_warps = 8).  A later process that loads the table skips the
 // timing of the candidate shapes for every plan it lists (the signature covers the mode, every
 // system's order, right-hand sides and offsets).
 extern "C" int32_t b2m_batch_tune_save(b2m_ctx* h, const char* path) {
@@ -712,10 +712,11 @@ extern "C" int32_t b2m_batch_tune_save(b2m_ctx* h, const char* path) {
     b2m::CallLock lk(ctx);
     FILE* f = std::fopen(path, "w");
     if (!f) return b2m::fail(ctx, B2M_ERR_ARG, "cannot write %s", path);
-    std::fprintf(f, "b2m-batch-tune 1\n");
+    std::fprintf(f, "b2m-batch-tune 2\n");
     for (const auto& e : ctx->batch_tunes)
-        std::fprintf(f, "%016llx %d %d %d %d %.6f\n", (unsigned long long)e.first, e.second.small_n,
-                     e.second.group_warps, e.second.pw_large, e.second.pw_small, (double)e.second.ms);
+        std::fprintf(f, "%016llx %d %d %d %d %d %.6f\n", (unsigned long long)e.first, e.second.small_n,
+                     e.second.group_warps, e.second.pw_large, e.second.pw_small, e.second.big_warps,
+                     (double)e.second.ms);
     return std::fclose(f) == 0 ? B2M_OK : b2m::fail(ctx, B2M_ERR_ARG, "cannot write %s", path);
 }
 
@@ -728,21 +729,26 @@ extern "C" int32_t b2m_batch_tune_load(b2m_ctx* h, const char* path, int32_t* lo
     if (!f) return b2m::fail(ctx, B2M_ERR_ARG, "cannot read %s", path);
     char head[32] = {0};
     int version = 0;
-    if (std::fscanf(f, "%31s %d", head, &version) != 2 || std::strcmp(head, "b2m-batch-tune") != 0 || version != 1) {
+    if (std::fscanf(f, "%31s %d", head, &version) != 2 || std::strcmp(head, "b2m-batch-tune") != 0 ||
+        (version != 1 && version != 2)) {
         std::fclose(f);
         return b2m::fail(ctx, B2M_ERR_FORMAT, "%s is not a batch tuning table", path);
     }
     unsigned long long sig;
-    int sn, g, pwl, pws;
+    int sn, g, pwl, pws, gb = 8;
     double ms;
     int n = 0;
-    while (std::fscanf(f, "%llx %d %d %d %d %lf", &sig, &sn, &g, &pwl, &pws, &ms) == 6) {
+    auto next = [&]() -> bool {
+        if (version == 1) return std::fscanf(f, "%llx %d %d %d %d %lf", &sig, &sn, &g, &pwl, &pws, &ms) == 6;
+        return std::fscanf(f, "%llx %d %d %d %d %d %lf", &sig, &sn, &g, &pwl, &pws, &gb, &ms) == 7;
+    };
+    while (next()) {
         // only shapes the kernel has: a damaged or foreign line is skipped, never launched
         const bool ok = sn == 64 && (g == 1 || g == 2 || g == 4) && (pwl == 8 || pwl == 16 || pwl == 32) &&
-                        (pws == 8 || pws == 16) &&
-                        b2m::batch_smem_bytes(sn, g, pwl, pws) <= ctx->smem_optin;
+                        (pws == 8 || pws == 16) && (gb == 4 || gb == 8) &&
+                        b2m::batch_smem_bytes(sn, g, pwl, pws, gb) <= ctx->smem_optin;
         if (!ok) continue;
-        ctx->batch_tunes[(uint64_t)sig] = b2m::BatchTune{sn, g, pwl, pws, (float)ms};
+        ctx->batch_tunes[(uint64_t)sig] = b2m::BatchTune{sn, g, pwl, pws, gb, (float)ms};
         ++n;
     }
     std::fclose(f);

@@ -77,6 +77,7 @@ struct BatchTune {
     int group_warps;
     int pw_large;     // panel widths of the two size buckets
     int pw_small;
+    int big_warps;    // warps per system of order > small_n (8: the whole CTA, 4: two per CTA)
     float ms;         // measured time of the whole batch with this shape
 };
 

@@ -434,6 +434,12 @@ extern "C" int32_t b2m_ctx_info(b2m_ctx* h, int32_t what, int64_t* value) {
         case B2M_INFO_CHAIN_CLUSTERS: *value = ctx->chain_clusters; return B2M_OK;
         case B2M_INFO_CHAIN_PROBE: *value = ctx->chain_probe_why; return B2M_OK;
         case B2M_INFO_CHAIN_CLUSTERS4: *value = ctx->chain_clusters4; return B2M_OK;
+        case B2M_INFO_BATCH_BIG_WARPS: {
+            const auto it = ctx->batch_tunes.find(ctx->batch_plan_sig);
+            *value = it != ctx->batch_tunes.end()       ? it->second.big_warps
+                     : ctx->batch_tunes.empty() ? 0 : ctx->batch_tunes.begin()->second.big_warps;
+            return B2M_OK;
+        }
         default: return b2m::fail(ctx, B2M_ERR_ARG, "unknown info key %d", what);
     }
 }

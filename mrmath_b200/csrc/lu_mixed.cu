@@ -79,11 +79,32 @@ __global__ void colmax_kernel(const double* R, int64_t ldr, int64_t n, int64_t k
     atomic_max_abs(&out[c], R[i * ldr + c]);
 }
 
-__global__ void f64_to_f32_kernel(const double* src, int64_t lds, float* dst, int64_t ldd, int64_t rows, int64_t cols) {
-    const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (e >= rows * cols) return;
-    const int64_t r = e / cols, c = e - r * cols;
-    dst[r * ldd + c] = (float)src[r * lds + c];
+// FP32 copy of A and ||A||inf in one pass over A: a warp per row (grid-stride over rows), each lane
+// converting and summing |a_ij| over its columns j = lane, lane + 32, ... in order (the same sum as
+// norm_inf_kernel), four loads in flight; the row sums meet in a global max on the bit pattern.
+__global__ void __launch_bounds__(256) f64_to_f32_norm_kernel(const double* src, int64_t lds, float* dst, int64_t ldd,
+                                                              int64_t n, unsigned long long* out) {
+    const int lane = threadIdx.x & 31;
+    const int64_t nwarps = (int64_t)gridDim.x * (blockDim.x / 32);
+    for (int64_t row = (int64_t)blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5); row < n; row += nwarps) {
+        const double* a = src + row * lds;
+        float* d = dst + row * ldd;
+        double s = 0.0;
+        int64_t j = lane;
+        for (; j + 96 < n; j += 128) {
+            const double v0 = a[j], v1 = a[j + 32], v2 = a[j + 64], v3 = a[j + 96];
+            d[j] = (float)v0; d[j + 32] = (float)v1; d[j + 64] = (float)v2; d[j + 96] = (float)v3;
+            s += fabs(v0); s += fabs(v1); s += fabs(v2); s += fabs(v3);
+        }
+        for (; j < n; j += 32) {
+            const double v = a[j];
+            d[j] = (float)v;
+            s += fabs(v);
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+        if (lane == 0) atomicMax(out, (unsigned long long)__double_as_longlong(s));
+    }
 }
 
 // pinv[perm[i]] = i
@@ -1071,13 +1092,12 @@ int32_t solve_mixed(Ctx* ctx, cudaStream_t st, const double* A, int64_t lda, int
     }
 
     B2M_CU(ctx, cudaMemsetAsync(ctx->d_status, 0, kNumStatus * sizeof(int32_t), st));
-    f64_to_f32_kernel<<<gsz(n * n), 256, 0, st>>>(A, lda, A32, ld32, n, n);
+    B2M_CU(ctx, cudaMemsetAsync(nrm, 0, sizeof(unsigned long long), st));
+    f64_to_f32_norm_kernel<<<(unsigned)std::min<int64_t>(ceil_div(n, 8), 8 * ctx->num_sms), 256, 0, st>>>(
+        A, lda, A32, ld32, n, nrm);
     B2M_LAUNCHED(ctx);
     B2M_TRY(chain_probe(ctx, st));
     B2M_TRY(lu_factor_f32(ctx, st, A32, ld32, n, perm, mode, sc));
-    B2M_CU(ctx, cudaMemsetAsync(nrm, 0, sizeof(unsigned long long), st));
-    norm_inf_kernel<<<gsz(n, 8), 256, 0, st>>>(A, lda, n, nrm);
-    B2M_LAUNCHED(ctx);
     B2M_CU(ctx, cudaMemcpyAsync(ctx->h_status, ctx->d_status, kNumStatus * sizeof(int32_t), cudaMemcpyDeviceToHost, st));
     B2M_CU(ctx, cudaMemcpyAsync(h.data(), nrm, sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
     B2M_CU(ctx, cudaStreamSynchronize(st));

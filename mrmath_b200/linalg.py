@@ -301,9 +301,10 @@ def batch_tune(ctx=None) -> dict:
     """The tile shape the batched solve's autotuner chose for the last plan."""
     vals = [C.c_int32(0) for _ in range(4)]
     ms = C.c_float(0.0)
-    _ctx_of(ctx).call("b2m_batch_tune_read", *[C.addressof(v) for v in vals], C.addressof(ms))
+    c = _ctx_of(ctx)
+    c.call("b2m_batch_tune_read", *[C.addressof(v) for v in vals], C.addressof(ms))
     return {"small_n": vals[0].value, "group_warps": vals[1].value, "pw_large": vals[2].value,
-            "pw_small": vals[3].value, "ms": ms.value}
+            "pw_small": vals[3].value, "big_warps": c.info("batch_big_warps"), "ms": ms.value}
 
 
 def batch_tune_save(path: str, ctx=None) -> None:
