@@ -237,7 +237,7 @@ constexpr int kDsNB = 64;
 constexpr int kDsRhs = 8;
 constexpr int kDsThreads = 128;
 constexpr int kDsMaxRhs = 16;  // right-hand sides per sweep launch
-constexpr int kDsSmem = 2 * kDsNB * kDsNB * (int)sizeof(double);  // T_bb^-1 and W_b, transposed
+constexpr int kDsSmem = 3 * kDsNB * kDsNB * (int)sizeof(double);  // T_bb^-1 and W_b transposed, T_bj
 constexpr int kDsTriSmem = 2 * kDsNB * (kDsNB + 1) * (int)sizeof(double);
 constexpr uint32_t kDsSpin = 1u << 22;
 constexpr unsigned long long kDsEmpty = ~0ull;        // a word not yet published
@@ -250,6 +250,29 @@ __device__ __forceinline__ unsigned long long ds_ld64(const unsigned long long* 
 }
 __device__ __forceinline__ void ds_st64(unsigned long long* p, unsigned long long v) {
     asm volatile("st.relaxed.gpu.global.b64 [%0], %1;\n" ::"l"(p), "l"(v) : "memory");
+}
+__device__ __forceinline__ void cp_async8(void* dst, const void* src, int src_bytes) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(smem_u32(dst)), "l"(src), "r"(src_bytes)
+                 : "memory");
+}
+
+// T_bj (64 x 64, zero past the matrix) into shared memory by asynchronous 8-byte copies that are
+// coalesced along the factor's rows: row-major triangles walk a row per 64 threads, transposed ones
+// a column.  Element (r, c) sits at r * 64 + (c ^ (r & 15)), so that the fold's reads of one column
+// by 32 consecutive rows take two shared-memory wavefronts.
+template <int MODE>
+__device__ __forceinline__ void ds_stage(double* s_tt, const double* LU, int64_t ld, int b0, int bs, int p0, int ps,
+                                         int t) {
+    constexpr bool trans = !(MODE == kTriL || MODE == kTriU);
+#pragma unroll 8
+    for (int i = 0; i < kDsNB * kDsNB / kDsThreads; ++i) {
+        const int e = t + kDsThreads * i;
+        const int rr = trans ? (e & (kDsNB - 1)) : e / kDsNB, cc = trans ? e / kDsNB : (e & (kDsNB - 1));
+        const bool in = rr < bs && cc < ps;
+        const double* src = trans ? LU + (int64_t)(p0 + cc) * ld + b0 + rr : LU + (int64_t)(b0 + rr) * ld + p0 + cc;
+        cp_async8(s_tt + rr * kDsNB + (cc ^ (rr & 15)), in ? src : LU, in ? 8 : 0);
+    }
+    cp_async_commit();
 }
 
 // inverse of the diagonal block b of the triangle (thread per column; zero past the matrix)
@@ -354,6 +377,7 @@ __global__ void __launch_bounds__(kDsThreads) dsweep_kernel(DsArgs a) {
     __shared__ int s_abort;
     double* s_inv = ds_dyn;                    // [k][r]: T_bb^-1 transposed
     double* s_w = ds_dyn + kDsNB * kDsNB;      // [k][r]: W_b transposed
+    double* s_tt = ds_dyn + 2 * kDsNB * kDsNB; // T_bj of the block being folded in (swizzled rows)
     if (a.status[kInfo] != 0) return;
     constexpr bool lower = tri_lower<MODE>();
     const int t = threadIdx.x, r = t & (kDsNB - 1), h = t >> 6;
@@ -398,6 +422,7 @@ __global__ void __launch_bounds__(kDsThreads) dsweep_kernel(DsArgs a) {
             const int idx = t + kDsThreads * e;
             s_p[idx >> 3][idx & 7] = __longlong_as_double((long long)w[e]);
         }
+        cp_async_wait<0>();  // this thread's part of T_bj has landed
         __syncthreads();
         return !s_abort;
     };
@@ -405,18 +430,16 @@ __global__ void __launch_bounds__(kDsThreads) dsweep_kernel(DsArgs a) {
     for (int jj = 0; ok && jj + 1 < bi; ++jj) {
         const int j = lower ? jj : nblk - 1 - jj;
         const int p0 = j * kDsNB, ps = min(kDsNB, a.n - p0);
-        double tv[32];  // this thread's half row of T_bj, all loads in flight
-#pragma unroll
-        for (int k = 0; k < 32; ++k) {
-            const int kk = 32 * h + k;
-            tv[k] = (r < bs && kk < ps) ? tri_at<MODE>(a.LU, a.ld, b0 + r, p0 + kk) : 0.0;
-        }
+        ds_stage<MODE>(s_tt, a.LU, a.ld, b0, bs, p0, ps, t);  // in flight during the wait
         ok = wait_block(j);
         if (!ok) break;
+        const double* trow = s_tt + r * kDsNB;
 #pragma unroll
-        for (int k = 0; k < 32; ++k)
+        for (int k = 0; k < 32; ++k) {
+            const double tv = trow[(32 * h + k) ^ (r & 15)];
 #pragma unroll
-            for (int q = 0; q < kDsRhs; ++q) acc[q] = fma(tv[k], s_p[32 * h + k][q], acc[q]);
+            for (int q = 0; q < kDsRhs; ++q) acc[q] = fma(tv, s_p[32 * h + k][q], acc[q]);
+        }
         __syncthreads();  // s_p is rewritten by the next wait
     }
     if (ok) {

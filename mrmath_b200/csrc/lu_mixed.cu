@@ -152,6 +152,27 @@ __device__ __forceinline__ float4 ld_row4(const float* row, int k, int kmax) {
     return v;
 }
 
+// T_bj (128 x 128, zero past the matrix and in the factors' padding columns) into shared memory by
+// asynchronous 16-byte copies, a row per 32 threads (coalesced).  Float4 c4 of row r sits at
+// r * 128 + 4 (c4 ^ (r & 7)), so that the fold's float4 reads of one column group by 32
+// consecutive rows take four wavefronts, the minimum.  The rows are 16-byte aligned (the FP32
+// factors' leading dimension is a multiple of 32).
+__device__ __forceinline__ void sw_stage(float* s_tt, const float* T, int64_t ld, int b0, int bs, int p0, int ps,
+                                         int t) {
+#pragma unroll 4
+    for (int i = 0; i < kTrsvNB * kTrsvNB / (4 * 256); ++i) {
+        const int e = t + 256 * i;
+        const int rr = e >> 5, c4 = e & 31;
+        const int nb = rr < bs ? 4 * max(0, min(4, ps - 4 * c4)) : 0;
+        const float* src = nb > 0 ? T + (int64_t)(b0 + rr) * ld + p0 + 4 * c4 : T;
+        cp_async16(s_tt + rr * kTrsvNB + 4 * (c4 ^ (rr & 7)), src, nb);
+    }
+    cp_async_commit();
+}
+__device__ __forceinline__ float4 sw_tile4(const float* s_tt, int r, int c4) {
+    return *reinterpret_cast<const float4*>(s_tt + r * kTrsvNB + 4 * (c4 ^ (r & 7)));
+}
+
 __global__ void __launch_bounds__(256) trsv_block_kernel(TrArgs a, int b) {
     __shared__ __align__(16) float s_p[kTrsvNB][kTrMaxRhs];  // solution of block prev
     __shared__ __align__(16) float s_y[kTrsvNB][kTrRhs];
@@ -326,7 +347,7 @@ __global__ void __launch_bounds__(256) trsv_block_kernel(TrArgs a, int b) {
 constexpr int kSwRhs = 8;
 constexpr uint32_t kSwSpin = 1u << 22;
 constexpr uint32_t kSwAbort = 0xFFFFFFFFu;
-constexpr int kSwSmem = 2 * kTrsvNB * kTrsvNB * (int)sizeof(float);  // T_bb^-1 and W_b
+constexpr int kSwSmem = 3 * kTrsvNB * kTrsvNB * (int)sizeof(float);  // T_bb^-1 and W_b, T_bj
 
 struct SwArgs {
     const float* T;
@@ -386,6 +407,7 @@ __global__ void __launch_bounds__(256, 1) trsv_sweep_kernel(SwArgs a) {
     __shared__ int s_abort;
     float4* s_inv = sw_dyn;                        // [32][128]: s_inv[kq][r] = inv[r][4kq .. 4kq+3]
     float4* s_w = sw_dyn + kTrsvNB * kTrsvNB / 4;  // same layout for W_b
+    float* s_tt = reinterpret_cast<float*>(sw_dyn + kTrsvNB * kTrsvNB / 2);  // T_bj being folded in
     const int t = threadIdx.x;
     if (a.status[kInfo] != 0) return;
     const int NB = kTrsvNB;
@@ -446,6 +468,7 @@ __global__ void __launch_bounds__(256, 1) trsv_sweep_kernel(SwArgs a) {
         const float4 v = make_float4(__uint_as_float((uint32_t)w[0]), __uint_as_float((uint32_t)w[1]),
                                      __uint_as_float((uint32_t)w[2]), __uint_as_float((uint32_t)w[3]));
         *reinterpret_cast<float4*>(&s_p[k][q0]) = v;
+        cp_async_wait<0>();  // this thread's part of T_bj has landed
         __syncthreads();
         if (s_abort) {
             abandon();
@@ -454,21 +477,16 @@ __global__ void __launch_bounds__(256, 1) trsv_sweep_kernel(SwArgs a) {
         return true;
     };
 
-    // all blocks before the last one: contributions with T_bj rows from registers
+    // all blocks before the last one: contributions with T_bj staged in shared memory
     for (int jj = 0; jj + 1 < bi; ++jj) {
         const int j = a.upper ? nblk - 1 - jj : jj;
         const int p0 = j * NB, ps = min(NB, a.n - p0);
-        float4 tv[16];
-        {
-            const float* trow = a.T + (int64_t)(b0 + min(r, bs - 1)) * a.ld + p0;
-#pragma unroll
-            for (int i = 0; i < 16; ++i)
-                tv[i] = r < bs ? ld_row4(trow, 64 * h + 4 * i, ps) : make_float4(0.f, 0.f, 0.f, 0.f);
-        }
+        sw_stage(s_tt, a.T, a.ld, b0, bs, p0, ps, t);  // in flight during the wait
         if (!wait_and_stage(j)) return;
 #pragma unroll
         for (int i = 0; i < 16; ++i) {
-            const float tk[4] = {tv[i].x, tv[i].y, tv[i].z, tv[i].w};
+            const float4 tvi = sw_tile4(s_tt, r, 16 * h + i);
+            const float tk[4] = {tvi.x, tvi.y, tvi.z, tvi.w};
 #pragma unroll
             for (int e = 0; e < 4; ++e) {
                 const int k = 64 * h + 4 * i + e;
@@ -560,7 +578,8 @@ __global__ void __cluster_dims__(kChCl, 1, 1) __launch_bounds__(256, 1) trsv_cha
     __shared__ int s_abort;
     float4* s_inv = sw_dyn;                        // [32][128]: s_inv[kq][r] = inv[r][4kq .. 4kq+3]
     float4* s_w = sw_dyn + kTrsvNB * kTrsvNB / 4;  // same layout for W_b
-    float (*s_rx)[kTrsvNB][kSwRhs] = reinterpret_cast<float (*)[kTrsvNB][kSwRhs]>(sw_dyn + kTrsvNB * kTrsvNB / 2);
+    float* s_tt = reinterpret_cast<float*>(sw_dyn + kTrsvNB * kTrsvNB / 2);  // T_bj being folded in
+    float (*s_rx)[kTrsvNB][kSwRhs] = reinterpret_cast<float (*)[kTrsvNB][kSwRhs]>(sw_dyn + 3 * kTrsvNB * kTrsvNB / 4);
     if (a.status[kInfo] != 0) return;  // uniform: written before the launch
     cg::cluster_group cluster = cg::this_cluster();
     const int t = threadIdx.x;
@@ -633,6 +652,7 @@ __global__ void __cluster_dims__(kChCl, 1, 1) __launch_bounds__(256, 1) trsv_cha
         const float4 v = make_float4(__uint_as_float((uint32_t)w[0]), __uint_as_float((uint32_t)w[1]),
                                      __uint_as_float((uint32_t)w[2]), __uint_as_float((uint32_t)w[3]));
         *reinterpret_cast<float4*>(&s_p[k][q0]) = v;
+        cp_async_wait<0>();  // this thread's part of T_bj has landed
         __syncthreads();
         return !s_abort;
     };
@@ -645,6 +665,7 @@ __global__ void __cluster_dims__(kChCl, 1, 1) __launch_bounds__(256, 1) trsv_cha
         }
         if (!ready && !bad) atomicCAS(tmo, 0, 504);
         if (!ready) s_abort = 1;
+        cp_async_wait<0>();  // this thread's part of T_bj has landed
         __syncthreads();
         return !s_abort;
     };
@@ -653,20 +674,15 @@ __global__ void __cluster_dims__(kChCl, 1, 1) __launch_bounds__(256, 1) trsv_cha
     for (int jj = 0; ok && jj + 1 < bi; ++jj) {
         const int j = a.upper ? nblk - 1 - jj : jj;
         const int p0 = j * NB, ps = min(NB, a.n - p0);
-        float4 tv[16];
-        {
-            const float* trow = a.T + (int64_t)(b0 + min(r, bs - 1)) * a.ld + p0;
-#pragma unroll
-            for (int i = 0; i < 16; ++i)
-                tv[i] = r < bs ? ld_row4(trow, 64 * h + 4 * i, ps) : make_float4(0.f, 0.f, 0.f, 0.f);
-        }
+        sw_stage(s_tt, a.T, a.ld, b0, bs, p0, ps, t);  // in flight during the wait
         const bool local = jj >= cl0;
         ok = local ? wait_push(jj - cl0) : wait_global(j);
         if (!ok) break;
         const float (*P)[kSwRhs] = local ? s_rx[jj - cl0] : s_p;
 #pragma unroll
         for (int i = 0; i < 16; ++i) {
-            const float tk[4] = {tv[i].x, tv[i].y, tv[i].z, tv[i].w};
+            const float4 tvi = sw_tile4(s_tt, r, 16 * h + i);
+            const float tk[4] = {tvi.x, tvi.y, tvi.z, tvi.w};
 #pragma unroll
             for (int e = 0; e < 4; ++e) {
                 const int k = 64 * h + 4 * i + e;
@@ -927,7 +943,7 @@ int32_t chain_probe(Ctx* ctx, cudaStream_t st) {
     int why8 = 0, why4 = 0;
     ctx->chain_clusters = chain_probe_one<8>(ctx, st, &why8);
     ctx->chain_clusters4 = chain_probe_one<4>(ctx, st, &why4);
-    ctx->chain_probe_why = why8 ? why8 : why4;
+    ctx->chain_probe_why = (ctx->chain_clusters > 0 || ctx->chain_clusters4 > 0) ? 0 : (why8 ? why8 : why4);
     return B2M_OK;
 }
 
