@@ -58,6 +58,8 @@ def parse():
                    help="solve: the headline (default); gemm / ozaki: m=n=k=8192 FP64 product with the "
                         "g*2^e distribution; batched: 20,000 uneven systems; adjoint: n=4096 gradient step")
     p.add_argument("--mode", type=int, default=0, help="batched: 0 plain FP64, 1 FP32 + FP64 refinement")
+    p.add_argument("--batch-count", type=int, default=20000,
+                   help="batched: number of systems (20,000 is the benchmark; smaller counts size profiler captures)")
     p.add_argument("--cpu-runs", type=int, default=3, help="solves in the CPU-baseline sample (median)")
     return p.parse_args()
 
@@ -482,7 +484,7 @@ def run_secondary(args, world, rank, local):
             config = {"workload": f"C = A B, m=n=k=8192, entries g*2^e (g Gaussian, e uniform in [-8, 8])", "n": n}
             dtype = "f64" if args.workload == "gemm" else "int8 slices -> f64"
         elif args.workload == "batched":
-            sizes, nrhs, mats, rhss = inputs.c5_batched(20000, seed=15 + rank)
+            sizes, nrhs, mats, rhss = inputs.c5_batched(args.batch_count, seed=15 + rank)
             nn, kk, a_off, b_off, Ah, Bh = L.pack_batch(mats, rhss)
             dA, dB = torch.from_numpy(Ah).to(dev), torch.from_numpy(Bh).to(dev)
             dX = torch.zeros_like(dB)
@@ -493,13 +495,13 @@ def run_secondary(args, world, rank, local):
             ms = _timed(fn, args.steps, args.warmup)
             work = sum(inputs.lu_solve_flops(int(x), int(y)) for x, y in zip(nn, kk))
             unit = "GFLOP/s"
-            metric = "batched uneven LU solves GFLOP/s (20,000 systems, n in [8, 256])"
+            metric = f"batched uneven LU solves GFLOP/s ({len(nn):,} systems, n in [8, 256])"
             extra.update({"solves_per_s": len(nn) / (ms / 1e3), "singular": int((info != 0).sum().item()),
                           "tile_shape": L.batch_tune(ctx)})
             if args.mode == 1:
                 it = iters.cpu().numpy()
                 extra.update({"mean_refinement_steps": float(it[it > 0].mean()), "fp64_fallbacks": int((it < 0).sum())})
-            config = {"workload": f"20,000 systems A = R + n I, 1-4 RHS, {'FP64' if args.mode == 0 else 'FP32 + FP64 IR'}",
+            config = {"workload": f"{len(nn):,} systems A = R + n I, 1-4 RHS, {'FP64' if args.mode == 0 else 'FP32 + FP64 IR'}",
                       "count": len(nn), "mode": args.mode}
             dtype = "f64" if args.mode == 0 else "f32 factor + f64 refinement"
         else:  # adjoint

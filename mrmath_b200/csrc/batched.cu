@@ -341,9 +341,18 @@ __device__ void grp_solve(const Grp& g, const Slice& s, const T* W, int n, int k
         for (int bi = 0; bi < nb; ++bi) {
             const int b = lower ? bi : nb - 1 - bi;
             const int b0 = 32 * b, bs = min(32, n - b0);
-            for (int e = g.tid; e < 32 * 32; e += g.nt) {
-                const int r = e >> 5, j = e & 31;
-                blk[r * 33 + j] = (r < bs && j < bs) ? (double)W[(int64_t)s.perm[b0 + r] * n + b0 + j] : 0.0;
+            for (int base = g.tid; base < 32 * 32; base += 4 * g.nt) {  // four loads in flight
+                double v[4];
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    const int e = base + u * g.nt, r = e >> 5, j = e & 31;
+                    v[u] = (e < 32 * 32 && r < bs && j < bs) ? (double)W[(int64_t)s.perm[b0 + r] * n + b0 + j] : 0.0;
+                }
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    const int e = base + u * g.nt;
+                    if (e < 32 * 32) blk[(e >> 5) * 33 + (e & 31)] = v[u];
+                }
             }
             g.sync();
             for (int q = w; q < kk; q += nw) {
@@ -403,9 +412,18 @@ __device__ int solve_plain(const Grp& g, const Slice& s, const BatchArgs& a, int
     const double* A = a.A + a.a_off[sys];
     if (grp_lu<double>(g, s, A, W, n, s.pw)) return 1;
     const double* B = a.B + a.b_off[sys];
-    for (int e = g.tid; e < n * kk; e += g.nt) {
-        const int i = e / kk, q = e - i * kk;
-        s.y[i * kBMaxK + q] = B[(int64_t)s.perm[i] * kk + q];
+    for (int base = g.tid; base < n * kk; base += 4 * g.nt) {  // four loads in flight
+        double v[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int e = base + u * g.nt;
+            v[u] = e < n * kk ? B[(int64_t)s.perm[e / kk] * kk + e % kk] : 0.0;
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int e = base + u * g.nt;
+            if (e < n * kk) s.y[(e / kk) * kBMaxK + e % kk] = v[u];
+        }
     }
     g.sync();
     grp_solve<double>(g, s, W, n, kk);

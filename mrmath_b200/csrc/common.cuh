@@ -268,6 +268,27 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int32_
     return false;
 }
 
+// A strided copy loop "for e = t; e < total; e += NT: put(e, get(e))" whose loads are issued CH at
+// a time before any of their results is used, so that a loop of global loads feeding shared
+// stores pays one memory latency per CH elements instead of one per element.  get(e) is only
+// called for e < total.
+template <int NT, int CH, typename T, typename Get, typename Put>
+__device__ __forceinline__ void batched_copy(int t, int total, Get get, Put put) {
+    for (int base = t; base < total; base += NT * CH) {
+        T v[CH];
+#pragma unroll
+        for (int i = 0; i < CH; ++i) {
+            const int e = base + NT * i;
+            v[i] = e < total ? get(e) : T(0);
+        }
+#pragma unroll
+        for (int i = 0; i < CH; ++i) {
+            const int e = base + NT * i;
+            if (e < total) put(e, v[i]);
+        }
+    }
+}
+
 // 16-byte asynchronous global -> shared copy (src_bytes < 16 zero-fills the rest), its commit
 // group and the wait for all but N groups.
 __device__ __forceinline__ void cp_async16(void* dst, const void* src, int src_bytes) {

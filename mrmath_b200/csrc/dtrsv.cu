@@ -286,7 +286,9 @@ __global__ void __launch_bounds__(kDsNB) dinv_kernel(const double* LU, int64_t l
     constexpr int SP = kDsNB + 1;
     double* s_t = dt_sm;
     double* s_x = dt_sm + kDsNB * SP;
-    for (int r = 0; r < kDsNB; ++r) s_t[r * SP + c] = (r < bs && c < bs) ? tri_at<MODE>(LU, ld, b0 + r, b0 + c) : 0.0;
+    batched_copy<1, 16, double>(0, kDsNB,
+        [&](int r) { return (r < bs && c < bs) ? tri_at<MODE>(LU, ld, b0 + r, b0 + c) : 0.0; },
+        [&](int r, double v) { s_t[r * SP + c] = v; });
     __syncthreads();
     if (lower) {
         for (int i = 0; i < kDsNB; ++i) {
@@ -328,11 +330,14 @@ __global__ void __launch_bounds__(256) dcouple_kernel(const double* LU, int64_t 
     double* s_i = dc_sm;
     double* s_t = dc_sm + kDsNB * SP;
     const int t = threadIdx.x;
-    for (int e = t; e < kDsNB * kDsNB; e += 256) {
-        const int r = e / kDsNB, c = e % kDsNB;
-        s_i[r * SP + c] = inv[(int64_t)b * kDsNB * kDsNB + e];
-        s_t[r * SP + c] = (r < bs && c < ps) ? tri_at<MODE>(LU, ld, b0 + r, p0 + c) : 0.0;
-    }
+    batched_copy<256, 8, double>(t, kDsNB * kDsNB, [&](int e) { return inv[(int64_t)b * kDsNB * kDsNB + e]; },
+                                 [&](int e, double v) { s_i[(e / kDsNB) * SP + e % kDsNB] = v; });
+    batched_copy<256, 8, double>(t, kDsNB * kDsNB,
+        [&](int e) {
+            const int r = e / kDsNB, c = e % kDsNB;
+            return (r < bs && c < ps) ? tri_at<MODE>(LU, ld, b0 + r, p0 + c) : 0.0;
+        },
+        [&](int e, double v) { s_t[(e / kDsNB) * SP + e % kDsNB] = v; });
     __syncthreads();
     const int r0 = 4 * (t >> 4), c0 = t & 15;
     double acc[4][4] = {};

@@ -160,10 +160,12 @@ __global__ void __launch_bounds__(kSuThreads)
     __shared__ T s_l[kPanelW][kPanelW + 1];  // L11 (strictly lower part), s_l[j][i] = L(c0 + j, c0 + i)
     if (status[kInfo] != 0) return;
     const int tid = threadIdx.x, lane = tid & 31;
-    for (int e = tid; e < kPanelW * kPanelW; e += kSuThreads) {
-        const int j = e / kPanelW, i = e - j * kPanelW;
-        s_l[j][i] = (i < j && j < w) ? A[(int64_t)(c0 + j) * ld + c0 + i] : T(0);
-    }
+    batched_copy<kSuThreads, kPanelW * kPanelW / kSuThreads, T>(tid, kPanelW * kPanelW,
+        [&](int e) {
+            const int j = e / kPanelW, i = e - j * kPanelW;
+            return (i < j && j < w) ? A[(int64_t)(c0 + j) * ld + c0 + i] : T(0);
+        },
+        [&](int e, T v) { s_l[e / kPanelW][e % kPanelW] = v; });
     if (tid < 32) {
         if (lane < w) src_main[lane] = c0 + lane;
         __syncwarp();
@@ -268,16 +270,18 @@ __global__ void __launch_bounds__(256, 2) panel_rank_update_kernel(double* A, in
     if (status[kInfo] != 0) return;
     const int t = threadIdx.x, tx = t & 15, ty = t >> 4;
     const int r0 = r_lo + blockIdx.y * kRuT, cb = cl + blockIdx.x * kRuT;
-    for (int e = t; e < kRuT * kPanelW; e += 256) {
-        const int rr = e >> 5, k = e & 31;
-        const int row = r0 + rr;
-        s_a[rr][k] = (row < n && k < w) ? A[(int64_t)row * ld + c0 + k] : 0.0;
-    }
-    for (int e = t; e < kPanelW * kRuT; e += 256) {
-        const int k = e / kRuT, cc = e - k * kRuT;
-        const int col = cb + cc;
-        s_b[k][cc] = (k < w && col < ch) ? A[(int64_t)(c0 + k) * ld + col] : 0.0;
-    }
+    batched_copy<256, kRuT * kPanelW / 256, double>(t, kRuT * kPanelW,
+        [&](int e) {
+            const int rr = e >> 5, k = e & 31, row = r0 + rr;
+            return (row < n && k < w) ? A[(int64_t)row * ld + c0 + k] : 0.0;
+        },
+        [&](int e, double v) { s_a[e >> 5][e & 31] = v; });
+    batched_copy<256, kPanelW * kRuT / 256, double>(t, kPanelW * kRuT,
+        [&](int e) {
+            const int k = e / kRuT, col = cb + e % kRuT;
+            return (k < w && col < ch) ? A[(int64_t)(c0 + k) * ld + col] : 0.0;
+        },
+        [&](int e, double v) { s_b[e / kRuT][e % kRuT] = v; });
     // the tile's own values, loaded while the slices arrive
     double c[4][4];
 #pragma unroll
@@ -351,10 +355,12 @@ __global__ void __launch_bounds__(256, 1) trsm_panel_kernel(const double* L, int
         cp_async_commit();
     };
     stage(0);
-    for (int e = t; e < kTpK * kTpC; e += 256) {
-        const int r = e / kTpC, c = e - r * kTpC;
-        s_x[e] = (r < k && cb + c < ncols) ? B[(int64_t)r * ldb + cb + c] : 0.0;
-    }
+    batched_copy<256, 8, double>(t, kTpK * kTpC,
+        [&](int e) {
+            const int r = e / kTpC, c = e - r * kTpC;
+            return (r < k && cb + c < ncols) ? B[(int64_t)r * ldb + cb + c] : 0.0;
+        },
+        [&](int e, double v) { s_x[e] = v; });
     for (int i = 0; i < nb; ++i) {
         if (i + 1 < nb) {
             stage(i + 1);

@@ -73,26 +73,35 @@ __device__ __forceinline__ float rcp_nr(float x) {
 // One column per iteration of a runtime loop (a compact body: unrolled multi-column steps spill
 // out of the instruction cache).  Register indices stay compile-time because every row shifts
 // left by one as its column is eliminated (the update writes v[k - 1]), so the current column is
-// always v[0].  One barrier per column: every warp's best lane publishes its candidate row (and
-// key) before the barrier (double-buffered by column parity); afterwards all threads pick the
-// winning warp with a warp reduction over the keys and read its row directly.  For the root
-// (lm given) the winner of column j is copied to s_u[j] (row j of U, from column j on) and every
-// row's multiplier of column j goes to lm[j][stack index] (global scratch), which gives the rows
-// of L; keeping them out of shared memory lets the CTA share an SM with a tensor-core GEMM.
+// always v[0].  One barrier per column: before it, every warp's best lane publishes its candidate
+// row, the reciprocal of its pivot value (computed by every lane while the warp reduction runs,
+// so it is off the chain) and its stack slot (double-buffered by column parity), and folds its key
+// into a shared maximum (atomicMax on the magnitude's bit pattern with the warp in the low 3 bits,
+// so the lowest warp wins among magnitudes that agree to 2^-20); after it, every thread reads the
+// maximum and then the winning row directly, with no further reduction.  The maximum words rotate
+// through three slots: thread 0 clears the one of column j + 2 after the barrier of column j, when
+// every read of it (column j - 1) is done and before any write (column j + 2).  For the root (lm
+// given) the winner of column j is copied to s_u[j] (row j of U, from column j on) and every row's
+// multiplier of column j goes to lm[j][stack index] (global scratch), which gives the rows of L;
+// keeping them out of shared memory lets the CTA share an SM with a tensor-core GEMM.
 struct GeppSmem {
-    float4 cand[2][kTsThreads / 32][8];  // candidate rows by column parity and warp (column j first)
-    unsigned key[2][kTsThreads / 32];
-    unsigned slot[2][kTsThreads / 32];
+    float4 cand[2][kTsThreads / 32][9];  // candidate rows by column parity and warp (column j first),
+                                         // then (reciprocal of the pivot, stack slot, -, -)
+    unsigned best[3];                    // packed maximum key of columns j, j + 1, j + 2 (mod 3)
     float4 u[32][8];                     // root: pivot rows as chosen
 };
 
 __device__ __forceinline__ void block_gepp(float (&v)[kTsRpt][32], const int (&rid)[kTsRpt], int w, int* s_win,
                                            int* s_loc, GeppSmem& g, float* lm) {
+    static_assert(kTsThreads / 32 <= 8, "the warp index must fit the key's low 3 bits");
     const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
     bool live[kTsRpt];
 #pragma unroll
     for (int r = 0; r < kTsRpt; ++r) live[r] = rid[r] >= 0;
     if (t < 32) { s_win[t] = -1; s_loc[t] = -1; }
+    if (t < 3) g.best[t] = 0u;
+    __syncthreads();
+    int b3 = 0;
 #pragma unroll 1
     for (int j = 0; j < w; ++j) {
         const int b = j & 1;
@@ -103,9 +112,13 @@ __device__ __forceinline__ void block_gepp(float (&v)[kTsRpt][32], const int (&r
             const unsigned k = live[r] ? __float_as_uint(fabsf(v[r][0])) + 1u : 0u;
             if (k > key) { key = k; rbest = r; }
         }
+        float vsel = v[0][0];
+#pragma unroll
+        for (int r = 1; r < kTsRpt; ++r) vsel = rbest == r ? v[r][0] : vsel;
+        const float rc = key > 1u ? rcp_nr(vsel) : 0.0f;  // a zero column eliminates nothing
         const unsigned wk = __reduce_max_sync(0xffffffffu, key);
         const unsigned bal = __ballot_sync(0xffffffffu, key == wk && key != 0u);
-        if (lane == (bal ? __ffs(bal) - 1 : 0)) {
+        if (wk != 0u && lane == __ffs(bal) - 1) {
 #pragma unroll
             for (int r = 0; r < kTsRpt; ++r) {
                 if (r == rbest) {
@@ -114,24 +127,25 @@ __device__ __forceinline__ void block_gepp(float (&v)[kTsRpt][32], const int (&r
                         g.cand[b][warp][q] = make_float4(v[r][4 * q], v[r][4 * q + 1], v[r][4 * q + 2], v[r][4 * q + 3]);
                 }
             }
-            g.key[b][warp] = wk;
-            g.slot[b][warp] = (unsigned)(rbest * kTsThreads + t);
+            g.cand[b][warp][8] = make_float4(rc, __uint_as_float((unsigned)(rbest * kTsThreads + t)), 0.f, 0.f);
+            atomicMax(&g.best[b3], ((wk > 8u ? wk : 8u) & ~7u) | (unsigned)(7 - warp));
         }
         __syncthreads();
-        // winning warp: largest key, lowest warp among equals
-        const unsigned kq = g.key[b][lane & (kTsThreads / 32 - 1)];
-        const unsigned pk = __reduce_max_sync(0xffffffffu, kq);
+        const unsigned pk = g.best[b3];
+        if (t == 0) g.best[b3 == 0 ? 2 : b3 - 1] = 0u;  // the slot of column j + 2
+        b3 = b3 == 2 ? 0 : b3 + 1;
         if (pk == 0u) break;  // no live row left anywhere (uniform)
-        const int pwarp = __ffs(__ballot_sync(0xffffffffu, kq == pk)) - 1;
-        const unsigned ps = g.slot[b][pwarp];
+        const int pwarp = 7 - (int)(pk & 7u);
         float pr[32];
 #pragma unroll
         for (int q = 0; q < 8; ++q) {
             const float4 f = g.cand[b][pwarp][q];
             pr[4 * q] = f.x; pr[4 * q + 1] = f.y; pr[4 * q + 2] = f.z; pr[4 * q + 3] = f.w;
         }
+        const float4 meta = g.cand[b][pwarp][8];
+        const float rcp = meta.x;
+        const unsigned ps = __float_as_uint(meta.y);
         if (lm && t < 8) g.u[j][t] = g.cand[b][pwarp][t];
-        const float rcp = pk > 1u ? rcp_nr(pr[0]) : 0.0f;  // a zero column eliminates nothing
 #pragma unroll
         for (int r = 0; r < kTsRpt; ++r) {
             if (ps == (unsigned)(r * kTsThreads + t)) {
@@ -223,21 +237,23 @@ __global__ void __launch_bounds__(kTsThreads) tslu_select_kernel(TsArgs a) {
 
     // ---- root: pivots s_win[0..w); rows of L\U from the multipliers and the published pivot rows
     const int lc0 = a.lc0, w = a.w;
-    for (int e = t; e < 32 * 32; e += kTsThreads) {
-        const int j = e >> 5, k = e & 31;
-        const int l = s_loc[j];
-        float x = 0.f;
-        if (j < w && l >= 0 && k < w) {
-            if (k < j) {
-                x = __ldcg(a.lmul + k * kTsRows + l);
-            } else {
-                const float4 f = s_g.u[j][(k - j) >> 2];
-                const int e4 = (k - j) & 3;
-                x = e4 == 0 ? f.x : e4 == 1 ? f.y : e4 == 2 ? f.z : f.w;
+    batched_copy<kTsThreads, 32 * 32 / kTsThreads, float>(t, 32 * 32,
+        [&](int e) {
+            const int j = e >> 5, k = e & 31;
+            const int l = s_loc[j];
+            float x = 0.f;
+            if (j < w && l >= 0 && k < w) {
+                if (k < j) {
+                    x = __ldcg(a.lmul + k * kTsRows + l);
+                } else {
+                    const float4 f = s_g.u[j][(k - j) >> 2];
+                    const int e4 = (k - j) & 3;
+                    x = e4 == 0 ? f.x : e4 == 1 ? f.y : e4 == 2 ? f.z : f.w;
+                }
             }
-        }
-        s_lu[j][k] = x;
-    }
+            return x;
+        },
+        [&](int e, float x) { s_lu[e >> 5][e & 31] = x; });
     __syncthreads();
     if (t < 32) {
         const bool bad = t < w && (s_win[t] < 0 || !(fabsf(s_lu[t][t]) > 10.0f / FLT_MAX));
@@ -607,8 +623,9 @@ __global__ void diag_inv_kernel(const float* LU, int64_t ld, int n, int nb, floa
     float* s_t = sm;             // [nb][SP] the triangle
     float* s_x = sm + nb * SP;   // [nb][SP] the inverse, column c owned by thread c
     const int c = threadIdx.x;
-    for (int r = 0; r < bs; ++r)
-        if (c < bs) s_t[r * SP + c] = LU[(int64_t)(b0 + r) * ld + b0 + c];
+    if (c < bs)
+        batched_copy<1, 16, float>(0, bs, [&](int r) { return LU[(int64_t)(b0 + r) * ld + b0 + c]; },
+                                   [&](int r, float v) { s_t[r * SP + c] = v; });
     __syncthreads();
     if (c < nb) {
         if (!upper) {
@@ -655,11 +672,14 @@ __global__ void __launch_bounds__(256) coupling_kernel(const float* LU, int64_t 
     float* s_t = sm + NB * kCpPitch; // [128][kCpPitch] T_{b,p}
     const float* inv = (upper ? uinv : linv) + (int64_t)blk * NB * NB;
     const int t = threadIdx.x;
-    for (int e = t; e < NB * NB; e += 256) {
-        const int r = e >> 7, c = e & (NB - 1);
-        s_i[r * kCpPitch + c] = inv[e];
-        s_t[r * kCpPitch + c] = (r < bs && c < ps) ? LU[(int64_t)(b0 + r) * ld + p0 + c] : 0.f;
-    }
+    batched_copy<256, 8, float>(t, NB * NB, [&](int e) { return inv[e]; },
+                                [&](int e, float v) { s_i[(e >> 7) * kCpPitch + (e & (NB - 1))] = v; });
+    batched_copy<256, 8, float>(t, NB * NB,
+        [&](int e) {
+            const int r = e >> 7, c = e & (NB - 1);
+            return (r < bs && c < ps) ? LU[(int64_t)(b0 + r) * ld + p0 + c] : 0.f;
+        },
+        [&](int e, float v) { s_t[(e >> 7) * kCpPitch + (e & (NB - 1))] = v; });
     __syncthreads();
     const int r0 = 8 * (t >> 4), c0 = t & 15;
     float acc[8][8];
