@@ -27,31 +27,38 @@ __global__ void scatter_rows_kernel(double* Lam, int64_t ldl, const double* Y, i
     Lam[(int64_t)perm[i] * ldl + c] = Y[i * ldy + c];
 }
 
-// dA[i][j] (op)= -sum_c Lam[i][c] X[j][c] over columns c in [c0, c0 + kc)
+// dA[i][j] (op)= -sum_c Lam[i][c] X[j][c] over columns c in [c0, c0 + kc), kc <= KC (the products
+// run over KC columns, the ones past kc being zero: KC is the smallest of 1, 4, 32 that holds kc,
+// so that a single right-hand side costs one FMA per entry and the kernel stays bound by the write)
+template <int KC>
 __global__ void __launch_bounds__(kRkCols) rank_update_kernel(double* dA, int64_t ldd, const double* Lam, int64_t ldl,
                                                               const double* X, int64_t ldx, int64_t n, int c0, int kc,
                                                               int accumulate) {
-    __shared__ double s_l[kRkRows][kRkK];
+    __shared__ double s_l[kRkRows][KC];
     const int t = threadIdx.x;
     const int64_t i0 = (int64_t)blockIdx.y * kRkRows;
     const int64_t j = (int64_t)blockIdx.x * kRkCols + t;
-    for (int e = t; e < kRkRows * kRkK; e += kRkCols) {
-        const int r = e / kRkK, c = e - r * kRkK;
+    for (int e = t; e < kRkRows * KC; e += kRkCols) {
+        const int r = e / KC, c = e - r * KC;
         s_l[r][c] = (i0 + r < n && c < kc) ? Lam[(i0 + r) * ldl + c0 + c] : 0.0;
     }
-    double xj[kRkK];
+    double xj[KC];
 #pragma unroll
-    for (int c = 0; c < kRkK; ++c) xj[c] = (j < n && c < kc) ? X[j * ldx + c0 + c] : 0.0;
+    for (int c = 0; c < KC; ++c) xj[c] = (j < n && c < kc) ? X[j * ldx + c0 + c] : 0.0;
     __syncthreads();
     if (j >= n) return;
-#pragma unroll 4
+    double old[kRkRows];
+    if (accumulate) {
+#pragma unroll
+        for (int r = 0; r < kRkRows; ++r) old[r] = i0 + r < n ? dA[(i0 + r) * ldd + j] : 0.0;
+    }
+#pragma unroll
     for (int r = 0; r < kRkRows; ++r) {
         if (i0 + r >= n) break;
         double acc = 0.0;
 #pragma unroll
-        for (int c = 0; c < kRkK; ++c) acc = fma(s_l[r][c], xj[c], acc);
-        double* p = dA + (i0 + r) * ldd + j;
-        *p = accumulate ? *p - acc : -acc;
+        for (int c = 0; c < KC; ++c) acc = fma(s_l[r][c], xj[c], acc);
+        dA[(i0 + r) * ldd + j] = accumulate ? old[r] - acc : -acc;
     }
 }
 
@@ -63,8 +70,7 @@ int32_t solve_adjoint_f64(Ctx* ctx, cudaStream_t st, const double* LU, int64_t l
     if (n <= 0 || nrhs <= 0) return B2M_OK;
     // Y = G; Y <- U^{-T} Y; Y <- L^{-T} Y; Lambda = P^T Y
     B2M_TRY(copy_matrix(ctx, st, Y, ldy * 8, G, ldg * 8, n, nrhs));
-    B2M_TRY(tri_solve_f64(ctx, st, LU, ld, n, kTriUt, Y, ldy, nrhs));
-    B2M_TRY(tri_solve_f64(ctx, st, LU, ld, n, kTriLt, Y, ldy, nrhs));
+    B2M_TRY(tri_solve2_f64(ctx, st, LU, ld, n, kTriUt, kTriLt, Y, ldy, nrhs));
     scatter_rows_kernel<<<(unsigned)ceil_div(n * nrhs, 256), 256, 0, st>>>(Lam, ldl, Y, ldy, perm, n, nrhs,
                                                                             ctx->d_status);
     B2M_LAUNCHED(ctx);
@@ -74,7 +80,12 @@ int32_t solve_adjoint_f64(Ctx* ctx, cudaStream_t st, const double* LU, int64_t l
         const int acc = (op == B2M_DO_ADD || c0 > 0) ? 1 : 0;
         dim3 grid((unsigned)ceil_div(n, kRkCols), (unsigned)ceil_div(n, kRkRows));
         prof_begin(ctx, st, kClsOther);
-        rank_update_kernel<<<grid, kRkCols, 0, st>>>(dA, ldd, Lam, ldl, X, ldx, n, (int)c0, kc, acc);
+        if (kc == 1)
+            rank_update_kernel<1><<<grid, kRkCols, 0, st>>>(dA, ldd, Lam, ldl, X, ldx, n, (int)c0, kc, acc);
+        else if (kc <= 4)
+            rank_update_kernel<4><<<grid, kRkCols, 0, st>>>(dA, ldd, Lam, ldl, X, ldx, n, (int)c0, kc, acc);
+        else
+            rank_update_kernel<kRkK><<<grid, kRkCols, 0, st>>>(dA, ldd, Lam, ldl, X, ldx, n, (int)c0, kc, acc);
         prof_end(ctx, st, kClsOther, 8.0 * n * n * (acc ? 2 : 1) + 16.0 * n * kc);  // bytes: dA once
         B2M_LAUNCHED(ctx);
     }

@@ -192,8 +192,7 @@ int32_t chol_solve_f64(Ctx* ctx, cudaStream_t st, const double* F, int64_t ldf, 
     B2M_CU(ctx, cudaMemcpy2DAsync(W, ldw * 8, F, ldf * 8, n * 8, n, cudaMemcpyDeviceToDevice, st));
     mirror_lower_kernel<<<blocks_for(n * n), 256, 0, st>>>(W, ldw, n);
     B2M_LAUNCHED(ctx);
-    B2M_TRY(tri_solve_f64(ctx, st, W, ldw, n, kTriUt, B, ldb, nrhs));
-    return tri_solve_f64(ctx, st, W, ldw, n, kTriU, B, ldb, nrhs);
+    return tri_solve2_f64(ctx, st, W, ldw, n, kTriUt, kTriU, B, ldb, nrhs);
 }
 
 int32_t copy_lower(Ctx* ctx, cudaStream_t st, double* dst, int64_t ldd, const double* src, int64_t lds, int64_t n,

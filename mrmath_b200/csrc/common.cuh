@@ -119,6 +119,8 @@ struct Ctx {
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     cudaStream_t side_stream = nullptr;                  // look-ahead trailing updates of the FP32 LU
     cudaEvent_t ev_side_fork = nullptr, ev_side_join = nullptr;
+    cudaStream_t leaf_stream = nullptr;  // FP64 LU: a leaf's work on its outer panel beyond the next leaf
+    cudaEvent_t ev_leaf_panel = nullptr, ev_leaf_side = nullptr;
     int chain_priority = 0;                               // stream priority of the panel kernels
     bool launch_hi = false;  // launch_k adds the launch attribute `priority = chain_priority` (PriorityScope)
     std::string last_error;
@@ -246,6 +248,14 @@ __device__ __forceinline__ void fence_proxy_async() {
 }
 __device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t bytes) {
     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+// bulk (non-tensor) asynchronous copy of `bytes` (a multiple of 16, both addresses 16-byte
+// aligned) from global memory into this CTA's shared memory, completing on `bar`
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
+                     smem_u32(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_u32(bar))
                  : "memory");
 }
 __device__ __forceinline__ void mbar_arrive(uint64_t* bar) {

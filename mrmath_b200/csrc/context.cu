@@ -39,6 +39,7 @@ int32_t ws_get(Ctx* ctx, int slot, size_t bytes, void** out) {
             B2M_CU(ctx, cudaStreamSynchronize(ctx->stream));
             if (ctx->own_stream) B2M_CU(ctx, cudaStreamSynchronize(ctx->own_stream));
             if (ctx->side_stream) B2M_CU(ctx, cudaStreamSynchronize(ctx->side_stream));
+            if (ctx->leaf_stream) B2M_CU(ctx, cudaStreamSynchronize(ctx->leaf_stream));
             for (auto& g : ctx->graphs) cudaGraphExecDestroy(g.second.exec);
             ctx->graphs.clear();
             B2M_CU(ctx, cudaFree(ctx->ws[slot]));
@@ -261,6 +262,9 @@ extern "C" int32_t b2m_destroy(b2m_ctx* h) {
     if (ctx->d_status) cudaFree(ctx->d_status);
     if (ctx->h_status) cudaFreeHost(ctx->h_status);
     if (ctx->side_stream) cudaStreamDestroy(ctx->side_stream);
+    if (ctx->leaf_stream) cudaStreamDestroy(ctx->leaf_stream);
+    if (ctx->ev_leaf_panel) cudaEventDestroy(ctx->ev_leaf_panel);
+    if (ctx->ev_leaf_side) cudaEventDestroy(ctx->ev_leaf_side);
     if (ctx->ev_side_fork) cudaEventDestroy(ctx->ev_side_fork);
     if (ctx->ev_side_join) cudaEventDestroy(ctx->ev_side_join);
     if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);

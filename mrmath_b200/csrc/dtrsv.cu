@@ -237,7 +237,8 @@ constexpr int kDsNB = 64;
 constexpr int kDsRhs = 8;
 constexpr int kDsThreads = 128;
 constexpr int kDsMaxRhs = 16;  // right-hand sides per sweep launch
-constexpr int kDsSmem = 3 * kDsNB * kDsNB * (int)sizeof(double);  // T_bb^-1 and W_b transposed, T_bj
+constexpr int kDsTS = kDsNB + 2;  // line stride of the staged T_bj (528 bytes: 16-byte aligned lines)
+constexpr int kDsSmem = (2 * kDsNB * kDsNB + kDsNB * kDsTS) * (int)sizeof(double);  // T_bb^-1, W_b, T_bj
 constexpr int kDsTriSmem = 2 * kDsNB * (kDsNB + 1) * (int)sizeof(double);
 constexpr uint32_t kDsSpin = 1u << 22;
 constexpr unsigned long long kDsEmpty = ~0ull;        // a word not yet published
@@ -256,23 +257,35 @@ __device__ __forceinline__ void cp_async8(void* dst, const void* src, int src_by
                  : "memory");
 }
 
-// T_bj (64 x 64, zero past the matrix) into shared memory by asynchronous 8-byte copies that are
-// coalesced along the factor's rows: row-major triangles walk a row per 64 threads, transposed ones
-// a column.  Element (r, c) sits at r * 64 + (c ^ (r & 15)), so that the fold's reads of one column
-// by 32 consecutive rows take two shared-memory wavefronts.
+// T_bj (64 x 64) into shared memory as 64 lines of kDsTS doubles: line r holds row r of T_bj for the
+// row-major triangles (L, U), line c holds column c for the transposed ones (U^T, L^T) -- in both
+// cases a 512-byte run of one row of the factors.  A full block whose lines are 16-byte aligned
+// comes in as 64 bulk copies (one instruction per line) completing on `bar`; otherwise
+// asynchronous 8-byte copies, zero past the matrix.  The fold reads column k of T_bj across 32
+// consecutive rows with at most four shared-memory wavefronts.
 template <int MODE>
-__device__ __forceinline__ void ds_stage(double* s_tt, const double* LU, int64_t ld, int b0, int bs, int p0, int ps,
-                                         int t) {
+__device__ __forceinline__ bool ds_stage(double* s_tt, const double* LU, int64_t ld, int b0, int bs, int p0, int ps,
+                                         int t, bool bulk_ok, uint64_t* bar) {
     constexpr bool trans = !(MODE == kTriL || MODE == kTriU);
+    if (bulk_ok && bs == kDsNB && ps == kDsNB) {
+        if (t == 0) mbar_arrive_expect_tx(bar, kDsNB * kDsNB * (int)sizeof(double));
+        if (t < kDsNB) {
+            const double* src = trans ? LU + (int64_t)(p0 + t) * ld + b0 : LU + (int64_t)(b0 + t) * ld + p0;
+            bulk_g2s(s_tt + t * kDsTS, src, kDsNB * (int)sizeof(double), bar);
+        }
+        return true;
+    }
 #pragma unroll 8
     for (int i = 0; i < kDsNB * kDsNB / kDsThreads; ++i) {
         const int e = t + kDsThreads * i;
-        const int rr = trans ? (e & (kDsNB - 1)) : e / kDsNB, cc = trans ? e / kDsNB : (e & (kDsNB - 1));
+        const int line = e / kDsNB, pos = e & (kDsNB - 1);  // pos runs along the factors' row
+        const int rr = trans ? pos : line, cc = trans ? line : pos;
         const bool in = rr < bs && cc < ps;
         const double* src = trans ? LU + (int64_t)(p0 + cc) * ld + b0 + rr : LU + (int64_t)(b0 + rr) * ld + p0 + cc;
-        cp_async8(s_tt + rr * kDsNB + (cc ^ (rr & 15)), in ? src : LU, in ? 8 : 0);
+        cp_async8(s_tt + line * kDsTS + pos, in ? src : LU, in ? 8 : 0);
     }
     cp_async_commit();
+    return false;
 }
 
 // inverse of the diagonal block b of the triangle (thread per column; zero past the matrix)
@@ -371,6 +384,7 @@ struct DsArgs {
     unsigned long long* pub;  // [nblk][ng][64][8] published blocks (double bits; preset to kDsEmpty)
     int32_t* status;
     uint32_t spin;
+    bool bulk;  // the factors' rows are 16-byte aligned: full blocks are staged by bulk copies
 };
 
 template <int MODE>
@@ -382,7 +396,8 @@ __global__ void __launch_bounds__(kDsThreads) dsweep_kernel(DsArgs a) {
     __shared__ int s_abort;
     double* s_inv = ds_dyn;                    // [k][r]: T_bb^-1 transposed
     double* s_w = ds_dyn + kDsNB * kDsNB;      // [k][r]: W_b transposed
-    double* s_tt = ds_dyn + 2 * kDsNB * kDsNB; // T_bj of the block being folded in (swizzled rows)
+    double* s_tt = ds_dyn + 2 * kDsNB * kDsNB; // T_bj of the block being folded in (kDsNB lines of kDsTS)
+    __shared__ __align__(8) uint64_t s_tbar;   // completion of a bulk-staged T_bj
     if (a.status[kInfo] != 0) return;
     constexpr bool lower = tri_lower<MODE>();
     const int t = threadIdx.x, r = t & (kDsNB - 1), h = t >> 6;
@@ -402,10 +417,18 @@ __global__ void __launch_bounds__(kDsThreads) dsweep_kernel(DsArgs a) {
         xb[q] = (h == 0 && r < bs && q < ncg) ? a.X[(int64_t)(b0 + r) * a.ldx + cg + q] : 0.0;
         acc[q] = 0.0;
     }
-    if (t == 0) s_abort = 0;
+    if (t == 0) {
+        s_abort = 0;
+        mbar_init(&s_tbar, 1);
+        fence_barrier_init();
+    }
     __syncthreads();
-    // block j published: its 64 x 8 values into s_p (thread t polls words t, t + 128, ...)
-    auto wait_block = [&](int j) -> bool {
+    uint32_t tphase = 0;
+    constexpr bool trans = !(MODE == kTriL || MODE == kTriU);
+    // block j published: its 64 x 8 values into s_p (thread t polls words t, t + 128, ...); also
+    // completes this thread's part of a staged T_bj (the bulk copies even when the wait gives up, so
+    // that no copy is in flight when the CTA leaves)
+    auto wait_block = [&](int j, bool bulk_staged) -> bool {
         const unsigned long long* src = a.pub + (size_t)(j * ng + g) * (kDsNB * kDsRhs);
         unsigned long long w[4];
         bool ready = false, bad = false;
@@ -428,6 +451,10 @@ __global__ void __launch_bounds__(kDsThreads) dsweep_kernel(DsArgs a) {
             s_p[idx >> 3][idx & 7] = __longlong_as_double((long long)w[e]);
         }
         cp_async_wait<0>();  // this thread's part of T_bj has landed
+        if (bulk_staged) {
+            if (!mbar_wait(&s_tbar, tphase, &a.status[kTimeout], 506)) s_abort = 1;
+            tphase ^= 1u;
+        }
         __syncthreads();
         return !s_abort;
     };
@@ -435,13 +462,14 @@ __global__ void __launch_bounds__(kDsThreads) dsweep_kernel(DsArgs a) {
     for (int jj = 0; ok && jj + 1 < bi; ++jj) {
         const int j = lower ? jj : nblk - 1 - jj;
         const int p0 = j * kDsNB, ps = min(kDsNB, a.n - p0);
-        ds_stage<MODE>(s_tt, a.LU, a.ld, b0, bs, p0, ps, t);  // in flight during the wait
-        ok = wait_block(j);
+        // T_bj is staged while this CTA waits for x_j
+        const bool bulk = ds_stage<MODE>(s_tt, a.LU, a.ld, b0, bs, p0, ps, t, a.bulk, &s_tbar);
+        ok = wait_block(j, bulk);
         if (!ok) break;
-        const double* trow = s_tt + r * kDsNB;
 #pragma unroll
         for (int k = 0; k < 32; ++k) {
-            const double tv = trow[(32 * h + k) ^ (r & 15)];
+            const int kk = 32 * h + k;
+            const double tv = trans ? s_tt[kk * kDsTS + r] : s_tt[r * kDsTS + kk];
 #pragma unroll
             for (int q = 0; q < kDsRhs; ++q) acc[q] = fma(tv, s_p[32 * h + k][q], acc[q]);
         }
@@ -469,7 +497,7 @@ __global__ void __launch_bounds__(kDsThreads) dsweep_kernel(DsArgs a) {
             for (int q = 0; q < kDsRhs; ++q) acc[q] = fma(m, s_y[kk][q], acc[q]);
         }
         if (bi > 0) {  // x_b = z - W_b x_p
-            ok = wait_block(lower ? b - 1 : b + 1);
+            ok = wait_block(lower ? b - 1 : b + 1, false);
             if (ok) {
 #pragma unroll 8
                 for (int k = 0; k < 32; ++k) {
@@ -505,11 +533,12 @@ __global__ void __launch_bounds__(kDsThreads) dsweep_kernel(DsArgs a) {
     }
 }
 
+// whether the persistent sweep of this triangle can run for nrhs right-hand sides (every CTA
+// co-resident with the others); sets the kernels' shared-memory attributes once per device
 template <int MODE>
-int32_t launch_chain(Ctx* ctx, cudaStream_t st, const double* LU, int64_t ld, int64_t n, double* X, int64_t ldx,
-                     int64_t nrhs, bool* used) {
-    *used = false;
-    const int nblk = (int)ceil_div(n, kDsNB);
+int32_t chain_usable(Ctx* ctx, int64_t n, int64_t nrhs, bool* usable) {
+    *usable = false;
+    if (n <= 2 * kDsNB) return B2M_OK;
     std::atomic<int>& attr = device_flag((const void*)dsweep_kernel<MODE>, 0, ctx->device);
     if (!attr.load()) {
         B2M_CU(ctx, cudaFuncSetAttribute(dsweep_kernel<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, kDsSmem));
@@ -523,15 +552,20 @@ int32_t launch_chain(Ctx* ctx, cudaStream_t st, const double* LU, int64_t ld, in
         B2M_CU(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, dsweep_kernel<MODE>, kDsThreads, kDsSmem));
         ctx->dsweep_ctas = coop ? per_sm * ctx->num_sms : 0;
     }
+    const int nblk = (int)ceil_div(n, kDsNB);
     const int ngmax = (int)ceil_div(std::min<int64_t>(nrhs, kDsMaxRhs), kDsRhs);
-    if ((int64_t)nblk * ngmax > ctx->dsweep_ctas) return B2M_OK;  // not co-resident: per-block launches
-    const size_t blk_doubles = (size_t)nblk * kDsNB * kDsNB;
-    const size_t pub_doubles = (size_t)nblk * 2 * kDsNB * kDsRhs;
-    void* p = nullptr;
-    B2M_TRY(ws_get(ctx, kWsTri, (2 * blk_doubles + pub_doubles) * sizeof(double), &p));
-    double* inv = static_cast<double*>(p);
-    double* w = inv + blk_doubles;
-    unsigned long long* pub = reinterpret_cast<unsigned long long*>(w + blk_doubles);
+    *usable = (int64_t)nblk * ngmax <= ctx->dsweep_ctas;
+    return B2M_OK;
+}
+
+size_t chain_blk_doubles(int64_t n) { return (size_t)ceil_div(n, kDsNB) * kDsNB * kDsNB; }
+size_t chain_pub_doubles(int64_t n) { return (size_t)ceil_div(n, kDsNB) * 2 * kDsNB * kDsRhs; }
+
+// the diagonal-block inverses and coupling blocks of the sweep
+template <int MODE>
+int32_t chain_prepare(Ctx* ctx, cudaStream_t st, const double* LU, int64_t ld, int64_t n, double* inv, double* w) {
+    const int nblk = (int)ceil_div(n, kDsNB);
+    const size_t blk_doubles = chain_blk_doubles(n);
     prof_begin(ctx, st, kClsSolve);
     dinv_kernel<MODE><<<nblk, kDsNB, kDsTriSmem, st>>>(LU, ld, (int)n, inv, ctx->d_status);
     prof_end(ctx, st, kClsSolve, 8.0 * 2 * blk_doubles);
@@ -540,12 +574,20 @@ int32_t launch_chain(Ctx* ctx, cudaStream_t st, const double* LU, int64_t ld, in
     dcouple_kernel<MODE><<<nblk, 256, kDsTriSmem, st>>>(LU, ld, (int)n, inv, w, ctx->d_status);
     prof_end(ctx, st, kClsSolve, 8.0 * 3 * blk_doubles);
     B2M_LAUNCHED(ctx);
+    return B2M_OK;
+}
+
+// the persistent sweeps (one cooperative launch per kDsMaxRhs right-hand sides)
+template <int MODE>
+int32_t chain_sweeps(Ctx* ctx, cudaStream_t st, const double* LU, int64_t ld, int64_t n, const double* inv,
+                     const double* w, unsigned long long* pub, double* X, int64_t ldx, int64_t nrhs) {
+    const int nblk = (int)ceil_div(n, kDsNB);
     for (int64_t c0 = 0; c0 < nrhs; c0 += kDsMaxRhs) {
         const int nc = (int)std::min<int64_t>(kDsMaxRhs, nrhs - c0);
         const int ng = (int)ceil_div(nc, kDsRhs);
         B2M_CU(ctx, cudaMemsetAsync(pub, 0xFF, (size_t)nblk * ng * kDsNB * kDsRhs * sizeof(double), st));  // kDsEmpty
         DsArgs da{LU, ld, (int)n, inv, w, X, ldx, (int)c0, nc, pub, ctx->d_status,
-                  ctx->wait_limit >= 0 ? (uint32_t)ctx->wait_limit : kDsSpin};
+                  ctx->wait_limit >= 0 ? (uint32_t)ctx->wait_limit : kDsSpin, aligned16(LU) && ld % 2 == 0};
         cudaLaunchConfig_t cfg{};
         cudaLaunchAttribute at[1];
         at[0].id = cudaLaunchAttributeCooperative;
@@ -561,8 +603,53 @@ int32_t launch_chain(Ctx* ctx, cudaStream_t st, const double* LU, int64_t ld, in
         prof_end(ctx, st, kClsSolve, 4.0 * (double)n * n + 16.0 * n * nc);
         B2M_LAUNCHED(ctx);
     }
-    *used = true;
     return B2M_OK;
+}
+
+template <int MODE>
+int32_t launch_chain(Ctx* ctx, cudaStream_t st, const double* LU, int64_t ld, int64_t n, double* X, int64_t ldx,
+                     int64_t nrhs, bool* used) {
+    B2M_TRY(chain_usable<MODE>(ctx, n, nrhs, used));
+    if (!*used) return B2M_OK;  // not co-resident: per-block launches
+    const size_t blk_doubles = chain_blk_doubles(n);
+    void* p = nullptr;
+    B2M_TRY(ws_get(ctx, kWsTri, (2 * blk_doubles + chain_pub_doubles(n)) * sizeof(double), &p));
+    double* inv = static_cast<double*>(p);
+    double* w = inv + blk_doubles;
+    unsigned long long* pub = reinterpret_cast<unsigned long long*>(w + blk_doubles);
+    B2M_TRY(chain_prepare<MODE>(ctx, st, LU, ld, n, inv, w));
+    return chain_sweeps<MODE>(ctx, st, LU, ld, n, inv, w, pub, X, ldx, nrhs);
+}
+
+// two sweeps in sequence; the second triangle's blocks are prepared on the side stream meanwhile
+template <int M1, int M2>
+int32_t solve_pair(Ctx* ctx, cudaStream_t st, const double* LU, int64_t ld, int64_t n, double* X, int64_t ldx,
+                   int64_t nrhs, bool* used) {
+    bool u1 = false, u2 = false;
+    B2M_TRY(chain_usable<M1>(ctx, n, nrhs, &u1));
+    B2M_TRY(chain_usable<M2>(ctx, n, nrhs, &u2));
+    *used = u1 && u2;
+    if (!*used) return B2M_OK;
+    B2M_TRY(ensure_side_stream(ctx));
+    const size_t blk_doubles = chain_blk_doubles(n);
+    void* p = nullptr;
+    B2M_TRY(ws_get(ctx, kWsTri, (4 * blk_doubles + chain_pub_doubles(n)) * sizeof(double), &p));
+    double* inv1 = static_cast<double*>(p);
+    double* w1 = inv1 + blk_doubles;
+    double* inv2 = w1 + blk_doubles;
+    double* w2 = inv2 + blk_doubles;
+    unsigned long long* pub = reinterpret_cast<unsigned long long*>(w2 + blk_doubles);
+    cudaStream_t q2 = ctx->side_stream;
+    B2M_CU(ctx, cudaEventRecord(ctx->ev_side_fork, st));
+    B2M_CU(ctx, cudaStreamWaitEvent(q2, ctx->ev_side_fork, 0));
+    B2M_TRY(chain_prepare<M2>(ctx, q2, LU, ld, n, inv2, w2));
+    B2M_CU(ctx, cudaEventRecord(ctx->ev_side_join, q2));
+    B2M_TRY(chain_prepare<M1>(ctx, st, LU, ld, n, inv1, w1));
+    // the first sweep is a cooperative launch that needs every SM free of the preparation kernels,
+    // so both preparations finish before it starts
+    B2M_CU(ctx, cudaStreamWaitEvent(st, ctx->ev_side_join, 0));
+    B2M_TRY(chain_sweeps<M1>(ctx, st, LU, ld, n, inv1, w1, pub, X, ldx, nrhs));
+    return chain_sweeps<M2>(ctx, st, LU, ld, n, inv2, w2, pub, X, ldx, nrhs);
 }
 
 template <int MODE>
@@ -577,6 +664,19 @@ int32_t solve_tri(Ctx* ctx, cudaStream_t st, const double* LU, int64_t ld, int64
 }
 
 }  // namespace
+
+int32_t tri_solve2_f64(Ctx* ctx, cudaStream_t st, const double* LU, int64_t ld, int64_t n, int mode1, int mode2,
+                       double* X, int64_t ldx, int64_t nrhs) {
+    if (n <= 0 || nrhs <= 0) return B2M_OK;
+    bool used = false;
+    if (mode1 == kTriL && mode2 == kTriU) B2M_TRY((solve_pair<kTriL, kTriU>(ctx, st, LU, ld, n, X, ldx, nrhs, &used)));
+    if (mode1 == kTriUt && mode2 == kTriLt)
+        B2M_TRY((solve_pair<kTriUt, kTriLt>(ctx, st, LU, ld, n, X, ldx, nrhs, &used)));
+    if (mode1 == kTriUt && mode2 == kTriU) B2M_TRY((solve_pair<kTriUt, kTriU>(ctx, st, LU, ld, n, X, ldx, nrhs, &used)));
+    if (used) return B2M_OK;
+    B2M_TRY(tri_solve_f64(ctx, st, LU, ld, n, mode1, X, ldx, nrhs));
+    return tri_solve_f64(ctx, st, LU, ld, n, mode2, X, ldx, nrhs);
+}
 
 int32_t tri_solve_f64(Ctx* ctx, cudaStream_t st, const double* LU, int64_t ld, int64_t n, int mode, double* X,
                       int64_t ldx, int64_t nrhs) {

@@ -36,6 +36,12 @@ int32_t lu_solve_f64(Ctx* ctx, cudaStream_t st, const double* LU, int64_t ld, in
 // Blocked FP64 triangular solve of X (n x nrhs, row stride ldx) in place with a triangle of the FP64
 // LU factors: kTriL unit-lower L, kTriU upper U, kTriUt = U^T (lower), kTriLt = L^T (unit upper).
 enum TriMode : int { kTriL = 0, kTriU = 1, kTriUt = 2, kTriLt = 3 };
+int32_t ensure_side_stream(Ctx* ctx);
+// two triangular solves in sequence on the same factors (X <- T2^-1 T1^-1 X); where both run the
+// persistent sweep, the diagonal-block inverses and coupling blocks of the second are formed on
+// the side stream while the first's are formed and swept
+int32_t tri_solve2_f64(Ctx* ctx, cudaStream_t st, const double* LU, int64_t ld, int64_t n, int mode1, int mode2,
+                       double* X, int64_t ldx, int64_t nrhs);
 int32_t tri_solve_f64(Ctx* ctx, cudaStream_t st, const double* LU, int64_t ld, int64_t n, int mode, double* X,
                       int64_t ldx, int64_t nrhs);
 

@@ -216,7 +216,7 @@ __global__ void __launch_bounds__(kSuThreads)
     __syncthreads();
     const int nm = n_moves;
     const int gc = col_lo + blockIdx.x * kSuThreads + tid;
-    const int col = gc < c0 ? gc : gc + w;  // the leaf's own columns are skipped
+    const int col = (gc < c0 || col_lo >= c0 + w) ? gc : gc + w;  // the leaf's own columns are skipped
     if (col < col_hi) {
         // every read of this column happens before its first write
         T v[2 * kPanelW];
@@ -269,56 +269,60 @@ __global__ void __launch_bounds__(256, 2) panel_rank_update_kernel(double* A, in
     __shared__ __align__(16) double s_b[kPanelW][kRuT];  // U12 columns of the tile
     if (status[kInfo] != 0) return;
     const int t = threadIdx.x, tx = t & 15, ty = t >> 4;
-    const int r0 = r_lo + blockIdx.y * kRuT, cb = cl + blockIdx.x * kRuT;
-    batched_copy<256, kRuT * kPanelW / 256, double>(t, kRuT * kPanelW,
-        [&](int e) {
-            const int rr = e >> 5, k = e & 31, row = r0 + rr;
-            return (row < n && k < w) ? A[(int64_t)row * ld + c0 + k] : 0.0;
-        },
-        [&](int e, double v) { s_a[e >> 5][e & 31] = v; });
-    batched_copy<256, kPanelW * kRuT / 256, double>(t, kPanelW * kRuT,
-        [&](int e) {
-            const int k = e / kRuT, col = cb + e % kRuT;
-            return (k < w && col < ch) ? A[(int64_t)(c0 + k) * ld + col] : 0.0;
-        },
-        [&](int e, double v) { s_b[e / kRuT][e % kRuT] = v; });
-    // the tile's own values, loaded while the slices arrive
-    double c[4][4];
-#pragma unroll
-    for (int i = 0; i < 4; ++i) {
-        const int row = r0 + 4 * ty + i;
-#pragma unroll
-        for (int j = 0; j < 4; ++j) {
-            const int col = cb + 4 * tx + j;
-            c[i][j] = (row < n && col < ch) ? A[(int64_t)row * ld + col] : 0.0;
-        }
-    }
-    __syncthreads();
-    double acc[4][4];
-#pragma unroll
-    for (int i = 0; i < 4; ++i)
-#pragma unroll
-        for (int j = 0; j < 4; ++j) acc[i][j] = 0.0;
-#pragma unroll 8
-    for (int k = 0; k < kPanelW; ++k) {
-        const double2 b01 = *reinterpret_cast<const double2*>(&s_b[k][4 * tx]);
-        const double2 b23 = *reinterpret_cast<const double2*>(&s_b[k][4 * tx + 2]);
-        const double bv[4] = {b01.x, b01.y, b23.x, b23.y};
-#pragma unroll
+    const int tiles_x = (ch - cl + kRuT - 1) / kRuT, tiles = tiles_x * ((n - r_lo + kRuT - 1) / kRuT);
+    for (int tl = blockIdx.x; tl < tiles; tl += gridDim.x) {  // a grid smaller than the tiles loops
+        const int r0 = r_lo + (tl / tiles_x) * kRuT, cb = cl + (tl % tiles_x) * kRuT;
+        batched_copy<256, kRuT * kPanelW / 256, double>(t, kRuT * kPanelW,
+            [&](int e) {
+                const int rr = e >> 5, k = e & 31, row = r0 + rr;
+                return (row < n && k < w) ? A[(int64_t)row * ld + c0 + k] : 0.0;
+            },
+            [&](int e, double v) { s_a[e >> 5][e & 31] = v; });
+        batched_copy<256, kPanelW * kRuT / 256, double>(t, kPanelW * kRuT,
+            [&](int e) {
+                const int k = e / kRuT, col = cb + e % kRuT;
+                return (k < w && col < ch) ? A[(int64_t)(c0 + k) * ld + col] : 0.0;
+            },
+            [&](int e, double v) { s_b[e / kRuT][e % kRuT] = v; });
+        // the tile's own values, loaded while the slices arrive
+        double c[4][4];
+    #pragma unroll
         for (int i = 0; i < 4; ++i) {
-            const double av = s_a[4 * ty + i][k];
-#pragma unroll
-            for (int j = 0; j < 4; ++j) acc[i][j] = fma(av, bv[j], acc[i][j]);
+            const int row = r0 + 4 * ty + i;
+    #pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const int col = cb + 4 * tx + j;
+                c[i][j] = (row < n && col < ch) ? A[(int64_t)row * ld + col] : 0.0;
+            }
         }
-    }
-#pragma unroll
-    for (int i = 0; i < 4; ++i) {
-        const int row = r0 + 4 * ty + i;
-#pragma unroll
-        for (int j = 0; j < 4; ++j) {
-            const int col = cb + 4 * tx + j;
-            if (row < n && col < ch) A[(int64_t)row * ld + col] = c[i][j] - acc[i][j];
+        __syncthreads();
+        double acc[4][4];
+    #pragma unroll
+        for (int i = 0; i < 4; ++i)
+    #pragma unroll
+            for (int j = 0; j < 4; ++j) acc[i][j] = 0.0;
+    #pragma unroll 8
+        for (int k = 0; k < kPanelW; ++k) {
+            const double2 b01 = *reinterpret_cast<const double2*>(&s_b[k][4 * tx]);
+            const double2 b23 = *reinterpret_cast<const double2*>(&s_b[k][4 * tx + 2]);
+            const double bv[4] = {b01.x, b01.y, b23.x, b23.y};
+    #pragma unroll
+            for (int i = 0; i < 4; ++i) {
+                const double av = s_a[4 * ty + i][k];
+    #pragma unroll
+                for (int j = 0; j < 4; ++j) acc[i][j] = fma(av, bv[j], acc[i][j]);
+            }
         }
+    #pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            const int row = r0 + 4 * ty + i;
+    #pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const int col = cb + 4 * tx + j;
+                if (row < n && col < ch) A[(int64_t)row * ld + col] = c[i][j] - acc[i][j];
+            }
+        }
+        __syncthreads();  // the tile's slices are no longer read
     }
 }
 
@@ -752,25 +756,59 @@ int32_t lu_blocked(Ctx* ctx, cudaStream_t q, double* A, int64_t ld, int64_t n, i
             B2M_CU(ctx, launch_k(ctx, iota_kernel, dim3((unsigned)ceil_div(n, 256)), dim3(256), 0, q, pmap, n));
             B2M_LAUNCHED(ctx);
         }
-        // the panel, right-looking by leaves (all of it on this stream: it is the critical path)
+        // The panel, right-looking by leaves.  The critical path, on this stream: a leaf's panel
+        // kernel, then its interchanges, U12 and rank-w update on the next leaf's columns only; the
+        // same for the other columns of the outer panel (the factored ones left of the leaf get the
+        // interchanges only) runs on the leaf stream, under the next leaf's panel kernel, and is
+        // waited for before that leaf's own updates touch those columns.  Column groups are
+        // disjoint between the two streams, and every column sees the leaves' interchanges and
+        // updates in leaf order, so the factors are those of the single-stream order.
+        cudaStream_t ql = ctx->leaf_stream;
+        bool leaf_busy = false;
+        auto swap_u12 = [&](cudaStream_t qs, int64_t c0, int64_t wl, int64_t lo, int64_t hi, bool maps) -> int32_t {
+            const int64_t cols = std::max<int64_t>(0, (lo >= c0 + wl || hi <= c0) ? hi - lo : hi - lo - wl);
+            if (cols == 0 && !maps) return B2M_OK;  // (the maps' update runs even without columns)
+            prof_begin(ctx, qs, kClsSwap);
+            B2M_CU(ctx, launch_k(ctx, leaf_swap_u12_kernel<double>,
+                                 dim3((unsigned)std::max<int64_t>(1, ceil_div(cols, kSuThreads))),
+                                 dim3(kSuThreads), 0, qs, A, ld, (int)lo, (int)hi, (int)c0, (int)wl, ipiv,
+                                 maps ? perm : (int32_t*)nullptr, maps ? pmap : (int32_t*)nullptr,
+                                 (const int32_t*)ctx->d_status));
+            prof_end(ctx, qs, kClsSwap, 16.0 * wl * (double)cols);
+            B2M_LAUNCHED(ctx);
+            return B2M_OK;
+        };
+        auto rank_update = [&](cudaStream_t qs, int64_t c0, int64_t wl, int64_t cl, int64_t ch, int max_ctas) -> int32_t {
+            const int64_t rl = c0 + wl;
+            if (ch <= cl || rl >= n) return B2M_OK;
+            const int64_t tiles = ceil_div(ch - cl, kRuT) * ceil_div(n - rl, kRuT);
+            prof_begin(ctx, qs, kClsGemm);
+            B2M_CU(ctx, launch_k(ctx, panel_rank_update_kernel, dim3((unsigned)std::min<int64_t>(tiles, max_ctas)),
+                                 dim3(256), 0, qs, A, ld, (int)n, (int)rl, (int)cl, (int)ch, (int)c0, (int)wl,
+                                 (const int32_t*)ctx->d_status));
+            prof_end(ctx, qs, kClsGemm, 2.0 * (double)(n - rl) * (double)(ch - cl) * (double)wl);  // flops
+            B2M_LAUNCHED(ctx);
+            return B2M_OK;
+        };
         for (int64_t c0 = k0; leaves && c0 < k1; c0 += leaf) {
             const int64_t wl = std::min(leaf, k1 - c0);
             B2M_TRY(launch_panel<double>(ctx, q, A + c0 * ld + c0, ld, (int)(n - c0), (int)wl, (int)c0, (int)c0, ipiv));
-            prof_begin(ctx, q, kClsSwap);
-            B2M_CU(ctx, launch_k(ctx, leaf_swap_u12_kernel<double>,
-                                 dim3((unsigned)std::max<int64_t>(1, ceil_div(w - wl, kSuThreads))), dim3(kSuThreads), 0,
-                                 q, A, ld, (int)k0, (int)k1, (int)c0, (int)wl, ipiv, perm, pmap,
-                                 (const int32_t*)ctx->d_status));
-            prof_end(ctx, q, kClsSwap, 16.0 * wl * (double)(w - wl));
-            B2M_LAUNCHED(ctx);
-            const int64_t rl = c0 + wl;
-            if (rl < k1) {
-                dim3 grid((unsigned)ceil_div(k1 - rl, kRuT), (unsigned)ceil_div(n - rl, kRuT));
-                prof_begin(ctx, q, kClsGemm);
-                B2M_CU(ctx, launch_k(ctx, panel_rank_update_kernel, grid, dim3(256), 0, q, A, ld, (int)n, (int)rl,
-                                     (int)rl, (int)k1, (int)c0, (int)wl, (const int32_t*)ctx->d_status));
-                prof_end(ctx, q, kClsGemm, 2.0 * (double)(n - rl) * (double)(k1 - rl) * (double)wl);  // flops
-                B2M_LAUNCHED(ctx);
+            const int64_t rl = c0 + wl, nx = std::min(rl + leaf, k1);  // the next leaf: columns [rl, nx)
+            B2M_CU(ctx, cudaEventRecord(ctx->ev_leaf_panel, q));
+            if (leaf_busy) {  // the previous leaf's updates of [rl, k1) are done
+                B2M_CU(ctx, cudaStreamWaitEvent(q, ctx->ev_leaf_side, 0));
+                leaf_busy = false;
+            }
+            B2M_TRY(swap_u12(q, c0, wl, rl, nx, true));
+            B2M_TRY(rank_update(q, c0, wl, rl, nx, 1 << 30));
+            if (nx < k1 || c0 > k0) {
+                PriorityScope side(ctx, false);
+                B2M_CU(ctx, cudaStreamWaitEvent(ql, ctx->ev_leaf_panel, 0));
+                B2M_TRY(swap_u12(ql, c0, wl, nx, k1, false));
+                B2M_TRY(swap_u12(ql, c0, wl, k0, c0, false));
+                B2M_TRY(rank_update(ql, c0, wl, nx, k1, 64));
+                B2M_CU(ctx, cudaEventRecord(ctx->ev_leaf_side, ql));
+                leaf_busy = true;
             }
             if (ctx->progress && ctx->progress_notes.size() < ctx->progress_notes.capacity()) {
                 ctx->progress_notes.push_back(
@@ -778,6 +816,7 @@ int32_t lu_blocked(Ctx* ctx, cudaStream_t q, double* A, int64_t ld, int64_t n, i
                 B2M_CU(ctx, cudaLaunchHostFunc(q, progress_trampoline, &ctx->progress_notes.back()));
             }
         }
+        if (leaf_busy) B2M_CU(ctx, cudaStreamWaitEvent(q, ctx->ev_leaf_side, 0));
         if (part == 0) return B2M_OK;
         B2M_TRY(join());  // the previous panel's wide update is done before rows move under it
         auto permute = [&](cudaStream_t qs, int64_t c_begin, int64_t c_end) -> int32_t {
@@ -821,18 +860,27 @@ int32_t lu_blocked(Ctx* ctx, cudaStream_t q, double* A, int64_t ld, int64_t n, i
     return join();
 }
 
+
+}  // namespace
+
+// the low-priority side stream (and its fork/join events) of this context, created on first use
 int32_t ensure_side_stream(Ctx* ctx) {
-    if (ctx->side_stream) return B2M_OK;
+    if (ctx->side_stream && ctx->leaf_stream) return B2M_OK;
     int least = 0, greatest = 0;
     B2M_CU(ctx, cudaDeviceGetStreamPriorityRange(&least, &greatest));
-    B2M_CU(ctx, cudaStreamCreateWithPriority(&ctx->side_stream, cudaStreamNonBlocking, least));
-    B2M_CU(ctx, cudaEventCreateWithFlags(&ctx->ev_side_fork, cudaEventDisableTiming));
-    B2M_CU(ctx, cudaEventCreateWithFlags(&ctx->ev_side_join, cudaEventDisableTiming));
+    if (!ctx->side_stream) {
+        B2M_CU(ctx, cudaStreamCreateWithPriority(&ctx->side_stream, cudaStreamNonBlocking, least));
+        B2M_CU(ctx, cudaEventCreateWithFlags(&ctx->ev_side_fork, cudaEventDisableTiming));
+        B2M_CU(ctx, cudaEventCreateWithFlags(&ctx->ev_side_join, cudaEventDisableTiming));
+    }
+    // the FP64 LU's in-panel look-ahead: the stream runs at the critical path's priority, since the
+    // leaf after next waits for it
+    B2M_CU(ctx, cudaStreamCreateWithPriority(&ctx->leaf_stream, cudaStreamNonBlocking, greatest));
+    B2M_CU(ctx, cudaEventCreateWithFlags(&ctx->ev_leaf_panel, cudaEventDisableTiming));
+    B2M_CU(ctx, cudaEventCreateWithFlags(&ctx->ev_leaf_side, cudaEventDisableTiming));
     ctx->chain_priority = greatest;
     return B2M_OK;
 }
-
-}  // namespace
 
 template <typename T>
 int32_t launch_swaps(Ctx* ctx, cudaStream_t st, T* A, int64_t ld, int ncols, int c0, int w, const int32_t* ipiv,
@@ -908,8 +956,7 @@ int32_t lu_solve_f64(Ctx* ctx, cudaStream_t st, const double* LU, int64_t ld, in
         gather_rows_kernel<<<(unsigned)ceil_div(n * nrhs, 256), 256, 0, s>>>(B, ldb, X, ldb, perm, n, nrhs);
         B2M_LAUNCHED(ctx);
         if (nrhs <= 64) {  // few right-hand sides: block-row sweeps (dtrsv.cu)
-            B2M_TRY(tri_solve_f64(ctx, s, LU, ld, n, kTriL, B, ldb, nrhs));
-            return tri_solve_f64(ctx, s, LU, ld, n, kTriU, B, ldb, nrhs);
+            return tri_solve2_f64(ctx, s, LU, ld, n, kTriL, kTriU, B, ldb, nrhs);
         }
         TriSolve t{LU, ld, n, B, ldb, n, nrhs, 0, nrhs};
         B2M_TRY(trsm_lower_rec(ctx, s, t, 0, 0, n));

@@ -836,14 +836,7 @@ int32_t lu_factor_f32(Ctx* ctx, cudaStream_t st, float* A, int64_t ld, int64_t n
                                              (int)cudaSharedmemCarveoutMaxShared));
         attr.store(1);
     }
-    if (!ctx->side_stream) {
-        int least = 0, greatest = 0;
-        B2M_CU(ctx, cudaDeviceGetStreamPriorityRange(&least, &greatest));
-        B2M_CU(ctx, cudaStreamCreateWithPriority(&ctx->side_stream, cudaStreamNonBlocking, least));
-        B2M_CU(ctx, cudaEventCreateWithFlags(&ctx->ev_side_fork, cudaEventDisableTiming));
-        B2M_CU(ctx, cudaEventCreateWithFlags(&ctx->ev_side_join, cudaEventDisableTiming));
-        ctx->chain_priority = greatest;
-    }
+    B2M_TRY(ensure_side_stream(ctx));
     const GraphKey key0{3 + mode * 10, A, perm, s.cand, s.bth, ld, n, 0, 1};
     const GraphKey key1{3 + mode * 10, A, perm, s.cand, s.bth, ld, n, 0, 2};
     // part 0: the first outer panel's leaves; part 1: everything after them.  Two graphs, so that the

@@ -36,7 +36,7 @@ constexpr int kReRows = 64;    // rows per residual CTA
 constexpr int kReRhs = 16;     // right-hand sides per residual CTA
 constexpr int kReK = 64;       // K chunk of the residual
 constexpr int kReSplit = 2;    // K halves inside a residual CTA (four warps each)
-constexpr int kReStages = 3;   // cp.async pipeline depth
+constexpr int kReStages = 5;   // cp.async pipeline depth (four 44 KiB stages in flight per SM)
 constexpr int kReAS = kReK + 2;                                   // A tile row stride (doubles)
 constexpr int kReXS = kReRhs + 4;                                 // X tile row stride (doubles)
 constexpr int kReStage = kReRows * kReAS + kReK * kReXS;          // doubles per stage
@@ -152,25 +152,33 @@ __device__ __forceinline__ float4 ld_row4(const float* row, int k, int kmax) {
     return v;
 }
 
-// T_bj (128 x 128, zero past the matrix and in the factors' padding columns) into shared memory by
-// asynchronous 16-byte copies, a row per 32 threads (coalesced).  Float4 c4 of row r sits at
-// r * 128 + 4 (c4 ^ (r & 7)), so that the fold's float4 reads of one column group by 32
-// consecutive rows take four wavefronts, the minimum.  The rows are 16-byte aligned (the FP32
-// factors' leading dimension is a multiple of 32).
-__device__ __forceinline__ void sw_stage(float* s_tt, const float* T, int64_t ld, int b0, int bs, int p0, int ps,
-                                         int t) {
+constexpr int kSwTS = kTrsvNB + 4;  // line stride of the staged T_bj (528 bytes: 16-byte aligned lines)
+
+// T_bj (128 x 128) into shared memory, row r at r * kSwTS floats (the stride keeps the fold's float4
+// reads of one column group by 32 consecutive rows at four wavefronts, the minimum).  A full block
+// comes in as 128 bulk copies of 512 bytes (one instruction per row, the FP32 factors' rows are
+// 16-byte aligned: their leading dimension is a multiple of 32) completing on `bar`; a partial one
+// by asynchronous 16-byte copies, zero past the matrix and in the factors' padding columns.
+__device__ __forceinline__ bool sw_stage(float* s_tt, const float* T, int64_t ld, int b0, int bs, int p0, int ps,
+                                         int t, uint64_t* bar) {
+    if (bs == kTrsvNB && ps == kTrsvNB) {
+        if (t == 0) mbar_arrive_expect_tx(bar, kTrsvNB * kTrsvNB * (int)sizeof(float));
+        if (t < kTrsvNB) bulk_g2s(s_tt + t * kSwTS, T + (int64_t)(b0 + t) * ld + p0, kTrsvNB * (int)sizeof(float), bar);
+        return true;
+    }
 #pragma unroll 4
     for (int i = 0; i < kTrsvNB * kTrsvNB / (4 * 256); ++i) {
         const int e = t + 256 * i;
         const int rr = e >> 5, c4 = e & 31;
         const int nb = rr < bs ? 4 * max(0, min(4, ps - 4 * c4)) : 0;
         const float* src = nb > 0 ? T + (int64_t)(b0 + rr) * ld + p0 + 4 * c4 : T;
-        cp_async16(s_tt + rr * kTrsvNB + 4 * (c4 ^ (rr & 7)), src, nb);
+        cp_async16(s_tt + rr * kSwTS + 4 * c4, src, nb);
     }
     cp_async_commit();
+    return false;
 }
 __device__ __forceinline__ float4 sw_tile4(const float* s_tt, int r, int c4) {
-    return *reinterpret_cast<const float4*>(s_tt + r * kTrsvNB + 4 * (c4 ^ (r & 7)));
+    return *reinterpret_cast<const float4*>(s_tt + r * kSwTS + 4 * c4);
 }
 
 __global__ void __launch_bounds__(256) trsv_block_kernel(TrArgs a, int b) {
@@ -347,7 +355,7 @@ __global__ void __launch_bounds__(256) trsv_block_kernel(TrArgs a, int b) {
 constexpr int kSwRhs = 8;
 constexpr uint32_t kSwSpin = 1u << 22;
 constexpr uint32_t kSwAbort = 0xFFFFFFFFu;
-constexpr int kSwSmem = 3 * kTrsvNB * kTrsvNB * (int)sizeof(float);  // T_bb^-1 and W_b, T_bj
+constexpr int kSwSmem = (2 * kTrsvNB * kTrsvNB + kTrsvNB * kSwTS) * (int)sizeof(float);  // T_bb^-1, W_b, T_bj
 
 struct SwArgs {
     const float* T;
@@ -419,8 +427,15 @@ __global__ void __launch_bounds__(256, 1) trsv_sweep_kernel(SwArgs a) {
     const int r = t & (NB - 1), h = t >> 7;
     const int cg = a.c0 + g * kSwRhs;
     const int ncg = min(kSwRhs, a.nc - g * kSwRhs);
-    if (t == 0) s_abort = 0;
+    __shared__ __align__(8) uint64_t s_tbar;  // completion of a bulk-staged T_bj
+    if (t == 0) {
+        s_abort = 0;
+        mbar_init(&s_tbar, 1);
+        fence_barrier_init();
+    }
     __syncthreads();
+    uint32_t tphase = 0;
+    bool tbulk = false;  // a bulk copy of T_bj is in flight (uniform)
     {
         const float* inv = a.inv + (int64_t)b * NB * NB;
         const float* w = a.w + (int64_t)b * NB * NB;
@@ -469,6 +484,11 @@ __global__ void __launch_bounds__(256, 1) trsv_sweep_kernel(SwArgs a) {
                                      __uint_as_float((uint32_t)w[2]), __uint_as_float((uint32_t)w[3]));
         *reinterpret_cast<float4*>(&s_p[k][q0]) = v;
         cp_async_wait<0>();  // this thread's part of T_bj has landed
+        if (tbulk) {  // so have the bulk copies (waited for even when the block wait gave up)
+            if (!mbar_wait(&s_tbar, tphase, &a.status[kTimeout], 507)) s_abort = 1;
+            tphase ^= 1u;
+            tbulk = false;
+        }
         __syncthreads();
         if (s_abort) {
             abandon();
@@ -481,7 +501,7 @@ __global__ void __launch_bounds__(256, 1) trsv_sweep_kernel(SwArgs a) {
     for (int jj = 0; jj + 1 < bi; ++jj) {
         const int j = a.upper ? nblk - 1 - jj : jj;
         const int p0 = j * NB, ps = min(NB, a.n - p0);
-        sw_stage(s_tt, a.T, a.ld, b0, bs, p0, ps, t);  // in flight during the wait
+        tbulk = sw_stage(s_tt, a.T, a.ld, b0, bs, p0, ps, t, &s_tbar);  // in flight during the wait
         if (!wait_and_stage(j)) return;
 #pragma unroll
         for (int i = 0; i < 16; ++i) {
@@ -579,7 +599,8 @@ __global__ void __cluster_dims__(kChCl, 1, 1) __launch_bounds__(256, 1) trsv_cha
     float4* s_inv = sw_dyn;                        // [32][128]: s_inv[kq][r] = inv[r][4kq .. 4kq+3]
     float4* s_w = sw_dyn + kTrsvNB * kTrsvNB / 4;  // same layout for W_b
     float* s_tt = reinterpret_cast<float*>(sw_dyn + kTrsvNB * kTrsvNB / 2);  // T_bj being folded in
-    float (*s_rx)[kTrsvNB][kSwRhs] = reinterpret_cast<float (*)[kTrsvNB][kSwRhs]>(sw_dyn + 3 * kTrsvNB * kTrsvNB / 4);
+    float (*s_rx)[kTrsvNB][kSwRhs] =
+        reinterpret_cast<float (*)[kTrsvNB][kSwRhs]>(sw_dyn + kTrsvNB * kTrsvNB / 2 + kTrsvNB * kSwTS / 4);
     if (a.status[kInfo] != 0) return;  // uniform: written before the launch
     cg::cluster_group cluster = cg::this_cluster();
     const int t = threadIdx.x;
@@ -588,12 +609,16 @@ __global__ void __cluster_dims__(kChCl, 1, 1) __launch_bounds__(256, 1) trsv_cha
     const int g = blockIdx.x / nbp, bi = blockIdx.x - g * nbp;
     const int rank = (int)cluster.block_rank();  // bi % kChCl: nbp is a multiple of kChCl
     const int cl0 = bi - rank;
+    __shared__ __align__(8) uint64_t s_tbar;  // completion of a bulk-staged T_bj
     if (t == 0) {
         for (int q = 0; q < rank; ++q) mbar_init(&s_bar[q], 1);
+        mbar_init(&s_tbar, 1);
         fence_barrier_init();
         for (int q = 0; q < rank; ++q) mbar_arrive_expect_tx(&s_bar[q], kChSlot);
         s_abort = 0;
     }
+    uint32_t tphase = 0;
+    bool tbulk = false;  // a bulk copy of T_bj is in flight (uniform)
     cluster.sync();  // every receiver's mbarriers are armed before the first push
     if (bi >= nblk) {  // padding CTA of the last cluster
         cluster.sync();
@@ -653,6 +678,11 @@ __global__ void __cluster_dims__(kChCl, 1, 1) __launch_bounds__(256, 1) trsv_cha
                                      __uint_as_float((uint32_t)w[2]), __uint_as_float((uint32_t)w[3]));
         *reinterpret_cast<float4*>(&s_p[k][q0]) = v;
         cp_async_wait<0>();  // this thread's part of T_bj has landed
+        if (tbulk) {  // so have the bulk copies (waited for even when the block wait gave up)
+            if (!mbar_wait(&s_tbar, tphase, &a.status[kTimeout], 508)) s_abort = 1;
+            tphase ^= 1u;
+            tbulk = false;
+        }
         __syncthreads();
         return !s_abort;
     };
@@ -666,6 +696,11 @@ __global__ void __cluster_dims__(kChCl, 1, 1) __launch_bounds__(256, 1) trsv_cha
         if (!ready && !bad) atomicCAS(tmo, 0, 504);
         if (!ready) s_abort = 1;
         cp_async_wait<0>();  // this thread's part of T_bj has landed
+        if (tbulk) {  // so have the bulk copies (waited for even when the block wait gave up)
+            if (!mbar_wait(&s_tbar, tphase, &a.status[kTimeout], 509)) s_abort = 1;
+            tphase ^= 1u;
+            tbulk = false;
+        }
         __syncthreads();
         return !s_abort;
     };
@@ -674,7 +709,7 @@ __global__ void __cluster_dims__(kChCl, 1, 1) __launch_bounds__(256, 1) trsv_cha
     for (int jj = 0; ok && jj + 1 < bi; ++jj) {
         const int j = a.upper ? nblk - 1 - jj : jj;
         const int p0 = j * NB, ps = min(NB, a.n - p0);
-        sw_stage(s_tt, a.T, a.ld, b0, bs, p0, ps, t);  // in flight during the wait
+        tbulk = sw_stage(s_tt, a.T, a.ld, b0, bs, p0, ps, t, &s_tbar);  // in flight during the wait
         const bool local = jj >= cl0;
         ok = local ? wait_push(jj - cl0) : wait_global(j);
         if (!ok) break;
