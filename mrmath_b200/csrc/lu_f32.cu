@@ -775,7 +775,7 @@ size_t f32_scratch_bytes(int64_t n) {
     b += 256 * sizeof(int);                                     // moves
     b += 32 * (size_t)kTsRows * sizeof(float);                  // root multipliers
     b += 2 * (size_t)round_up(n, 64) * sizeof(int32_t);          // panel row maps (by panel parity)
-    b += (size_t)kNB * 32 * sizeof(float);                      // leaf L11^-1 blocks
+    b += 2 * (size_t)kNB * 32 * sizeof(float);                  // leaf L11^-1 blocks (by panel parity)
     b += 4 * (size_t)round_up(n, 32) * kNB * sizeof(float);     // bth, btl, ah, al
     b += 4 * (size_t)nblk * kTrsvNB * kTrsvNB * sizeof(float);  // diagonal inverses, coupling blocks
     b += 2 * (size_t)nblk * kSweepGroups * kTrsvNB * 8 * sizeof(unsigned long long);  // sweep words
@@ -800,7 +800,7 @@ F32Scratch f32_scratch_carve(void* base, int64_t n) {
     s.moves = reinterpret_cast<int*>(take(256 * sizeof(int)));
     s.lmul = reinterpret_cast<float*>(take(32 * (size_t)kTsRows * sizeof(float)));
     s.pmap = reinterpret_cast<int32_t*>(take(2 * (size_t)round_up(n, 64) * sizeof(int32_t)));
-    s.lpinv = reinterpret_cast<float*>(take((size_t)kNB * 32 * sizeof(float)));
+    s.lpinv = reinterpret_cast<float*>(take(2 * (size_t)kNB * 32 * sizeof(float)));
     const size_t panel = (size_t)round_up(n, 32) * kNB * sizeof(float);
     s.bth = reinterpret_cast<float*>(take(panel));
     s.btl = reinterpret_cast<float*>(take(panel));
@@ -875,11 +875,15 @@ int32_t lu_factor_f32(Ctx* ctx, cudaStream_t st, float* A, int64_t ld, int64_t n
             // be permuting the previous panel's left columns with its map while this panel's first
             // leaf initialises the other one (the join below orders the reuse two panels later)
             int32_t* pmap = s.pmap + ((oc0 / kNB) & 1) * round_up(n, 64);
+            // the leaves' L11^-1 blocks alternate the same way: the side stream's U12 of the columns
+            // beyond the next panel still reads this panel's blocks while the next panel's leaves
+            // write theirs (without the second buffer those reads raced with the writes)
+            float* lpinv = s.lpinv + ((oc0 / kNB) & 1) * (size_t)kNB * 32;
             const bool leaves = (part == 0) == (oc0 == 0);
             for (int64_t lc0 = oc0; leaves && lc0 < oc0 + pw; lc0 += 32) {
                 const int w = (int)std::min<int64_t>(32, n - lc0);
                 TsArgs ta{A, ld, (int)n, (int)lc0, w, (int)oc0, pw, s.cand, s.counters, s.top, s.mvals, s.wmat,
-                          s.moves, s.lmul, lc0 == oc0 ? pmap : nullptr, s.lpinv, ctx->d_status};
+                          s.moves, s.lmul, lc0 == oc0 ? pmap : nullptr, lpinv, ctx->d_status};
                 prof_begin(ctx, q, kClsPanel);
                 {
                     const cudaLaunchConfig_t c = cfg_of((unsigned)ceil_div(n - lc0, kTsRows), kTsThreads, 0);
@@ -938,7 +942,7 @@ int32_t lu_factor_f32(Ctx* ctx, cudaStream_t st, float* A, int64_t ld, int64_t n
             const int nL = mode == 3 ? (int)ceil_div(M * pw, 1024) : 0;
             auto outer = [&](cudaStream_t qs, int64_t cs0, int64_t ncols, int nl) -> int32_t {
                 OuArgs oa{A, ld, (int)n, (int)oc0, pw, mode, (int)ceil_div(ncols, 32), (int)cs0, (int)ncols,
-                          s.bth, s.btl, s.ah, s.al, s.lpinv, ctx->d_status};
+                          s.bth, s.btl, s.ah, s.al, lpinv, ctx->d_status};
                 prof_begin(ctx, qs, kClsTrsm);
                 B2M_CU(ctx, launch_k(ctx, lu_outer_kernel, dim3((unsigned)(oa.nU + nl)), dim3(256), (size_t)ou_smem, qs, oa));
                 // bytes: U12 read and written, its GEMM copies written, L21 read and split (3xTF32)
