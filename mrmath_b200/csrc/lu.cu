@@ -156,7 +156,7 @@ __global__ void __launch_bounds__(kSuThreads)
                          int32_t* pmap, const int32_t* status) {
     __shared__ int src_main[kPanelW];
     __shared__ int mv_dst[2 * kPanelW], mv_src[2 * kPanelW];
-    __shared__ int n_moves;
+    __shared__ int n_moves, n_main;
     __shared__ T s_l[kPanelW][kPanelW + 1];  // L11 (strictly lower part), s_l[j][i] = L(c0 + j, c0 + i)
     if (status[kInfo] != 0) return;
     const int tid = threadIdx.x, lane = tid & 31;
@@ -167,18 +167,22 @@ __global__ void __launch_bounds__(kSuThreads)
         },
         [&](int e, T v) { s_l[e / kPanelW][e % kPanelW] = v; });
     if (tid < 32) {
-        if (lane < w) src_main[lane] = c0 + lane;
-        __syncwarp();
+        // The interchanges composed into moves.  Lane i holds sm = the original row whose content
+        // ends in row c0 + i; lane e < n_extra holds a row q outside the leaf's rows that an
+        // interchange reached (my_pos) and the original row whose content ends there (my_src).
+        // Each interchange swaps two of these entries through shuffles (one warp, no shared
+        // memory round trip per interchange).
+        int sm = c0 + lane;
         int my_pos = -1, my_src = -1, n_extra = 0;
         const int qv = lane < w ? ipiv[c0 + lane] : 0;
         for (int j = 0; j < w; ++j) {
             const int q = __shfl_sync(0xffffffffu, qv, j);
+            const int a = __shfl_sync(0xffffffffu, sm, j);
             if (q < c0 + w) {
-                if (lane == 0 && q != c0 + j) {
-                    const int t = src_main[j];
-                    src_main[j] = src_main[q - c0];
-                    src_main[q - c0] = t;
-                }
+                const int qi = q - c0;
+                const int b = __shfl_sync(0xffffffffu, sm, qi);
+                if (lane == j) sm = b;
+                else if (lane == qi) sm = a;
             } else {
                 const unsigned hit = __ballot_sync(0xffffffffu, my_pos == q);
                 int owner;
@@ -188,15 +192,13 @@ __global__ void __launch_bounds__(kSuThreads)
                     owner = n_extra++;
                     if (lane == owner) { my_pos = q; my_src = q; }
                 }
-                if (lane == owner) {
-                    const int t = src_main[j];
-                    src_main[j] = my_src;
-                    my_src = t;
-                }
+                const int b = __shfl_sync(0xffffffffu, my_src, owner);
+                if (lane == j) sm = b;
+                if (lane == owner) my_src = a;
             }
-            __syncwarp();
         }
-        const bool mv_main = lane < w && src_main[lane] != c0 + lane;
+        if (lane < w) src_main[lane] = sm;
+        const bool mv_main = lane < w && sm != c0 + lane;
         const bool mv_extra = lane < n_extra && my_src != my_pos;
         const unsigned bm = __ballot_sync(0xffffffffu, mv_main);
         const unsigned be = __ballot_sync(0xffffffffu, mv_extra);
@@ -204,14 +206,14 @@ __global__ void __launch_bounds__(kSuThreads)
         if (mv_main) {
             const int k = __popc(bm & below);
             mv_dst[k] = c0 + lane;
-            mv_src[k] = src_main[lane];
+            mv_src[k] = sm;
         }
         if (mv_extra) {
             const int k = __popc(bm) + __popc(be & below);
             mv_dst[k] = my_pos;
             mv_src[k] = my_src;
         }
-        if (lane == 0) n_moves = __popc(bm) + __popc(be);
+        if (lane == 0) { n_moves = __popc(bm) + __popc(be); n_main = __popc(bm); }
     }
     __syncthreads();
     const int nm = n_moves;
@@ -219,17 +221,19 @@ __global__ void __launch_bounds__(kSuThreads)
     const int col = (gc < c0 || col_lo >= c0 + w) ? gc : gc + w;  // the leaf's own columns are skipped
     if (col < col_hi) {
         // every read of this column happens before its first write
-        T v[2 * kPanelW];
-#pragma unroll
-        for (int k = 0; k < 2 * kPanelW; ++k)
-            if (k < nm) v[k] = A[(int64_t)mv_src[k] * ld + col];
         if (col > c0) {  // right of the leaf: the leaf's rows after the interchanges, then U12
-            T x[kPanelW];
+            // the moves into the leaf's rows are covered by x; only the moves out of them (the
+            // extra entries, after the n_main moves into the leaf's rows) need their own values
+            const int nmain = n_main, nx = nm - n_main;
+            T x[kPanelW], v[kPanelW];
 #pragma unroll
             for (int j = 0; j < kPanelW; ++j) x[j] = j < w ? A[(int64_t)src_main[j] * ld + col] : T(0);
 #pragma unroll
-            for (int k = 0; k < 2 * kPanelW; ++k)
-                if (k < nm && (mv_dst[k] < c0 || mv_dst[k] >= c0 + w)) A[(int64_t)mv_dst[k] * ld + col] = v[k];
+            for (int e = 0; e < kPanelW; ++e)
+                if (e < nx) v[e] = A[(int64_t)mv_src[nmain + e] * ld + col];
+#pragma unroll
+            for (int e = 0; e < kPanelW; ++e)
+                if (e < nx) A[(int64_t)mv_dst[nmain + e] * ld + col] = v[e];
 #pragma unroll
             for (int i = 0; i < kPanelW - 1; ++i) {
 #pragma unroll
@@ -239,6 +243,10 @@ __global__ void __launch_bounds__(kSuThreads)
             for (int j = 0; j < kPanelW; ++j)
                 if (j < w) A[(int64_t)(c0 + j) * ld + col] = x[j];
         } else {
+            T v[2 * kPanelW];
+#pragma unroll
+            for (int k = 0; k < 2 * kPanelW; ++k)
+                if (k < nm) v[k] = A[(int64_t)mv_src[k] * ld + col];
 #pragma unroll
             for (int k = 0; k < 2 * kPanelW; ++k)
                 if (k < nm) A[(int64_t)mv_dst[k] * ld + col] = v[k];
