@@ -32,7 +32,7 @@ N_DEFAULT, NRHS_DEFAULT, KAPPA_DEFAULT = 8192, 16, 1e5
 # DRAM bytes per algorithmic byte of a dominant kernel class, from a single-launch ncu capture
 # (dram__bytes_read.sum + dram__bytes_write.sum over the bytes the event profiler charges to that
 # launch): the tournament leaf of the mixed solve, profiles/tslu_select_n8192_dram.md
-NCU_TRAFFIC_RATIO = {"panel": 1.146}
+NCU_TRAFFIC_RATIO = {"panel": 1.147}
 METRIC = "LU-solve GFLOP/s at n=8192 to FP64 backward error: mixed-precision IR vs plain FP64"
 
 
