@@ -129,9 +129,13 @@ def dist_setup():
 
         import torch
         import torch.distributed as dist
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
-                                device_id=torch.device("cuda", local))
+        timeout = datetime.timedelta(seconds=120)
+        if torch.cuda.is_available():
+            torch.cuda.set_device(local)
+            dist.init_process_group("nccl", timeout=timeout, device_id=torch.device("cuda", local))
+        else:
+            # host-only ranks (the reference arm's plumbing, the CPU tests of this code): gloo
+            dist.init_process_group("gloo", timeout=timeout)
     return world, rank, local
 
 
@@ -146,9 +150,16 @@ def max_over_ranks(world, value: float) -> float:
         return value
     import torch
     import torch.distributed as dist
-    t = torch.tensor([value], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([value], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def job_gflops(steps: int, world: int, flops_per_solve: float, ms_max: float) -> float:
+    """Whole-job rate: every rank solves its own system each step (replicas), so the job does
+    steps x world solves in the slowest rank's time."""
+    return steps * world * flops_per_solve / (ms_max / 1e3) / 1e9
 
 
 # ----------------------------------------------------------------------------- CPU baseline (oracle)
@@ -307,7 +318,7 @@ def run_b200(args, world, rank, local):
         step()
     prof = ctx.profile_read()
     ctx.profile(False)
-    value = args.steps * world * flops / (ms_max / 1e3) / 1e9
+    value = job_gflops(args.steps, world, flops, ms_max)
 
     # ---- end to end through the host-buffer C ABI (pinned host buffers, copies inside the region)
     e2e = None
@@ -331,7 +342,7 @@ def run_b200(args, world, rank, local):
         torch.cuda.synchronize()
         ems = max_over_ranks(world, e0.elapsed_time(e1))
         eta_e2e = backward_error_torch(A, torch.from_numpy(x_np).to(A.device), B)
-        e2e = {"value": args.steps * world * flops / (ems / 1e3) / 1e9, "unit": "GFLOP/s",
+        e2e = {"value": job_gflops(args.steps, world, flops, ems), "unit": "GFLOP/s",
                "h2d_bytes_per_step": int(a_np.nbytes + b_np.nbytes), "d2h_bytes_per_step": int(x_np.nbytes),
                "backward_error": eta_e2e, "api": "b2m_MatrixLinEQSolve" + ("Mixed" if form == "mixed" else "")}
         del hA, hB, hX
@@ -349,7 +360,7 @@ def run_b200(args, world, rank, local):
         p1.record()
         torch.cuda.synchronize()
         pms = max_over_ranks(world, p0.elapsed_time(p1))
-        pv = args.steps * world * flops / (pms / 1e3) / 1e9
+        pv = job_gflops(args.steps, world, flops, pms)
         plain = {"value": pv, "unit": "GFLOP/s", "ms_per_step": pms / args.steps,
                  "backward_error": backward_error_torch(A, X, B), "mixed_over_plain": value / pv}
 
@@ -370,7 +381,7 @@ def run_b200(args, world, rank, local):
             torch.cuda.synchronize()
             qms = max_over_ranks(world, q0.elapsed_time(q1))
             library = {"what": "torch.linalg.solve, cuSOLVER getrf + getrs (context only)",
-                       "value": args.steps * world * flops / (qms / 1e3) / 1e9, "unit": "GFLOP/s",
+                       "value": job_gflops(args.steps, world, flops, qms), "unit": "GFLOP/s",
                        "ms_per_step": qms / args.steps, "backward_error": backward_error_torch(A, Xl, B)}
             del Xl
         except Exception as exc:

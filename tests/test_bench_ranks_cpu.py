@@ -1,0 +1,107 @@
+"""The benchmark's multi-rank plumbing on two host ranks (gloo, world size 2, no GPU).
+
+`bench.py --gpus N` under torchrun runs one independent solve per rank (replicas, no collective on
+the data path); the only cross-rank steps are the barriers around the timed region and the maximum
+of the ranks' device times.  These tests run that plumbing as two spawned gloo processes:
+- `max_over_ranks` returns the slowest rank's time on every rank, and `job_gflops` charges
+  steps x world solves to it;
+- the reference arm (`--impl reference`) runs on rank 0 alone, prints exactly one JSON line, and the
+  other rank exits 0 without work.
+"""
+import json
+import os
+import socket
+import sys
+
+import pytest
+import torch.multiprocessing as mp
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _free_port() -> int:
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def _env(rank: int, world: int, port: int):
+    os.environ.update({"RANK": str(rank), "LOCAL_RANK": str(rank), "WORLD_SIZE": str(world),
+                       "MASTER_ADDR": "127.0.0.1", "MASTER_PORT": str(port)})
+    if ROOT not in sys.path:
+        sys.path.insert(0, ROOT)
+
+
+def _plumbing_rank(rank, world, port, q):
+    _env(rank, world, port)
+    import torch.distributed as dist
+
+    import bench
+    w, r, _ = bench.dist_setup()
+    try:
+        bench.barrier(w)
+        ms = 10.0 + 5.0 * r  # rank 1 is the slow one
+        q.put((r, w, dist.get_backend(), bench.max_over_ranks(w, ms)))
+        bench.barrier(w)
+    finally:
+        dist.destroy_process_group()
+
+
+def _reference_rank(rank, world, port, out_dir, q):
+    _env(rank, world, port)
+    import contextlib
+    import io
+
+    import bench
+    sys.argv = ["bench.py", "--impl", "reference", "--gpus", str(world), "--steps", "2", "--warmup", "1",
+                "--n", "96", "--nrhs", "2", "--kappa", "100"]
+    buf = io.StringIO()
+    with contextlib.redirect_stdout(buf):
+        rc = bench.main()
+    q.put((rank, rc, buf.getvalue()))
+
+
+def _run(target, args, world=2, timeout=300):
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=target, args=(r, world, port, *args, q)) for r in range(world)]
+    for p in procs:
+        p.start()
+    out = [q.get(timeout=timeout) for _ in range(world)]
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    return sorted(out)
+
+
+def test_max_over_ranks_gloo_two_ranks():
+    out = _run(_plumbing_rank, ())
+    assert [o[0] for o in out] == [0, 1]
+    for _, w, backend, ms_max in out:
+        assert w == 2 and backend == "gloo"
+        assert ms_max == 15.0
+
+
+def test_job_rate_counts_every_replica():
+    import bench
+    flops = 2.0 / 3.0 * 8192 ** 3 + 2.0 * 8192 ** 2 * 16
+    one = bench.job_gflops(20, 1, flops, 400.0)
+    assert one == pytest.approx(20 * flops / 0.4 / 1e9)
+    # two replicas in the same (slowest-rank) time: twice the job's throughput
+    assert bench.job_gflops(20, 2, flops, 400.0) == pytest.approx(2 * one)
+
+
+def test_reference_arm_rank0_only(tmp_path):
+    pytest.importorskip("oracle")
+    out = _run(_reference_rank, (str(tmp_path),))
+    (r0, rc0, s0), (r1, rc1, s1) = out
+    assert (r0, r1) == (0, 1) and rc0 == 0 and rc1 == 0
+    assert s1.strip() == ""
+    lines = [ln for ln in s0.splitlines() if ln.strip()]
+    assert len(lines) == 1
+    line = json.loads(lines[0])
+    assert line["impl"] == "reference" and line["n_gpus"] == 2
+    assert line["config"]["n"] == 96 and line["status"] == 0
+    assert line["backward_error"] <= line["backward_error_bound"]
+    assert line["e2e"]["h2d_bytes_per_step"] == 0 and line["cpu_baseline"]["kind"] == "port"
