@@ -63,3 +63,34 @@ def test_status_strings_without_gpu():
     assert _lib.lib.b2m_status_string(-1) == b"dimension error"
     # null context is rejected without touching a device
     assert _lib.lib.b2m_MatrixLUDecompInPlace(None, None, 0, 0, None) == _lib.ERR_ARG
+
+
+def _c_arg_count(args: str) -> int:
+    args = re.sub(r"/\*.*?\*/", "", args, flags=re.S).strip()
+    return 0 if args in ("", "void") else len(args.split(","))
+
+
+def _pascal_arg_count(args: str) -> int:
+    n = 0
+    for group in args.split(";"):
+        names = re.sub(r"^(out|var|const)\s+", "", group.split(":")[0].strip())
+        n += len([x for x in names.split(",") if x.strip()])
+    return n
+
+
+def test_integration_bindings_match_header():
+    """The Pascal unit and the ctypes stub in INTEGRATION.md bind only entry points that the header
+    declares, each `cdecl; external` with the header's argument count."""
+    header = "".join(open(h).read() for h in glob.glob(os.path.join(ROOT, "include", "*.h")))
+    decl = {m.group(1): m.group(2) for m in
+            re.finditer(r"B2M_API\s+[\w\s\*]+?\b(b2m_\w+)\s*\((.*?)\)\s*;", header, re.S)}
+    doc = open(os.path.join(ROOT, "INTEGRATION.md")).read()
+    externals = re.findall(r"function\s+(b2m_\w+)\s*\((.*?)\)\s*:\s*\w+\s*;\s*cdecl;\s*external", doc, re.S)
+    assert len(externals) >= 30
+    for name, args in externals:
+        assert name in decl, f"{name} bound in the Pascal unit but not declared"
+        assert _pascal_arg_count(args) == _c_arg_count(decl[name]), name
+    for name in set(re.findall(r"lib\.(b2m_\w+)", doc)):
+        assert name in decl, f"{name} used by the ctypes stub but not declared"
+    argtypes = re.search(r"lib\.b2m_MatrixLinEQSolve\.argtypes\s*=\s*\[(.*?)\]", doc, re.S).group(1)
+    assert argtypes.count("ctypes.") == _c_arg_count(decl["b2m_MatrixLinEQSolve"])
