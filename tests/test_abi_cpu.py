@@ -94,3 +94,35 @@ def test_integration_bindings_match_header():
         assert name in decl, f"{name} used by the ctypes stub but not declared"
     argtypes = re.search(r"lib\.b2m_MatrixLinEQSolve\.argtypes\s*=\s*\[(.*?)\]", doc, re.S).group(1)
     assert argtypes.count("ctypes.") == _c_arg_count(decl["b2m_MatrixLinEQSolve"])
+
+
+def test_null_context_and_no_device_are_errors_not_crashes():
+    """Every entry point that takes a context returns B2M_ERR_ARG for a null one (and null
+    buffers) before it touches a device; b2m_create on a machine without a usable device returns
+    B2M_ERR_CUDA and leaves the handle null.  Runs without a GPU."""
+    import ctypes
+
+    import torch
+
+    from mrmath_b200 import _lib
+    lib = _lib.lib
+    not_ctx = {"b2m_last_error", "b2m_status_string", "b2m_kernel_launches", "b2m_create",
+               "b2m_ReadMatrixFile", "b2m_WriteMatrixFile"}
+
+    def zero(t):
+        is_ptr = t is _lib.vp or t is ctypes.c_char_p or (hasattr(t, "_type_") and not isinstance(t._type_, str))
+        return None if is_ptr else 0
+
+    checked = 0
+    for name, (_, argtypes) in _lib.SIGNATURES.items():
+        if name in not_ctx:
+            continue
+        assert getattr(lib, name)(*[zero(t) for t in argtypes]) == _lib.ERR_ARG, name
+        checked += 1
+    assert checked >= 50
+    assert lib.b2m_kernel_launches(None) == -1
+    assert lib.b2m_last_error(None) == b"null context"
+    if not torch.cuda.is_available():
+        h = _lib.vp()
+        assert lib.b2m_create(0, ctypes.byref(h)) == _lib.ERR_CUDA
+        assert h.value is None
