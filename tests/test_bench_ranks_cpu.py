@@ -105,3 +105,13 @@ def test_reference_arm_rank0_only(tmp_path):
     assert line["config"]["n"] == 96 and line["status"] == 0
     assert line["backward_error"] <= line["backward_error_bound"]
     assert line["e2e"]["h2d_bytes_per_step"] == 0 and line["cpu_baseline"]["kind"] == "port"
+
+
+def test_tuned_blas_context_line():
+    """The tuned CPU BLAS context (numpy's dgesv) beside the CPU baseline: labelled as context,
+    solves the benchmark's system construction to FP64 backward error."""
+    import bench
+    a, b = bench.headline_system_host(256, 1e4, 4, seed=15)
+    line = bench.cpu_tuned_blas_context(a, b, runs=1)
+    assert "not the reference" in line["what"] and line["unit"] == "GFLOP/s"
+    assert line["value"] > 0 and line["backward_error"] <= 256 * 2.0 ** -53
