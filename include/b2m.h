@@ -193,7 +193,9 @@ B2M_API int32_t b2m_dev_MatrixMultErrorReport(b2m_ctx* ctx, const double* dest, 
                                               int64_t LineWidth2, int32_t trans, int32_t sample_rows,
                                               b2m_gemm_report* report);
 
-/* ------------------------------------------------------------------ LU (src/LinAlgLU.pas) */
+/* ------------------------------------------------------------------ LU (src/LinAlgLU.pas)
+ * Orders up to 32768 (the FP64 pivot panel is held on chip by one 16-CTA cluster, 8 columns wide at
+ * the largest orders); larger orders return B2M_ERR_UNSUPPORTED.  The reference has no such limit. */
 /* MatrixLUDecompInPlace LinAlgLU.pas:283-295 */
 B2M_API int32_t b2m_MatrixLUDecompInPlace(b2m_ctx* ctx, double* A, int64_t LineWidthA, int64_t width, int32_t* indx);
 /* MatrixLUDecomp LinAlgLU.pas:297-305 (A is left untouched) */
