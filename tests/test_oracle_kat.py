@@ -292,3 +292,16 @@ def test_oracle_against_lapack_real_and_complex():
         zdet = oracle.cplx_determinant(z)
         zref_det = np.linalg.det(z)
         assert abs(zdet - zref_det) <= 1e-10 * abs(zref_det)
+
+
+def test_oracle_cholesky_against_lapack():
+    """The oracle's blocked Cholesky (MatrixCholeskyInPlace4) against numpy's LAPACK potrf on a
+    seeded SPD matrix x x^T + n I."""
+    r = oracle.Mersenne(seed=99)
+    n = 150
+    x = r.gaussian(n, n)
+    a = x @ x.T + n * np.eye(n)
+    f = a.copy()
+    assert oracle.cholesky_inplace4(f, 32) == 0
+    ref = np.linalg.cholesky(a)
+    assert np.linalg.norm(np.tril(f) - ref) <= 1e-13 * np.linalg.norm(ref)
