@@ -26,8 +26,9 @@ def _free_port() -> int:
 
 
 def _env(rank: int, world: int, port: int):
+    # host ranks even where GPUs are visible: the gloo path is the one under test
     os.environ.update({"RANK": str(rank), "LOCAL_RANK": str(rank), "WORLD_SIZE": str(world),
-                       "MASTER_ADDR": "127.0.0.1", "MASTER_PORT": str(port)})
+                       "MASTER_ADDR": "127.0.0.1", "MASTER_PORT": str(port), "CUDA_VISIBLE_DEVICES": ""})
     if ROOT not in sys.path:
         sys.path.insert(0, ROOT)
 
