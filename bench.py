@@ -66,7 +66,8 @@ def parse():
 
 # ----------------------------------------------------------------------------- clocks
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons, sampled every 100 ms during the timed region."""
+    """nvidia-smi clocks and throttle reasons, sampled every 100 ms during the timed region (the
+    sampler is running before the region starts; only its samples from then on count)."""
 
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
@@ -76,6 +77,7 @@ class ClockSampler:
         self.index = index
         self.proc = None
         self.lines: list[str] = []
+        self.first = 0
 
     def __enter__(self):
         try:
@@ -84,6 +86,13 @@ class ClockSampler:
                  "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
+            # nvidia-smi takes a moment to print its first sample: wait for it (at most 3 s) so
+            # that the sampling covers the timed region from its start, and count only what
+            # arrives after this point
+            deadline = time.monotonic() + 3.0
+            while not self.lines and time.monotonic() < deadline and self.proc.poll() is None:
+                time.sleep(0.02)
+            self.first = len(self.lines)
         except Exception:
             self.proc = None
         return self
@@ -103,7 +112,8 @@ class ClockSampler:
     def summary(self) -> dict:
         sm, mx, reasons = [], [], set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
+        lines = self.lines[self.first:] or self.lines  # a region shorter than one period keeps the last
+        for ln in lines:
             f = [x.strip() for x in ln.split(",")]
             if len(f) < 9:
                 continue

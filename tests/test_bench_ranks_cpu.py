@@ -7,6 +7,8 @@ of the ranks' device times.  These tests run that plumbing as two spawned gloo p
   steps x world solves to it;
 - the reference arm (`--impl reference`) runs on rank 0 alone, prints exactly one JSON line, and the
   other rank exits 0 without work.
+The file also checks two host-side pieces of the bench line: the tuned CPU BLAS context and the
+clock record (against a fake nvidia-smi).
 """
 import json
 import os
@@ -116,3 +118,30 @@ def test_tuned_blas_context_line():
     line = bench.cpu_tuned_blas_context(a, b, runs=1)
     assert "not the reference" in line["what"] and line["unit"] == "GFLOP/s"
     assert line["value"] > 0 and line["backward_error"] <= 256 * 2.0 ** -53
+
+
+def test_clock_sampler_covers_the_region(tmp_path, monkeypatch):
+    """The clock record: the sampler waits for nvidia-smi's first sample before the timed region
+    starts, counts only the samples taken after that, and reports the median SM clock, the maximum
+    and every throttle reason seen active.  A fake nvidia-smi on PATH stands in for the real one."""
+    import time
+
+    import bench
+    fake = tmp_path / "nvidia-smi"
+    fake.write_text(
+        "#!/usr/bin/env python3\n"
+        "import sys, time\n"
+        "time.sleep(0.3)\n"
+        "print('0, 1200, 1965, 300, 0x0, Not Active, Not Active, Not Active, Not Active', flush=True)\n"
+        "for i in range(100):\n"
+        "    time.sleep(0.05)\n"
+        "    cap = 'Active' if i == 2 else 'Not Active'\n"
+        "    print(f'0, 1965, 1965, 900, 0x4, Not Active, Not Active, Not Active, {cap}', flush=True)\n")
+    fake.chmod(0o755)
+    monkeypatch.setenv("PATH", f"{tmp_path}{os.pathsep}{os.environ['PATH']}")
+    with bench.ClockSampler(0) as clk:
+        assert clk.first == 1  # the idle sample before the region is excluded
+        time.sleep(0.4)
+    s = clk.summary()
+    assert s["samples"] >= 3 and s["sm_mhz"] == 1965.0 and s["sm_max_mhz"] == 1965.0
+    assert s["reasons"] == ["sw_power_cap"]
